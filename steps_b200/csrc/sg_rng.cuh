@@ -1,0 +1,346 @@
+// Counter-based random streams and exact discrete samplers for the
+// operator-split SSA step.
+//
+// Everything here is __host__ __device__ and uses only IEEE-754 operations
+// that are correctly rounded on both the GPU and an x86 host (+, -, *, /,
+// sqrt, explicit fma, floor).  With FMA contraction disabled on both sides
+// (-fmad=false for nvcc device code, -ffp-contract=off for gcc) the same
+// counters produce bit-identical samples on CPU and GPU.
+//
+// Reference behaviour replaced:
+//   * src/steps/rng/r123.cpp:43-82      Philox4x32 buffered serial stream (key 0,
+//                                        seed in the counter) -> one independent
+//                                        counter stream per (unit, window).
+//   * src/steps/rng/rng.hpp:87-105      getUnfII / getUnfIE / getUnfEE.
+//   * src/steps/rng/rng.cpp:512-514     getExp (Ahrens-Dieter in float) -> -log(U)/a0
+//                                        with the project log below.
+//   * src/steps/rng/rng.cpp:516-527     getBinom (small_binomial / libstdc++) ->
+//                                        BINV inversion and BTRD rejection.
+#pragma once
+#include <stdint.h>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define SG_HD __host__ __device__ __forceinline__
+#define SG_HD_NOINLINE __host__ __device__ __noinline__
+#else
+#define SG_HD static inline
+#define SG_HD_NOINLINE static
+#endif
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+// as 1, 2, 3", SC'11).  Multipliers and Weyl constants are the published ones.
+// ---------------------------------------------------------------------------
+#define SG_PHILOX_M0 0xD2511F53u
+#define SG_PHILOX_M1 0xCD9E8D57u
+#define SG_PHILOX_W0 0x9E3779B9u
+#define SG_PHILOX_W1 0xBB67AE85u
+#define SG_PHILOX_ROUNDS 10
+
+struct sg_u32x4 {
+    uint32_t x, y, z, w;
+};
+
+SG_HD void sg_mulhilo32(uint32_t a, uint32_t b, uint32_t* hi, uint32_t* lo) {
+#if defined(__CUDA_ARCH__)
+    *hi = __umulhi(a, b);
+    *lo = a * b;
+#else
+    uint64_t p = (uint64_t)a * (uint64_t)b;
+    *hi = (uint32_t)(p >> 32);
+    *lo = (uint32_t)p;
+#endif
+}
+
+SG_HD sg_u32x4 sg_philox4x32(sg_u32x4 c, uint32_t k0, uint32_t k1) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+    for (int r = 0; r < SG_PHILOX_ROUNDS; ++r) {
+        uint32_t hi0, lo0, hi1, lo1;
+        sg_mulhilo32(SG_PHILOX_M0, c.x, &hi0, &lo0);
+        sg_mulhilo32(SG_PHILOX_M1, c.z, &hi1, &lo1);
+        sg_u32x4 n;
+        n.x = hi1 ^ c.y ^ k0;
+        n.y = lo1;
+        n.z = hi0 ^ c.w ^ k1;
+        n.w = lo0;
+        c = n;
+        k0 += SG_PHILOX_W0;
+        k1 += SG_PHILOX_W1;
+    }
+    return c;
+}
+
+// Stream purposes (top byte of counter word w).
+#define SG_PURPOSE_WINDOW 0u   // SSA + diffusion of one unit in one split window
+#define SG_PURPOSE_SETUP 1u    // host-side placement of molecules (setters)
+#define SG_PURPOSE_EFIELD 2u   // reserved
+
+// One independent stream: counter = (block, unit, window_lo, purpose<<24 | window_hi24),
+// key = (seed_lo, seed_hi + realization * W0).  Draw j of the stream is word
+// (j mod 4) of Philox(block = j / 4).  Values are consumed through a 4-word
+// shift register so that the state stays in registers on the GPU.
+struct sg_stream {
+    uint32_t k0, k1;
+    uint32_t unit, wlo, whi;
+    uint32_t block;
+    uint32_t b0, b1, b2, b3;
+    uint32_t left;
+};
+
+SG_HD void sg_stream_init(sg_stream* s, uint64_t seed, uint32_t realization, uint32_t unit,
+                          uint64_t window, uint32_t purpose) {
+    s->k0 = (uint32_t)seed;
+    s->k1 = (uint32_t)(seed >> 32) + realization * SG_PHILOX_W0;
+    s->unit = unit;
+    s->wlo = (uint32_t)window;
+    s->whi = (purpose << 24) | ((uint32_t)(window >> 32) & 0xFFFFFFu);
+    s->block = 0;
+    s->left = 0;
+    s->b0 = s->b1 = s->b2 = s->b3 = 0;
+}
+
+SG_HD uint32_t sg_next_u32(sg_stream* s) {
+    if (s->left == 0) {
+        sg_u32x4 c;
+        c.x = s->block;
+        c.y = s->unit;
+        c.z = s->wlo;
+        c.w = s->whi;
+        sg_u32x4 r = sg_philox4x32(c, s->k0, s->k1);
+        s->block += 1;
+        s->b0 = r.x;
+        s->b1 = r.y;
+        s->b2 = r.z;
+        s->b3 = r.w;
+        s->left = 4;
+    }
+    uint32_t v = s->b0;
+    s->b0 = s->b1;
+    s->b1 = s->b2;
+    s->b2 = s->b3;
+    s->left -= 1;
+    return v;
+}
+
+#define SG_TWO_M32 2.3283064365386963e-10  // 2^-32, exact
+
+// [0,1): x * 2^-32   (reference getUnfIE, rng.hpp:93-96)
+SG_HD double sg_u01_co(uint32_t x) { return (double)x * SG_TWO_M32; }
+// (0,1]: (x + 1) * 2^-32   (argument of the waiting-time log, never 0)
+SG_HD double sg_u01_oc(uint32_t x) { return ((double)x + 1.0) * SG_TWO_M32; }
+// (0,1): (x + 0.5) * 2^-32 (reference getUnfEE, rng.hpp:99-102)
+SG_HD double sg_u01_oo(uint32_t x) { return ((double)x + 0.5) * SG_TWO_M32; }
+
+// ---------------------------------------------------------------------------
+// Natural logarithm written from the mathematics (no libm call, so host and
+// device agree bit for bit).  x = m * 2^e with m in [sqrt(1/2), sqrt(2));
+// log m = 2 atanh(s), s = (m - 1)/(m + 1), |s| <= 0.1716, expanded as the
+// Taylor series 2 s (1 + z/3 + z^2/5 + ... + z^11/23), z = s^2 (truncation
+// error below 1e-19 relative).  ln 2 is split into a 32-bit head and a tail
+// so that e * ln2_head is exact.
+// ---------------------------------------------------------------------------
+#define SG_LN2_HEAD 0.6931471803691238
+#define SG_LN2_TAIL 1.9082149292705877e-10
+#define SG_SQRT2 1.4142135623730951
+
+SG_HD uint64_t sg_f64_bits(double x) {
+#if defined(__CUDA_ARCH__)
+    return (uint64_t)__double_as_longlong(x);
+#else
+    union {
+        double d;
+        uint64_t u;
+    } c;
+    c.d = x;
+    return c.u;
+#endif
+}
+
+SG_HD double sg_bits_f64(uint64_t b) {
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double((long long)b);
+#else
+    union {
+        double d;
+        uint64_t u;
+    } c;
+    c.u = b;
+    return c.d;
+#endif
+}
+
+// Valid for finite x > 0 (callers never pass 0, negatives or non-finite values).
+SG_HD double sg_log(double x) {
+    uint64_t b = sg_f64_bits(x);
+    int e = (int)((b >> 52) & 0x7FF);
+    if (e == 0) {  // subnormal: scale by 2^54
+        x = x * 18014398509481984.0;
+        b = sg_f64_bits(x);
+        e = (int)((b >> 52) & 0x7FF) - 54;
+    }
+    e -= 1023;
+    double m = sg_bits_f64((b & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull);
+    if (m > SG_SQRT2) {
+        m = m * 0.5;
+        e += 1;
+    }
+    double s = (m - 1.0) / (m + 1.0);
+    double z = s * s;
+    double p = 1.0 / 23.0;
+    p = fma(p, z, 1.0 / 21.0);
+    p = fma(p, z, 1.0 / 19.0);
+    p = fma(p, z, 1.0 / 17.0);
+    p = fma(p, z, 1.0 / 15.0);
+    p = fma(p, z, 1.0 / 13.0);
+    p = fma(p, z, 1.0 / 11.0);
+    p = fma(p, z, 1.0 / 9.0);
+    p = fma(p, z, 1.0 / 7.0);
+    p = fma(p, z, 1.0 / 5.0);
+    p = fma(p, z, 1.0 / 3.0);
+    double t = 2.0 * s;
+    double lm = fma(t * z, p, t);
+    double de = (double)e;
+    return fma(de, SG_LN2_HEAD, fma(de, SG_LN2_TAIL, lm));
+}
+
+// q^n by binary powering (multiplications only).
+SG_HD double sg_pow_u(double q, uint32_t n) {
+    double r = 1.0;
+    double b = q;
+    while (n) {
+        if (n & 1u) r = r * b;
+        b = b * b;
+        n >>= 1;
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Binomial(n, p) sampling.
+//   n * min(p, 1-p) < SG_BINV_CUT : BINV sequential-search inversion
+//       (Kachitvichyanukul & Schmeiser, "Binomial random variate generation",
+//        CACM 31(2), 1988), one uniform per sample.
+//   otherwise                     : BTRD transformed rejection with decomposition
+//       (Hormann, "The generation of binomial random variates", J. Statist.
+//        Comput. Simul. 46, 1993).
+// ---------------------------------------------------------------------------
+#define SG_BINV_CUT 10.0
+#define SG_BTRD_MAX_ITERS 256
+
+SG_HD uint32_t sg_binv(sg_stream* st, uint32_t n, double p) {
+    double q = 1.0 - p;
+    double s = p / q;
+    double a = ((double)n + 1.0) * s;
+    double r = sg_pow_u(q, n);
+    double u = sg_u01_co(sg_next_u32(st));
+    uint32_t x = 0;
+    while (u >= r && x < n) {
+        u = u - r;
+        x += 1;
+        r = r * (a / (double)x - s);
+    }
+    return x;
+}
+
+// Stirling-series remainder fc(k) = ln k! - ((k + 1/2) ln(k + 1) - (k + 1) + ln(2 pi)/2),
+// tabulated for k < 10 (values computed from the definition), series beyond.
+SG_HD double sg_stirling_fc(uint32_t k) {
+    switch (k) {
+        case 0: return 0.08106146679532733;
+        case 1: return 0.04134069595540946;
+        case 2: return 0.027677925684997717;
+        case 3: return 0.02079067210376584;
+        case 4: return 0.01664469118982126;
+        case 5: return 0.013876128823072875;
+        case 6: return 0.011896709945893313;
+        case 7: return 0.010411265261973668;
+        case 8: return 0.00925546218270945;
+        case 9: return 0.008330563433359472;
+        default: break;
+    }
+    double k1 = (double)k + 1.0;
+    double k1sq = k1 * k1;
+    return (1.0 / 12.0 - (1.0 / 360.0 - 1.0 / 1260.0 / k1sq) / k1sq) / k1;
+}
+
+// BTRD for p <= 1/2 and n p >= SG_BINV_CUT.  Candidates outside [0, n] are
+// rejected.  The iteration cap is never reached in practice (acceptance rate
+// is above 0.8 per round); if it were, the mode is returned.
+SG_HD_NOINLINE uint32_t sg_btrd(sg_stream* st, uint32_t n, double p) {
+    double dn = (double)n;
+    double q = 1.0 - p;
+    double m = floor((dn + 1.0) * p);
+    double r = p / q;
+    double nr = (dn + 1.0) * r;
+    double npq = dn * p * q;
+    double sq = sqrt(npq);
+    double b = 1.15 + 2.53 * sq;
+    double a = -0.0873 + 0.0248 * b + 0.01 * p;
+    double c = dn * p + 0.5;
+    double alpha = (2.83 + 5.1 / b) * sq;
+    double vr = 0.92 - 4.2 / b;
+    double urvr = 0.86 * vr;
+    uint32_t mi = (uint32_t)m;
+    for (int iter = 0; iter < SG_BTRD_MAX_ITERS; ++iter) {
+        double v = sg_u01_co(sg_next_u32(st));
+        double u;
+        if (v <= urvr) {
+            u = v / vr - 0.43;
+            double kq = floor((2.0 * a / (0.5 - fabs(u)) + b) * u + c);
+            if (kq < 0.0 || kq > dn) continue;
+            return (uint32_t)kq;
+        }
+        if (v >= vr) {
+            u = sg_u01_co(sg_next_u32(st)) - 0.5;
+        } else {
+            u = v / vr - 0.93;
+            u = (u < 0.0 ? -0.5 : 0.5) - u;
+            v = sg_u01_co(sg_next_u32(st)) * vr;
+        }
+        double us = 0.5 - fabs(u);
+        double kd = floor((2.0 * a / us + b) * u + c);
+        if (kd < 0.0 || kd > dn) continue;
+        v = v * alpha / (a / (us * us) + b);
+        double km = fabs(kd - m);
+        uint32_t k = (uint32_t)kd;
+        if (km <= 15.0) {
+            // Recursive evaluation of f(k)/f(m).
+            double f = 1.0;
+            if (mi < k) {
+                for (uint32_t i = mi + 1; i <= k; ++i) f = f * (nr / (double)i - r);
+            } else if (mi > k) {
+                for (uint32_t i = k + 1; i <= mi; ++i) v = v * (nr / (double)i - r);
+            }
+            if (v <= f) return k;
+            continue;
+        }
+        // Squeeze on log f(k)/f(m), then the exact test with Stirling corrections.
+        v = sg_log(v);
+        double rho = (km / npq) * (((km / 3.0 + 0.625) * km + 1.0 / 6.0) / npq + 0.5);
+        double t = -km * km / (2.0 * npq);
+        if (v < t - rho) return k;
+        if (v > t + rho) continue;
+        double nm = dn - m + 1.0;
+        double h = (m + 0.5) * sg_log((m + 1.0) / (r * nm)) + sg_stirling_fc(mi) +
+                   sg_stirling_fc(n - mi);
+        double nk = dn - kd + 1.0;
+        double bound = h + (dn + 1.0) * sg_log(nm / nk) + (kd + 0.5) * sg_log(nk * r / (kd + 1.0)) -
+                       sg_stirling_fc(k) - sg_stirling_fc(n - k);
+        if (v <= bound) return k;
+    }
+    return mi;
+}
+
+// Binomial(n, p) for any p (values <= 0 give 0, >= 1 give n).  For p > 1/2
+// the sample is n - Binomial(n, 1 - p) (1 - p is exact there).
+SG_HD uint32_t sg_binom(sg_stream* st, uint32_t n, double p) {
+    if (n == 0 || !(p > 0.0)) return 0;
+    if (p >= 1.0) return n;
+    bool flip = p > 0.5;
+    double pp = flip ? 1.0 - p : p;
+    uint32_t k = ((double)n * pp < SG_BINV_CUT) ? sg_binv(st, n, pp) : sg_btrd(st, n, pp);
+    return flip ? n - k : k;
+}

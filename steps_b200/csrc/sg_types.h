@@ -1,0 +1,83 @@
+// Device-side tables of the operator-split SSA step.  Plain structs shared by
+// the host solver (which fills them) and the CUDA kernels (which read them).
+//
+// Layout in HBM (T = tets over all realizations, S = volume species,
+// D = diffusing species, R = reactions):
+//   counts   uint32  [S][T]        species-major, tet contiguous (coalesced)
+//   outflow  uint4   [2][D][T]     per (diffusing species, tet): molecules leaving
+//                                  through faces 0..3 in one window; double
+//                                  buffered by window parity
+//   nbr      int4    [T]           per face: (neighbour << 2) | face-of-neighbour,
+//                                  or -1 when nothing diffuses through the face
+//   geo      float4  [T]           (c0, c1, c2, G): conditional face selectors and
+//                                  G = sum_f A_f / (V d_f)
+//   ivs      double  [T]           1 / (1e3 V N_A): order scaling of reaction constants
+#pragma once
+#include <stdint.h>
+
+#define SG_MAX_LHS 4   // distinct reactant species of one reaction
+#define SG_MAX_UPD 8   // distinct species whose count a reaction changes
+
+// One volume reaction, compacted from the dense lhs / upd rows of the reference
+// Compdef (src/steps/solver/compdef.hpp:252-266).  Entries are in increasing
+// species order.
+typedef struct sg_reac {
+    int32_t comp;                      // compartment the reaction lives in
+    int32_t order;                     // sum of lhs stoichiometry
+    int32_t nlhs;                      // number of distinct reactants
+    int32_t nupd;                      // number of species changed
+    int32_t lhs_spec[SG_MAX_LHS];      // reactant species (global volume index)
+    int32_t lhs_ord[SG_MAX_LHS];       // its stoichiometry (1..4)
+    int32_t upd_spec[SG_MAX_UPD];      // changed species
+    int32_t upd_delta[SG_MAX_UPD];     // signed change
+} sg_reac;
+
+// Per realization bookkeeping, advanced on the device by the last block of each
+// window launch so that the window kernel can be replayed from a CUDA graph.
+typedef struct sg_real {
+    int32_t tet_begin;                 // first tet of this realization
+    int32_t tet_end;                   // one past its last tet
+    double t;                          // current time (s)
+    double t_end;                      // end time of the current run() call
+    double period;                     // operator-split update period (s)
+    unsigned long long window;         // windows completed since reset
+    int32_t pending;                   // outflow of the last window not yet gathered
+    int32_t pad_;
+} sg_real;
+
+// Device status word bits (checked by the host after every run()).
+#define SG_ERR_CONSERVATION 1u         // species totals moved other than by reactions
+#define SG_ERR_OVERFLOW 2u             // a count would exceed UINT32_MAX
+#define SG_ERR_TABLE 4u                // a table index out of range
+#define SG_ERR_CG 8u                   // EField CG did not converge
+#define SG_ERR_NEGATIVE 16u            // a count would go below zero
+
+// Window-kernel arguments.
+typedef struct sg_window_args {
+    uint32_t* counts;
+    uint32_t* outflow;                 // base of [2][D][T] uint4 buffers (as uint32*)
+    const int32_t* nbr;                // [T][4]
+    const float* geo;                  // [T][4]
+    const double* ivs;                 // [T]
+    const int32_t* comp;               // [T] or null when every tet is in compartment 0
+    const uint32_t* clamp;             // [T] bit per species, or null
+    const sg_reac* reacs;              // [R]
+    const int32_t* comp_reac_begin;    // [ncomp + 1]
+    const double* kcst;                // [nreal][R]
+    const double* dcst;                // [nreal][ncomp][S]
+    const int32_t* diff_slot;          // [S]: compact diffusing index or -1
+    sg_real* reals;                    // [nreal]
+    unsigned long long* totals;        // [2][S]  species totals at window start
+    unsigned long long* ext;           // [2][R]  reaction events per window
+    unsigned long long* ext_total;     // [R]     reaction events since reset
+    unsigned long long* diff_total;    // [1]     diffused molecules since reset
+    unsigned long long* launch_state;  // [4]: done blocks, launch parity, active count, prev valid
+    uint32_t* status;                  // device error word
+    int32_t ntets;                     // total tets over realizations
+    int32_t nspec;
+    int32_t ndiff;
+    int32_t nreac;
+    int32_t ncomp;
+    int32_t nreal;
+    uint64_t seed;
+} sg_window_args;

@@ -1,0 +1,396 @@
+// One operator-split window for every unit (tet) of every active realization.
+//
+// Reference path restated (src/steps/mpi/tetopsplit/tetopsplit.cpp, "TOS"):
+//   TOS:1528-1839  _runWithoutEField: SSA over the window, then diffusion, then sync.
+//   TOS:1569-1588  SSA loop: dt ~ Exp(a0); stop when cumulative dt passes the window.
+//   TOS:1633-1712  diffusion: population, occupancy-weighted mean, Bernoulli on the
+//                  fraction, Binomial(mean_n, min(1, window * scaledDcst)).
+//   diff.cpp:515-585  multinomial face split by sequential conditional binomials.
+//   reac.cpp:184-251  propensity h_mu * ccst and apply with occupancy integration
+//                  (tet.cpp:318-340).
+//
+// The reference runs one composition-rejection SSA over all reactions of a rank.
+// Reactions only touch one tet, so an independent direct-method SSA per tet inside
+// the window has the same law.  Diffusion is two-phase: each (tet, species) writes
+// its per-face outflow in window w; window w+1 first gathers the inflow through
+// the reverse-face table, so every tet only writes its own counts.
+#pragma once
+#include "sg_rng.cuh"
+#include "sg_types.h"
+
+namespace sg {
+
+__device__ __forceinline__ double reac_ccst(const sg_reac* rc, double k, double ivs) {
+    int o = rc->order;
+    if (o == 1) return k;
+    if (o == 0) return k / ivs;
+    double c = k * ivs;
+    for (int i = 2; i < o; ++i) c = c * ivs;
+    return c;
+}
+
+// h_mu * ccst, counts read from this thread's column of shared memory.
+__device__ __forceinline__ double reac_prop(const sg_reac* rc, const uint32_t* sc, int stride,
+                                            double ccst) {
+    double h = 1.0;
+    int nl = rc->nlhs;
+    for (int i = 0; i < nl; ++i) {
+        int s = rc->lhs_spec[i];
+        uint32_t o = (uint32_t)rc->lhs_ord[i];
+        uint32_t c = sc[s * stride];
+        if (o > c) return 0.0;
+        if (o >= 4) h = h * (double)(c - 3);
+        if (o >= 3) h = h * (double)(c - 2);
+        if (o >= 2) h = h * (double)(c - 1);
+        h = h * (double)c;
+    }
+    return h * ccst;
+}
+
+__device__ __forceinline__ int find_real(const sg_real* reals, int nreal, int t) {
+    if (nreal == 1) return 0;
+    int lo = 0, hi = nreal - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&reals[mid].tet_begin) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Shared-memory carve-up for a block of BLOCK threads.
+struct smem_layout {
+    uint32_t* cnt;             // [S][BLOCK]
+    double* occ;               // [S][BLOCK]
+    double* last;              // [S][BLOCK]
+    unsigned long long* tot;   // [S]
+    unsigned long long* moved; // [1]
+    unsigned int* ext;         // [R]
+    int* flag;                 // [2]
+};
+
+__host__ __device__ inline size_t smem_bytes(int block, int nspec, int nreac) {
+    size_t b = (size_t)block * nspec * 4;
+    b = (b + 7) & ~(size_t)7;
+    b += (size_t)block * nspec * 16;
+    b += (size_t)nspec * 8 + 8;
+    b += (size_t)nreac * 4 + 4;
+    b = (b + 7) & ~(size_t)7;
+    b += 16;
+    return b;
+}
+
+__device__ inline smem_layout carve(unsigned char* base, int block, int nspec, int nreac) {
+    smem_layout L;
+    size_t b = (size_t)block * nspec * 4;
+    L.cnt = (uint32_t*)base;
+    b = (b + 7) & ~(size_t)7;
+    L.occ = (double*)(base + b);
+    b += (size_t)block * nspec * 8;
+    L.last = (double*)(base + b);
+    b += (size_t)block * nspec * 8;
+    L.tot = (unsigned long long*)(base + b);
+    b += (size_t)nspec * 8;
+    L.moved = (unsigned long long*)(base + b);
+    b += 8;
+    L.ext = (unsigned int*)(base + b);
+    b += (size_t)nreac * 4 + 4;
+    b = (b + 7) & ~(size_t)7;
+    L.flag = (int*)(base + b);
+    return L;
+}
+
+// SSA for one tet over [0, T): direct method with FP64 propensities, waiting
+// times -log(U)/a0, occupancy integration per changed species.
+__device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layout& L, int tid,
+                                        int BLOCK, int rb, int re, const double* K, double ivs,
+                                        uint32_t clampm, double T, sg_stream* st) {
+    uint32_t* sc = L.cnt + tid;
+    double* so = L.occ + tid;
+    double* sl = L.last + tid;
+    double tt = 0.0;
+    for (;;) {
+        double a0 = 0.0;
+        for (int q = rb; q < re; ++q) {
+            const sg_reac* rc = &a.reacs[q];
+            a0 = a0 + reac_prop(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
+        }
+        if (!(a0 > 0.0)) break;
+        double dt = -sg_log(sg_u01_oc(sg_next_u32(st))) / a0;
+        if (tt + dt > T) break;
+        tt = tt + dt;
+        double target = sg_u01_co(sg_next_u32(st)) * a0;
+        double cum = 0.0;
+        int sel = -1, lastnz = -1;
+        for (int q = rb; q < re; ++q) {
+            const sg_reac* rc = &a.reacs[q];
+            double p = reac_prop(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
+            if (p > 0.0) {
+                lastnz = q;
+                cum = cum + p;
+                if (target < cum) {
+                    sel = q;
+                    break;
+                }
+            }
+        }
+        if (sel < 0) sel = lastnz;
+        const sg_reac* rc = &a.reacs[sel];
+        int nu = rc->nupd;
+        for (int i = 0; i < nu; ++i) {
+            int s = rc->upd_spec[i];
+            if ((clampm >> s) & 1u) continue;
+            uint32_t old = sc[s * BLOCK];
+            so[s * BLOCK] = so[s * BLOCK] + (double)old * (tt - sl[s * BLOCK]);
+            sl[s * BLOCK] = tt;
+            long long nc = (long long)old + rc->upd_delta[i];
+            if (nc < 0 || nc > 0xFFFFFFFFll) {
+                atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
+                nc = nc < 0 ? 0 : 0xFFFFFFFFll;
+            }
+            sc[s * BLOCK] = (uint32_t)nc;
+        }
+        atomicAdd(&L.ext[sel], 1u);
+    }
+}
+
+// Window kernel: gather (if pending) -> totals -> SSA -> diffusion leave -> store.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) window_kernel(sg_window_args a, int check) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int S = a.nspec;
+    const int R = a.nreac;
+    const int tid = threadIdx.x;
+    smem_layout L = carve(smem_raw, BLOCK, S, R);
+    for (int i = tid; i < S; i += BLOCK) L.tot[i] = 0ull;
+    for (int i = tid; i < R; i += BLOCK) L.ext[i] = 0u;
+    if (tid == 0) L.moved[0] = 0ull;
+    __syncthreads();
+
+    const int lane = tid & 31;
+    const unsigned long long parity = __ldcg(&a.launch_state[1]) & 1ull;
+    const size_t plane = (size_t)a.ntets * 4;  // uint32 words per diffusing species
+    unsigned long long moved = 0ull;
+
+    for (int base = blockIdx.x * BLOCK; base < a.ntets; base += gridDim.x * BLOCK) {
+        const int t = base + tid;
+        bool active = t < a.ntets;
+        int r = 0, comp = 0, tlocal = 0;
+        double T = 0.0;
+        unsigned long long w = 0;
+        int pending = 0;
+        if (active) {
+            r = find_real(a.reals, a.nreal, t);
+            const sg_real* rl = &a.reals[r];
+            double rt = rl->t, rend = rl->t_end, per = rl->period;
+            active = rt < rend;
+            T = (rt + per > rend) ? rend - rt : per;
+            w = rl->window;
+            pending = rl->pending;
+            tlocal = t - rl->tet_begin;
+            if (a.comp) comp = __ldg(&a.comp[t]);
+            if (comp < 0) active = false;
+        }
+        int4 nb = make_int4(-1, -1, -1, -1);
+        uint32_t clampm = 0u;
+        const double* Dc = a.dcst;
+        if (active) {
+            nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
+            if (a.clamp) clampm = __ldg(&a.clamp[t]);
+            Dc = a.dcst + ((size_t)r * a.ncomp + comp) * S;
+        }
+        // Phase 1: gather last window's inflow, stage counts in shared memory.
+        const uint32_t* in = a.outflow + (size_t)((w + 1) & 1ull) * a.ndiff * plane;
+        for (int s = 0; s < S; ++s) {
+            uint32_t c = 0u;
+            if (active) {
+                c = a.counts[(size_t)s * a.ntets + t];
+                int ds = __ldg(&a.diff_slot[s]);
+                if (pending && ds >= 0 && __ldg(&Dc[s]) > 0.0 && !((clampm >> s) & 1u)) {
+                    const uint32_t* src = in + (size_t)ds * plane;
+                    unsigned long long sum = c;
+                    if (nb.x >= 0) sum += __ldg(&src[nb.x]);
+                    if (nb.y >= 0) sum += __ldg(&src[nb.y]);
+                    if (nb.z >= 0) sum += __ldg(&src[nb.z]);
+                    if (nb.w >= 0) sum += __ldg(&src[nb.w]);
+                    if (sum > 0xFFFFFFFFull) {
+                        atomicOr(a.status, SG_ERR_OVERFLOW);
+                        sum = 0xFFFFFFFFull;
+                    }
+                    c = (uint32_t)sum;
+                }
+                L.occ[s * BLOCK + tid] = 0.0;
+                L.last[s * BLOCK + tid] = 0.0;
+            }
+            L.cnt[s * BLOCK + tid] = c;
+            unsigned long long v = warp_sum_u64((unsigned long long)c);
+            if (lane == 0 && v) atomicAdd(&L.tot[s], v);
+        }
+        if (!active) continue;
+
+        sg_stream st;
+        sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)tlocal, w, SG_PURPOSE_WINDOW);
+        const double ivs = __ldg(&a.ivs[t]);
+        const double* K = a.kcst + (size_t)r * R;
+        const int rb = __ldg(&a.comp_reac_begin[comp]);
+        const int re = __ldg(&a.comp_reac_begin[comp + 1]);
+
+        // Phase 2: reaction SSA over the window.
+        if (re > rb) tet_ssa(a, L, tid, BLOCK, rb, re, K, ivs, clampm, T, &st);
+
+        // Phase 3: diffusion leave, one (tet, species) at a time.
+        const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
+        const double G = (double)g.w;
+        uint4* out = reinterpret_cast<uint4*>(a.outflow + (size_t)(w & 1ull) * a.ndiff * plane);
+        for (int s = 0; s < S; ++s) {
+            int ds = __ldg(&a.diff_slot[s]);
+            if (ds < 0) continue;
+            double D = __ldg(&Dc[s]);
+            if (!(D > 0.0)) continue;
+            uint32_t pop = L.cnt[s * BLOCK + tid];
+            uint4 k = make_uint4(0u, 0u, 0u, 0u);
+            if (pop > 0u) {
+                double t1 = T * (D * G);
+                if (t1 >= 1.0) t1 = 1.0;
+                double so = L.occ[s * BLOCK + tid], sl = L.last[s * BLOCK + tid];
+                uint32_t mean_n = pop;
+                if (so != 0.0 || sl != 0.0) {
+                    double nbar = (so + (double)pop * (T - sl)) / T;
+                    if (nbar > (double)pop) nbar = (double)pop;
+                    double nint = floor(nbar);
+                    double frc = nbar - nint;
+                    mean_n = (uint32_t)nint;
+                    if (frc > 0.0) {
+                        if (sg_u01_co(sg_next_u32(&st)) < frc) mean_n += 1u;
+                    }
+                }
+                uint32_t Kn = sg_binom(&st, mean_n, t1);
+                if (Kn > 0u) {
+                    uint32_t rem = Kn;
+                    k.x = sg_binom(&st, rem, (double)g.x);
+                    rem -= k.x;
+                    k.y = sg_binom(&st, rem, (double)g.y);
+                    rem -= k.y;
+                    k.z = sg_binom(&st, rem, (double)g.z);
+                    rem -= k.z;
+                    k.w = rem;
+                    if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
+                    moved += Kn;
+                }
+            }
+            out[(size_t)ds * a.ntets + t] = k;
+        }
+        // Phase 4: store counts.
+        for (int s = 0; s < S; ++s) a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
+    }
+
+    // Block partials -> global accumulators of this launch parity.
+    moved = warp_sum_u64(moved);
+    if (lane == 0 && moved) atomicAdd(L.moved, moved);
+    __syncthreads();
+    for (int i = tid; i < S; i += BLOCK)
+        if (L.tot[i]) atomicAdd(&a.totals[parity * S + i], L.tot[i]);
+    for (int i = tid; i < R; i += BLOCK)
+        if (L.ext[i]) atomicAdd(&a.ext[parity * R + i], (unsigned long long)L.ext[i]);
+    if (tid == 0 && L.moved[0]) atomicAdd(a.diff_total, L.moved[0]);
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long prev = atomicAdd(&a.launch_state[0], 1ull);
+        L.flag[0] = (prev == (unsigned long long)(gridDim.x - 1)) ? 1 : 0;
+        L.flag[1] = 0;
+    }
+    __syncthreads();
+    if (!L.flag[0]) return;
+    __threadfence();
+
+    // Last block: conservation check, counters, device-side time advance.
+    const unsigned long long p = parity, q = parity ^ 1ull;
+    int nact = 0;
+    for (int i = tid; i < a.nreal; i += BLOCK) {
+        const sg_real* rl = &a.reals[i];
+        if (__ldcg(&rl->t) < __ldcg(&rl->t_end)) nact += 1;
+    }
+    for (int o = 16; o > 0; o >>= 1) nact += __shfl_down_sync(0xffffffffu, nact, o);
+    if (lane == 0) atomicAdd(&L.flag[1], nact);
+    __syncthreads();
+    nact = L.flag[1];
+    const bool do_check = check && __ldcg(&a.launch_state[3]) != 0ull &&
+                          (unsigned long long)nact == __ldcg(&a.launch_state[2]);
+    for (int s = tid; s < S && do_check; s += BLOCK) {
+        long long expect = (long long)__ldcg(&a.totals[q * S + s]);
+        for (int rr = 0; rr < R; ++rr) {
+            const sg_reac* rc = &a.reacs[rr];
+            for (int i = 0; i < rc->nupd; ++i)
+                if (rc->upd_spec[i] == s)
+                    expect += (long long)rc->upd_delta[i] * (long long)__ldcg(&a.ext[q * R + rr]);
+        }
+        if ((unsigned long long)expect != __ldcg(&a.totals[p * S + s]))
+            atomicOr(a.status, SG_ERR_CONSERVATION);
+    }
+    __syncthreads();
+    for (int rr = tid; rr < R; rr += BLOCK) {
+        a.ext_total[rr] += __ldcg(&a.ext[p * R + rr]);
+        a.ext[q * R + rr] = 0ull;
+    }
+    for (int s = tid; s < S; s += BLOCK) a.totals[q * S + s] = 0ull;
+    for (int i = tid; i < a.nreal; i += BLOCK) {
+        sg_real* rl = &a.reals[i];
+        double rt = __ldcg(&rl->t), rend = __ldcg(&rl->t_end), per = __ldcg(&rl->period);
+        if (rt < rend) {
+            rl->t = (rt + per > rend) ? rend : rt + per;
+            rl->window = __ldcg(&rl->window) + 1ull;
+            rl->pending = 1;
+        }
+    }
+    if (tid == 0) {
+        a.launch_state[2] = (unsigned long long)nact;
+        a.launch_state[3] = 1ull;
+        a.launch_state[1] = p + 1ull;
+        a.launch_state[0] = 0ull;
+    }
+}
+
+// Apply the pending inflow of the last window to the counts (enter phase only).
+__global__ void flush_kernel(sg_window_args a) {
+    const size_t plane = (size_t)a.ntets * 4;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.ntets; t += gridDim.x * blockDim.x) {
+        int r = find_real(a.reals, a.nreal, t);
+        const sg_real* rl = &a.reals[r];
+        if (!rl->pending) continue;
+        int comp = a.comp ? a.comp[t] : 0;
+        if (comp < 0) continue;
+        int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
+        uint32_t clampm = a.clamp ? a.clamp[t] : 0u;
+        const double* Dc = a.dcst + ((size_t)r * a.ncomp + comp) * a.nspec;
+        const uint32_t* in = a.outflow + (size_t)((rl->window + 1) & 1ull) * a.ndiff * plane;
+        for (int s = 0; s < a.nspec; ++s) {
+            int ds = a.diff_slot[s];
+            if (ds < 0 || !(Dc[s] > 0.0) || ((clampm >> s) & 1u)) continue;
+            const uint32_t* src = in + (size_t)ds * plane;
+            unsigned long long sum = a.counts[(size_t)s * a.ntets + t];
+            if (nb.x >= 0) sum += src[nb.x];
+            if (nb.y >= 0) sum += src[nb.y];
+            if (nb.z >= 0) sum += src[nb.z];
+            if (nb.w >= 0) sum += src[nb.w];
+            if (sum > 0xFFFFFFFFull) {
+                atomicOr(a.status, SG_ERR_OVERFLOW);
+                sum = 0xFFFFFFFFull;
+            }
+            a.counts[(size_t)s * a.ntets + t] = (uint32_t)sum;
+        }
+    }
+}
+
+__global__ void clear_pending_kernel(sg_real* reals, int nreal) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreal; i += gridDim.x * blockDim.x)
+        reals[i].pending = 0;
+}
+
+}  // namespace sg
