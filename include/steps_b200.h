@@ -1,0 +1,127 @@
+/*
+ * steps_b200 — C ABI of the B200 operator-split spatial SSA solver.
+ *
+ * The library replaces the implementation of STEPS' TetOpSplitP
+ * (src/steps/mpi/tetopsplit/tetopsplit.hpp:79) behind the solver API of
+ * src/steps/solver/api.hpp:58.  Plain C types only: pointers, sizes, indices.
+ * Every function returns an sg_status; on failure sg_last_error() gives the
+ * message (thread-local).  Status codes mirror the reference's exception
+ * classes (src/steps/util/error.hpp:161-234): ArgErr, ProgErr, NotImplErr.
+ *
+ * Units follow the reference API: seconds, metres, m^3, molecule counts as
+ * double at the boundary (fractional values are rounded stochastically),
+ * reaction constants in the reference's units (M, s), diffusion constants m^2/s.
+ *
+ * Typical use (what a TetOpSplitP-replacement class does in its constructor):
+ *   sg_create -> sg_set_nspecs -> sg_set_mesh -> sg_add_reac* -> sg_add_diff*
+ *   [-> sg_set_realizations] -> sg_setup; then sg_run / getters / setters.
+ */
+#ifndef STEPS_B200_H
+#define STEPS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SG_ABI_VERSION 1
+
+typedef enum sg_status {
+    SG_OK = 0,
+    SG_EARG = 1,     /* steps::ArgErr      (bad argument)            */
+    SG_EPROG = 2,    /* steps::ProgErr     (internal / usage error)  */
+    SG_ENOTIMPL = 3, /* steps::NotImplErr                             */
+    SG_ECUDA = 4,    /* CUDA runtime failure                          */
+    SG_EDEVICE = 5   /* device status word: conservation, overflow, CG */
+} sg_status;
+
+typedef struct sg_solver sg_solver; /* opaque */
+
+/* Message of the last failed call on this thread. */
+const char* sg_last_error(void);
+int sg_version(void);
+
+/* ---- construction ------------------------------------------------------ */
+
+/* Replaces TetOpSplitP::TetOpSplitP (tetopsplit.hpp:81-87, TOS:84-127).  seed keys
+ * the Philox streams (the reference reads RNG::seed, rng.hpp:60). */
+int sg_create(sg_solver** out, uint64_t seed, int device);
+int sg_destroy(sg_solver* h);
+
+/* Volume species count (global species of the Statedef, statedef.hpp:40). */
+int sg_set_nspecs(sg_solver* h, int32_t nspec);
+
+/* Mesh as the reference Tet objects see it (TOS:644-681): per tet volume (m^3), per
+ * face neighbour tet (-1 = none), face area (m^2) and barycentre distance (m), and
+ * the compartment of each tet (-1 = outside every compartment). */
+int sg_set_mesh(sg_solver* h, int32_t ntets, const double* vol, const int32_t* neighb,
+                const double* area, const double* dist, const int32_t* tet_comp, int32_t ncomp);
+
+/* One volume reaction of a compartment: dense lhs/upd rows over nspec species as in
+ * Compdef::reac_lhs / reac_upd (compdef.hpp:252-266); kcst as Reacdef kcst. */
+int sg_add_reac(sg_solver* h, int32_t comp, const uint32_t* lhs, const int32_t* upd, double kcst,
+                int32_t* out_idx);
+
+/* One diffusion rule (Diffdef: ligand species, dcst in m^2/s) of a compartment. */
+int sg_add_diff(sg_solver* h, int32_t comp, int32_t spec, double dcst, int32_t* out_idx);
+
+/* Batched form: the mesh holds nreal independent realizations, realization r owning
+ * tets [tet_offsets[r], tet_offsets[r+1]).  No reference counterpart (the reference runs
+ * one realization per process). */
+int sg_set_realizations(sg_solver* h, int32_t nreal, const int32_t* tet_offsets);
+
+/* Flatten tables and upload (TOS:479-1088 _setup). */
+int sg_setup(sg_solver* h);
+
+/* ---- simulation control (api.hpp:103-140) ---------------------------------- */
+
+int sg_reset(sg_solver* h);                       /* API::reset        TOS reset          */
+int sg_run(sg_solver* h, double endtime);         /* API::run          TOS:1507           */
+int sg_advance(sg_solver* h, double adv);         /* API::advance      TOS:1955           */
+int sg_get_time(sg_solver* h, double* t);         /* API::getTime                          */
+int sg_get_update_period(sg_solver* h, int32_t real, double* period); /* TOS:5373 updPeriod */
+int sg_get_nsteps(sg_solver* h, uint64_t* n);     /* API::getNSteps                        */
+int sg_get_niteration(sg_solver* h, uint64_t* n); /* TetOpSplitP::getNIteration TOS:8322   */
+int sg_get_reac_extent(sg_solver* h, int32_t reac, uint64_t* n); /* getReacExtent TOS:8302 */
+int sg_get_diff_extent(sg_solver* h, uint64_t* n);               /* getDiffExtent TOS:8314 */
+int sg_set_diff_apply_threshold(sg_solver* h, int32_t threshold); /* TOS:8296 */
+
+/* ---- counts (api.hpp:2324-2325, 2582-2583) --------------------------------- */
+
+/* API::getTetSpecCount / setTetSpecCount -> TOS:3830 / TOS:3849. */
+int sg_get_tet_count(sg_solver* h, int32_t tet, int32_t spec, double* n);
+int sg_set_tet_count(sg_solver* h, int32_t tet, int32_t spec, double n);
+
+/* API::getCompSpecCount / setCompSpecCount -> TOS:2045 / TOS:2051 (distribute_quantity).
+ * real selects one realization, or -1 for all. */
+int sg_get_comp_count(sg_solver* h, int32_t comp, int32_t spec, int32_t real, double* n);
+int sg_set_comp_count(sg_solver* h, int32_t comp, int32_t spec, int32_t real, double n);
+
+/* Whole species row over all tets: getBatchTetSpecCountsNP (TOS:5715) for every tet,
+ * and its setter counterpart.  out/in hold ntets uint32 values. */
+int sg_get_spec_counts(sg_solver* h, int32_t spec, uint32_t* out);
+int sg_set_spec_counts(sg_solver* h, int32_t spec, const uint32_t* in);
+
+/* API::setTetSpecClamped (TOS setTetSpecClamped). */
+int sg_set_tet_clamped(sg_solver* h, int32_t tet, int32_t spec, int32_t clamped);
+
+/* API::setCompReacK / getCompReacK and setCompDiffD (api_comp.cpp). real = -1: all. */
+int sg_set_reac_k(sg_solver* h, int32_t reac, int32_t real, double k);
+int sg_get_reac_k(sg_solver* h, int32_t reac, int32_t real, double* k);
+int sg_set_diff_d(sg_solver* h, int32_t comp, int32_t spec, int32_t real, double d);
+
+/* ---- device options (no reference counterpart) ------------------------------ */
+
+/* Window-kernel launch shape: block in {64,128,256}; grid 0 = occupancy-sized. */
+int sg_set_launch(sg_solver* h, int32_t block, int32_t grid);
+/* Per-window bit-exact molecule-conservation check (on by default). */
+int sg_set_conservation_check(sg_solver* h, int32_t on);
+/* Device status word (SG_ERR_* bits). */
+int sg_get_status(sg_solver* h, uint32_t* status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STEPS_B200_H */

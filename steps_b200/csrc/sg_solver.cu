@@ -1,0 +1,1064 @@
+// Host side of the B200 operator-split solver: owns the device state, flattens the
+// model x mesh tables, runs the split-window loop and implements the
+// get/set entry points of the reference solver API behind a C ABI.
+//
+// Replaces the implementation of steps::mpi::tetopsplit::TetOpSplitP
+// (src/steps/mpi/tetopsplit/tetopsplit.hpp:79, tetopsplit.cpp "TOS").
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "sg_rng.cuh"
+#include "sg_types.h"
+#include "sg_window.cuh"
+#include "sg_errors.h"
+#include "../../include/steps_b200.h"
+
+namespace sg {
+
+static const double AVOGADRO = 6.02214076e23;  // src/steps/math/constants.hpp
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (count) SG_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+};
+
+struct Solver {
+    int device = 0;
+    uint64_t seed = 0;
+    cudaStream_t stream = nullptr;
+    int nsm = 148;
+
+    // ---- model x mesh, host copies ----
+    int ntets = 0, ncomp = 1, nspec = 0, nreal = 1;
+    std::vector<double> vol, area, dist;        // [T], [T*4], [T*4]
+    std::vector<int32_t> neighb, tet_comp;      // [T*4], [T]
+    std::vector<int32_t> real_begin{0, 0};      // [nreal + 1]
+    std::vector<sg_reac> reacs;                 // global reaction list, sorted by comp at setup
+    std::vector<double> reac_kdef;              // model kcst per reaction
+    std::vector<int32_t> reac_order_user;       // user reaction index -> sorted slot
+    std::vector<double> dcst_def;               // [ncomp][S] model diffusion constants
+    std::vector<int32_t> diff_comp, diff_spec;  // user diffusion rules
+    std::vector<double> kcst;                   // [nreal][R] current constants
+    std::vector<double> dcst;                   // [nreal][ncomp][S]
+    std::vector<int32_t> comp_reac_begin;       // [ncomp + 1]
+    std::vector<int32_t> diff_slot;             // [S]
+    std::vector<float> geo;                     // [T*4]
+    std::vector<int32_t> nbrp;                  // [T*4]
+    std::vector<double> ivs;                    // [T]
+    std::vector<uint32_t> clampm;               // [T]
+    bool any_clamp = false;
+    bool any_unassigned = false;
+    int ndiff = 0;
+    int diff_apply_threshold = 10;              // TOS:995; accepted, does not change the law
+    bool is_setup = false;
+
+    // ---- device state ----
+    DevBuf<uint32_t> d_counts, d_outflow, d_clamp, d_status;
+    DevBuf<int32_t> d_nbr, d_comp, d_crb, d_dslot;
+    DevBuf<float> d_geo;
+    DevBuf<double> d_ivs, d_kcst, d_dcst;
+    DevBuf<sg_reac> d_reacs;
+    DevBuf<sg_real> d_reals;
+    DevBuf<unsigned long long> d_totals, d_ext, d_ext_total, d_diff_total, d_launch;
+    std::vector<sg_real> reals;                 // host mirror
+    bool pending_host = false;
+    uint64_t niteration = 0;
+    uint64_t setup_calls = 0;                   // counter of the host placement stream
+    int block = 128;
+    int grid = 0;
+    bool check = true;
+
+    Solver(uint64_t s, int dev) : device(dev), seed(s) {
+        SG_CUDA(cudaSetDevice(device));
+        SG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        cudaDeviceProp prop;
+        SG_CUDA(cudaGetDeviceProperties(&prop, device));
+        nsm = prop.multiProcessorCount;
+    }
+    ~Solver() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void require_setup() const {
+        if (!is_setup) throw ProgErr("solver tables are not set up (call sg_setup first)");
+    }
+    void require_not_setup() const {
+        if (is_setup) throw ProgErr("model and mesh are fixed once sg_setup has been called");
+    }
+    void check_tet(int t) const {
+        if (t < 0 || t >= ntets) throw ArgErr("tetrahedron index out of range: " + std::to_string(t));
+    }
+    void check_spec(int s) const {
+        if (s < 0 || s >= nspec) throw ArgErr("species index out of range: " + std::to_string(s));
+    }
+    void check_comp(int c) const {
+        if (c < 0 || c >= ncomp) throw ArgErr("compartment index out of range: " + std::to_string(c));
+    }
+    void check_real(int r) const {
+        if (r < 0 || r >= nreal) throw ArgErr("realization index out of range: " + std::to_string(r));
+    }
+
+    template <typename T>
+    void h2d(T* dst, const T* src, size_t n) {
+        if (n) SG_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, stream));
+    }
+    template <typename T>
+    void d2h(T* dst, const T* src, size_t n) {
+        if (n) SG_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, stream));
+    }
+    void sync() { SG_CUDA(cudaStreamSynchronize(stream)); }
+
+    int realization_of(int t) const {
+        if (nreal == 1) return 0;
+        auto it = std::upper_bound(real_begin.begin(), real_begin.end(), t);
+        return (int)(it - real_begin.begin()) - 1;
+    }
+
+    // ------------------------------------------------------------------
+    // Setup: flatten model x mesh into the device tables (TOS:479-1088,
+    // diff.cpp:41-90 for the scaled diffusion constant and face selector,
+    // reac.cpp:44-53 for the volume scaling of reaction constants).
+    // ------------------------------------------------------------------
+    void setup() {
+        require_not_setup();
+        if (ntets <= 0) throw ArgErr("mesh has no tetrahedra");
+        if (nspec <= 0) throw ArgErr("model has no volume species");
+        if ((int)real_begin.size() != nreal + 1 || real_begin[0] != 0 || real_begin[nreal] != ntets)
+            throw ArgErr("realization tet offsets do not cover the mesh");
+        for (int r = 0; r < nreal; ++r)
+            if (real_begin[r + 1] < real_begin[r]) throw ArgErr("realization offsets decrease");
+
+        // Reactions grouped by compartment (model order kept inside a compartment).
+        const int R = (int)reacs.size();
+        std::vector<int32_t> order(R);
+        for (int i = 0; i < R; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return reacs[a].comp < reacs[b].comp; });
+        std::vector<sg_reac> sorted(R);
+        std::vector<double> ksorted(R);
+        reac_order_user.assign(R, 0);
+        for (int i = 0; i < R; ++i) {
+            sorted[i] = reacs[order[i]];
+            ksorted[i] = reac_kdef[order[i]];
+            reac_order_user[order[i]] = i;
+        }
+        reacs = sorted;
+        reac_kdef = ksorted;
+        comp_reac_begin.assign(ncomp + 1, 0);
+        for (int i = 0; i < R; ++i) comp_reac_begin[reacs[i].comp + 1] += 1;
+        for (int c = 0; c < ncomp; ++c) comp_reac_begin[c + 1] += comp_reac_begin[c];
+
+        // Diffusion: one compact slot per species that has a rule somewhere.
+        diff_slot.assign(nspec, -1);
+        ndiff = 0;
+        for (size_t i = 0; i < diff_spec.size(); ++i)
+            if (diff_slot[diff_spec[i]] < 0) diff_slot[diff_spec[i]] = ndiff++;
+
+        build_geometry();
+
+        // Per-realization parameter copies.
+        kcst.assign((size_t)nreal * R, 0.0);
+        dcst.assign((size_t)nreal * ncomp * nspec, 0.0);
+
+        // Device buffers.
+        d_counts.alloc((size_t)nspec * ntets);
+        d_outflow.alloc((size_t)2 * std::max(ndiff, 1) * ntets * 4);
+        SG_CUDA(cudaMemsetAsync(d_outflow.p, 0, d_outflow.n * 4, stream));
+        d_nbr.alloc((size_t)ntets * 4);
+        d_geo.alloc((size_t)ntets * 4);
+        d_ivs.alloc(ntets);
+        d_clamp.alloc(ntets);
+        d_comp.alloc(ntets);
+        d_reacs.alloc(std::max(R, 1));
+        d_crb.alloc(ncomp + 1);
+        d_dslot.alloc(nspec);
+        d_kcst.alloc(std::max<size_t>(kcst.size(), 1));
+        d_dcst.alloc(dcst.size());
+        d_reals.alloc(nreal);
+        d_totals.alloc((size_t)2 * nspec);
+        d_ext.alloc((size_t)2 * std::max(R, 1));
+        d_ext_total.alloc(std::max(R, 1));
+        d_diff_total.alloc(1);
+        d_launch.alloc(4);
+        d_status.alloc(1);
+        h2d(d_nbr.p, nbrp.data(), nbrp.size());
+        h2d(d_geo.p, geo.data(), geo.size());
+        h2d(d_ivs.p, ivs.data(), ivs.size());
+        h2d(d_comp.p, tet_comp.data(), tet_comp.size());
+        if (R) h2d(d_reacs.p, reacs.data(), reacs.size());
+        h2d(d_crb.p, comp_reac_begin.data(), comp_reac_begin.size());
+        h2d(d_dslot.p, diff_slot.data(), diff_slot.size());
+        reals.assign(nreal, sg_real{});
+        for (int r = 0; r < nreal; ++r) {
+            reals[r].tet_begin = real_begin[r];
+            reals[r].tet_end = real_begin[r + 1];
+        }
+        clampm.assign(ntets, 0u);
+        is_setup = true;
+        set_kernel_smem_limits();
+        reset();
+    }
+
+    void build_geometry() {
+        geo.assign((size_t)ntets * 4, 0.0f);
+        nbrp.assign((size_t)ntets * 4, -1);
+        ivs.assign(ntets, 0.0);
+        any_unassigned = false;
+        for (int t = 0; t < ntets; ++t) {
+            int c = tet_comp[t];
+            if (c < 0) any_unassigned = true;
+            if (!(vol[t] > 0.0)) throw ArgErr("tetrahedron " + std::to_string(t) + " has no volume");
+            ivs[t] = 1.0 / (1.0e3 * vol[t] * AVOGADRO);
+            double g[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int f = 0; f < 4; ++f) {
+                int n = neighb[(size_t)t * 4 + f];
+                if (n < -1 || n >= ntets) throw ArgErr("neighbour index out of range");
+                if (n < 0) continue;
+                int rf = -1;
+                for (int j = 0; j < 4; ++j)
+                    if (neighb[(size_t)n * 4 + j] == t) rf = j;
+                if (rf < 0) throw ArgErr("neighbour table is not symmetric at tet " + std::to_string(t));
+                if (realization_of(t) != realization_of(n)) throw ArgErr("neighbour crosses realizations");
+                double d = dist[(size_t)t * 4 + f];
+                if (c >= 0 && d > 0.0 && tet_comp[n] == c) {
+                    g[f] = area[(size_t)t * 4 + f] / (vol[t] * d);
+                    nbrp[(size_t)t * 4 + f] = (n << 2) | rf;
+                }
+            }
+            double G = g[0] + g[1] + g[2] + g[3];
+            int lastf = -1;
+            for (int f = 0; f < 4; ++f)
+                if (g[f] > 0.0) lastf = f;
+            double rem = G;
+            for (int f = 0; f < 3; ++f) {
+                double cf = 0.0;
+                if (g[f] > 0.0) {
+                    cf = (f == lastf) ? 1.0 : g[f] / rem;
+                    if (cf > 1.0) cf = 1.0;
+                    rem -= g[f];
+                }
+                geo[(size_t)t * 4 + f] = (float)cf;
+            }
+            geo[(size_t)t * 4 + 3] = (float)G;
+        }
+    }
+
+    // Largest scaled diffusion constant per realization -> update period
+    // (TOS:5373-5411 _computeUpdPeriod; the MPI max-reduction becomes a host max).
+    void recompute_periods() {
+        for (int r = 0; r < nreal; ++r) {
+            double mx = 0.0;
+            for (int t = real_begin[r]; t < real_begin[r + 1]; ++t) {
+                int c = tet_comp[t];
+                if (c < 0) continue;
+                double G = (double)geo[(size_t)t * 4 + 3];
+                for (int s = 0; s < nspec; ++s) {
+                    if (diff_slot[s] < 0) continue;
+                    double sd = dcst[((size_t)r * ncomp + c) * nspec + s] * G;
+                    if (sd > mx) mx = sd;
+                }
+            }
+            reals[r].period = (mx > 0.0) ? 1.0 / mx : std::numeric_limits<double>::infinity();
+        }
+    }
+
+    void upload_params() {
+        h2d(d_kcst.p, kcst.data(), kcst.size());
+        h2d(d_dcst.p, dcst.data(), dcst.size());
+        recompute_periods();
+        upload_reals();
+    }
+    void upload_reals() { h2d(d_reals.p, reals.data(), reals.size()); }
+    void download_reals() {
+        d2h(reals.data(), d_reals.p, reals.size());
+        sync();
+    }
+
+    // Reference reset (TOS reset): counts to zero, time to zero, constants to the
+    // model values, extents cleared, clamps released.
+    void reset() {
+        require_setup();
+        SG_CUDA(cudaMemsetAsync(d_counts.p, 0, d_counts.n * 4, stream));
+        SG_CUDA(cudaMemsetAsync(d_totals.p, 0, d_totals.n * 8, stream));
+        SG_CUDA(cudaMemsetAsync(d_ext.p, 0, d_ext.n * 8, stream));
+        SG_CUDA(cudaMemsetAsync(d_ext_total.p, 0, d_ext_total.n * 8, stream));
+        SG_CUDA(cudaMemsetAsync(d_diff_total.p, 0, 8, stream));
+        SG_CUDA(cudaMemsetAsync(d_launch.p, 0, 32, stream));
+        SG_CUDA(cudaMemsetAsync(d_status.p, 0, 4, stream));
+        const int R = (int)reacs.size();
+        for (int r = 0; r < nreal; ++r)
+            for (int i = 0; i < R; ++i) kcst[(size_t)r * R + i] = reac_kdef[i];
+        for (int r = 0; r < nreal; ++r)
+            for (int c = 0; c < ncomp; ++c)
+                for (int s = 0; s < nspec; ++s)
+                    dcst[((size_t)r * ncomp + c) * nspec + s] = dcst_def[(size_t)c * nspec + s];
+        std::fill(clampm.begin(), clampm.end(), 0u);
+        any_clamp = false;
+        h2d(d_clamp.p, clampm.data(), clampm.size());
+        for (auto& rl : reals) {
+            rl.t = 0.0;
+            rl.t_end = 0.0;
+            rl.window = 0;
+            rl.pending = 0;
+        }
+        pending_host = false;
+        niteration = 0;
+        upload_params();
+        sync();
+    }
+
+    // ------------------------------------------------------------------
+    // Split-window loop (TOS:1507-1527 run, TOS:1528-1839 _runWithoutEField).
+    // ------------------------------------------------------------------
+    static bool almost_equal(double x, double y) {  // src/steps/util/collections.hpp:144-148
+        double d = std::fabs(x - y);
+        return d <= std::numeric_limits<double>::epsilon() * std::fabs(x + y) * 4 ||
+               d < std::numeric_limits<double>::min();
+    }
+
+    sg_window_args window_args() {
+        sg_window_args a;
+        std::memset(&a, 0, sizeof(a));
+        a.counts = d_counts.p;
+        a.outflow = d_outflow.p;
+        a.nbr = d_nbr.p;
+        a.geo = d_geo.p;
+        a.ivs = d_ivs.p;
+        a.comp = (ncomp > 1 || any_unassigned) ? d_comp.p : nullptr;
+        a.clamp = any_clamp ? d_clamp.p : nullptr;
+        a.reacs = d_reacs.p;
+        a.comp_reac_begin = d_crb.p;
+        a.kcst = d_kcst.p;
+        a.dcst = d_dcst.p;
+        a.diff_slot = d_dslot.p;
+        a.reals = d_reals.p;
+        a.totals = d_totals.p;
+        a.ext = d_ext.p;
+        a.ext_total = d_ext_total.p;
+        a.diff_total = d_diff_total.p;
+        a.launch_state = d_launch.p;
+        a.status = d_status.p;
+        a.ntets = ntets;
+        a.nspec = nspec;
+        a.ndiff = ndiff;
+        a.nreac = (int)reacs.size();
+        a.ncomp = ncomp;
+        a.nreal = nreal;
+        a.seed = seed;
+        return a;
+    }
+
+    size_t window_smem() const { return smem_bytes(block, nspec, (int)reacs.size()); }
+
+    void set_kernel_smem_limits() {
+        size_t sm = smem_bytes(256, nspec, (int)reacs.size());
+        if (sm > 227 * 1024) throw NotImplErr("too many species for the shared-memory staging");
+        if (sm > 48 * 1024) {
+            SG_CUDA(cudaFuncSetAttribute(window_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            SG_CUDA(cudaFuncSetAttribute(window_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            SG_CUDA(cudaFuncSetAttribute(window_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        }
+    }
+
+    int window_grid() {
+        if (grid > 0) return grid;
+        size_t sm = window_smem();
+        int per_sm = 0;
+        switch (block) {
+            case 64: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<64>, 64, sm)); break;
+            case 128: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<128>, 128, sm)); break;
+            case 256: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<256>, 256, sm)); break;
+            default: throw ArgErr("block size must be 64, 128 or 256");
+        }
+        if (per_sm < 1) per_sm = 1;
+        long need = ((long)ntets + block - 1) / block;
+        long cap = (long)per_sm * nsm;
+        return (int)std::max(1L, std::min(need, cap));
+    }
+
+    void launch_window(const sg_window_args& a, int g) {
+        size_t sm = window_smem();
+        int chk = (check && !any_clamp) ? 1 : 0;
+        switch (block) {
+            case 64: window_kernel<64><<<g, 64, sm, stream>>>(a, chk); break;
+            case 128: window_kernel<128><<<g, 128, sm, stream>>>(a, chk); break;
+            case 256: window_kernel<256><<<g, 256, sm, stream>>>(a, chk); break;
+            default: throw ArgErr("block size must be 64, 128 or 256");
+        }
+        SG_CUDA(cudaGetLastError());
+    }
+
+    // Number of windows the device time recurrence takes to reach t_end.
+    static uint64_t count_windows(double t, double t_end, double period) {
+        uint64_t n = 0;
+        while (t < t_end) {
+            t = (t + period > t_end) ? t_end : t + period;
+            n += 1;
+        }
+        return n;
+    }
+
+    double time() const { return reals.empty() ? 0.0 : reals[0].t; }
+
+    void run(double endtime) {
+        require_setup();
+        double t = time();
+        if (endtime < t) throw ArgErr("Endtime is before current simulation time");
+        if (almost_equal(t, endtime)) {
+            for (auto& rl : reals) rl.t = endtime;
+            upload_reals();
+            sync();
+            return;
+        }
+        enqueue_windows(endtime);
+        download_reals();
+        check_status();
+    }
+
+    // Enqueue every window up to endtime for all realizations (no host sync).
+    uint64_t enqueue_windows(double endtime) {
+        uint64_t n = 0;
+        std::vector<uint64_t> k(nreal);
+        for (int r = 0; r < nreal; ++r) {
+            reals[r].t_end = endtime;
+            k[r] = count_windows(reals[r].t, endtime, reals[r].period);
+            n = std::max(n, k[r]);
+        }
+        upload_reals();
+        if (n == 0) return 0;
+        sg_window_args a = window_args();
+        int g = window_grid();
+        for (uint64_t i = 0; i < n; ++i) launch_window(a, g);
+        for (int r = 0; r < nreal; ++r) {
+            reals[r].window += k[r];
+            if (k[r]) reals[r].pending = 1;
+            reals[r].t = endtime;
+        }
+        niteration += n;
+        pending_host = true;
+        return n;
+    }
+
+    void check_status() {
+        uint32_t st = 0;
+        d2h(&st, d_status.p, 1);
+        sync();
+        if (st) {
+            SG_CUDA(cudaMemsetAsync(d_status.p, 0, 4, stream));
+            sync();
+            std::string m = "device status error:";
+            if (st & SG_ERR_CONSERVATION) m += " molecule conservation violated;";
+            if (st & SG_ERR_OVERFLOW) m += " count overflow;";
+            if (st & SG_ERR_NEGATIVE) m += " negative count;";
+            if (st & SG_ERR_TABLE) m += " table index out of range;";
+            if (st & SG_ERR_CG) m += " EField CG did not converge;";
+            throw DeviceErr(m);
+        }
+    }
+
+    // Gather the pending inflow so that counts are complete (getters, setters).
+    void flush() {
+        if (!pending_host) return;
+        sg_window_args a = window_args();
+        int g = std::min((ntets + 255) / 256, nsm * 8);
+        flush_kernel<<<std::max(g, 1), 256, 0, stream>>>(a);
+        SG_CUDA(cudaGetLastError());
+        clear_pending_kernel<<<(nreal + 255) / 256, 256, 0, stream>>>(d_reals.p, nreal);
+        SG_CUDA(cudaGetLastError());
+        for (auto& rl : reals) rl.pending = 0;
+        pending_host = false;
+        sync();
+        check_status();
+    }
+
+    // A host write to the counts breaks the window-to-window conservation link.
+    void invalidate_check() {
+        static const unsigned long long zero = 0ull;
+        h2d(d_launch.p + 3, &zero, 1);
+    }
+
+    // ------------------------------------------------------------------
+    // Host placement stream: one fresh Philox stream per setter call.
+    // ------------------------------------------------------------------
+    sg_stream setup_stream() {
+        sg_stream st;
+        sg_stream_init(&st, seed, 0u, (uint32_t)(setup_calls & 0xFFFFFFFFu), setup_calls >> 32,
+                       SG_PURPOSE_SETUP);
+        setup_calls += 1;
+        return st;
+    }
+
+    // Stochastic rounding of a fractional count (TOS:3849-3890 _setTetSpecCount).
+    static uint32_t round_count(double n, sg_stream* st) {
+        if (!(n >= 0.0)) throw ArgErr("count must be non-negative");
+        if (n > 4294967295.0)
+            throw ArgErr("Can't set count greater than maximum unsigned integer (4294967295).");
+        double ni = std::floor(n);
+        double fr = n - ni;
+        uint32_t c = (uint32_t)ni;
+        if (fr > 0.0 && sg_u01_co(sg_next_u32(st)) < fr) c += 1;
+        return c;
+    }
+
+    std::vector<uint32_t> row(int s) {
+        std::vector<uint32_t> v(ntets);
+        d2h(v.data(), d_counts.p + (size_t)s * ntets, ntets);
+        sync();
+        return v;
+    }
+    void put_row(int s, const std::vector<uint32_t>& v) {
+        h2d(d_counts.p + (size_t)s * ntets, v.data(), (size_t)ntets);
+        invalidate_check();
+        sync();
+    }
+
+    double get_tet_count(int t, int s) {
+        require_setup();
+        check_tet(t);
+        check_spec(s);
+        flush();
+        uint32_t c = 0;
+        d2h(&c, d_counts.p + (size_t)s * ntets + t, 1);
+        sync();
+        return (double)c;
+    }
+
+    void set_tet_count(int t, int s, double n) {
+        require_setup();
+        check_tet(t);
+        check_spec(s);
+        if (tet_comp[t] < 0) throw ArgErr("Species undefined in tetrahedron.");
+        flush();
+        sg_stream st = setup_stream();
+        uint32_t c = round_count(n, &st);
+        h2d(d_counts.p + (size_t)s * ntets + t, &c, 1);
+        invalidate_check();
+        sync();
+    }
+
+    // Tets of compartment c (in realization r, or in all realizations when r < 0).
+    std::vector<int> comp_tets(int c, int r) const {
+        std::vector<int> v;
+        int b = r < 0 ? 0 : real_begin[r], e = r < 0 ? ntets : real_begin[r + 1];
+        for (int t = b; t < e; ++t)
+            if (tet_comp[t] == c) v.push_back(t);
+        return v;
+    }
+
+    double get_comp_count(int c, int s, int r) {
+        require_setup();
+        check_comp(c);
+        check_spec(s);
+        if (r >= 0) check_real(r);
+        flush();
+        std::vector<uint32_t> v = row(s);
+        unsigned long long sum = 0;
+        for (int t : comp_tets(c, r)) sum += v[t];
+        return (double)sum;
+    }
+
+    // util::distribute_quantity (src/steps/util/distribute.hpp:102-193): volume-weighted
+    // floor allocation, then the remainder placed by adjusted Pareto order sampling
+    // (src/steps/math/sample.hpp:59-200) with the fractional parts as inclusion weights.
+    void distribute(double x, const std::vector<int>& tets, std::vector<uint32_t>& v, sg_stream* st) {
+        if (tets.empty()) return;
+        if (x == 0.0) {
+            for (int t : tets) v[t] = 0;
+            return;
+        }
+        double total = 0.0;
+        for (int t : tets) total += vol[t];
+        if (!(total > 0.0)) throw ArgErr("non-positive total weight for distribution");
+        if (sg_u01_co(sg_next_u32(st)) < x - std::floor(x))
+            x = 1.0 + std::floor(x);
+        else
+            x = std::floor(x);
+        double xot = x / total;
+        unsigned long long allocated = 0;
+        std::vector<double> pi(tets.size());
+        for (size_t i = 0; i < tets.size(); ++i) {
+            double xi = xot * vol[tets[i]];
+            double fl = std::floor(xi);
+            pi[i] = xi - fl;
+            v[tets[i]] = (uint32_t)fl;
+            allocated += (unsigned long long)fl;
+        }
+        if ((double)allocated > x) throw ProgErr("internal error in count rounding");
+        size_t rem = (size_t)(x - (double)allocated);
+        if (rem == 0) return;
+        // Adjusted Pareto order sampling: rank Q_i = q_i U_i / (1 - U_i), keep the rem smallest.
+        double psum = 0.0;
+        for (double p : pi) psum += p;
+        double rescale = (double)rem / psum;
+        double d = 0.0;
+        for (double& p : pi) {
+            p *= rescale;
+            if (p > 1.0) p = 1.0;
+            d += p * (1.0 - p);
+        }
+        double ood2 = (d == 0.0) ? 1.0 : 1.0 / (d * d);
+        std::vector<std::pair<double, size_t>> keys;
+        keys.reserve(tets.size());
+        for (size_t i = 0; i < tets.size(); ++i) {
+            double q = pi[i];
+            if (q == 0.0) continue;
+            double loga = q * (1.0 - q) * (q - 0.5) * ood2;
+            double aa = 1.0 + loga + 0.5 * loga * loga;
+            double qc = (1.0 - q) / q * aa;
+            double u = sg_u01_co(sg_next_u32(st));
+            keys.emplace_back(qc * u / (1.0 - u), i);
+        }
+        if (keys.size() < rem) rem = keys.size();
+        if (rem == 0) return;
+        std::nth_element(keys.begin(), keys.begin() + (rem - 1), keys.end());
+        for (size_t j = 0; j < rem; ++j) v[tets[keys[j].second]] += 1;
+    }
+
+    void set_comp_count(int c, int s, double n, int r) {
+        require_setup();
+        check_comp(c);
+        check_spec(s);
+        if (r >= 0) check_real(r);
+        if (!(n >= 0.0)) throw ArgErr("count must be non-negative");
+        if (n > 4294967295.0) throw ArgErr("count exceeds the maximum unsigned integer");
+        flush();
+        std::vector<uint32_t> v = row(s);
+        int rb = r < 0 ? 0 : r, re = r < 0 ? nreal : r + 1;
+        for (int rr = rb; rr < re; ++rr) {
+            sg_stream st = setup_stream();
+            distribute(n, comp_tets(c, rr), v, &st);
+        }
+        put_row(s, v);
+    }
+
+    void get_spec_row(int s, uint32_t* out) {
+        require_setup();
+        check_spec(s);
+        flush();
+        d2h(out, d_counts.p + (size_t)s * ntets, ntets);
+        sync();
+    }
+
+    void set_spec_row(int s, const uint32_t* in) {
+        require_setup();
+        check_spec(s);
+        flush();
+        h2d(d_counts.p + (size_t)s * ntets, in, (size_t)ntets);
+        invalidate_check();
+        sync();
+    }
+
+    void set_tet_clamped(int t, int s, bool on) {
+        require_setup();
+        check_tet(t);
+        check_spec(s);
+        flush();
+        if (on)
+            clampm[t] |= (1u << s);
+        else
+            clampm[t] &= ~(1u << s);
+        any_clamp = false;
+        for (uint32_t m : clampm)
+            if (m) any_clamp = true;
+        h2d(d_clamp.p + t, &clampm[t], 1);
+        invalidate_check();
+        sync();
+    }
+
+    void check_reac(int user_reac) const {
+        if (user_reac < 0 || user_reac >= (int)reacs.size()) throw ArgErr("reaction index out of range");
+    }
+
+    void set_reac_k(int user_reac, int r, double k) {
+        require_setup();
+        check_reac(user_reac);
+        if (r >= 0) check_real(r);
+        if (!(k >= 0.0)) throw ArgErr("reaction constant must be non-negative");
+        int slot = reac_order_user[user_reac];
+        const int R = (int)reacs.size();
+        int rb = r < 0 ? 0 : r, re = r < 0 ? nreal : r + 1;
+        for (int rr = rb; rr < re; ++rr) kcst[(size_t)rr * R + slot] = k;
+        h2d(d_kcst.p, kcst.data(), kcst.size());
+        sync();
+    }
+
+    double get_reac_k(int user_reac, int r) const {
+        check_reac(user_reac);
+        if (r >= 0) check_real(r);
+        return kcst[(size_t)std::max(r, 0) * reacs.size() + reac_order_user[user_reac]];
+    }
+
+    void set_diff_d(int c, int s, double d, int r) {
+        require_setup();
+        check_comp(c);
+        check_spec(s);
+        if (r >= 0) check_real(r);
+        if (!(d >= 0.0)) throw ArgErr("diffusion constant must be non-negative");
+        if (diff_slot[s] < 0) throw ArgErr("species has no diffusion rule");
+        flush();
+        int rb = r < 0 ? 0 : r, re = r < 0 ? nreal : r + 1;
+        for (int rr = rb; rr < re; ++rr) dcst[((size_t)rr * ncomp + c) * nspec + s] = d;
+        upload_params();
+        sync();
+    }
+
+    unsigned long long reac_extent(int user_reac) {
+        require_setup();
+        check_reac(user_reac);
+        unsigned long long v = 0;
+        d2h(&v, d_ext_total.p + reac_order_user[user_reac], 1);
+        sync();
+        return v;
+    }
+    unsigned long long diff_extent() {
+        require_setup();
+        unsigned long long v = 0;
+        d2h(&v, d_diff_total.p, 1);
+        sync();
+        return v;
+    }
+    unsigned long long nsteps() {
+        unsigned long long v = diff_extent();
+        for (int i = 0; i < (int)reacs.size(); ++i) v += reac_extent(i);
+        return v;
+    }
+};
+
+}  // namespace sg
+
+// ===========================================================================
+// C ABI.  Every entry point returns an sg_status; the message of the last
+// failure on the calling thread is available from sg_last_error().
+// ===========================================================================
+using sg::Solver;
+
+static thread_local std::string g_last_error;
+
+template <typename F>
+static int guarded(F&& f) {
+    try {
+        f();
+        return SG_OK;
+    } catch (const sg::ArgErr& e) {
+        g_last_error = e.what();
+        return SG_EARG;
+    } catch (const sg::NotImplErr& e) {
+        g_last_error = e.what();
+        return SG_ENOTIMPL;
+    } catch (const sg::CudaErr& e) {
+        g_last_error = e.what();
+        return SG_ECUDA;
+    } catch (const sg::DeviceErr& e) {
+        g_last_error = e.what();
+        return SG_EDEVICE;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return SG_EPROG;
+    }
+}
+
+static Solver* S(sg_solver* h) {
+    if (!h) throw sg::ArgErr("null solver handle");
+    return reinterpret_cast<Solver*>(h);
+}
+
+template <typename T>
+static void need(T* p, const char* what) {
+    if (!p) throw sg::ArgErr(std::string("null pointer: ") + what);
+}
+
+extern "C" {
+
+const char* sg_last_error(void) { return g_last_error.c_str(); }
+
+int sg_version(void) { return SG_ABI_VERSION; }
+
+int sg_create(sg_solver** out, uint64_t seed, int device) {
+    return guarded([&] {
+        need(out, "out");
+        *out = reinterpret_cast<sg_solver*>(new Solver(seed, device));
+    });
+}
+
+int sg_destroy(sg_solver* h) {
+    return guarded([&] { delete S(h); });
+}
+
+int sg_set_nspecs(sg_solver* h, int32_t nspec) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (nspec <= 0 || nspec > 32) throw sg::ArgErr("volume species count must be in 1..32");
+        if (!s->reacs.empty() || !s->diff_spec.empty())
+            throw sg::ProgErr("species count must be set before reactions and diffusions");
+        s->nspec = nspec;
+        s->dcst_def.assign((size_t)s->ncomp * nspec, 0.0);
+    });
+}
+
+int sg_set_mesh(sg_solver* h, int32_t ntets, const double* vol, const int32_t* neighb,
+                const double* area, const double* dist, const int32_t* tet_comp, int32_t ncomp) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        need(vol, "vol");
+        need(neighb, "neighb");
+        need(area, "area");
+        need(dist, "dist");
+        need(tet_comp, "tet_comp");
+        if (ntets <= 0) throw sg::ArgErr("ntets must be positive");
+        if (ntets >= (1 << 29)) throw sg::ArgErr("at most 2^29 - 1 tetrahedra per solver");
+        if (ncomp <= 0) throw sg::ArgErr("at least one compartment is required");
+        if (!s->reacs.empty() || !s->diff_spec.empty())
+            throw sg::ProgErr("mesh must be set before reactions and diffusions");
+        for (int32_t i = 0; i < ntets; ++i)
+            if (tet_comp[i] < -1 || tet_comp[i] >= ncomp) throw sg::ArgErr("tet compartment index out of range");
+        s->ntets = ntets;
+        s->ncomp = ncomp;
+        s->vol.assign(vol, vol + ntets);
+        s->neighb.assign(neighb, neighb + (size_t)ntets * 4);
+        s->area.assign(area, area + (size_t)ntets * 4);
+        s->dist.assign(dist, dist + (size_t)ntets * 4);
+        s->tet_comp.assign(tet_comp, tet_comp + ntets);
+        s->real_begin = {0, ntets};
+        s->nreal = 1;
+        s->dcst_def.assign((size_t)ncomp * std::max(s->nspec, 0), 0.0);
+    });
+}
+
+int sg_add_reac(sg_solver* h, int32_t comp, const uint32_t* lhs, const int32_t* upd, double kcst,
+                int32_t* out_idx) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (s->nspec <= 0 || s->ntets <= 0) throw sg::ProgErr("set species count and mesh first");
+        s->check_comp(comp);
+        need(lhs, "lhs");
+        need(upd, "upd");
+        if (!(kcst >= 0.0)) throw sg::ArgErr("reaction constant must be non-negative");
+        sg_reac r;
+        std::memset(&r, 0, sizeof(r));
+        r.comp = comp;
+        for (int i = 0; i < s->nspec; ++i) {
+            if (lhs[i] == 0) continue;
+            if (lhs[i] > 4) throw sg::ArgErr("reactant stoichiometry above 4 is not supported");
+            if (r.nlhs == SG_MAX_LHS) throw sg::ArgErr("more than 4 distinct reactants");
+            r.lhs_spec[r.nlhs] = i;
+            r.lhs_ord[r.nlhs] = (int32_t)lhs[i];
+            r.nlhs += 1;
+            r.order += (int32_t)lhs[i];
+        }
+        if (r.order > 4) throw sg::ArgErr("reaction order above 4 is not supported");
+        for (int i = 0; i < s->nspec; ++i) {
+            if (upd[i] == 0) continue;
+            if (r.nupd == SG_MAX_UPD) throw sg::ArgErr("a reaction changes more than 8 species");
+            r.upd_spec[r.nupd] = i;
+            r.upd_delta[r.nupd] = upd[i];
+            r.nupd += 1;
+        }
+        s->reacs.push_back(r);
+        s->reac_kdef.push_back(kcst);
+        if (out_idx) *out_idx = (int32_t)s->reacs.size() - 1;
+    });
+}
+
+int sg_add_diff(sg_solver* h, int32_t comp, int32_t spec, double dcst, int32_t* out_idx) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (s->nspec <= 0 || s->ntets <= 0) throw sg::ProgErr("set species count and mesh first");
+        s->check_comp(comp);
+        s->check_spec(spec);
+        if (!(dcst >= 0.0)) throw sg::ArgErr("diffusion constant must be non-negative");
+        for (size_t i = 0; i < s->diff_spec.size(); ++i)
+            if (s->diff_spec[i] == spec && s->diff_comp[i] == comp)
+                throw sg::ArgErr("duplicate diffusion rule for species in compartment");
+        s->diff_comp.push_back(comp);
+        s->diff_spec.push_back(spec);
+        s->dcst_def[(size_t)comp * s->nspec + spec] = dcst;
+        if (out_idx) *out_idx = (int32_t)s->diff_spec.size() - 1;
+    });
+}
+
+int sg_set_realizations(sg_solver* h, int32_t nreal, const int32_t* tet_offsets) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        need(tet_offsets, "tet_offsets");
+        if (nreal <= 0) throw sg::ArgErr("need nreal > 0");
+        s->nreal = nreal;
+        s->real_begin.assign(tet_offsets, tet_offsets + nreal + 1);
+    });
+}
+
+int sg_setup(sg_solver* h) {
+    return guarded([&] { S(h)->setup(); });
+}
+
+int sg_reset(sg_solver* h) {
+    return guarded([&] { S(h)->reset(); });
+}
+
+int sg_run(sg_solver* h, double endtime) {
+    return guarded([&] { S(h)->run(endtime); });
+}
+
+int sg_advance(sg_solver* h, double adv) {
+    return guarded([&] {
+        if (adv < 0.0) throw sg::ArgErr("Time to advance cannot be negative");
+        Solver* s = S(h);
+        s->run(s->time() + adv);
+    });
+}
+
+int sg_get_time(sg_solver* h, double* t) {
+    return guarded([&] {
+        need(t, "t");
+        *t = S(h)->time();
+    });
+}
+
+int sg_get_update_period(sg_solver* h, int32_t real, double* period) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_setup();
+        s->check_real(real);
+        need(period, "period");
+        *period = s->reals[real].period;
+    });
+}
+
+int sg_get_tet_count(sg_solver* h, int32_t tet, int32_t spec, double* n) {
+    return guarded([&] {
+        need(n, "n");
+        *n = S(h)->get_tet_count(tet, spec);
+    });
+}
+
+int sg_set_tet_count(sg_solver* h, int32_t tet, int32_t spec, double n) {
+    return guarded([&] { S(h)->set_tet_count(tet, spec, n); });
+}
+
+int sg_get_comp_count(sg_solver* h, int32_t comp, int32_t spec, int32_t real, double* n) {
+    return guarded([&] {
+        need(n, "n");
+        *n = S(h)->get_comp_count(comp, spec, real);
+    });
+}
+
+int sg_set_comp_count(sg_solver* h, int32_t comp, int32_t spec, int32_t real, double n) {
+    return guarded([&] { S(h)->set_comp_count(comp, spec, n, real); });
+}
+
+int sg_get_spec_counts(sg_solver* h, int32_t spec, uint32_t* out) {
+    return guarded([&] {
+        need(out, "out");
+        S(h)->get_spec_row(spec, out);
+    });
+}
+
+int sg_set_spec_counts(sg_solver* h, int32_t spec, const uint32_t* in) {
+    return guarded([&] {
+        need(in, "in");
+        S(h)->set_spec_row(spec, in);
+    });
+}
+
+int sg_set_tet_clamped(sg_solver* h, int32_t tet, int32_t spec, int32_t clamped) {
+    return guarded([&] { S(h)->set_tet_clamped(tet, spec, clamped != 0); });
+}
+
+int sg_set_reac_k(sg_solver* h, int32_t reac, int32_t real, double k) {
+    return guarded([&] { S(h)->set_reac_k(reac, real, k); });
+}
+
+int sg_get_reac_k(sg_solver* h, int32_t reac, int32_t real, double* k) {
+    return guarded([&] {
+        need(k, "k");
+        *k = S(h)->get_reac_k(reac, real);
+    });
+}
+
+int sg_set_diff_d(sg_solver* h, int32_t comp, int32_t spec, int32_t real, double d) {
+    return guarded([&] { S(h)->set_diff_d(comp, spec, d, real); });
+}
+
+int sg_set_diff_apply_threshold(sg_solver* h, int32_t threshold) {
+    return guarded([&] {
+        if (threshold < 0) throw sg::ArgErr("threshold must be non-negative");
+        S(h)->diff_apply_threshold = threshold;
+    });
+}
+
+int sg_get_reac_extent(sg_solver* h, int32_t reac, uint64_t* n) {
+    return guarded([&] {
+        need(n, "n");
+        *n = S(h)->reac_extent(reac);
+    });
+}
+
+int sg_get_diff_extent(sg_solver* h, uint64_t* n) {
+    return guarded([&] {
+        need(n, "n");
+        *n = S(h)->diff_extent();
+    });
+}
+
+int sg_get_nsteps(sg_solver* h, uint64_t* n) {
+    return guarded([&] {
+        need(n, "n");
+        *n = S(h)->nsteps();
+    });
+}
+
+int sg_get_niteration(sg_solver* h, uint64_t* n) {
+    return guarded([&] {
+        need(n, "n");
+        *n = S(h)->niteration;
+    });
+}
+
+int sg_set_launch(sg_solver* h, int32_t block, int32_t grid) {
+    return guarded([&] {
+        if (block != 64 && block != 128 && block != 256) throw sg::ArgErr("block must be 64, 128 or 256");
+        if (grid < 0) throw sg::ArgErr("grid must be >= 0 (0 = occupancy-sized)");
+        S(h)->block = block;
+        S(h)->grid = grid;
+    });
+}
+
+int sg_set_conservation_check(sg_solver* h, int32_t on) {
+    return guarded([&] { S(h)->check = on != 0; });
+}
+
+int sg_get_status(sg_solver* h, uint32_t* status) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_setup();
+        need(status, "status");
+        s->d2h(status, s->d_status.p, 1);
+        s->sync();
+    });
+}
+
+}  // extern "C"
