@@ -1,0 +1,313 @@
+"""Python mirror of the reference's TetOpSplit solver class.
+
+Same constructor arguments and method names as the Cython binding
+``_py_TetOpSplitP`` (pysteps/cysteps_mpi.pyx:74-200 and the get/set methods at
+:2593-2609, :3728-3742, :4831) and its API_1 aliases (getTetCount, setCompCount, ...).
+The model and mesh are flattened here and handed to the C ABI of libsteps_b200.so;
+every call below goes to the GPU solver.  Host lists (tet_hosts, tri_hosts,
+wm_hosts) are accepted and ignored: the whole mesh lives on one GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import ArgErr, check, ptr
+
+EF_NONE = 0
+EF_DEFAULT = 1
+EF_DV_BDSYS = 2
+EF_DV_PETSC = 3
+
+AVOGADRO = 6.02214076e23
+
+
+def flatten(model, geom):
+    """Model x mesh -> index tables (the role of the reference Statedef / Compdef,
+    src/steps/solver/statedef.hpp:40, compdef.hpp:252-266): volume species in model
+    order, compartments in mesh order, per compartment its reactions (dense lhs/upd rows)
+    in model order and its diffusion rules."""
+    from .model import ChanState
+
+    spec_names = [n for n, s in model.specs.items() if not isinstance(s, ChanState)]
+    if not spec_names:
+        raise ArgErr("model has no volume species")
+    spec_index = {n: i for i, n in enumerate(spec_names)}
+    comp_names = list(geom.comps.keys())
+    comp_index = {n: i for i, n in enumerate(comp_names)}
+    S = len(spec_names)
+
+    def sidx(name):
+        try:
+            return spec_index[name]
+        except KeyError:
+            raise ArgErr(f"unknown species '{name}'") from None
+
+    tet_comp = np.full(geom.ntets, -1, dtype=np.int32)
+    for ci, name in enumerate(comp_names):
+        tet_comp[geom.comps[name].tets] = ci
+    reacs, diffs = [], []
+    for ci, cname in enumerate(comp_names):
+        for vsname in geom.comps[cname].volsys:
+            vs = model.volsys[vsname]
+            for rid, r in vs.reacs.items():
+                lhs = np.zeros(S, dtype=np.uint32)
+                upd = np.zeros(S, dtype=np.int32)
+                for s in r.lhs:
+                    lhs[sidx(s)] += 1
+                    upd[sidx(s)] -= 1
+                for s in r.rhs:
+                    upd[sidx(s)] += 1
+                reacs.append((ci, rid, lhs, upd, r.kcst))
+            for did, d in vs.diffs.items():
+                diffs.append((ci, did, sidx(d.lig), d.dcst))
+    return {
+        "spec_names": spec_names, "spec_index": spec_index,
+        "comp_names": comp_names, "comp_index": comp_index,
+        "tet_comp": tet_comp, "reacs": reacs, "diffs": diffs,
+        "vol": np.ascontiguousarray(geom.tet_vol, dtype=np.float64),
+        "neighb": np.ascontiguousarray(geom.tet_neighb, dtype=np.int32),
+        "area": np.ascontiguousarray(geom.tet_area, dtype=np.float64),
+        "dist": np.ascontiguousarray(geom.tet_dist, dtype=np.float64),
+    }
+
+
+class TetOpSplit:
+    def __init__(self, model, geom, rng, calcMembPot=EF_NONE, tet_hosts=None, tri_hosts=None,
+                 wm_hosts=None, device=0, realizations=None, block=128):
+        self._h = None
+        self._L = _lib.load()
+        self.model, self.geom, self.rng = model, geom, rng
+        if calcMembPot not in (EF_NONE, 0):
+            raise _lib.NotImplErr("membrane potential is not available through this class")
+        h = C.c_void_p()
+        check(self._L.sg_create(C.byref(h), C.c_uint64(rng.seed), device))
+        self._h = h
+        try:
+            self._flatten(model, geom, realizations)
+            check(self._L.sg_set_launch(self._h, block, 0))
+            check(self._L.sg_setup(self._h))
+        except Exception:
+            self._L.sg_destroy(self._h)
+            self._h = None
+            raise
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._L.sg_destroy(h)
+            self._h = None
+
+    # ------------------------------------------------------------------ tables
+    def _flatten(self, model, geom, realizations):
+        F = flatten(model, geom)
+        self.tables = F
+        self.spec_names, self.spec_index = F["spec_names"], F["spec_index"]
+        self.comp_names, self.comp_index = F["comp_names"], F["comp_index"]
+        self.tet_comp = F["tet_comp"]
+        L, h = self._L, self._h
+        check(L.sg_set_nspecs(h, len(self.spec_names)))
+        check(L.sg_set_mesh(h, geom.ntets, ptr(F["vol"], C.c_double), ptr(F["neighb"], C.c_int32),
+                            ptr(F["area"], C.c_double), ptr(F["dist"], C.c_double),
+                            ptr(F["tet_comp"], C.c_int32), max(len(self.comp_names), 1)))
+        self.reac_index = {}   # (comp, reac id) -> ABI reaction index
+        self.diff_index = {}   # (comp, diff id) -> species index
+        for (ci, rid, lhs, upd, k) in F["reacs"]:
+            out = C.c_int32()
+            check(L.sg_add_reac(h, ci, ptr(lhs, C.c_uint32), ptr(upd, C.c_int32), k, C.byref(out)))
+            self.reac_index[(self.comp_names[ci], rid)] = out.value
+        for (ci, did, s, d) in F["diffs"]:
+            out = C.c_int32()
+            check(L.sg_add_diff(h, ci, s, d, C.byref(out)))
+            self.diff_index[(self.comp_names[ci], did)] = s
+        if realizations is not None:
+            off = np.ascontiguousarray(realizations, dtype=np.int32)
+            self.nreal = len(off) - 1
+            check(L.sg_set_realizations(h, self.nreal, ptr(off, C.c_int32)))
+            self.real_offsets = off
+        else:
+            self.nreal = 1
+            self.real_offsets = np.array([0, geom.ntets], dtype=np.int32)
+
+    def _spec(self, name):
+        try:
+            return self.spec_index[name]
+        except KeyError:
+            raise ArgErr(f"unknown species '{name}'") from None
+
+    def _comp(self, name):
+        try:
+            return self.comp_index[name]
+        except KeyError:
+            raise ArgErr(f"unknown compartment '{name}'") from None
+
+    def _reac(self, c, r):
+        try:
+            return self.reac_index[(c, r)]
+        except KeyError:
+            raise ArgErr(f"reaction '{r}' undefined in compartment '{c}'") from None
+
+    # ------------------------------------------------------------ solver info
+    def getSolverName(self):
+        return "TetOpSplitB200"
+
+    def getSolverDesc(self):
+        return "Operator-split spatial SSA on one B200 GPU (Philox counter streams)"
+
+    def getSolverAuthors(self):
+        return "steps_b200 developers"
+
+    def getSolverEmail(self):
+        return ""
+
+    # --------------------------------------------------------------- control
+    def reset(self):
+        check(self._L.sg_reset(self._h))
+
+    def run(self, endtime):
+        check(self._L.sg_run(self._h, float(endtime)))
+
+    def advance(self, adv):
+        check(self._L.sg_advance(self._h, float(adv)))
+
+    def step(self):
+        raise _lib.NotImplErr("step() is not implemented for operator-split solvers")
+
+    def getTime(self):
+        t = C.c_double()
+        check(self._L.sg_get_time(self._h, C.byref(t)))
+        return t.value
+
+    def getUpdPeriod(self, realization=0):
+        p = C.c_double()
+        check(self._L.sg_get_update_period(self._h, realization, C.byref(p)))
+        return p.value
+
+    def getNSteps(self):
+        n = C.c_uint64()
+        check(self._L.sg_get_nsteps(self._h, C.byref(n)))
+        return n.value
+
+    def getNIteration(self):
+        n = C.c_uint64()
+        check(self._L.sg_get_niteration(self._h, C.byref(n)))
+        return n.value
+
+    def getDiffExtent(self):
+        n = C.c_uint64()
+        check(self._L.sg_get_diff_extent(self._h, C.byref(n)))
+        return n.value
+
+    def getCompReacExtent(self, c, r):
+        n = C.c_uint64()
+        check(self._L.sg_get_reac_extent(self._h, self._reac(c, r), C.byref(n)))
+        return n.value
+
+    def setDiffApplyThreshold(self, threshold):
+        check(self._L.sg_set_diff_apply_threshold(self._h, int(threshold)))
+
+    # ---------------------------------------------------------------- counts
+    def getTetSpecCount(self, idx, s):
+        n = C.c_double()
+        check(self._L.sg_get_tet_count(self._h, int(idx), self._spec(s), C.byref(n)))
+        return n.value
+
+    def setTetSpecCount(self, idx, s, n):
+        check(self._L.sg_set_tet_count(self._h, int(idx), self._spec(s), float(n)))
+
+    def getCompSpecCount(self, c, s, realization=-1):
+        n = C.c_double()
+        check(self._L.sg_get_comp_count(self._h, self._comp(c), self._spec(s), int(realization),
+                                        C.byref(n)))
+        return n.value
+
+    def setCompSpecCount(self, c, s, n, realization=-1):
+        check(self._L.sg_set_comp_count(self._h, self._comp(c), self._spec(s), int(realization),
+                                        float(n)))
+
+    def _comp_vol(self, c, realization=-1):
+        tets = self.geom.comps[c].tets
+        if realization >= 0:
+            b, e = self.real_offsets[realization], self.real_offsets[realization + 1]
+            tets = tets[(tets >= b) & (tets < e)]
+        return float(self.geom.tet_vol[tets].sum())
+
+    def getTetSpecConc(self, idx, s):
+        return self.getTetSpecCount(idx, s) / (AVOGADRO * self.geom.tet_vol[idx] * 1.0e3)
+
+    def setTetSpecConc(self, idx, s, c):
+        self.setTetSpecCount(idx, s, c * AVOGADRO * self.geom.tet_vol[idx] * 1.0e3)
+
+    def getCompSpecConc(self, c, s, realization=-1):
+        v = self._comp_vol(c, realization)
+        return self.getCompSpecCount(c, s, realization) / (AVOGADRO * v * 1.0e3)
+
+    def setCompSpecConc(self, c, s, conc, realization=-1):
+        if realization >= 0:
+            self.setCompSpecCount(c, s, conc * AVOGADRO * self._comp_vol(c, realization) * 1.0e3,
+                                  realization)
+        else:
+            for r in range(self.nreal):
+                self.setCompSpecCount(c, s, conc * AVOGADRO * self._comp_vol(c, r) * 1.0e3, r)
+
+    def setTetSpecClamped(self, idx, s, clamped):
+        check(self._L.sg_set_tet_clamped(self._h, int(idx), self._spec(s), 1 if clamped else 0))
+
+    def getSpecCounts(self, s, out=None):
+        """All tets' counts of species s as uint32 (device -> host of one row)."""
+        if out is None:
+            out = np.empty(self.geom.ntets, dtype=np.uint32)
+        check(self._L.sg_get_spec_counts(self._h, self._spec(s), ptr(out, C.c_uint32)))
+        return out
+
+    def setSpecCounts(self, s, counts):
+        a = np.ascontiguousarray(counts, dtype=np.uint32)
+        if a.size != self.geom.ntets:
+            raise ArgErr("need one count per tet")
+        check(self._L.sg_set_spec_counts(self._h, self._spec(s), ptr(a, C.c_uint32)))
+
+    def getBatchTetSpecCountsNP(self, tets, s, counts):
+        """Reference getBatchTetSpecCountsNP (TOS:5715): counts[i] = count of s in tets[i]."""
+        row = self.getSpecCounts(s)
+        counts[:] = row[np.asarray(tets, dtype=np.int64)]
+
+    def getBatchTetSpecCounts(self, tets, s):
+        out = np.empty(len(tets), dtype=np.float64)
+        self.getBatchTetSpecCountsNP(tets, s, out)
+        return list(out)
+
+    # ------------------------------------------------------------- constants
+    def setCompReacK(self, c, r, k, realization=-1):
+        check(self._L.sg_set_reac_k(self._h, self._reac(c, r), int(realization), float(k)))
+
+    def getCompReacK(self, c, r, realization=0):
+        k = C.c_double()
+        check(self._L.sg_get_reac_k(self._h, self._reac(c, r), int(realization), C.byref(k)))
+        return k.value
+
+    def setCompDiffD(self, c, d, dcst, realization=-1):
+        try:
+            s = self.diff_index[(c, d)]
+        except KeyError:
+            raise ArgErr(f"diffusion '{d}' undefined in compartment '{c}'") from None
+        check(self._L.sg_set_diff_d(self._h, self._comp(c), s, int(realization), float(dcst)))
+
+    # --------------------------------------------------------- device knobs
+    def setLaunch(self, block, grid=0):
+        check(self._L.sg_set_launch(self._h, int(block), int(grid)))
+
+    def setConservationCheck(self, on):
+        check(self._L.sg_set_conservation_check(self._h, 1 if on else 0))
+
+    # ----------------------------------------------------------- API_1 names
+    getTetCount = getTetSpecCount
+    setTetCount = setTetSpecCount
+    getCompCount = getCompSpecCount
+    setCompCount = setCompSpecCount
+    getTetConc = getTetSpecConc
+    setTetConc = setTetSpecConc
+    getCompConc = getCompSpecConc
+    setCompConc = setCompSpecConc
+    setTetClamped = setTetSpecClamped
