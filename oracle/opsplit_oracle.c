@@ -1,0 +1,623 @@
+/*
+ * TEST INFRASTRUCTURE ONLY — CPU oracle of the operator-split SSA step.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arms
+ * may load this file's library, and only as the checker or the timed CPU baseline,
+ * never as part of the product path.
+ *
+ * It restates, in plain C, the algorithm of STEPS' TetOpSplitP split window
+ * (src/steps/mpi/tetopsplit/tetopsplit.cpp, "TOS") with the project's counter-based
+ * random streams, so that the GPU solver fed the same Philox counters must match it
+ * bit for bit.  It is written independently of the CUDA sources: its own Philox, its
+ * own samplers (same published algorithms, same operation order), its own table build.
+ *
+ * Pinning:
+ *   - Philox4x32-10 is checked against the reference's vendored Random123
+ *     (src/third_party/Random123/philox.h) by tests/golden/philox_kat.json, produced
+ *     by oracle/ref_philox_kat.c compiled from that header.
+ *   - The binomial sampler is checked by the chi-squared test of the reference's
+ *     test/unit/cpp/test_rng.cpp:51-90 (same n, p grid and thresholds) and by a
+ *     proper chi-squared goodness of fit over the BINV and BTRD regimes.
+ *   - Trajectory statistics are checked against the analytic kinetics of
+ *     test/validation/API_1/validation_rd_mpi/parallel_spatial_tetopsplit.py.
+ *
+ * Compile with -ffp-contract=off (explicit fma() only).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------- */
+/* Philox4x32-10 (Salmon et al., SC'11)                                       */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    uint32_t v[4];
+} or_ctr;
+
+static or_ctr or_philox(or_ctr c, uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c.v[0];
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c.v[2];
+        or_ctr n;
+        n.v[0] = (uint32_t)(p1 >> 32) ^ c.v[1] ^ k0;
+        n.v[1] = (uint32_t)p1;
+        n.v[2] = (uint32_t)(p0 >> 32) ^ c.v[3] ^ k1;
+        n.v[3] = (uint32_t)p0;
+        c = n;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+/* Exported for the known-answer test. */
+void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    or_ctr c = {{ctr[0], ctr[1], ctr[2], ctr[3]}};
+    or_ctr r = or_philox(c, key[0], key[1]);
+    memcpy(out, r.v, 16);
+}
+
+/* Stream of one (realization, unit, window): draw j = word j%4 of Philox(block j/4). */
+typedef struct {
+    uint32_t k0, k1, unit, wlo, whi, block;
+    uint32_t buf[4];
+    int pos;
+} or_stream;
+
+static void or_stream_init(or_stream* s, uint64_t seed, uint32_t real, uint32_t unit,
+                           uint64_t window, uint32_t purpose) {
+    s->k0 = (uint32_t)seed;
+    s->k1 = (uint32_t)(seed >> 32) + real * 0x9E3779B9u;
+    s->unit = unit;
+    s->wlo = (uint32_t)window;
+    s->whi = (purpose << 24) | ((uint32_t)(window >> 32) & 0xFFFFFFu);
+    s->block = 0;
+    s->pos = 4;
+}
+
+static uint32_t or_u32(or_stream* s) {
+    if (s->pos == 4) {
+        or_ctr c = {{s->block, s->unit, s->wlo, s->whi}};
+        or_ctr r = or_philox(c, s->k0, s->k1);
+        memcpy(s->buf, r.v, 16);
+        s->block += 1;
+        s->pos = 0;
+    }
+    return s->buf[s->pos++];
+}
+
+static const double TWO_M32 = 2.3283064365386963e-10;
+static double u_co(uint32_t x) { return (double)x * TWO_M32; }
+static double u_oc(uint32_t x) { return ((double)x + 1.0) * TWO_M32; }
+
+/* ------------------------------------------------------------------------- */
+/* log via 2 atanh((m-1)/(m+1)) Taylor series (same terms and order as the GPU) */
+/* ------------------------------------------------------------------------- */
+static double or_log(double x) {
+    uint64_t b;
+    memcpy(&b, &x, 8);
+    int e = (int)((b >> 52) & 0x7FF);
+    if (e == 0) {
+        x = x * 18014398509481984.0;
+        memcpy(&b, &x, 8);
+        e = (int)((b >> 52) & 0x7FF) - 54;
+    }
+    e -= 1023;
+    uint64_t mb = (b & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull;
+    double m;
+    memcpy(&m, &mb, 8);
+    if (m > 1.4142135623730951) {
+        m = m * 0.5;
+        e += 1;
+    }
+    double s = (m - 1.0) / (m + 1.0);
+    double z = s * s;
+    static const double inv_odd[10] = {1.0 / 21.0, 1.0 / 19.0, 1.0 / 17.0, 1.0 / 15.0, 1.0 / 13.0,
+                                       1.0 / 11.0, 1.0 / 9.0,  1.0 / 7.0,  1.0 / 5.0,  1.0 / 3.0};
+    double p = 1.0 / 23.0;
+    for (int i = 0; i < 10; ++i) p = fma(p, z, inv_odd[i]);
+    double t = 2.0 * s;
+    double lm = fma(t * z, p, t);
+    double de = (double)e;
+    return fma(de, 0.6931471803691238, fma(de, 1.9082149292705877e-10, lm));
+}
+
+double or_log_export(double x) { return or_log(x); }
+
+/* ------------------------------------------------------------------------- */
+/* Binomial: BINV (Kachitvichyanukul & Schmeiser 1988) / BTRD (Hormann 1993)  */
+/* ------------------------------------------------------------------------- */
+static double or_powu(double q, uint32_t n) {
+    double r = 1.0, b = q;
+    while (n) {
+        if (n & 1u) r = r * b;
+        b = b * b;
+        n >>= 1;
+    }
+    return r;
+}
+
+static uint32_t or_binv(or_stream* st, uint32_t n, double p) {
+    double q = 1.0 - p;
+    double s = p / q;
+    double a = ((double)n + 1.0) * s;
+    double r = or_powu(q, n);
+    double u = u_co(or_u32(st));
+    uint32_t x = 0;
+    while (u >= r && x < n) {
+        u = u - r;
+        x += 1;
+        r = r * (a / (double)x - s);
+    }
+    return x;
+}
+
+static double or_fc(uint32_t k) {
+    static const double tab[10] = {0.08106146679532733,  0.04134069595540946,
+                                   0.027677925684997717, 0.02079067210376584,
+                                   0.01664469118982126,  0.013876128823072875,
+                                   0.011896709945893313, 0.010411265261973668,
+                                   0.00925546218270945,  0.008330563433359472};
+    if (k < 10) return tab[k];
+    double k1 = (double)k + 1.0;
+    double k1sq = k1 * k1;
+    return (1.0 / 12.0 - (1.0 / 360.0 - 1.0 / 1260.0 / k1sq) / k1sq) / k1;
+}
+
+static uint32_t or_btrd(or_stream* st, uint32_t n, double p) {
+    double dn = (double)n, q = 1.0 - p;
+    double m = floor((dn + 1.0) * p);
+    double r = p / q, nr = (dn + 1.0) * r, npq = dn * p * q;
+    double sq = sqrt(npq);
+    double b = 1.15 + 2.53 * sq;
+    double a = -0.0873 + 0.0248 * b + 0.01 * p;
+    double c = dn * p + 0.5;
+    double alpha = (2.83 + 5.1 / b) * sq;
+    double vr = 0.92 - 4.2 / b;
+    double urvr = 0.86 * vr;
+    uint32_t mi = (uint32_t)m;
+    for (int iter = 0; iter < 256; ++iter) {
+        double v = u_co(or_u32(st)), u;
+        if (v <= urvr) {
+            u = v / vr - 0.43;
+            double kq = floor((2.0 * a / (0.5 - fabs(u)) + b) * u + c);
+            if (kq < 0.0 || kq > dn) continue;
+            return (uint32_t)kq;
+        }
+        if (v >= vr) {
+            u = u_co(or_u32(st)) - 0.5;
+        } else {
+            u = v / vr - 0.93;
+            u = (u < 0.0 ? -0.5 : 0.5) - u;
+            v = u_co(or_u32(st)) * vr;
+        }
+        double us = 0.5 - fabs(u);
+        double kd = floor((2.0 * a / us + b) * u + c);
+        if (kd < 0.0 || kd > dn) continue;
+        v = v * alpha / (a / (us * us) + b);
+        double km = fabs(kd - m);
+        uint32_t k = (uint32_t)kd;
+        if (km <= 15.0) {
+            double f = 1.0;
+            if (mi < k) {
+                for (uint32_t i = mi + 1; i <= k; ++i) f = f * (nr / (double)i - r);
+            } else if (mi > k) {
+                for (uint32_t i = k + 1; i <= mi; ++i) v = v * (nr / (double)i - r);
+            }
+            if (v <= f) return k;
+            continue;
+        }
+        v = or_log(v);
+        double rho = (km / npq) * (((km / 3.0 + 0.625) * km + 1.0 / 6.0) / npq + 0.5);
+        double t = -km * km / (2.0 * npq);
+        if (v < t - rho) return k;
+        if (v > t + rho) continue;
+        double nm = dn - m + 1.0;
+        double h = (m + 0.5) * or_log((m + 1.0) / (r * nm)) + or_fc(mi) + or_fc(n - mi);
+        double nk = dn - kd + 1.0;
+        double bound = h + (dn + 1.0) * or_log(nm / nk) + (kd + 0.5) * or_log(nk * r / (kd + 1.0)) -
+                       or_fc(k) - or_fc(n - k);
+        if (v <= bound) return k;
+    }
+    return mi;
+}
+
+static uint32_t or_binom(or_stream* st, uint32_t n, double p) {
+    if (n == 0 || !(p > 0.0)) return 0;
+    if (p >= 1.0) return n;
+    int flip = p > 0.5;
+    double pp = flip ? 1.0 - p : p;
+    uint32_t k = ((double)n * pp < 10.0) ? or_binv(st, n, pp) : or_btrd(st, n, pp);
+    return flip ? n - k : k;
+}
+
+/* Draw count binomials from one stream (sampler tests): out[i] = Binom(n, p). */
+void or_binom_many(uint64_t seed, uint32_t unit, uint32_t n, double p, uint32_t count, uint32_t* out) {
+    or_stream st;
+    or_stream_init(&st, seed, 0, unit, 0, 0);
+    for (uint32_t i = 0; i < count; ++i) out[i] = or_binom(&st, n, p);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Model x mesh tables                                                        */
+/* ------------------------------------------------------------------------- */
+#define OR_MAXR 256
+#define OR_MAXS 32
+
+typedef struct {
+    int comp;
+    uint32_t lhs[OR_MAXS];
+    int32_t upd[OR_MAXS];
+    int order;
+} or_reac;
+
+typedef struct {
+    uint64_t seed;
+    int ntets, nspec, ncomp, nreal, nreac;
+    const double* vol;
+    const int32_t* neighb;
+    const double* area;
+    const double* dist;
+    const int32_t* tcomp;
+    const int32_t* real_begin; /* nreal + 1 */
+    or_reac reac[OR_MAXR];
+    double* kcst;              /* [nreal][nreac] */
+    double* dcst;              /* [nreal][ncomp][nspec] */
+    int has_rule[OR_MAXS];
+    /* derived */
+    float* geo;                /* [T][4]: c0 c1 c2 G */
+    int32_t* nbr;              /* [T][4]: neighbour or -1 */
+    int32_t* rface;            /* [T][4]: face of the neighbour pointing back */
+    double* ivs;               /* [T] */
+    uint32_t* clamp;           /* [T] */
+    uint32_t* counts;          /* [S][T] */
+    uint32_t* outflow;         /* [S][T][4] scratch of one window */
+    double* t;                 /* [nreal] */
+    double* period;            /* [nreal] */
+    uint64_t* window;          /* [nreal] */
+    uint64_t ext[OR_MAXR];
+    uint64_t diff_moved;
+} or_solver;
+
+or_solver* or_create(uint64_t seed, int ntets, int nspec, int ncomp, const double* vol,
+                     const int32_t* neighb, const double* area, const double* dist,
+                     const int32_t* tcomp, int nreal, const int32_t* real_begin) {
+    if (nspec > OR_MAXS) return NULL;
+    or_solver* s = (or_solver*)calloc(1, sizeof(or_solver));
+    s->seed = seed;
+    s->ntets = ntets;
+    s->nspec = nspec;
+    s->ncomp = ncomp;
+    s->nreal = nreal;
+    s->vol = vol;
+    s->neighb = neighb;
+    s->area = area;
+    s->dist = dist;
+    s->tcomp = tcomp;
+    s->real_begin = real_begin;
+    s->dcst = (double*)calloc((size_t)nreal * ncomp * nspec, sizeof(double));
+    s->counts = (uint32_t*)calloc((size_t)nspec * ntets, 4);
+    s->outflow = (uint32_t*)calloc((size_t)nspec * ntets * 4, 4);
+    s->clamp = (uint32_t*)calloc((size_t)ntets, 4);
+    s->t = (double*)calloc(nreal, sizeof(double));
+    s->period = (double*)calloc(nreal, sizeof(double));
+    s->window = (uint64_t*)calloc(nreal, sizeof(uint64_t));
+    return s;
+}
+
+void or_destroy(or_solver* s) {
+    if (!s) return;
+    free(s->kcst);
+    free(s->dcst);
+    free(s->geo);
+    free(s->nbr);
+    free(s->rface);
+    free(s->ivs);
+    free(s->clamp);
+    free(s->counts);
+    free(s->outflow);
+    free(s->t);
+    free(s->period);
+    free(s->window);
+    free(s);
+}
+
+/* Reactions are appended per compartment in the order given (the caller passes them
+ * grouped by compartment, keeping the model order inside a compartment). */
+int or_add_reac(or_solver* s, int comp, const uint32_t* lhs, const int32_t* upd, double kcst) {
+    if (s->nreac >= OR_MAXR) return -1;
+    or_reac* r = &s->reac[s->nreac];
+    r->comp = comp;
+    r->order = 0;
+    for (int i = 0; i < s->nspec; ++i) {
+        r->lhs[i] = lhs[i];
+        r->upd[i] = upd[i];
+        r->order += (int)lhs[i];
+    }
+    int R = s->nreac;
+    double* k = (double*)malloc(sizeof(double) * (size_t)s->nreal * (R + 1));
+    for (int rr = 0; rr < s->nreal; ++rr) {
+        for (int i = 0; i < R; ++i) k[(size_t)rr * (R + 1) + i] = s->kcst[(size_t)rr * R + i];
+        k[(size_t)rr * (R + 1) + R] = kcst;
+    }
+    free(s->kcst);
+    s->kcst = k;
+    s->nreac = R + 1;
+    return R;
+}
+
+void or_add_diff(or_solver* s, int comp, int spec, double dcst) {
+    s->has_rule[spec] = 1;
+    for (int r = 0; r < s->nreal; ++r) s->dcst[((size_t)r * s->ncomp + comp) * s->nspec + spec] = dcst;
+}
+
+void or_set_reac_k(or_solver* s, int reac, int real, double k) {
+    s->kcst[(size_t)real * s->nreac + reac] = k;
+}
+
+static void or_periods(or_solver* s) {
+    for (int r = 0; r < s->nreal; ++r) {
+        double mx = 0.0;
+        for (int t = s->real_begin[r]; t < s->real_begin[r + 1]; ++t) {
+            int c = s->tcomp[t];
+            if (c < 0) continue;
+            double G = (double)s->geo[(size_t)t * 4 + 3];
+            for (int sp = 0; sp < s->nspec; ++sp) {
+                if (!s->has_rule[sp]) continue;
+                double sd = s->dcst[((size_t)r * s->ncomp + c) * s->nspec + sp] * G;
+                if (sd > mx) mx = sd;
+            }
+        }
+        s->period[r] = (mx > 0.0) ? 1.0 / mx : INFINITY;
+    }
+}
+
+/* Scaled diffusion constant and face selector as Diff::Diff (diff.cpp:41-90): faces to a
+ * neighbour of the same compartment with positive distance carry A_f / (V d_f); the
+ * conditional selectors c_f = g_f / (G - sum_{j<f} g_j) drive the sequential binomial split
+ * of Diff::apply (diff.cpp:515-585); the last active face takes the remainder. */
+int or_setup(or_solver* s) {
+    int T = s->ntets;
+    s->geo = (float*)calloc((size_t)T * 4, sizeof(float));
+    s->nbr = (int32_t*)malloc((size_t)T * 4 * 4);
+    s->rface = (int32_t*)malloc((size_t)T * 4 * 4);
+    s->ivs = (double*)calloc(T, sizeof(double));
+    for (int t = 0; t < T; ++t) {
+        int c = s->tcomp[t];
+        s->ivs[t] = 1.0 / (1.0e3 * s->vol[t] * 6.02214076e23);
+        double g[4] = {0, 0, 0, 0};
+        for (int f = 0; f < 4; ++f) {
+            int n = s->neighb[(size_t)t * 4 + f];
+            s->nbr[(size_t)t * 4 + f] = -1;
+            s->rface[(size_t)t * 4 + f] = -1;
+            if (n < 0) continue;
+            int rf = -1;
+            for (int j = 0; j < 4; ++j)
+                if (s->neighb[(size_t)n * 4 + j] == t) rf = j;
+            if (rf < 0) return -1;
+            double d = s->dist[(size_t)t * 4 + f];
+            if (c >= 0 && d > 0.0 && s->tcomp[n] == c) {
+                g[f] = s->area[(size_t)t * 4 + f] / (s->vol[t] * d);
+                s->nbr[(size_t)t * 4 + f] = n;
+                s->rface[(size_t)t * 4 + f] = rf;
+            }
+        }
+        double G = g[0] + g[1] + g[2] + g[3];
+        int lastf = -1;
+        for (int f = 0; f < 4; ++f)
+            if (g[f] > 0.0) lastf = f;
+        double rem = G;
+        for (int f = 0; f < 3; ++f) {
+            double cf = 0.0;
+            if (g[f] > 0.0) {
+                cf = (f == lastf) ? 1.0 : g[f] / rem;
+                if (cf > 1.0) cf = 1.0;
+                rem -= g[f];
+            }
+            s->geo[(size_t)t * 4 + f] = (float)cf;
+        }
+        s->geo[(size_t)t * 4 + 3] = (float)G;
+    }
+    or_periods(s);
+    return 0;
+}
+
+void or_set_counts(or_solver* s, int spec, const uint32_t* row) {
+    memcpy(s->counts + (size_t)spec * s->ntets, row, (size_t)s->ntets * 4);
+}
+void or_get_counts(or_solver* s, int spec, uint32_t* row) {
+    memcpy(row, s->counts + (size_t)spec * s->ntets, (size_t)s->ntets * 4);
+}
+void or_set_clamped(or_solver* s, int tet, int spec, int on) {
+    if (on)
+        s->clamp[tet] |= 1u << spec;
+    else
+        s->clamp[tet] &= ~(1u << spec);
+}
+void or_set_time(or_solver* s, int real, double t, uint64_t window) {
+    s->t[real] = t;
+    s->window[real] = window;
+}
+double or_get_time(or_solver* s, int real) { return s->t[real]; }
+uint64_t or_get_window(or_solver* s, int real) { return s->window[real]; }
+double or_get_period(or_solver* s, int real) { return s->period[real]; }
+uint64_t or_get_reac_extent(or_solver* s, int reac) { return s->ext[reac]; }
+uint64_t or_get_diff_extent(or_solver* s) { return s->diff_moved; }
+
+/* ------------------------------------------------------------------------- */
+/* One split window                                                           */
+/* ------------------------------------------------------------------------- */
+
+/* Reac::rate (reac.cpp:184-232): h_mu = prod falling factorials, times
+ * ccst = k (1e3 V N_A)^(1 - order) (reac.cpp:44-53). */
+static double or_prop(const or_solver* s, const or_reac* r, const uint32_t* cnt, double k, double ivs) {
+    double ccst;
+    if (r->order == 1)
+        ccst = k;
+    else if (r->order == 0)
+        ccst = k / ivs;
+    else {
+        ccst = k * ivs;
+        for (int i = 2; i < r->order; ++i) ccst = ccst * ivs;
+    }
+    double h = 1.0;
+    for (int i = 0; i < s->nspec; ++i) {
+        uint32_t o = r->lhs[i];
+        if (o == 0) continue;
+        uint32_t c = cnt[i];
+        if (o > c) return 0.0;
+        if (o >= 4) h = h * (double)(c - 3);
+        if (o >= 3) h = h * (double)(c - 2);
+        if (o >= 2) h = h * (double)(c - 1);
+        h = h * (double)c;
+    }
+    return h * ccst;
+}
+
+/* SSA phase (TOS:1565-1588) then diffusion phase (TOS:1633-1712) of tet t. */
+static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
+    const int S = s->nspec;
+    const int c = s->tcomp[t];
+    uint32_t cnt[OR_MAXS];
+    double occ[OR_MAXS], last[OR_MAXS];
+    for (int i = 0; i < S; ++i) {
+        cnt[i] = s->counts[(size_t)i * s->ntets + t];
+        occ[i] = 0.0;
+        last[i] = 0.0;
+    }
+    const uint32_t clampm = s->clamp[t];
+    or_stream st;
+    or_stream_init(&st, s->seed, (uint32_t)r, (uint32_t)(t - s->real_begin[r]), w, 0u);
+    const double ivs = s->ivs[t];
+    const double* K = s->kcst + (size_t)r * s->nreac;
+
+    int rb = -1, re = -1;
+    for (int q = 0; q < s->nreac; ++q) {
+        if (s->reac[q].comp == c) {
+            if (rb < 0) rb = q;
+            re = q + 1;
+        }
+    }
+    if (rb >= 0) {
+        double tt = 0.0;
+        for (;;) {
+            double a0 = 0.0;
+            for (int q = rb; q < re; ++q) a0 = a0 + or_prop(s, &s->reac[q], cnt, K[q], ivs);
+            if (!(a0 > 0.0)) break;
+            double dt = -or_log(u_oc(or_u32(&st))) / a0;
+            if (tt + dt > T) break;
+            tt = tt + dt;
+            double target = u_co(or_u32(&st)) * a0;
+            double cum = 0.0;
+            int sel = -1, lastnz = -1;
+            for (int q = rb; q < re; ++q) {
+                double p = or_prop(s, &s->reac[q], cnt, K[q], ivs);
+                if (p > 0.0) {
+                    lastnz = q;
+                    cum = cum + p;
+                    if (target < cum) {
+                        sel = q;
+                        break;
+                    }
+                }
+            }
+            if (sel < 0) sel = lastnz;
+            /* Reac::apply (reac.cpp:235-251) with Tet::setCount occupancy (tet.cpp:318-340). */
+            for (int i = 0; i < S; ++i) {
+                int32_t d = s->reac[sel].upd[i];
+                if (d == 0 || ((clampm >> i) & 1u)) continue;
+                occ[i] = occ[i] + (double)cnt[i] * (tt - last[i]);
+                last[i] = tt;
+                cnt[i] = (uint32_t)((int64_t)cnt[i] + d);
+            }
+#pragma omp atomic
+            s->ext[sel] += 1;
+        }
+    }
+
+    const float* g = s->geo + (size_t)t * 4;
+    const double G = (double)g[3];
+    const double* Dc = s->dcst + ((size_t)r * s->ncomp + c) * S;
+    uint64_t moved = 0;
+    for (int i = 0; i < S; ++i) {
+        if (!s->has_rule[i]) continue;
+        double D = Dc[i];
+        if (!(D > 0.0)) continue;
+        uint32_t* o = s->outflow + ((size_t)i * s->ntets + t) * 4;
+        o[0] = o[1] = o[2] = o[3] = 0;
+        uint32_t pop = cnt[i];
+        if (pop == 0) continue;
+        double t1 = T * (D * G);
+        if (t1 >= 1.0) t1 = 1.0;
+        uint32_t mean_n = pop;
+        if (occ[i] != 0.0 || last[i] != 0.0) {
+            double nbar = (occ[i] + (double)pop * (T - last[i])) / T;
+            if (nbar > (double)pop) nbar = (double)pop;
+            double nint = floor(nbar);
+            double frc = nbar - nint;
+            mean_n = (uint32_t)nint;
+            if (frc > 0.0 && u_co(or_u32(&st)) < frc) mean_n += 1;
+        }
+        uint32_t Kn = or_binom(&st, mean_n, t1);
+        if (Kn == 0) continue;
+        uint32_t rem = Kn;
+        for (int f = 0; f < 3; ++f) {
+            o[f] = or_binom(&st, rem, (double)g[f]);
+            rem -= o[f];
+        }
+        o[3] = rem;
+        if (!((clampm >> i) & 1u)) cnt[i] = pop - Kn;
+        moved += Kn;
+    }
+    for (int i = 0; i < S; ++i) s->counts[(size_t)i * s->ntets + t] = cnt[i];
+#pragma omp atomic
+    s->diff_moved += moved;
+}
+
+/* Arrivals: Tet::incCount on the receiving tet (tet.cpp:342-370), skipped when clamped. */
+static void or_tet_enter(or_solver* s, int r, int t) {
+    const int c = s->tcomp[t];
+    const double* Dc = s->dcst + ((size_t)r * s->ncomp + c) * s->nspec;
+    for (int i = 0; i < s->nspec; ++i) {
+        if (!s->has_rule[i] || !(Dc[i] > 0.0) || ((s->clamp[t] >> i) & 1u)) continue;
+        uint64_t sum = s->counts[(size_t)i * s->ntets + t];
+        for (int f = 0; f < 4; ++f) {
+            int n = s->nbr[(size_t)t * 4 + f];
+            if (n < 0) continue;
+            sum += s->outflow[((size_t)i * s->ntets + n) * 4 + s->rface[(size_t)t * 4 + f]];
+        }
+        s->counts[(size_t)i * s->ntets + t] = (uint32_t)sum;
+    }
+}
+
+/* run(endtime) for every realization (TOS:1507-1527, window recurrence TOS:1550-1558 and
+ * the time update at the end of each window TOS:1818-1823). Returns windows run. */
+uint64_t or_run(or_solver* s, double endtime) {
+    uint64_t total = 0;
+    for (int r = 0; r < s->nreal; ++r) {
+        int tb = s->real_begin[r], te = s->real_begin[r + 1];
+        /* TOS:1513: a run to (almost) the current time only sets the time
+         * (util::almost_equal, src/steps/util/collections.hpp:144-148). */
+        double d = fabs(s->t[r] - endtime);
+        if (d <= 2.220446049250313e-16 * fabs(s->t[r] + endtime) * 4 || d < 2.2250738585072014e-308) {
+            s->t[r] = endtime;
+            continue;
+        }
+        while (s->t[r] < endtime) {
+            double t = s->t[r], per = s->period[r];
+            double T = (t + per > endtime) ? endtime - t : per;
+            uint64_t w = s->window[r];
+#pragma omp parallel for schedule(dynamic, 256)
+            for (int tet = tb; tet < te; ++tet)
+                if (s->tcomp[tet] >= 0) or_tet_window(s, r, tet, T, w);
+#pragma omp parallel for schedule(static)
+            for (int tet = tb; tet < te; ++tet)
+                if (s->tcomp[tet] >= 0) or_tet_enter(s, r, tet);
+            s->t[r] = (t + per > endtime) ? endtime : t + per;
+            s->window[r] = w + 1;
+            total += 1;
+        }
+    }
+    return total;
+}

@@ -1,0 +1,148 @@
+"""TEST INFRASTRUCTURE ONLY — ctypes wrapper of the CPU oracle (liboracle.so).
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline and reference arms.
+The product (steps_b200) never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import build_oracle
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        path = build_oracle.build_oracle()
+        lib = C.CDLL(path)
+        P = C.c_void_p
+        pf, pi, pu = (C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_uint32))
+        lib.or_create.restype = P
+        lib.or_create.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, pf, pi, pf, pf, pi, C.c_int, pi]
+        lib.or_destroy.argtypes = [P]
+        lib.or_add_reac.argtypes = [P, C.c_int, pu, pi, C.c_double]
+        lib.or_add_reac.restype = C.c_int
+        lib.or_add_diff.argtypes = [P, C.c_int, C.c_int, C.c_double]
+        lib.or_set_reac_k.argtypes = [P, C.c_int, C.c_int, C.c_double]
+        lib.or_setup.argtypes = [P]
+        lib.or_setup.restype = C.c_int
+        lib.or_set_counts.argtypes = [P, C.c_int, pu]
+        lib.or_get_counts.argtypes = [P, C.c_int, pu]
+        lib.or_set_clamped.argtypes = [P, C.c_int, C.c_int, C.c_int]
+        lib.or_set_time.argtypes = [P, C.c_int, C.c_double, C.c_uint64]
+        lib.or_get_time.argtypes = [P, C.c_int]
+        lib.or_get_time.restype = C.c_double
+        lib.or_get_window.argtypes = [P, C.c_int]
+        lib.or_get_window.restype = C.c_uint64
+        lib.or_get_period.argtypes = [P, C.c_int]
+        lib.or_get_period.restype = C.c_double
+        lib.or_get_reac_extent.argtypes = [P, C.c_int]
+        lib.or_get_reac_extent.restype = C.c_uint64
+        lib.or_get_diff_extent.argtypes = [P]
+        lib.or_get_diff_extent.restype = C.c_uint64
+        lib.or_run.argtypes = [P, C.c_double]
+        lib.or_run.restype = C.c_uint64
+        lib.or_philox4x32_10.argtypes = [pu, pu, pu]
+        lib.or_log_export.argtypes = [C.c_double]
+        lib.or_log_export.restype = C.c_double
+        lib.or_binom_many.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, pu]
+        _lib = lib
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class Oracle:
+    """CPU oracle over tables from steps_b200.solver.flatten (same species/reaction order).
+
+    The number of OpenMP threads is taken from OMP_NUM_THREADS at library load."""
+
+    def __init__(self, tables, seed, realizations=None):
+        self.L = load()
+        F = tables
+        self.F = F
+        self.ntets = int(F["vol"].size)
+        self.nspec = len(F["spec_names"])
+        off = np.ascontiguousarray(realizations if realizations is not None else [0, self.ntets],
+                                   dtype=np.int32)
+        self._keep = [F["vol"], F["neighb"], F["area"], F["dist"], F["tet_comp"], off]
+        self.off = off
+        self.nreal = len(off) - 1
+        self.h = self.L.or_create(C.c_uint64(seed), self.ntets, self.nspec, max(len(F["comp_names"]), 1),
+                                  _p(F["vol"], C.c_double), _p(F["neighb"], C.c_int32),
+                                  _p(F["area"], C.c_double), _p(F["dist"], C.c_double),
+                                  _p(F["tet_comp"], C.c_int32), self.nreal, _p(off, C.c_int32))
+        if not self.h:
+            raise ValueError("oracle supports at most 32 species")
+        for (ci, _rid, lhs, upd, k) in F["reacs"]:
+            self.L.or_add_reac(self.h, ci, _p(lhs, C.c_uint32), _p(upd, C.c_int32), k)
+        for (ci, _did, s, d) in F["diffs"]:
+            self.L.or_add_diff(self.h, ci, s, d)
+        if self.L.or_setup(self.h) != 0:
+            raise ValueError("neighbour table is not symmetric")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.or_destroy(self.h)
+            self.h = None
+
+    def set_counts(self, s, row):
+        a = np.ascontiguousarray(row, dtype=np.uint32)
+        self.L.or_set_counts(self.h, s, _p(a, C.c_uint32))
+
+    def get_counts(self, s):
+        a = np.empty(self.ntets, dtype=np.uint32)
+        self.L.or_get_counts(self.h, s, _p(a, C.c_uint32))
+        return a
+
+    def set_reac_k(self, reac, real, k):
+        self.L.or_set_reac_k(self.h, reac, real, k)
+
+    def set_clamped(self, tet, s, on):
+        self.L.or_set_clamped(self.h, tet, s, 1 if on else 0)
+
+    def set_time(self, real, t, window):
+        self.L.or_set_time(self.h, real, t, window)
+
+    def time(self, real=0):
+        return self.L.or_get_time(self.h, real)
+
+    def window(self, real=0):
+        return self.L.or_get_window(self.h, real)
+
+    def period(self, real=0):
+        return self.L.or_get_period(self.h, real)
+
+    def reac_extent(self, reac):
+        return self.L.or_get_reac_extent(self.h, reac)
+
+    def diff_extent(self):
+        return self.L.or_get_diff_extent(self.h)
+
+    def run(self, endtime):
+        return self.L.or_run(self.h, endtime)
+
+
+def philox(ctr, key):
+    L = load()
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    o = np.empty(4, dtype=np.uint32)
+    L.or_philox4x32_10(_p(c, C.c_uint32), _p(k, C.c_uint32), _p(o, C.c_uint32))
+    return [int(x) for x in o]
+
+
+def log(x):
+    return load().or_log_export(float(x))
+
+
+def binom_many(seed, unit, n, p, count):
+    out = np.empty(count, dtype=np.uint32)
+    load().or_binom_many(seed, unit, n, p, count, _p(out, C.c_uint32))
+    return out
