@@ -119,6 +119,14 @@ int sg_set_launch(sg_solver* h, int32_t block, int32_t grid);
 int sg_set_conservation_check(sg_solver* h, int32_t on);
 /* Device status word (SG_ERR_* bits). */
 int sg_get_status(sg_solver* h, uint32_t* status);
+/* The CUDA stream (cudaStream_t) every kernel of this solver is launched on. */
+int sg_get_stream(sg_solver* h, void** stream);
+/* CUDA-event timing of the window launches of each run() (resets the totals).  The
+ * reference's MPI_PROFILING timers (getCompTime etc., TOS:8330-8359) have this role. */
+int sg_set_profiling(sg_solver* h, int32_t on);
+/* Device ms spent in window launches and their count since profiling was switched on,
+ * and the number of kernels this solver has launched since creation. */
+int sg_get_profile(sg_solver* h, double* window_ms, uint64_t* windows, uint64_t* launches);
 
 #ifdef __cplusplus
 }

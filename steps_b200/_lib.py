@@ -76,6 +76,9 @@ PROTOTYPES = {
     "sg_set_launch": [_P, _i32, _i32],
     "sg_set_conservation_check": [_P, _i32],
     "sg_get_status": [_P, _pu32],
+    "sg_get_stream": [_P, C.POINTER(_P)],
+    "sg_set_profiling": [_P, _i32],
+    "sg_get_profile": [_P, _pf64, _pu64, _pu64],
 }
 
 _lib = None

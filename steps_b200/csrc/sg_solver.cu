@@ -88,14 +88,25 @@ struct Solver {
     int grid = 0;
     bool check = true;
 
+    // ---- launch accounting and optional per-run CUDA-event timing ----
+    uint64_t launches = 0;                      // kernels launched by this solver
+    bool profiling = false;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    double prof_ms = 0.0;                       // device time of window launches
+    uint64_t prof_windows = 0;
+
     Solver(uint64_t s, int dev) : device(dev), seed(s) {
         SG_CUDA(cudaSetDevice(device));
         SG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        SG_CUDA(cudaEventCreate(&ev_begin));
+        SG_CUDA(cudaEventCreate(&ev_end));
         cudaDeviceProp prop;
         SG_CUDA(cudaGetDeviceProperties(&prop, device));
         nsm = prop.multiProcessorCount;
     }
     ~Solver() {
+        if (ev_begin) cudaEventDestroy(ev_begin);
+        if (ev_end) cudaEventDestroy(ev_end);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -448,7 +459,17 @@ struct Solver {
         if (n == 0) return 0;
         sg_window_args a = window_args();
         int g = window_grid();
+        if (profiling) SG_CUDA(cudaEventRecord(ev_begin, stream));
         for (uint64_t i = 0; i < n; ++i) launch_window(a, g);
+        launches += n;
+        if (profiling) {
+            SG_CUDA(cudaEventRecord(ev_end, stream));
+            SG_CUDA(cudaEventSynchronize(ev_end));
+            float ms = 0.0f;
+            SG_CUDA(cudaEventElapsedTime(&ms, ev_begin, ev_end));
+            prof_ms += ms;
+            prof_windows += n;
+        }
         for (int r = 0; r < nreal; ++r) {
             reals[r].window += k[r];
             if (k[r]) reals[r].pending = 1;
@@ -485,6 +506,7 @@ struct Solver {
         SG_CUDA(cudaGetLastError());
         clear_pending_kernel<<<(nreal + 255) / 256, 256, 0, stream>>>(d_reals.p, nreal);
         SG_CUDA(cudaGetLastError());
+        launches += 2;
         for (auto& rl : reals) rl.pending = 0;
         pending_host = false;
         sync();
@@ -1049,6 +1071,31 @@ int sg_set_launch(sg_solver* h, int32_t block, int32_t grid) {
 
 int sg_set_conservation_check(sg_solver* h, int32_t on) {
     return guarded([&] { S(h)->check = on != 0; });
+}
+
+int sg_get_stream(sg_solver* h, void** stream) {
+    return guarded([&] {
+        need(stream, "stream");
+        *stream = (void*)S(h)->stream;
+    });
+}
+
+int sg_set_profiling(sg_solver* h, int32_t on) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->profiling = on != 0;
+        s->prof_ms = 0.0;
+        s->prof_windows = 0;
+    });
+}
+
+int sg_get_profile(sg_solver* h, double* window_ms, uint64_t* windows, uint64_t* launches) {
+    return guarded([&] {
+        Solver* s = S(h);
+        if (window_ms) *window_ms = s->prof_ms;
+        if (windows) *windows = s->prof_windows;
+        if (launches) *launches = s->launches;
+    });
 }
 
 int sg_get_status(sg_solver* h, uint32_t* status) {

@@ -301,6 +301,26 @@ class TetOpSplit:
     def setConservationCheck(self, on):
         check(self._L.sg_set_conservation_check(self._h, 1 if on else 0))
 
+    def getStream(self):
+        """The cudaStream_t (as an int) all kernels of this solver run on."""
+        p = C.c_void_p()
+        check(self._L.sg_get_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def setProfiling(self, on):
+        check(self._L.sg_set_profiling(self._h, 1 if on else 0))
+
+    def getProfile(self):
+        """(device ms in window launches, windows timed, kernels launched since creation)."""
+        ms, w, n = C.c_double(), C.c_uint64(), C.c_uint64()
+        check(self._L.sg_get_profile(self._h, C.byref(ms), C.byref(w), C.byref(n)))
+        return ms.value, w.value, n.value
+
+    def getStatus(self):
+        s = C.c_uint32()
+        check(self._L.sg_get_status(self._h, C.byref(s)))
+        return s.value
+
     # ----------------------------------------------------------- API_1 names
     getTetCount = getTetSpecCount
     setTetCount = setTetSpecCount
