@@ -1,0 +1,344 @@
+"""Benchmark: operator-split spatial SSA throughput (tet-species updates/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): 40^3 Kuhn cubes of 0.1 um (384,000 tets), the seeded 8-species /
+12-reaction network, species 0-3 Poisson(50) per tet, run at the update period the
+solver derives from the largest scaled diffusion constant.  One step advances 1 ms of
+simulated time (all split windows in it); K = 10 steps cover the configuration's 10 ms.
+
+value: updates = tets x species x windows over the timed steps, divided by the device
+time of the steps (CUDA events on the solver's stream, L2 flushed between steps).
+e2e:   the same metric through the C ABI with host buffers: each step uploads every
+species row from pinned host memory, runs 1 ms and downloads every row.
+N > 1: independent replicas, one per GPU (the path is not sharded).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+STEP_SIM_S = 1.0e-3
+SEED = 1
+NCUBE = 40
+NSPEC = 8
+BYTES_PER_TET_SPEC = 40    # count r/w 8 B + 4 face outflows written 16 B + 4 inflows read 16 B
+BYTES_PER_TET = 32         # neighbour table 16 B + face coefficients 16 B
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload():
+    from steps_b200 import workloads as W
+
+    mesh = W.cube_mesh(NCUBE)
+    mdl = W.random_network(SEED)
+    rows = W.poisson_counts(mesh.ntets, 50.0, SEED, nspec=NSPEC)
+    return mdl, mesh, rows
+
+
+def config_dict(mesh):
+    return {
+        "workload": "plain_384k: 40^3 Kuhn cubes (0.1 um), 384,000 tets, 8 species, 12 reactions, "
+                    "Poisson(50) species 0-3, 10 ms",
+        "tets": int(mesh.ntets), "species": NSPEC, "reactions": 12,
+        "sim_ms_per_step": STEP_SIM_S * 1e3,
+        "network_seed": SEED,
+        "l2": "flushed between timed steps (256 MiB device write)",
+    }
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(mdl, mesh, rows, windows=4):
+    """The CPU oracle (C restatement, OpenMP over tets) on a bounded sample of the workload."""
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle.pyoracle import Oracle
+    from steps_b200.solver import flatten
+
+    ora = Oracle(flatten(mdl, mesh), seed=SEED)
+    for i in range(NSPEC):
+        ora.set_counts(i, rows[i])
+    per = ora.period()
+    ora.run(per)  # warm-up window
+    t0 = time.perf_counter()
+    n = ora.run(per * (1 + windows))
+    dt = time.perf_counter() - t0
+    upd = mesh.ntets * NSPEC * n
+    return {"value": upd / dt, "unit": "tet-species updates/s", "cores": threads, "kind": "port",
+            "sample": f"{n} split windows of the same workload (384,000 tets x 8 species), "
+                      f"{dt:.2f} s on {threads} host threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    mdl, mesh, rows = workload()
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle.pyoracle import Oracle
+    from steps_b200.solver import flatten
+
+    ora = Oracle(flatten(mdl, mesh), seed=SEED)
+    for i in range(NSPEC):
+        ora.set_counts(i, rows[i])
+    per = ora.period()
+    wins_per_step = 2
+    t = 0.0
+    for _ in range(args.warmup):
+        t += wins_per_step * per
+        ora.run(t)
+    total, upd = 0.0, 0
+    for _ in range(args.steps):
+        t += wins_per_step * per
+        t0 = time.perf_counter()
+        n = ora.run(t)
+        total += time.perf_counter() - t0
+        upd += mesh.ntets * NSPEC * n
+    v = upd / total
+    line = {
+        "metric": "tet-species updates/s", "value": v, "unit": "tet-species updates/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32+f64", "data": "synthetic",
+        "config": dict(config_dict(mesh), step=f"{wins_per_step} split windows (bounded CPU sample)"),
+        "cpu_baseline": {"value": v, "unit": "tet-species updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{wins_per_step} split windows per step on {threads} host threads; the "
+                                   "reference TetOpSplitP does not build here, so its CPU restatement runs"},
+        "e2e": {"value": v, "unit": "tet-species updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from steps_b200 import rng as srng
+    from steps_b200.solver import TetOpSplit
+
+    mdl, mesh, rows = workload()
+    r = srng.create("r123", 512)
+    r.initialize(SEED + rank)
+    sim = TetOpSplit(mdl, mesh, r, device=local)
+    for i, s in enumerate(sim.spec_names):
+        sim.setSpecCounts(s, rows[i])
+    ext = torch.cuda.ExternalStream(sim.getStream(), device=local)
+    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    t_sim = 0.0
+    for _ in range(args.warmup):
+        t_sim += STEP_SIM_S
+        sim.run(t_sim)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    sim.setProfiling(True)
+    _, _, launches0 = sim.getProfile()
+    it0 = sim.getNIteration()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush_buf.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+        t_sim += STEP_SIM_S
+        sim.run(t_sim)
+        with torch.cuda.stream(ext):
+            e1.record(ext)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    barrier()
+    clk = clocks.stop()
+    win_ms, nwin, launches1 = sim.getProfile()
+    windows = sim.getNIteration() - it0
+    sim.setProfiling(False)
+    updates = mesh.ntets * NSPEC * windows
+
+    t_max = total_ms
+    upd_all = updates
+    if dist is not None:
+        tt = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        uu = torch.tensor([updates], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(uu, op=dist.ReduceOp.SUM)
+        upd_all = float(uu.item())
+    value = upd_all / (t_max * 1e-3)
+
+    # End-to-end through the C ABI with pinned host buffers.
+    host = [torch.empty(mesh.ntets, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+            for _ in range(NSPEC)]
+    for i, s in enumerate(sim.spec_names):
+        sim.getSpecCounts(s, host[i])
+    barrier()
+    e2e_s, e2e_upd = 0.0, 0
+    for _ in range(args.steps):
+        it_a = sim.getNIteration()
+        t0 = time.perf_counter()
+        for i, s in enumerate(sim.spec_names):
+            sim.setSpecCounts(s, host[i])
+        t_sim += STEP_SIM_S
+        sim.run(t_sim)
+        for i, s in enumerate(sim.spec_names):
+            sim.getSpecCounts(s, host[i])
+        e2e_s += time.perf_counter() - t0
+        e2e_upd += mesh.ntets * NSPEC * (sim.getNIteration() - it_a)
+    e2e_val = e2e_upd / e2e_s
+    if dist is not None:
+        ee = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(ee, op=dist.ReduceOp.MAX)
+        e2e_val = e2e_upd * world / float(ee.item())
+
+    peak, peak_kind = peaks()
+    bytes_per_window = mesh.ntets * (BYTES_PER_TET_SPEC * NSPEC + BYTES_PER_TET)
+    avg_win_s = (win_ms * 1e-3) / max(nwin, 1)
+    achieved = bytes_per_window / avg_win_s / 1e9
+    traffic = None
+    prof_path = os.path.join(ROOT, "profiles", "traffic_window_kernel.json")
+    if os.path.exists(prof_path):
+        with open(prof_path) as f:
+            traffic = json.load(f).get("bytes_per_launch_scaled_to_384k")
+
+    if rank == 0:
+        mdl_cpu, mesh_cpu, rows_cpu = (mdl, mesh, rows)
+        cpu = cpu_baseline(mdl_cpu, mesh_cpu, rows_cpu) if world == 1 else None
+        line = {
+            "metric": "tet-species updates/s", "value": value, "unit": "tet-species updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32+f64", "data": "synthetic",
+            "config": dict(config_dict(mesh), parallelism=f"replicas{world}"),
+            "sim_ms_per_wall_s": (STEP_SIM_S * 1e3 * args.steps) / (t_max * 1e-3),
+            "windows_per_step": windows / args.steps,
+            "e2e": {"value": e2e_val, "unit": "tet-species updates/s",
+                    "h2d_bytes_per_step": NSPEC * mesh.ntets * 4, "d2h_bytes_per_step": NSPEC * mesh.ntets * 4},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                         else "fallback 6650 GB/s",
+                         "kernel": "sg::window_kernel<128>",
+                         "algorithmic_bytes_per_launch": bytes_per_window,
+                         "avg_launch_us": avg_win_s * 1e6},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": int(launches1 - launches0),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    del sim
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

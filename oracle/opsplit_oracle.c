@@ -149,6 +149,7 @@ static uint32_t or_binv(or_stream* st, uint32_t n, double p) {
         u = u - r;
         x += 1;
         r = r * (a / (double)x - s);
+        if (!(r > 0.0)) break;
     }
     return x;
 }
@@ -523,6 +524,7 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
                 }
             }
             if (sel < 0) sel = lastnz;
+            if (sel < 0) break;
             /* Reac::apply (reac.cpp:235-251) with Tet::setCount occupancy (tet.cpp:318-340). */
             for (int i = 0; i < S; ++i) {
                 int32_t d = s->reac[sel].upd[i];

@@ -241,6 +241,7 @@ SG_HD uint32_t sg_binv(sg_stream* st, uint32_t n, double p) {
         u = u - r;
         x += 1;
         r = r * (a / (double)x - s);
+        if (!(r > 0.0)) break;  // pmf underflowed past the mass: stop at x
     }
     return x;
 }

@@ -141,6 +141,7 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
             }
         }
         if (sel < 0) sel = lastnz;
+        if (sel < 0) break;
         const sg_reac* rc = &a.reacs[sel];
         int nu = rc->nupd;
         for (int i = 0; i < nu; ++i) {

@@ -1,0 +1,139 @@
+"""GPU split windows vs the CPU oracle, bit for bit, through the C ABI.
+
+The oracle restates TetOpSplitP's window (src/steps/mpi/tetopsplit/tetopsplit.cpp:1528-1839)
+with the same Philox counters; every count of every tet must agree after every run().
+"""
+import numpy as np
+import pytest
+
+from steps_b200 import workloads as W
+from tests.helpers import assert_same, pair, sync_counts, two_comp_mesh, two_comp_model
+
+pytestmark = pytest.mark.gpu
+
+
+def test_plain_small_ab_c(steps_lib):
+    """A + B <-> C with diffusion on 10^3 Kuhn cubes, recorded every 1 ms (4 windows/ms)."""
+    sim, ora = pair(W.ab_c_model(), W.cube_mesh(10), seed=1)
+    sim.setCompSpecCount("comp", "A", 10000)
+    sim.setCompSpecCount("comp", "B", 10000)
+    assert sim.getCompSpecCount("comp", "A") == 10000
+    sync_counts(sim, ora)
+    assert sim.getUpdPeriod() == ora.period()
+    for k in range(1, 21):
+        t = k * 1.0e-3
+        sim.run(t)
+        ora.run(t)
+        assert_same(sim, ora, f"t={t}")
+        assert sim.getTime() == t
+    assert sim.getNIteration() == ora.window() == 80
+    assert sim.getCompSpecCount("comp", "A") + sim.getCompSpecCount("comp", "C") == 10000
+    for r, name in enumerate(["fwd", "bwd"]):
+        assert sim.getCompReacExtent("comp", name) == ora.reac_extent(r)
+    assert sim.getDiffExtent() == ora.diff_extent()
+    assert sim.getStatus() == 0
+
+
+def test_diffusion_only_large_counts(steps_lib):
+    """Pure diffusion with counts in the BTRD regime (n p >= 10)."""
+    mdl = W.ab_c_model(kf=0.0, kb=0.0)
+    sim, ora = pair(mdl, W.cube_mesh(5), seed=99)
+    row = np.zeros(sim.geom.ntets, dtype=np.uint32)
+    row[::7] = 200000
+    row[3] = 4000000000
+    sim.setSpecCounts("A", row)
+    sim.setSpecCounts("B", np.full(sim.geom.ntets, 3, dtype=np.uint32))
+    sync_counts(sim, ora)
+    total = int(row.sum(dtype=np.uint64))
+    for k in range(1, 6):
+        t = k * 3.0 * sim.getUpdPeriod()
+        sim.run(t)
+        ora.run(t)
+        assert_same(sim, ora, f"window {k}")
+        assert int(sim.getSpecCounts("A").sum(dtype=np.uint64)) == total
+
+
+def test_random_network_poisson(steps_lib):
+    """8 species, 12 reactions (zeroth, first, second order) on 6^3 cubes, Poisson(50) counts."""
+    mdl = W.random_network(2025)
+    sim, ora = pair(mdl, W.cube_mesh(6), seed=2025)
+    rows = W.poisson_counts(sim.geom.ntets, 50.0, 2025)
+    for i, s in enumerate(sim.spec_names):
+        sim.setSpecCounts(s, rows[i])
+    sync_counts(sim, ora)
+    per = sim.getUpdPeriod()
+    for k in range(1, 9):
+        t = k * 2.5 * per
+        sim.run(t)
+        ora.run(t)
+        assert_same(sim, ora, f"t={t}")
+    for r in range(12):
+        assert sim.getCompReacExtent("comp", f"r{r}") == ora.reac_extent(r)
+
+
+def test_two_compartments(steps_lib):
+    """Different reactions and diffusion rules per compartment; no diffusion across."""
+    sim, ora = pair(two_comp_model(), two_comp_mesh(6), seed=5)
+    for c in ("left", "right"):
+        for s in ("A", "B"):
+            sim.setCompSpecCount(c, s, 2500.5)
+    sync_counts(sim, ora)
+    for k in range(1, 7):
+        t = k * 1.7e-4
+        sim.run(t)
+        ora.run(t)
+        assert_same(sim, ora, f"t={t}")
+
+
+def test_clamped_species(steps_lib):
+    sim, ora = pair(W.ab_c_model(), W.cube_mesh(5), seed=11)
+    sim.setCompSpecCount("comp", "A", 5000)
+    sim.setCompSpecCount("comp", "B", 5000)
+    for t in (0, 17, 400):
+        sim.setTetSpecClamped(t, "A", True)
+        ora.set_clamped(t, 0, True)
+    sync_counts(sim, ora)
+    clamped_before = [sim.getTetSpecCount(t, "A") for t in (0, 17, 400)]
+    for k in range(1, 6):
+        t = k * 1.0e-3
+        sim.run(t)
+        ora.run(t)
+        assert_same(sim, ora, f"t={t}")
+    assert [sim.getTetSpecCount(t, "A") for t in (0, 17, 400)] == clamped_before
+
+
+def test_batched_realizations_with_jitter(steps_lib):
+    """Realizations of different sizes in one launch, per-realization rate constants."""
+    sizes = [3, 5, 4, 6]
+    mesh = W.batched_mesh(sizes)
+    mdl = W.random_network(7)
+    sim, ora = pair(mdl, mesh, seed=3, realizations=mesh.offsets)
+    jit = W.rate_jitter(len(sizes), 12, 3)
+    for r in range(len(sizes)):
+        for q in range(12):
+            k = sim.getCompReacK("comp", f"r{q}", r) * jit[r, q]
+            sim.setCompReacK("comp", f"r{q}", k, realization=r)
+            ora.set_reac_k(q, r, k)
+    rows = W.poisson_counts(mesh.ntets, 20.0, 3)
+    for i, s in enumerate(sim.spec_names):
+        sim.setSpecCounts(s, rows[i])
+    sync_counts(sim, ora)
+    per = sim.getUpdPeriod()
+    for k in range(1, 5):
+        t = k * 3.0 * per
+        sim.run(t)
+        ora.run(t)
+        assert_same(sim, ora, f"t={t}")
+
+
+@pytest.mark.parametrize("block", [64, 256])
+def test_launch_shapes_agree(steps_lib, block):
+    """The result does not depend on the block size (counter-based streams)."""
+    sim, ora = pair(W.ab_c_model(), W.cube_mesh(7), seed=4, block=block)
+    sim.setCompSpecCount("comp", "A", 7000)
+    sim.setCompSpecCount("comp", "B", 3000)
+    sync_counts(sim, ora)
+    for k in range(1, 4):
+        sim.run(k * 1.0e-3)
+        ora.run(k * 1.0e-3)
+        assert_same(sim, ora, f"block {block} step {k}")
