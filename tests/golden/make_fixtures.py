@@ -1,0 +1,65 @@
+"""Regenerate the golden fixtures from the reference tree (run in the build container only).
+
+    python tests/golden/make_fixtures.py
+
+  sphere_rad1_37tets.npz  vertices (m, scale 1e-6 as the reference test imports them) and
+                          tets of test/validation/API_1/validation_rd_mpi/meshes/
+                          sphere_rad1_37tets.inp, the mesh of the reference's analytic
+                          TetOpSplit kinetics validation (parallel_spatial_tetopsplit.py).
+  philox_kat.json         Philox4x32-10 known answers from the reference's vendored Random123
+                          (oracle/ref_philox_kat.c, built by oracle/build_oracle.py).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = "/root/reference"
+
+
+def read_abaqus(path, scale):
+    """Nodes and C3D4 elements of an Abaqus .inp file (1-based ids in the file)."""
+    nodes, elems, mode = {}, [], None
+    with open(path) as f:
+        for line in f:
+            s = line.strip()
+            if not s or s.startswith("**"):
+                continue
+            if s.startswith("*"):
+                u = s.upper()
+                mode = "node" if u.startswith("*NODE") else ("elem" if u.startswith("*ELEMENT") else None)
+                continue
+            parts = [p for p in s.replace(",", " ").split()]
+            if mode == "node":
+                nodes[int(parts[0])] = [float(x) * scale for x in parts[1:4]]
+            elif mode == "elem":
+                elems.append([int(x) for x in parts[1:5]])
+    ids = sorted(nodes)
+    remap = {nid: i for i, nid in enumerate(ids)}
+    verts = np.array([nodes[i] for i in ids])
+    tets = np.array([[remap[n] for n in e] for e in elems], dtype=np.int64)
+    return verts, tets
+
+
+def main():
+    inp = os.path.join(REF, "test/validation/API_1/validation_rd_mpi/meshes/sphere_rad1_37tets.inp")
+    v, t = read_abaqus(inp, 1.0e-6)
+    np.savez(os.path.join(HERE, "sphere_rad1_37tets.npz"), verts=v, tets=t)
+    print("sphere:", v.shape, t.shape)
+    sys.path.insert(0, ROOT)
+    from oracle import build_oracle
+
+    exe = build_oracle.build_ref(force=True)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    with open(os.path.join(HERE, "philox_kat.json"), "w") as f:
+        f.write(out)
+    print("philox_kat.json written")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,98 @@
+"""Pins of the CPU oracle: known answers and distribution tests (CPU only).
+
+- Philox4x32-10 against tests/golden/philox_kat.json, produced by the reference's own
+  vendored Random123 header (src/third_party/Random123/philox.h) via oracle/ref_philox_kat.c.
+- The project log against math.log.
+- The binomial sampler with the chi-squared check of the reference's
+  test/unit/cpp/test_rng.cpp:51-90 (same (n, p) grid, sample sizes and levels), and a
+  goodness-of-fit test with the proper degrees of freedom over both sampler regimes.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+from scipy import stats
+
+from oracle import pyoracle
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def test_philox_known_answers():
+    with open(os.path.join(HERE, "golden", "philox_kat.json")) as f:
+        kat = json.load(f)
+    assert len(kat) >= 8
+    for c in kat:
+        assert pyoracle.philox(c["ctr"], c["key"]) == c["out"]
+
+
+def test_philox_published_zero_vector():
+    # Random123 known-answer for philox4x32_10 with zero counter and key.
+    assert pyoracle.philox([0, 0, 0, 0], [0, 0]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+
+
+def test_log_matches_libm():
+    rng = np.random.default_rng(1)
+    xs = np.concatenate([np.exp(rng.uniform(-700, 700, 20000)), rng.uniform(0, 1, 20000) + 1e-300,
+                         1.0 + rng.uniform(-1e-6, 1e-6, 2000), [1.0, 2.0, 0.5, 2.3283064365386963e-10,
+                                                                 5e-324, 1.7e308]])
+    for x in xs:
+        ref = math.log(x)
+        got = pyoracle.log(x)
+        assert abs(got - ref) <= 4e-16 * max(abs(ref), 1e-300) + 1e-300, (x, got, ref)
+
+
+def _ref_style_pvalue(sample, t, p_test, t_test):
+    """Chi-squared statistic and p-value exactly as test_rng.cpp:51-90 forms them
+    (degrees of freedom = n_sample - 1)."""
+    n = len(sample)
+    obs = np.bincount(sample, minlength=t + 1)[: t + 1]
+    k = np.arange(t + 1)
+    exp = n * stats.binom.pmf(k, t_test, p_test)
+    chi = float(np.sum((exp - obs) ** 2 / exp))
+    return 1.0 - stats.chi2.cdf(chi, n - 1)
+
+
+@pytest.mark.parametrize("t,p", [(10, 0.3), (8, 0.4)])
+def test_binomial_reference_grid_accepts(t, p):
+    sample = pyoracle.binom_many(12345, 0, t, p, 10000).astype(np.int64)
+    assert _ref_style_pvalue(sample, t, p, t) >= 1 - 0.999
+
+
+@pytest.mark.parametrize("t_test,p_test", [(10, 0.45), (15, 0.4)])
+def test_binomial_reference_grid_rejects_wrong(t_test, p_test):
+    sample = pyoracle.binom_many(12345, 1, 10, 0.3, 100).astype(np.int64)
+    assert _ref_style_pvalue(sample, 10, p_test, t_test) <= 0.9
+
+
+@pytest.mark.parametrize("n,p", [(10, 0.3), (40, 0.2), (1000, 0.3), (200, 0.93), (5000, 0.5),
+                                 (1 << 20, 3e-6), (60, 0.999), (4000000000, 2e-9), (25, 0.4)])
+def test_binomial_goodness_of_fit(n, p):
+    m = 200000
+    x = pyoracle.binom_many(777, n % 1000, n, p, m).astype(np.int64)
+    mean, var = n * p, n * p * (1 - p)
+    assert abs(x.mean() - mean) < 5 * math.sqrt(var / m) + 1e-12
+    lo, hi = stats.binom.ppf(1e-6, n, p), stats.binom.ppf(1 - 1e-6, n, p)
+    ks = np.arange(int(lo), int(hi) + 1)
+    pmf = stats.binom.pmf(ks, n, p)
+    keep = pmf * m >= 5
+    ks, pmf = ks[keep], pmf[keep]
+    obs = np.array([(x == k).sum() for k in ks])
+    rest_obs = m - obs.sum()
+    rest_exp = m * (1 - pmf.sum())
+    chi = float(np.sum((obs - m * pmf) ** 2 / (m * pmf)))
+    dof = len(ks) - 1
+    if rest_exp >= 5:
+        chi += (rest_obs - rest_exp) ** 2 / rest_exp
+        dof += 1
+    assert stats.chi2.sf(chi, dof) > 1e-4, (n, p, chi, dof)
+
+
+def test_binomial_edges():
+    assert (pyoracle.binom_many(1, 0, 0, 0.5, 10) == 0).all()
+    assert (pyoracle.binom_many(1, 0, 17, 0.0, 10) == 0).all()
+    assert (pyoracle.binom_many(1, 0, 17, 1.0, 10) == 17).all()
+    x = pyoracle.binom_many(1, 0, 3, 0.9999999, 1000)
+    assert x.max() <= 3
