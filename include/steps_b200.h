@@ -128,6 +128,42 @@ int sg_set_profiling(sg_solver* h, int32_t on);
  * and the number of kernels this solver has launched since creation. */
 int sg_get_profile(sg_solver* h, double* window_ms, uint64_t* windows, uint64_t* launches);
 
+/* ---- allocation-free entry point (no counterpart in the reference) ----------
+ *
+ * For callers that cannot call cudaMalloc: code running while a stream is being
+ * captured into a CUDA graph, programs whose device memory comes only from their own
+ * pool allocator, and loops that cannot afford an allocation's device synchronisation.
+ * It advances one realization in one compartment (every tet) from t0 to t_end with the
+ * same window kernel as sg_run, and returns with counts complete.  The caller owns all
+ * inputs and outputs; the library allocates nothing.  Its scratch (packed mesh tables,
+ * face-outflow double buffer, counters) is one fixed device array of
+ * SG_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until exit.
+ *
+ * Limits: ntets <= SG_NOALLOC_MAX_TETS, ntets * nspec <= SG_NOALLOC_MAX_TET_SPECIES,
+ * nspec <= 32, nreac <= SG_NOALLOC_MAX_REACS; larger problems return SG_EARG.
+ *
+ * Device buffers (current device): counts [nspec][ntets] uint32 (in/out); vol [ntets],
+ * neighb [ntets][4] (-1 = none), area [ntets][4], dist [ntets][4] as in sg_set_mesh.
+ * Host arrays: lhs / upd [nreac][nspec] dense rows as in sg_add_reac, kcst [nreac],
+ * dcst [nspec] (0 = species does not diffuse).  seed, window0 (windows already run in
+ * earlier calls: continues the same Philox streams) and t0 give the same results as a
+ * solver created with that seed and run over the same times.  stream is a cudaStream_t
+ * (NULL = legacy default stream); the call synchronises it before returning.
+ * windows_out / period_out (optional) receive the windows run and the update period.
+ *
+ * The first call on a device looks up the scratch array's device address; make that
+ * first call before any stream capture.  Every call reuses the same array and clears
+ * what must start at zero; calls that overlap on the GPU race on it. */
+#define SG_NOALLOC_MAX_TETS 65536
+#define SG_NOALLOC_MAX_TET_SPECIES 262144
+#define SG_NOALLOC_MAX_REACS 64
+#define SG_NOALLOC_SCRATCH_BYTES 11021312
+int sg_run_noalloc(int32_t ntets, int32_t nspec, int32_t nreac, uint32_t* counts, const double* vol,
+                   const int32_t* neighb, const double* area, const double* dist, const uint32_t* lhs,
+                   const int32_t* upd, const double* kcst, const double* dcst, uint64_t seed, double t0,
+                   double t_end, uint64_t window0, void* stream, uint64_t* windows_out,
+                   double* period_out);
+
 #ifdef __cplusplus
 }
 #endif

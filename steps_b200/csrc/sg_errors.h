@@ -25,6 +25,9 @@ struct DeviceErr : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
 
+// Sets the message returned by sg_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
+
 }  // namespace sg
 
 #define SG_CUDA(call)                                                                    \

@@ -22,7 +22,7 @@
 
 #if defined(__CUDACC__)
 #define SG_HD __host__ __device__ __forceinline__
-#define SG_HD_NOINLINE __host__ __device__ __noinline__
+#define SG_HD_NOINLINE static __host__ __device__ __noinline__
 #else
 #define SG_HD static inline
 #define SG_HD_NOINLINE static

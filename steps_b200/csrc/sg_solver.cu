@@ -776,6 +776,8 @@ using sg::Solver;
 
 static thread_local std::string g_last_error;
 
+void sg::set_last_error(const std::string& msg) { g_last_error = msg; }
+
 template <typename F>
 static int guarded(F&& f) {
     try {

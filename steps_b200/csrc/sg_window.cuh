@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(BLOCK) window_kernel(sg_window_args a, int che
 }
 
 // Apply the pending inflow of the last window to the counts (enter phase only).
-__global__ void flush_kernel(sg_window_args a) {
+static __global__ void flush_kernel(sg_window_args a) {
     const size_t plane = (size_t)a.ntets * 4;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.ntets; t += gridDim.x * blockDim.x) {
         int r = find_real(a.reals, a.nreal, t);
@@ -389,7 +389,7 @@ __global__ void flush_kernel(sg_window_args a) {
     }
 }
 
-__global__ void clear_pending_kernel(sg_real* reals, int nreal) {
+static __global__ void clear_pending_kernel(sg_real* reals, int nreal) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreal; i += gridDim.x * blockDim.x)
         reals[i].pending = 0;
 }
