@@ -148,7 +148,7 @@ static uint32_t or_binv(or_stream* st, uint32_t n, double p) {
     while (u >= r && x < n) {
         u = u - r;
         x += 1;
-        r = r * (a / (double)x - s);
+        r = r * (a * (1.0 / (double)x) - s);
         if (!(r > 0.0)) break;
     }
     return x;
@@ -229,7 +229,7 @@ static uint32_t or_binom(or_stream* st, uint32_t n, double p) {
     if (p >= 1.0) return n;
     int flip = p > 0.5;
     double pp = flip ? 1.0 - p : p;
-    uint32_t k = ((double)n * pp < 10.0) ? or_binv(st, n, pp) : or_btrd(st, n, pp);
+    uint32_t k = ((double)n * pp < 24.0) ? or_binv(st, n, pp) : or_btrd(st, n, pp);
     return flip ? n - k : k;
 }
 
@@ -386,7 +386,7 @@ int or_setup(or_solver* s) {
     s->ivs = (double*)calloc(T, sizeof(double));
     for (int t = 0; t < T; ++t) {
         int c = s->tcomp[t];
-        s->ivs[t] = 1.0 / (1.0e3 * s->vol[t] * 6.02214076e23);
+        s->ivs[t] = 1.0 / (1.0e3 * s->vol[t] * 6.02214179e23); /* math/constants.hpp:45 */
         double g[4] = {0, 0, 0, 0};
         for (int f = 0; f < 4; ++f) {
             int n = s->neighb[(size_t)t * 4 + f];

@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libsteps_b200.so")
+# STEPS_B200_LIB may point at another build of the same sources (e.g. a tuning variant).
+LIB_PATH = os.environ.get("STEPS_B200_LIB") or os.path.join(_HERE, "libsteps_b200.so")
 
 
 class StepsError(RuntimeError):

@@ -61,7 +61,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 namespace {
 
-const double kAvogadro = 6.02214076e23;  // src/steps/math/constants.hpp
+const double kAvogadro = 6.02214179e23;  // src/steps/math/constants.hpp:45
 
 // Per-tet tables from the raw mesh arrays, exactly as the solver object builds them on
 // the host (diff.cpp:41-90 face coefficients; one compartment holding every tet), plus

@@ -102,21 +102,30 @@ SG_HD void sg_stream_init(sg_stream* s, uint64_t seed, uint32_t realization, uin
     s->b0 = s->b1 = s->b2 = s->b3 = 0;
 }
 
+// Refill of the 4-word buffer.  With SG_NOINLINE_REFILL the Philox rounds exist once
+// in the device code instead of at every draw site (smaller instruction footprint).
+#if defined(__CUDACC__) && defined(SG_NOINLINE_REFILL)
+static __host__ __device__ __noinline__
+#else
+SG_HD
+#endif
+void sg_stream_refill(sg_stream* s) {
+    sg_u32x4 c;
+    c.x = s->block;
+    c.y = s->unit;
+    c.z = s->wlo;
+    c.w = s->whi;
+    sg_u32x4 r = sg_philox4x32(c, s->k0, s->k1);
+    s->block += 1;
+    s->b0 = r.x;
+    s->b1 = r.y;
+    s->b2 = r.z;
+    s->b3 = r.w;
+    s->left = 4;
+}
+
 SG_HD uint32_t sg_next_u32(sg_stream* s) {
-    if (s->left == 0) {
-        sg_u32x4 c;
-        c.x = s->block;
-        c.y = s->unit;
-        c.z = s->wlo;
-        c.w = s->whi;
-        sg_u32x4 r = sg_philox4x32(c, s->k0, s->k1);
-        s->block += 1;
-        s->b0 = r.x;
-        s->b1 = r.y;
-        s->b2 = r.z;
-        s->b3 = r.w;
-        s->left = 4;
-    }
+    if (s->left == 0) sg_stream_refill(s);
     uint32_t v = s->b0;
     s->b0 = s->b1;
     s->b1 = s->b2;
@@ -227,10 +236,18 @@ SG_HD double sg_pow_u(double q, uint32_t n) {
 //       (Hormann, "The generation of binomial random variates", J. Statist.
 //        Comput. Simul. 46, 1993).
 // ---------------------------------------------------------------------------
-#define SG_BINV_CUT 10.0
+#define SG_BINV_CUT 24.0
 #define SG_BTRD_MAX_ITERS 256
+#define SG_RCP_TABLE 128   // 1/x for x < SG_RCP_TABLE, precomputed (same value as 1.0/x)
 
-SG_HD uint32_t sg_binv(sg_stream* st, uint32_t n, double p) {
+// 1/x, read from a table of correctly rounded reciprocals when one is given.
+SG_HD double sg_rcp(const double* tab, uint32_t x) {
+    return (tab && x < SG_RCP_TABLE) ? tab[x] : 1.0 / (double)x;
+}
+
+// Sequential search from 0: pmf recurrence f(x) = f(x-1) * ((n+1) s / x - s), s = p/q,
+// with 1/x from the reciprocal table (one multiply instead of a division per step).
+SG_HD uint32_t sg_binv(sg_stream* st, uint32_t n, double p, const double* rcp) {
     double q = 1.0 - p;
     double s = p / q;
     double a = ((double)n + 1.0) * s;
@@ -240,7 +257,7 @@ SG_HD uint32_t sg_binv(sg_stream* st, uint32_t n, double p) {
     while (u >= r && x < n) {
         u = u - r;
         x += 1;
-        r = r * (a / (double)x - s);
+        r = r * (a * sg_rcp(rcp, x) - s);
         if (!(r > 0.0)) break;  // pmf underflowed past the mass: stop at x
     }
     return x;
@@ -337,11 +354,11 @@ SG_HD_NOINLINE uint32_t sg_btrd(sg_stream* st, uint32_t n, double p) {
 
 // Binomial(n, p) for any p (values <= 0 give 0, >= 1 give n).  For p > 1/2
 // the sample is n - Binomial(n, 1 - p) (1 - p is exact there).
-SG_HD uint32_t sg_binom(sg_stream* st, uint32_t n, double p) {
+SG_HD uint32_t sg_binom(sg_stream* st, uint32_t n, double p, const double* rcp = nullptr) {
     if (n == 0 || !(p > 0.0)) return 0;
     if (p >= 1.0) return n;
     bool flip = p > 0.5;
     double pp = flip ? 1.0 - p : p;
-    uint32_t k = ((double)n * pp < SG_BINV_CUT) ? sg_binv(st, n, pp) : sg_btrd(st, n, pp);
+    uint32_t k = ((double)n * pp < SG_BINV_CUT) ? sg_binv(st, n, pp, rcp) : sg_btrd(st, n, pp);
     return flip ? n - k : k;
 }

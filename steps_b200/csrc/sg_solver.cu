@@ -23,7 +23,7 @@
 
 namespace sg {
 
-static const double AVOGADRO = 6.02214076e23;  // src/steps/math/constants.hpp
+static const double AVOGADRO = 6.02214179e23;  // src/steps/math/constants.hpp:45
 
 template <typename T>
 struct DevBuf {

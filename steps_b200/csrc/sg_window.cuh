@@ -161,14 +161,22 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
     }
 }
 
+// Resident threads per SM the window kernel is compiled for (caps registers per thread).
+#ifndef SG_WINDOW_THREADS_PER_SM
+#define SG_WINDOW_THREADS_PER_SM 768
+#endif
+
 // Window kernel: gather (if pending) -> totals -> SSA -> diffusion leave -> store.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) window_kernel(sg_window_args a, int check) {
+__global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
+    window_kernel(sg_window_args a, int check) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double s_rcp[SG_RCP_TABLE];
     const int S = a.nspec;
     const int R = a.nreac;
     const int tid = threadIdx.x;
     smem_layout L = carve(smem_raw, BLOCK, S, R);
+    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
     for (int i = tid; i < S; i += BLOCK) L.tot[i] = 0ull;
     for (int i = tid; i < R; i += BLOCK) L.ext[i] = 0u;
     if (tid == 0) L.moved[0] = 0ull;
@@ -271,16 +279,32 @@ __global__ void __launch_bounds__(BLOCK) window_kernel(sg_window_args a, int che
                         if (sg_u01_co(sg_next_u32(&st)) < frc) mean_n += 1u;
                     }
                 }
-                uint32_t Kn = sg_binom(&st, mean_n, t1);
+                // Stage 0: molecules leaving, Binomial(mean_n, t1); stages 1-3: conditional
+                // face split of them; the last face takes the rest.  One sampler call site.
+                uint32_t n = mean_n, Kn = 0u;
+                double pst = t1;
+#pragma unroll 1
+                for (int stage = 0; stage < 4; ++stage) {
+                    uint32_t v = sg_binom(&st, n, pst, s_rcp);
+                    if (stage == 0) {
+                        Kn = v;
+                        n = v;
+                        pst = (double)g.x;
+                    } else if (stage == 1) {
+                        k.x = v;
+                        n -= v;
+                        pst = (double)g.y;
+                    } else if (stage == 2) {
+                        k.y = v;
+                        n -= v;
+                        pst = (double)g.z;
+                    } else {
+                        k.z = v;
+                        n -= v;
+                    }
+                }
+                k.w = n;
                 if (Kn > 0u) {
-                    uint32_t rem = Kn;
-                    k.x = sg_binom(&st, rem, (double)g.x);
-                    rem -= k.x;
-                    k.y = sg_binom(&st, rem, (double)g.y);
-                    rem -= k.y;
-                    k.z = sg_binom(&st, rem, (double)g.z);
-                    rem -= k.z;
-                    k.w = rem;
                     if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
                     moved += Kn;
                 }

@@ -21,7 +21,7 @@ EF_DEFAULT = 1
 EF_DV_BDSYS = 2
 EF_DV_PETSC = 3
 
-AVOGADRO = 6.02214076e23
+AVOGADRO = 6.02214179e23  # src/steps/math/constants.hpp:45
 
 
 def flatten(model, geom):
