@@ -163,7 +163,7 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
 
 // Resident threads per SM the window kernel is compiled for (caps registers per thread).
 #ifndef SG_WINDOW_THREADS_PER_SM
-#define SG_WINDOW_THREADS_PER_SM 768
+#define SG_WINDOW_THREADS_PER_SM 1024
 #endif
 
 // Window kernel: gather (if pending) -> totals -> SSA -> diffusion leave -> store.
