@@ -111,6 +111,33 @@ int sg_set_reac_k(sg_solver* h, int32_t reac, int32_t real, double k);
 int sg_get_reac_k(sg_solver* h, int32_t reac, int32_t real, double* k);
 int sg_set_diff_d(sg_solver* h, int32_t comp, int32_t spec, int32_t real, double d);
 
+/* ---- membrane potential (EField; api.hpp:140, 2874-2875; efield.hpp:59) ----------
+ * Units at this boundary are the reference API's: V, A, s, F/m^2, ohm m, ohm m^2.
+ * Inside, the EField works in um, ms, mV, pA, pF, nS like src/steps/solver/efield. */
+
+/* Membrane mesh: all mesh vertices (m, [nverts][3]), every tet's 4 vertices (tets of a
+ * compartment conduct; efield.cpp:48-112 initMesh), and the membrane triangles' vertices.
+ * method: 0 = FP64 Jacobi-PCG, 1 = FP32 PCG inside FP64 residual refinement.  Replaces
+ * TetOpSplitP::_setupEField (TOS:1092-1279); switches run() to the EField loop (TOS:1851). */
+int sg_set_efield_mesh(sg_solver* h, int32_t nverts, const double* verts, const int32_t* tet_verts,
+                       int32_t ntris, const int32_t* tri_verts, int32_t method);
+int sg_set_efield_dt(sg_solver* h, double dt);                     /* API::setEfieldDT  */
+int sg_get_efield_dt(sg_solver* h, double* dt);                    /* API::getEfieldDT  */
+/* Relative residual of the solve, of each FP32 inner solve, and the iteration cap. */
+int sg_set_efield_tolerance(sg_solver* h, double rel_tol, double inner_rel_tol, int32_t max_iter);
+int sg_set_memb_potential(sg_solver* h, double v);                 /* API::setMembPotential */
+int sg_set_memb_capac(sg_solver* h, double cm);                    /* API::setMembCapac     */
+int sg_set_memb_vol_res(sg_solver* h, double ra);                  /* API::setMembVolRes    */
+int sg_set_memb_res(sg_solver* h, double ro, double vrev);         /* API::setMembRes       */
+int sg_get_vert_v(sg_solver* h, int32_t vert, double* v);          /* API::getVertV  TOS:5215 */
+int sg_set_vert_v(sg_solver* h, int32_t vert, double v);           /* API::setVertV  TOS:5225 */
+int sg_get_tri_v(sg_solver* h, int32_t memb_tri, double* v);       /* API::getTriV (membrane index) */
+int sg_set_vert_v_clamped(sg_solver* h, int32_t vert, int32_t clamped); /* API::setVertVClamped */
+int sg_set_vert_iclamp(sg_solver* h, int32_t vert, double amps);   /* API::setVertIClamp    */
+/* EField steps taken, CG iterations, device ms in the solves, last relative residual. */
+int sg_get_efield_stats(sg_solver* h, uint64_t* steps, uint64_t* iterations, double* solve_ms,
+                        double* last_rel_residual);
+
 /* ---- device options (no reference counterpart) ------------------------------ */
 
 /* Window-kernel launch shape: block in {64,128,256}; grid 0 = occupancy-sized. */
@@ -157,7 +184,7 @@ int sg_get_profile(sg_solver* h, double* window_ms, uint64_t* windows, uint64_t*
 #define SG_NOALLOC_MAX_TETS 65536
 #define SG_NOALLOC_MAX_TET_SPECIES 262144
 #define SG_NOALLOC_MAX_REACS 64
-#define SG_NOALLOC_SCRATCH_BYTES 11021312
+#define SG_NOALLOC_SCRATCH_BYTES 11021824
 int sg_run_noalloc(int32_t ntets, int32_t nspec, int32_t nreac, uint32_t* counts, const double* vol,
                    const int32_t* neighb, const double* area, const double* dist, const uint32_t* lhs,
                    const int32_t* upd, const double* kcst, const double* dcst, uint64_t seed, double t0,

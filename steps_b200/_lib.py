@@ -77,6 +77,20 @@ PROTOTYPES = {
     "sg_set_launch": [_P, _i32, _i32],
     "sg_set_conservation_check": [_P, _i32],
     "sg_get_status": [_P, _pu32],
+    "sg_set_efield_mesh": [_P, _i32, _pf64, _pi32, _i32, _pi32, _i32],
+    "sg_set_efield_dt": [_P, _f64],
+    "sg_get_efield_dt": [_P, _pf64],
+    "sg_set_efield_tolerance": [_P, _f64, _f64, _i32],
+    "sg_set_memb_potential": [_P, _f64],
+    "sg_set_memb_capac": [_P, _f64],
+    "sg_set_memb_vol_res": [_P, _f64],
+    "sg_set_memb_res": [_P, _f64, _f64],
+    "sg_get_vert_v": [_P, _i32, _pf64],
+    "sg_set_vert_v": [_P, _i32, _f64],
+    "sg_get_tri_v": [_P, _i32, _pf64],
+    "sg_set_vert_v_clamped": [_P, _i32, _i32],
+    "sg_set_vert_iclamp": [_P, _i32, _f64],
+    "sg_get_efield_stats": [_P, _pu64, _pu64, _pf64, _pf64],
     "sg_get_stream": [_P, C.POINTER(_P)],
     "sg_set_profiling": [_P, _i32],
     "sg_get_profile": [_P, _pf64, _pu64, _pu64],

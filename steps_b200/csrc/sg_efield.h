@@ -1,0 +1,97 @@
+// EField: vertex-based membrane-potential solve on the GPU.
+//
+// Reference: src/steps/solver/efield/ (efield.cpp:48-112 initMesh, dVsolver.hpp:126-180
+// _advance, tetcoupler.cpp:48-300 coupling coefficients, tetmesh.cpp:231-262 surface).
+// Units as in the reference EField: um, ms, mV, pA, pF, nS.
+//
+// Each EField step assembles the backward-Euler system of dVsolver.hpp:126-180,
+//     A_ii = C_i/dt + g_i + sum_j cc_ij,   A_ij = -cc_ij,
+//     b_i  = I_i + g_i (V_ext - V_i) + sum_j cc_ij (V_j - V_i),
+// solves A dV = b with Jacobi-preconditioned CG (FP64, or FP32 CG inside an FP64
+// residual-refinement loop) and updates V += dV on unclamped vertices.  Clamped rows
+// are identity rows with b = 0, so their columns drop out and A stays SPD.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+namespace sg {
+
+enum EFieldMethod { EF_CG_FP64 = 0, EF_CG_MIXED = 1 };
+
+struct EFieldStats {
+    uint64_t steps = 0;
+    uint64_t iterations = 0;        // inner CG iterations (FP32 ones in mixed mode)
+    uint64_t refinements = 0;       // FP64 residual evaluations
+    double last_rel_residual = 0.0;
+    double solve_ms = 0.0;          // device time of the solves (CUDA events)
+};
+
+struct EFieldSystem {
+    // ---- host model ----
+    int nverts = 0;
+    int ntris = 0;                        // membrane triangles
+    std::vector<int32_t> tri_verts;       // [ntris][3]
+    std::vector<double> tri_area_um2;     // [ntris]
+    std::vector<double> vert_area_um2;    // [nverts] membrane area attributed to the vertex
+    std::vector<int32_t> nbr_ptr, nbr_idx;// vertex adjacency (CSR, no diagonal)
+    std::vector<double> geo_cc;           // geometric coupling per adjacency entry (um)
+    double cm = 0.01;                     // pF/um^2   (1 uF/cm^2, efield.cpp:81)
+    double sigma = 1.0 / 1.0e-3;          // nS/um     (1 ohm m, efield.cpp:87)
+    double g_leak = 0.0;                  // nS/um^2   surface conductance
+    double v_leak = 0.0;                  // mV
+    int method = EF_CG_FP64;
+    double tol = 1.0e-10;                 // relative residual of the FP64 solve
+    int max_iter = 20000;
+    std::vector<uint8_t> vclamped;        // [nverts]
+    std::vector<double> vert_iclamp;      // pA, [nverts]
+    std::vector<double> tri_iclamp;       // pA, [ntris]
+
+    // ---- device ----
+    int width = 0;                        // ELL width (max off-diagonal entries per row)
+    double* V = nullptr;                  // mV [nverts]
+    double* tri_V = nullptr;              // mV [ntris]
+    double* tri_I = nullptr;              // pA [ntris] (outward membrane current of the step)
+    int32_t* d_tri_verts = nullptr;
+    int32_t* d_vt_ptr = nullptr;          // vertex -> membrane tris (CSR)
+    int32_t* d_vt_idx = nullptr;
+    double* d_vert_iclamp = nullptr;
+    double* d_tri_iclamp = nullptr;
+    int32_t* ell_col = nullptr;           // [width][nverts], -1 = padding
+    double* ell_cc = nullptr;             // [width][nverts] cc_ij (nS), all neighbours (RHS)
+    double* ell_a64 = nullptr;            // [width][nverts] -cc_ij, clamped columns removed
+    float* ell_a32 = nullptr;
+    double* diag64 = nullptr;             // A_ii
+    double* cap_gext = nullptr;           // [2][nverts]: C_i (pF), g_i (nS)
+    uint8_t* d_vclamped = nullptr;
+    int32_t* acol_dev = nullptr;          // [width][nverts] matrix columns (clamped ones removed)
+    double inner_tol = 1.0e-4;            // relative residual of each FP32 inner solve
+    double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
+    float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr, *x32 = nullptr, *s32 = nullptr;
+    double* red = nullptr;                // reduction partials
+    double* scal = nullptr;               // device scalars
+    unsigned int* red_count = nullptr;
+    double dt_built = -1.0;
+    bool dirty = true;                    // clamps / membrane properties changed
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    EFieldStats stats;
+    int nsm = 148;
+
+    ~EFieldSystem();
+    // verts in um, tets [ntet][4] (all tets that conduct), membrane tris [ntris][3] with areas.
+    void setup(int nverts, const double* verts_um, int ntet, const int32_t* tets, int ntris,
+               const int32_t* tris, cudaStream_t stream, int nsm);
+    void set_potential(double v_mV, cudaStream_t stream);
+    void build_matrix(double dt_ms, cudaStream_t stream);
+    // One EField step of dt_ms with tri_I already set on the device.
+    void advance(double dt_ms, cudaStream_t stream);
+    void release();
+};
+
+// Geometric coupling of a tet mesh: for every edge ij, sum over tets of the linear-FEM
+// stiffness -V_T grad(phi_i).grad(phi_j) (um).  Exposed for the tests.
+void efield_couple(int nverts, const double* verts_um, int ntet, const int32_t* tets,
+                   std::vector<int32_t>& ptr, std::vector<int32_t>& idx, std::vector<double>& cc);
+
+}  // namespace sg

@@ -154,6 +154,7 @@ std::vector<sg_reac> compact_reacs(int nspec, int nreac, const uint32_t* lhs, co
             r.lhs_ord[r.nlhs] = (int32_t)l;
             r.nlhs += 1;
             r.order += (int32_t)l;
+            r.lhs_mask |= 1u << i;
         }
         if (r.order > 4) throw sg::ArgErr("reaction order above 4 is not supported");
         for (int i = 0; i < nspec; ++i) {
@@ -163,6 +164,7 @@ std::vector<sg_reac> compact_reacs(int nspec, int nreac, const uint32_t* lhs, co
             r.upd_spec[r.nupd] = i;
             r.upd_delta[r.nupd] = u;
             r.nupd += 1;
+            r.upd_mask |= 1u << i;
         }
         out[q] = r;
     }

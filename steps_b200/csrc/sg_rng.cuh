@@ -102,20 +102,26 @@ SG_HD void sg_stream_init(sg_stream* s, uint64_t seed, uint32_t realization, uin
     s->b0 = s->b1 = s->b2 = s->b3 = 0;
 }
 
-// Refill of the 4-word buffer.  With SG_NOINLINE_REFILL the Philox rounds exist once
-// in the device code instead of at every draw site (smaller instruction footprint).
+// One Philox block of a stream.  With SG_NOINLINE_REFILL the rounds exist once in the
+// device code instead of at every draw site (smaller instruction footprint); arguments
+// and result pass by value so the caller's stream state stays in registers.
 #if defined(__CUDACC__) && defined(SG_NOINLINE_REFILL)
 static __host__ __device__ __noinline__
 #else
 SG_HD
 #endif
-void sg_stream_refill(sg_stream* s) {
+sg_u32x4 sg_philox_block(uint32_t block, uint32_t unit, uint32_t wlo, uint32_t whi, uint32_t k0,
+                         uint32_t k1) {
     sg_u32x4 c;
-    c.x = s->block;
-    c.y = s->unit;
-    c.z = s->wlo;
-    c.w = s->whi;
-    sg_u32x4 r = sg_philox4x32(c, s->k0, s->k1);
+    c.x = block;
+    c.y = unit;
+    c.z = wlo;
+    c.w = whi;
+    return sg_philox4x32(c, k0, k1);
+}
+
+SG_HD void sg_stream_refill(sg_stream* s) {
+    sg_u32x4 r = sg_philox_block(s->block, s->unit, s->wlo, s->whi, s->k0, s->k1);
     s->block += 1;
     s->b0 = r.x;
     s->b1 = r.y;
@@ -247,9 +253,8 @@ SG_HD double sg_rcp(const double* tab, uint32_t x) {
 
 // Sequential search from 0: pmf recurrence f(x) = f(x-1) * ((n+1) s / x - s), s = p/q,
 // with 1/x from the reciprocal table (one multiply instead of a division per step).
-SG_HD uint32_t sg_binv(sg_stream* st, uint32_t n, double p, const double* rcp) {
+SG_HD uint32_t sg_binv(sg_stream* st, uint32_t n, double p, const double* rcp, double s) {
     double q = 1.0 - p;
-    double s = p / q;
     double a = ((double)n + 1.0) * s;
     double r = sg_pow_u(q, n);
     double u = sg_u01_co(sg_next_u32(st));
@@ -287,7 +292,7 @@ SG_HD double sg_stirling_fc(uint32_t k) {
 // BTRD for p <= 1/2 and n p >= SG_BINV_CUT.  Candidates outside [0, n] are
 // rejected.  The iteration cap is never reached in practice (acceptance rate
 // is above 0.8 per round); if it were, the mode is returned.
-SG_HD_NOINLINE uint32_t sg_btrd(sg_stream* st, uint32_t n, double p) {
+SG_HD uint32_t sg_btrd(sg_stream* st, uint32_t n, double p) {
     double dn = (double)n;
     double q = 1.0 - p;
     double m = floor((dn + 1.0) * p);
@@ -354,11 +359,25 @@ SG_HD_NOINLINE uint32_t sg_btrd(sg_stream* st, uint32_t n, double p) {
 
 // Binomial(n, p) for any p (values <= 0 give 0, >= 1 give n).  For p > 1/2
 // the sample is n - Binomial(n, 1 - p) (1 - p is exact there).
-SG_HD uint32_t sg_binom(sg_stream* st, uint32_t n, double p, const double* rcp = nullptr) {
+// Odds ratio of the smaller tail, pp / (1 - pp) with pp = min(p, 1 - p): the value the
+// samplers below use; callers with a fixed p may compute it once.
+SG_HD double sg_binom_odds(double p) {
+    double pp = (p > 0.5) ? 1.0 - p : p;
+    return pp / (1.0 - pp);
+}
+
+// Binomial(n, p) with odds = sg_binom_odds(p) supplied by the caller.
+SG_HD uint32_t sg_binom_o(sg_stream* st, uint32_t n, double p, double odds, const double* rcp) {
     if (n == 0 || !(p > 0.0)) return 0;
     if (p >= 1.0) return n;
     bool flip = p > 0.5;
     double pp = flip ? 1.0 - p : p;
-    uint32_t k = ((double)n * pp < SG_BINV_CUT) ? sg_binv(st, n, pp, rcp) : sg_btrd(st, n, pp);
+    uint32_t k = ((double)n * pp < SG_BINV_CUT) ? sg_binv(st, n, pp, rcp, odds) : sg_btrd(st, n, pp);
     return flip ? n - k : k;
+}
+
+SG_HD uint32_t sg_binom(sg_stream* st, uint32_t n, double p, const double* rcp = nullptr) {
+    if (n == 0 || !(p > 0.0)) return 0;
+    if (p >= 1.0) return n;
+    return sg_binom_o(st, n, p, sg_binom_odds(p), rcp);
 }

@@ -19,6 +19,7 @@
 #include "sg_types.h"
 #include "sg_window.cuh"
 #include "sg_errors.h"
+#include "sg_efield.h"
 #include "../../include/steps_b200.h"
 
 namespace sg {
@@ -87,6 +88,11 @@ struct Solver {
     int block = 128;
     int grid = 0;
     bool check = true;
+
+    // ---- EField (membrane potential) ----
+    EFieldSystem ef;
+    bool ef_on = false;
+    double efdt = 1.0e-5;                       // s, TOS:938 default EField dt
 
     // ---- launch accounting and optional per-run CUDA-event timing ----
     uint64_t launches = 0;                      // kernels launched by this solver
@@ -441,9 +447,68 @@ struct Solver {
             sync();
             return;
         }
+        if (ef_on) {
+            run_with_efield(endtime);
+            return;
+        }
         enqueue_windows(endtime);
         download_reals();
         check_status();
+    }
+
+    // TOS:1851-1952 _runWithEField: per EField step, the reaction-diffusion windows up to
+    // min(t + efdt, endtime), then the membrane currents and the EField solve over the
+    // step actually taken; the new triangle potentials feed the next windows.
+    void run_with_efield(double endtime) {
+        if (nreal != 1) throw NotImplErr("EField with batched realizations");
+        while (time() < endtime) {
+            double t0 = time();
+            double t1 = std::min(t0 + efdt, endtime);
+            if (almost_equal(t1, endtime)) t1 = endtime;
+            if (almost_equal(t0, t1)) {
+                for (auto& rl : reals) rl.t = t1;
+                upload_reals();
+                break;
+            }
+            enqueue_windows(t1);
+            download_reals();
+            check_status();
+            double real_dt = time() - t0;
+            // Membrane currents of the step (no channel currents on this path: tri_I = 0).
+            SG_CUDA(cudaMemsetAsync(ef.tri_I, 0, std::max(ef.ntris, 1) * 8, stream));
+            ef.advance(real_dt * 1.0e3, stream);  // efield.cpp:229-234: s -> ms
+        }
+        sync();
+    }
+
+    void require_ef() const {
+        if (!ef_on) throw ProgErr("Method not available: this solver has no membrane potential");
+    }
+    void check_vert(int v) const {
+        if (v < 0 || v >= ef.nverts) throw ArgErr("vertex index out of range: " + std::to_string(v));
+    }
+    double get_vert_v(int v) {
+        require_ef();
+        check_vert(v);
+        double x = 0.0;
+        d2h(&x, ef.V + v, 1);
+        sync();
+        return x * 1.0e-3;  // mV -> V
+    }
+    void set_vert_v(int v, double volts) {
+        require_ef();
+        check_vert(v);
+        double x = volts * 1.0e3;
+        h2d(ef.V + v, &x, 1);
+        sync();
+    }
+    double get_tri_v(int t) {
+        require_ef();
+        if (t < 0 || t >= ef.ntris) throw ArgErr("membrane triangle index out of range");
+        double x = 0.0;
+        d2h(&x, ef.tri_V + t, 1);
+        sync();
+        return x * 1.0e-3;
     }
 
     // Enqueue every window up to endtime for all realizations (no host sync).
@@ -891,6 +956,7 @@ int sg_add_reac(sg_solver* h, int32_t comp, const uint32_t* lhs, const int32_t* 
             r.lhs_ord[r.nlhs] = (int32_t)lhs[i];
             r.nlhs += 1;
             r.order += (int32_t)lhs[i];
+            r.lhs_mask |= 1u << i;
         }
         if (r.order > 4) throw sg::ArgErr("reaction order above 4 is not supported");
         for (int i = 0; i < s->nspec; ++i) {
@@ -899,6 +965,7 @@ int sg_add_reac(sg_solver* h, int32_t comp, const uint32_t* lhs, const int32_t* 
             r.upd_spec[r.nupd] = i;
             r.upd_delta[r.nupd] = upd[i];
             r.nupd += 1;
+            r.upd_mask |= 1u << i;
         }
         s->reacs.push_back(r);
         s->reac_kdef.push_back(kcst);
@@ -1073,6 +1140,143 @@ int sg_set_launch(sg_solver* h, int32_t block, int32_t grid) {
 
 int sg_set_conservation_check(sg_solver* h, int32_t on) {
     return guarded([&] { S(h)->check = on != 0; });
+}
+
+int sg_set_efield_mesh(sg_solver* h, int32_t nverts, const double* verts, const int32_t* tet_verts,
+                       int32_t ntris, const int32_t* tri_verts, int32_t method) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_setup();
+        need(verts, "verts");
+        need(tet_verts, "tet_verts");
+        if (ntris > 0) need(tri_verts, "tri_verts");
+        if (method != sg::EF_CG_FP64 && method != sg::EF_CG_MIXED) throw sg::ArgErr("unknown EField method");
+        // Conducting volume: the tets of every compartment (efield.cpp:48 initMesh).
+        std::vector<int32_t> tets;
+        for (int t = 0; t < s->ntets; ++t)
+            if (s->tet_comp[t] >= 0) tets.insert(tets.end(), tet_verts + (size_t)t * 4, tet_verts + (size_t)t * 4 + 4);
+        std::vector<double> um((size_t)nverts * 3);
+        for (size_t i = 0; i < um.size(); ++i) um[i] = verts[i] * 1.0e6;  // m -> um (efield units)
+        s->ef.setup(nverts, um.data(), (int)(tets.size() / 4), tets.data(), ntris, tri_verts, s->stream, s->nsm);
+        s->ef.method = method;
+        s->ef_on = true;
+        s->sync();
+    });
+}
+
+int sg_set_efield_dt(sg_solver* h, double dt) {
+    return guarded([&] {
+        if (!(dt > 0.0)) throw sg::ArgErr("EField dt must be positive");
+        S(h)->efdt = dt;
+    });
+}
+
+int sg_get_efield_dt(sg_solver* h, double* dt) {
+    return guarded([&] {
+        need(dt, "dt");
+        *dt = S(h)->efdt;
+    });
+}
+
+int sg_set_efield_tolerance(sg_solver* h, double rel_tol, double inner_rel_tol, int32_t max_iter) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        if (!(rel_tol > 0.0) || !(inner_rel_tol > 0.0) || max_iter <= 0) throw sg::ArgErr("bad tolerance");
+        s->ef.tol = rel_tol;
+        s->ef.inner_tol = inner_rel_tol;
+        s->ef.max_iter = max_iter;
+    });
+}
+
+int sg_set_memb_potential(sg_solver* h, double v) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        s->ef.set_potential(v * 1.0e3, s->stream);
+        s->sync();
+    });
+}
+
+int sg_set_memb_capac(sg_solver* h, double cm) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        if (!(cm >= 0.0)) throw sg::ArgErr("capacitance must be non-negative");
+        s->ef.cm = cm;  // F/m^2 == pF/um^2
+        s->ef.dirty = true;
+    });
+}
+
+int sg_set_memb_vol_res(sg_solver* h, double ra) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        if (!(ra > 0.0)) throw sg::ArgErr("resistivity must be positive");
+        s->ef.sigma = 1.0 / (ra * 1.0e-3);  // ohm m -> nS/um  (efield.cpp:83-87)
+        s->ef.dirty = true;
+    });
+}
+
+int sg_set_memb_res(sg_solver* h, double ro, double vrev) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        if (!(ro > 0.0)) throw sg::ArgErr("membrane resistance must be positive");
+        s->ef.g_leak = (1.0 / ro) * 1.0e-3;  // S/m^2 -> nS/um^2 (dVsolver.cpp:85)
+        s->ef.v_leak = vrev * 1.0e3;
+        s->ef.dirty = true;
+    });
+}
+
+int sg_get_vert_v(sg_solver* h, int32_t v, double* volts) {
+    return guarded([&] {
+        need(volts, "volts");
+        *volts = S(h)->get_vert_v(v);
+    });
+}
+
+int sg_set_vert_v(sg_solver* h, int32_t v, double volts) {
+    return guarded([&] { S(h)->set_vert_v(v, volts); });
+}
+
+int sg_get_tri_v(sg_solver* h, int32_t tri, double* volts) {
+    return guarded([&] {
+        need(volts, "volts");
+        *volts = S(h)->get_tri_v(tri);
+    });
+}
+
+int sg_set_vert_v_clamped(sg_solver* h, int32_t v, int32_t clamped) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        s->check_vert(v);
+        s->ef.vclamped[v] = clamped ? 1 : 0;
+        s->ef.dirty = true;
+    });
+}
+
+int sg_set_vert_iclamp(sg_solver* h, int32_t v, double amps) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        s->check_vert(v);
+        s->ef.vert_iclamp[v] = amps * 1.0e12;  // A -> pA, positive = into the cell (efield.cpp:214-225)
+        s->ef.dirty = true;
+    });
+}
+
+int sg_get_efield_stats(sg_solver* h, uint64_t* steps, uint64_t* iterations, double* solve_ms,
+                        double* last_rel_residual) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        if (steps) *steps = s->ef.stats.steps;
+        if (iterations) *iterations = s->ef.stats.iterations;
+        if (solve_ms) *solve_ms = s->ef.stats.solve_ms;
+        if (last_rel_residual) *last_rel_residual = s->ef.stats.last_rel_residual;
+    });
 }
 
 int sg_get_stream(sg_solver* h, void** stream) {

@@ -30,6 +30,8 @@ typedef struct sg_reac {
     int32_t lhs_ord[SG_MAX_LHS];       // its stoichiometry (1..4)
     int32_t upd_spec[SG_MAX_UPD];      // changed species
     int32_t upd_delta[SG_MAX_UPD];     // signed change
+    uint32_t lhs_mask;                 // bit per reactant species (propensity dependencies)
+    uint32_t upd_mask;                 // bit per changed species
 } sg_reac;
 
 // Per realization bookkeeping, advanced on the device by the last block of each

@@ -69,6 +69,8 @@ struct smem_layout {
     uint32_t* cnt;             // [S][BLOCK]
     double* occ;               // [S][BLOCK]
     double* last;              // [S][BLOCK]
+    double* prop;              // [R][BLOCK] propensities of this thread's tet
+    sg_reac* reac;             // [R] copy of the reaction table
     unsigned long long* tot;   // [S]
     unsigned long long* moved; // [1]
     unsigned int* ext;         // [R]
@@ -77,8 +79,11 @@ struct smem_layout {
 
 __host__ __device__ inline size_t smem_bytes(int block, int nspec, int nreac) {
     size_t b = (size_t)block * nspec * 4;
-    b = (b + 7) & ~(size_t)7;
+    b = (b + 15) & ~(size_t)15;
     b += (size_t)block * nspec * 16;
+    b += (size_t)block * nreac * 8;
+    b += (size_t)nreac * sizeof(sg_reac);
+    b = (b + 7) & ~(size_t)7;
     b += (size_t)nspec * 8 + 8;
     b += (size_t)nreac * 4 + 4;
     b = (b + 7) & ~(size_t)7;
@@ -90,11 +95,16 @@ __device__ inline smem_layout carve(unsigned char* base, int block, int nspec, i
     smem_layout L;
     size_t b = (size_t)block * nspec * 4;
     L.cnt = (uint32_t*)base;
-    b = (b + 7) & ~(size_t)7;
+    b = (b + 15) & ~(size_t)15;
     L.occ = (double*)(base + b);
     b += (size_t)block * nspec * 8;
     L.last = (double*)(base + b);
     b += (size_t)block * nspec * 8;
+    L.prop = (double*)(base + b);
+    b += (size_t)block * nreac * 8;
+    L.reac = (sg_reac*)(base + b);
+    b += (size_t)nreac * sizeof(sg_reac);
+    b = (b + 7) & ~(size_t)7;
     L.tot = (unsigned long long*)(base + b);
     b += (size_t)nspec * 8;
     L.moved = (unsigned long long*)(base + b);
@@ -114,12 +124,19 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
     uint32_t* sc = L.cnt + tid;
     double* so = L.occ + tid;
     double* sl = L.last + tid;
+    double* sp = L.prop + tid;  // sp[q * BLOCK]: propensity of reaction q in this tet
     double tt = 0.0;
+    // Propensities are kept per reaction and only the ones whose reactants changed are
+    // re-evaluated after an event; a0 is always re-summed in reaction order, so every
+    // value equals a full re-evaluation.
+    uint32_t changed = 0xFFFFFFFFu;
     for (;;) {
         double a0 = 0.0;
         for (int q = rb; q < re; ++q) {
-            const sg_reac* rc = &a.reacs[q];
-            a0 = a0 + reac_prop(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
+            const sg_reac* rc = &L.reac[q];
+            if (rc->lhs_mask & changed) sp[q * BLOCK] = reac_prop(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
+            else if (changed == 0xFFFFFFFFu) sp[q * BLOCK] = reac_prop(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
+            a0 = a0 + sp[q * BLOCK];
         }
         if (!(a0 > 0.0)) break;
         double dt = -sg_log(sg_u01_oc(sg_next_u32(st))) / a0;
@@ -129,8 +146,7 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
         double cum = 0.0;
         int sel = -1, lastnz = -1;
         for (int q = rb; q < re; ++q) {
-            const sg_reac* rc = &a.reacs[q];
-            double p = reac_prop(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
+            double p = sp[q * BLOCK];
             if (p > 0.0) {
                 lastnz = q;
                 cum = cum + p;
@@ -142,7 +158,8 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
         }
         if (sel < 0) sel = lastnz;
         if (sel < 0) break;
-        const sg_reac* rc = &a.reacs[sel];
+        const sg_reac* rc = &L.reac[sel];
+        changed = rc->upd_mask & ~clampm;
         int nu = rc->nupd;
         for (int i = 0; i < nu; ++i) {
             int s = rc->upd_spec[i];
@@ -177,6 +194,7 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     const int tid = threadIdx.x;
     smem_layout L = carve(smem_raw, BLOCK, S, R);
     for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
+    for (int i = tid; i < R; i += BLOCK) L.reac[i] = a.reacs[i];
     for (int i = tid; i < S; i += BLOCK) L.tot[i] = 0ull;
     for (int i = tid; i < R; i += BLOCK) L.ext[i] = 0u;
     if (tid == 0) L.moved[0] = 0ull;
@@ -222,12 +240,13 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
                 c = a.counts[(size_t)s * a.ntets + t];
                 int ds = __ldg(&a.diff_slot[s]);
                 if (pending && ds >= 0 && __ldg(&Dc[s]) > 0.0 && !((clampm >> s) & 1u)) {
-                    const uint32_t* src = in + (size_t)ds * plane;
+                    // Slot f of this tet holds what the neighbour behind face f sent.
+                    const uint4 v = __ldg(reinterpret_cast<const uint4*>(in + (size_t)ds * plane) + t);
                     unsigned long long sum = c;
-                    if (nb.x >= 0) sum += __ldg(&src[nb.x]);
-                    if (nb.y >= 0) sum += __ldg(&src[nb.y]);
-                    if (nb.z >= 0) sum += __ldg(&src[nb.z]);
-                    if (nb.w >= 0) sum += __ldg(&src[nb.w]);
+                    if (nb.x >= 0) sum += v.x;
+                    if (nb.y >= 0) sum += v.y;
+                    if (nb.z >= 0) sum += v.z;
+                    if (nb.w >= 0) sum += v.w;
                     if (sum > 0xFFFFFFFFull) {
                         atomicOr(a.status, SG_ERR_OVERFLOW);
                         sum = 0xFFFFFFFFull;
@@ -256,7 +275,11 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
         // Phase 3: diffusion leave, one (tet, species) at a time.
         const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
         const double G = (double)g.w;
-        uint4* out = reinterpret_cast<uint4*>(a.outflow + (size_t)(w & 1ull) * a.ndiff * plane);
+        // Odds ratios of the three face selectors, once per tet instead of once per draw.
+        const double odd1 = sg_binom_odds((double)g.x);
+        const double odd2 = sg_binom_odds((double)g.y);
+        const double odd3 = sg_binom_odds((double)g.z);
+        uint32_t* out = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane;
         for (int s = 0; s < S; ++s) {
             int ds = __ldg(&a.diff_slot[s]);
             if (ds < 0) continue;
@@ -283,21 +306,25 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
                 // face split of them; the last face takes the rest.  One sampler call site.
                 uint32_t n = mean_n, Kn = 0u;
                 double pst = t1;
+                double ost = (t1 > 0.0 && t1 < 1.0) ? sg_binom_odds(t1) : 0.0;
 #pragma unroll 1
                 for (int stage = 0; stage < 4; ++stage) {
-                    uint32_t v = sg_binom(&st, n, pst, s_rcp);
+                    uint32_t v = sg_binom_o(&st, n, pst, ost, s_rcp);
                     if (stage == 0) {
                         Kn = v;
                         n = v;
                         pst = (double)g.x;
+                        ost = odd1;
                     } else if (stage == 1) {
                         k.x = v;
                         n -= v;
                         pst = (double)g.y;
+                        ost = odd2;
                     } else if (stage == 2) {
                         k.y = v;
                         n -= v;
                         pst = (double)g.z;
+                        ost = odd3;
                     } else {
                         k.z = v;
                         n -= v;
@@ -309,7 +336,13 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
                     moved += Kn;
                 }
             }
-            out[(size_t)ds * a.ntets + t] = k;
+            // Scatter into the receiving tets' slots: nb.f = (neighbour << 2) | its face,
+            // i.e. the word index inside this species' plane.  Each slot has one writer.
+            uint32_t* po = out + (size_t)ds * plane;
+            if (nb.x >= 0) po[nb.x] = k.x;
+            if (nb.y >= 0) po[nb.y] = k.y;
+            if (nb.z >= 0) po[nb.z] = k.z;
+            if (nb.w >= 0) po[nb.w] = k.w;
         }
         // Phase 4: store counts.
         for (int s = 0; s < S; ++s) a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
@@ -398,12 +431,12 @@ static __global__ void flush_kernel(sg_window_args a) {
         for (int s = 0; s < a.nspec; ++s) {
             int ds = a.diff_slot[s];
             if (ds < 0 || !(Dc[s] > 0.0) || ((clampm >> s) & 1u)) continue;
-            const uint32_t* src = in + (size_t)ds * plane;
+            const uint4 v = reinterpret_cast<const uint4*>(in + (size_t)ds * plane)[t];
             unsigned long long sum = a.counts[(size_t)s * a.ntets + t];
-            if (nb.x >= 0) sum += src[nb.x];
-            if (nb.y >= 0) sum += src[nb.y];
-            if (nb.z >= 0) sum += src[nb.z];
-            if (nb.w >= 0) sum += src[nb.w];
+            if (nb.x >= 0) sum += v.x;
+            if (nb.y >= 0) sum += v.y;
+            if (nb.z >= 0) sum += v.z;
+            if (nb.w >= 0) sum += v.w;
             if (sum > 0xFFFFFFFFull) {
                 atomicOr(a.status, SG_ERR_OVERFLOW);
                 sum = 0xFFFFFFFFull;

@@ -170,6 +170,22 @@ class TmPatch:
         return float(self.mesh.tri_area[self.tris].sum())
 
 
+class Memb:
+    """A membrane for the EField: the triangles of its patches (src/steps/geom/memb.hpp:49).
+    The conducting volume is every tet of every compartment."""
+
+    def __init__(self, id, mesh, patches, supplementary_comps=None, opt_method=1, search_percent=100.0,
+                 opt_file_name=""):
+        self.id = id
+        self.mesh = mesh
+        self.patches = list(patches)
+        tris = np.unique(np.concatenate([p.tris for p in self.patches])) if self.patches else np.zeros(0, int)
+        self.tris = tris.astype(np.int64)
+        if not hasattr(mesh, "membs"):
+            mesh.membs = {}
+        mesh.membs[id] = self
+
+
 def kuhn_box(nx, ny, nz, h=1.0e-7, origin=(0.0, 0.0, 0.0)):
     """Box of nx*ny*nz cubes of side h, each cut into 6 tets along its main diagonal
     (Kuhn / Freudenthal triangulation; conforming across cubes).

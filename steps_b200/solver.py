@@ -20,6 +20,11 @@ EF_NONE = 0
 EF_DEFAULT = 1
 EF_DV_BDSYS = 2
 EF_DV_PETSC = 3
+# GPU membrane-potential solvers: Jacobi-preconditioned CG in FP64, or FP32 CG inside an
+# FP64 residual-refinement loop.  The reference's direct/PETSc choices map to FP64 CG.
+EF_DV_CG_FP64 = 10
+EF_DV_CG_MIXED = 11
+_EF_METHOD = {EF_DEFAULT: 0, EF_DV_BDSYS: 0, EF_DV_PETSC: 0, EF_DV_CG_FP64: 0, EF_DV_CG_MIXED: 1}
 
 AVOGADRO = 6.02214179e23  # src/steps/math/constants.hpp:45
 
@@ -33,7 +38,7 @@ def flatten(model, geom):
 
     spec_names = [n for n, s in model.specs.items() if not isinstance(s, ChanState)]
     if not spec_names:
-        raise ArgErr("model has no volume species")
+        spec_names = ["__inert__"]  # membrane-only models: one species that never changes
     spec_index = {n: i for i, n in enumerate(spec_names)}
     comp_names = list(geom.comps.keys())
     comp_index = {n: i for i, n in enumerate(comp_names)}
@@ -80,8 +85,8 @@ class TetOpSplit:
         self._h = None
         self._L = _lib.load()
         self.model, self.geom, self.rng = model, geom, rng
-        if calcMembPot not in (EF_NONE, 0):
-            raise _lib.NotImplErr("membrane potential is not available through this class")
+        if calcMembPot not in _EF_METHOD and calcMembPot != EF_NONE:
+            raise ArgErr(f"unknown calcMembPot {calcMembPot}")
         h = C.c_void_p()
         check(self._L.sg_create(C.byref(h), C.c_uint64(rng.seed), device))
         self._h = h
@@ -89,6 +94,8 @@ class TetOpSplit:
             self._flatten(model, geom, realizations)
             check(self._L.sg_set_launch(self._h, block, 0))
             check(self._L.sg_setup(self._h))
+            if calcMembPot != EF_NONE:
+                self._setup_efield(geom, _EF_METHOD[calcMembPot])
         except Exception:
             self._L.sg_destroy(self._h)
             self._h = None
@@ -130,6 +137,19 @@ class TetOpSplit:
         else:
             self.nreal = 1
             self.real_offsets = np.array([0, geom.ntets], dtype=np.int32)
+
+    def _setup_efield(self, geom, method):
+        membs = getattr(geom, "membs", {})
+        if len(membs) != 1:
+            raise ArgErr("the membrane potential needs exactly one Memb on the mesh")
+        memb = next(iter(membs.values()))
+        self.memb_tris = memb.tris
+        self.memb_index = {int(t): i for i, t in enumerate(memb.tris)}
+        verts = np.ascontiguousarray(geom.verts, dtype=np.float64)
+        tets = np.ascontiguousarray(geom.tets, dtype=np.int32)
+        tris = np.ascontiguousarray(geom.tris[memb.tris], dtype=np.int32)
+        check(self._L.sg_set_efield_mesh(self._h, geom.nverts, ptr(verts, C.c_double), ptr(tets, C.c_int32),
+                                         len(memb.tris), ptr(tris, C.c_int32), method))
 
     def _spec(self, name):
         try:
@@ -293,6 +313,59 @@ class TetOpSplit:
         except KeyError:
             raise ArgErr(f"diffusion '{d}' undefined in compartment '{c}'") from None
         check(self._L.sg_set_diff_d(self._h, self._comp(c), s, int(realization), float(dcst)))
+
+    # ------------------------------------------------ membrane potential (EField)
+    def setEfieldDT(self, dt):
+        check(self._L.sg_set_efield_dt(self._h, float(dt)))
+
+    def getEfieldDT(self):
+        x = C.c_double()
+        check(self._L.sg_get_efield_dt(self._h, C.byref(x)))
+        return x.value
+
+    def setEfieldTolerance(self, rel_tol, inner_rel_tol=1e-4, max_iter=20000):
+        check(self._L.sg_set_efield_tolerance(self._h, float(rel_tol), float(inner_rel_tol), int(max_iter)))
+
+    def setMembPotential(self, memb, v):
+        check(self._L.sg_set_memb_potential(self._h, float(v)))
+
+    def setMembCapac(self, memb, cm):
+        check(self._L.sg_set_memb_capac(self._h, float(cm)))
+
+    def setMembVolRes(self, memb, ra):
+        check(self._L.sg_set_memb_vol_res(self._h, float(ra)))
+
+    def setMembRes(self, memb, ro, vrev):
+        check(self._L.sg_set_memb_res(self._h, float(ro), float(vrev)))
+
+    def getVertV(self, vidx):
+        x = C.c_double()
+        check(self._L.sg_get_vert_v(self._h, int(vidx), C.byref(x)))
+        return x.value
+
+    def setVertV(self, vidx, v):
+        check(self._L.sg_set_vert_v(self._h, int(vidx), float(v)))
+
+    def setVertVClamped(self, vidx, cl):
+        check(self._L.sg_set_vert_v_clamped(self._h, int(vidx), 1 if cl else 0))
+
+    def setVertIClamp(self, vidx, cur):
+        check(self._L.sg_set_vert_iclamp(self._h, int(vidx), float(cur)))
+
+    def getTriV(self, tidx):
+        try:
+            m = self.memb_index[int(tidx)]
+        except (AttributeError, KeyError):
+            raise ArgErr(f"triangle {tidx} is not on the membrane") from None
+        x = C.c_double()
+        check(self._L.sg_get_tri_v(self._h, m, C.byref(x)))
+        return x.value
+
+    def getEfieldStats(self):
+        """(EField steps, CG iterations, device ms in the solves, last relative residual)."""
+        s, it, ms, rr = C.c_uint64(), C.c_uint64(), C.c_double(), C.c_double()
+        check(self._L.sg_get_efield_stats(self._h, C.byref(s), C.byref(it), C.byref(ms), C.byref(rr)))
+        return s.value, it.value, ms.value, rr.value
 
     # --------------------------------------------------------- device knobs
     def setLaunch(self, block, grid=0):

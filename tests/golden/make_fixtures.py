@@ -46,11 +46,32 @@ def read_abaqus(path, scale):
     return verts, tets
 
 
+def read_steps_xml(path):
+    """Vertices and tets of a STEPS XML mesh (<nodes><node><coords>, <tetrahedrons><tet><nodes>)."""
+    import re
+
+    txt = open(path).read()
+    nodes = re.search(r"<nodes size\s*=\s*\"\d+\">(.*?)</nodes>\s*<triangles", txt, re.S).group(1)
+    verts = np.array([[float(x) for x in m.split(",")] for m in re.findall(r"<coords>(.*?)</coords>", nodes)])
+    tets_blk = re.search(r"<tetrahedrons.*?</tetrahedrons>", txt, re.S).group(0)
+    tets = np.array([[int(x) for x in m.split(",")] for m in re.findall(r"<nodes>(.*?)</nodes>", tets_blk)],
+                    dtype=np.int64)
+    return verts, tets
+
+
 def main():
     inp = os.path.join(REF, "test/validation/API_1/validation_rd_mpi/meshes/sphere_rad1_37tets.inp")
     v, t = read_abaqus(inp, 1.0e-6)
     np.savez(os.path.join(HERE, "sphere_rad1_37tets.npz"), verts=v, tets=t)
     print("sphere:", v.shape, t.shape)
+    # Rallpack1 passive cable: mesh and the reference V(t) at 0 um and 1000 um
+    # (test/validation/API_1/validation_efield/, used by test_rallpack1_membres.py).
+    ef = os.path.join(REF, "test/validation/API_1/validation_efield")
+    v, t = read_steps_xml(os.path.join(ef, "meshes/axon_cube_L1000um_D866nm_1978tets.xml"))
+    v0 = np.loadtxt(os.path.join(ef, "data/rallpack1_correct/v0"))
+    vx = np.loadtxt(os.path.join(ef, "data/rallpack1_correct/vx"))
+    np.savez_compressed(os.path.join(HERE, "rallpack1.npz"), verts=v, tets=t, v0=v0, vx=vx)
+    print("rallpack1:", v.shape, t.shape, v0.shape, vx.shape)
     sys.path.insert(0, ROOT)
     from oracle import build_oracle
 

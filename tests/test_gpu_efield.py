@@ -1,0 +1,78 @@
+"""EField on the GPU against the reference's golden data and an FP64 direct solve.
+
+Rallpack1 (passive cable, 1000 um x 0.866 um, 1978 tets) as the reference's
+test/validation/API_1/validation_efield/rallpack1_membres.py sets it up: membrane on the
+lateral surface, R_A = 1 ohm m, R_M = 4 ohm m^2, C_M = 0.01 F/m^2 (both corrected by the
+mesh's area factor), E_M = -65 mV, 0.1 nA injected over the z-min vertices, EField dt
+10 us.  V(t) at the radial extrema of both ends must match the reference's
+rallpack1_correct/{v0,vx} curves with RMS error below 1 mV (test_rallpack1_membres.py:45).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from steps_b200 import geom as sgeom
+from steps_b200 import model as smodel
+from steps_b200.solver import EF_DV_CG_FP64, EF_DV_CG_MIXED, TetOpSplit
+from tests.helpers import make_rng
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+P = dict(R_A=1.0, R_M=4.0, C_M=0.01, E_M=-0.065, Iinj=0.1e-9, diameter=1.0e-6, length=1.0e-3,
+         sim_end=0.25, EF_dt=1.0e-5)
+
+
+def rallpack1_sim(method):
+    d = np.load(os.path.join(HERE, "golden", "rallpack1.npz"))
+    mesh = sgeom.Tetmesh(d["verts"], d["tets"])
+    sgeom.TmComp("cyto", mesh, np.arange(mesh.ntets))
+    minz, maxz = mesh.getBoundMin()[2], mesh.getBoundMax()[2]
+    zeps = (maxz - minz) / mesh.ntets
+    surf = mesh.getSurfTris()
+    z = mesh.verts[mesh.tris[surf]][:, :, 2]
+    zmin = surf[np.all(z <= minz + zeps, axis=1)]
+    zmax = surf[np.all(z >= maxz - zeps, axis=1)]
+    memb_tris = np.setdiff1d(surf, np.concatenate([zmin, zmax]))
+    patch = sgeom.TmPatch("memb", mesh, memb_tris, mesh.comps["cyto"])
+    sgeom.Memb("membrane", mesh, [patch])
+    zmin_v = np.unique(mesh.tris[zmin])
+    zmax_v = np.unique(mesh.tris[zmax])
+
+    def extrema(vs):
+        r2 = (mesh.verts[vs, :2] ** 2).sum(axis=1)
+        return [int(vs[np.argmin(r2)]), int(vs[np.argmax(r2)])]
+
+    mdl = smodel.Model()
+    smodel.Volsys("vsys", mdl)
+    sim = TetOpSplit(mdl, mesh, make_rng(1), method)
+    area_cyl = np.pi * P["diameter"] * P["length"]
+    factor = patch.getArea() / area_cyl
+    sim.setEfieldDT(P["EF_dt"])
+    sim.setMembPotential("membrane", P["E_M"])
+    sim.setMembVolRes("membrane", P["R_A"])
+    sim.setMembCapac("membrane", P["C_M"] / factor)
+    sim.setMembRes("membrane", P["R_M"] * factor, P["E_M"])
+    for v in zmin_v:
+        sim.setVertIClamp(int(v), P["Iinj"] / len(zmin_v))
+    return sim, extrema(zmin_v), extrema(zmax_v), d["v0"], d["vx"]
+
+
+@pytest.mark.parametrize("method", [EF_DV_CG_FP64, EF_DV_CG_MIXED])
+def test_rallpack1_membres(steps_lib, method):
+    sim, v0s, vxs, ref0, refx = rallpack1_sim(method)
+    sim.setEfieldTolerance(1e-10)
+    dt = 5.0e-5
+    n = int(np.ceil(P["sim_end"] / dt)) + 1
+    out0, outx = np.zeros(n), np.zeros(n)
+    for k in range(n):
+        sim.run(k * dt)
+        out0[k] = np.mean([sim.getVertV(v) for v in v0s])
+        outx[k] = np.mean([sim.getVertV(v) for v in vxs])
+    npt = min(n, len(ref0))
+    rms0 = np.linalg.norm(ref0[:npt, 1] - out0[:npt]) / np.sqrt(npt)
+    rmsx = np.linalg.norm(refx[:npt, 1] - outx[:npt]) / np.sqrt(npt)
+    steps, iters, ms, rr = sim.getEfieldStats()
+    assert steps == 25000
+    assert rms0 < 1.0e-3 and rmsx < 1.0e-3, (rms0, rmsx, iters / steps)
