@@ -59,6 +59,46 @@ def rallpack1_sim(method):
     return sim, extrema(zmin_v), extrema(zmax_v), d["v0"], d["vx"]
 
 
+@pytest.mark.parametrize("method,rtol", [(EF_DV_CG_FP64, 1e-9), (EF_DV_CG_MIXED, 1e-7)])
+def test_efield_steps_match_fp64_direct_solve(steps_lib, method, rtol):
+    """20 EField steps on a 4x4x10 Kuhn box (membrane = every boundary triangle, leak,
+    a current clamp, one voltage-clamped vertex) against the FP64 direct-solve oracle."""
+    from oracle.efield_oracle import EFieldOracle
+
+    mesh = sgeom.kuhn_box(4, 4, 10, 1e-7)
+    sgeom.TmComp("cyto", mesh, np.arange(mesh.ntets))
+    surf = mesh.getSurfTris()
+    patch = sgeom.TmPatch("memb", mesh, surf, mesh.comps["cyto"])
+    sgeom.Memb("membrane", mesh, [patch])
+    mdl = smodel.Model()
+    smodel.Volsys("vsys", mdl)
+    sim = TetOpSplit(mdl, mesh, make_rng(3), method)
+    sim.setEfieldTolerance(1e-12, 1e-4)
+    sim.setEfieldDT(1e-6)
+    sim.setMembPotential("membrane", -0.065)
+    sim.setMembCapac("membrane", 0.01)
+    sim.setMembVolRes("membrane", 1.0)
+    sim.setMembRes("membrane", 1.0 / 0.3, -0.065)
+    ora = EFieldOracle(mesh.verts, mesh.tets, mesh.tris[surf])
+    ora.cm, ora.sigma, ora.g, ora.vext = 0.01, 1.0e3, 0.3e-3, -65.0
+    zmin = np.unique(mesh.tris[surf][np.all(mesh.verts[mesh.tris[surf]][:, :, 2] <= 1e-12, axis=1)])
+    for v in zmin:
+        sim.setVertIClamp(int(v), 1e-9 / len(zmin))
+        ora.iclamp[v] = 1e-9 / len(zmin) * 1e12
+    top = int(np.argmax(mesh.verts[:, 2]))
+    sim.setVertV(top, -0.070)
+    sim.setVertVClamped(top, True)
+    ora.V[top] = -70.0
+    ora.clamped[top] = True
+    for k in range(1, 21):
+        sim.run(k * 1e-6)
+        ora.advance(1e-3)
+    got = np.array([sim.getVertV(v) for v in range(mesh.nverts)]) * 1e3
+    assert got[top] == -70.0
+    assert np.max(np.abs(got - ora.V) / np.abs(ora.V)) < rtol
+    assert np.ptp(got) > 1e-3  # the clamp and the injection actually moved V
+
+
 @pytest.mark.parametrize("method", [EF_DV_CG_FP64, EF_DV_CG_MIXED])
 def test_rallpack1_membres(steps_lib, method):
     sim, v0s, vxs, ref0, refx = rallpack1_sim(method)
