@@ -142,6 +142,8 @@ int sg_get_efield_stats(sg_solver* h, uint64_t* steps, uint64_t* iterations, dou
 
 /* Window-kernel launch shape: block in {64,128,256}; grid 0 = occupancy-sized. */
 int sg_set_launch(sg_solver* h, int32_t block, int32_t grid);
+/* Replay window launches from a captured CUDA graph of 16 windows (on by default). */
+int sg_set_graphs(sg_solver* h, int32_t on);
 /* Per-window bit-exact molecule-conservation check (on by default). */
 int sg_set_conservation_check(sg_solver* h, int32_t on);
 /* Device status word (SG_ERR_* bits). */

@@ -76,6 +76,7 @@ PROTOTYPES = {
     "sg_set_diff_d": [_P, _i32, _i32, _i32, _f64],
     "sg_set_launch": [_P, _i32, _i32],
     "sg_set_conservation_check": [_P, _i32],
+    "sg_set_graphs": [_P, _i32],
     "sg_get_status": [_P, _pu32],
     "sg_set_efield_mesh": [_P, _i32, _pf64, _pi32, _i32, _pi32, _i32],
     "sg_set_efield_dt": [_P, _f64],

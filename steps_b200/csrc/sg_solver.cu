@@ -111,6 +111,7 @@ struct Solver {
         nsm = prop.multiProcessorCount;
     }
     ~Solver() {
+        drop_graph();
         if (ev_begin) cudaEventDestroy(ev_begin);
         if (ev_end) cudaEventDestroy(ev_end);
         if (stream) cudaStreamDestroy(stream);
@@ -425,6 +426,44 @@ struct Solver {
         SG_CUDA(cudaGetLastError());
     }
 
+    // ---- CUDA graph of kGraphChunk window launches, rebuilt when the launch changes ----
+    static constexpr int kGraphChunk = 16;
+    bool use_graphs = true;
+    cudaGraphExec_t graph_exec = nullptr;
+    sg_window_args graph_args{};
+    int graph_grid = -1, graph_block = -1, graph_check = -1;
+
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+
+    cudaGraphExec_t window_graph(const sg_window_args& a, int g) {
+        int chk = (check && !any_clamp) ? 1 : 0;
+        if (graph_exec && g == graph_grid && block == graph_block && chk == graph_check &&
+            std::memcmp(&a, &graph_args, sizeof(a)) == 0)
+            return graph_exec;
+        drop_graph();
+        cudaGraph_t graph = nullptr;
+        SG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            for (int i = 0; i < kGraphChunk; ++i) launch_window(a, g);
+        } catch (...) {
+            cudaStreamEndCapture(stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        SG_CUDA(cudaStreamEndCapture(stream, &graph));
+        cudaError_t e = cudaGraphInstantiate(&graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        SG_CUDA(e);
+        graph_args = a;
+        graph_grid = g;
+        graph_block = block;
+        graph_check = chk;
+        return graph_exec;
+    }
+
     // Number of windows the device time recurrence takes to reach t_end.
     static uint64_t count_windows(double t, double t_end, double period) {
         uint64_t n = 0;
@@ -525,7 +564,14 @@ struct Solver {
         sg_window_args a = window_args();
         int g = window_grid();
         if (profiling) SG_CUDA(cudaEventRecord(ev_begin, stream));
-        for (uint64_t i = 0; i < n; ++i) launch_window(a, g);
+        // Windows advance their own time on the device, so a captured chunk of window
+        // launches replays unchanged; the remainder is launched directly.
+        uint64_t done = 0;
+        if (use_graphs && n >= (uint64_t)kGraphChunk) {
+            cudaGraphExec_t ge = window_graph(a, g);
+            for (; done + kGraphChunk <= n; done += kGraphChunk) SG_CUDA(cudaGraphLaunch(ge, stream));
+        }
+        for (; done < n; ++done) launch_window(a, g);
         launches += n;
         if (profiling) {
             SG_CUDA(cudaEventRecord(ev_end, stream));
@@ -1135,6 +1181,13 @@ int sg_set_launch(sg_solver* h, int32_t block, int32_t grid) {
         if (grid < 0) throw sg::ArgErr("grid must be >= 0 (0 = occupancy-sized)");
         S(h)->block = block;
         S(h)->grid = grid;
+    });
+}
+
+int sg_set_graphs(sg_solver* h, int32_t on) {
+    return guarded([&] {
+        S(h)->use_graphs = on != 0;
+        if (!on) S(h)->drop_graph();
     });
 }
 

@@ -374,6 +374,9 @@ class TetOpSplit:
     def setConservationCheck(self, on):
         check(self._L.sg_set_conservation_check(self._h, 1 if on else 0))
 
+    def setGraphs(self, on):
+        check(self._L.sg_set_graphs(self._h, 1 if on else 0))
+
     def getStream(self):
         """The cudaStream_t (as an int) all kernels of this solver run on."""
         p = C.c_void_p()

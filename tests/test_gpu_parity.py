@@ -126,6 +126,25 @@ def test_batched_realizations_with_jitter(steps_lib):
         assert_same(sim, ora, f"t={t}")
 
 
+@pytest.mark.parametrize("graphs", [True, False])
+def test_long_runs_graph_replay(steps_lib, graphs):
+    """run() calls of 40+ windows replay a captured graph of 16 windows; the result must
+    not depend on it."""
+    sim, ora = pair(W.random_network(11), W.cube_mesh(6), seed=12)
+    sim.setGraphs(graphs)
+    rows = W.poisson_counts(sim.geom.ntets, 30.0, 12)
+    for i, s in enumerate(sim.spec_names):
+        sim.setSpecCounts(s, rows[i])
+    sync_counts(sim, ora)
+    per = sim.getUpdPeriod()
+    for k in (1, 2):
+        t = k * 41.5 * per
+        sim.run(t)
+        ora.run(t)
+        assert_same(sim, ora, f"graphs={graphs} call {k}")
+    assert sim.getNIteration() == ora.window() >= 80
+
+
 @pytest.mark.parametrize("block", [64, 256])
 def test_launch_shapes_agree(steps_lib, block):
     """The result does not depend on the block size (counter-based streams)."""
