@@ -111,6 +111,28 @@ int sg_set_reac_k(sg_solver* h, int32_t reac, int32_t real, double k);
 int sg_get_reac_k(sg_solver* h, int32_t reac, int32_t real, double* k);
 int sg_set_diff_d(sg_solver* h, int32_t comp, int32_t spec, int32_t real, double d);
 
+/* ---- membrane triangles and surface reactions (Patchdef, Tri; tri.hpp:339) ------
+ * Builder calls (before sg_setup).  The membrane triangles m = 0..ntris-1 each join the
+ * SSA unit of their inner tet (the reference's Tri in the same rank as its iTet). */
+int sg_set_surface(sg_solver* h, int32_t nsspec, int32_t ntris, const int32_t* tri_inner_tet,
+                   const int32_t* tri_patch, const double* tri_area, int32_t npatch);
+/* SReac (sreac.cpp:40-68, 305-520): dense rows slhs/supd over nsspec surface species and
+ * ilhs/iupd over nspec inner-volume species; kcst in the reference's units. */
+int sg_add_sreac(sg_solver* h, int32_t patch, const uint32_t* slhs, const uint32_t* ilhs, const int32_t* supd,
+                 const int32_t* iupd, double kcst, int32_t* out_idx);
+/* VDepSReac (vdepsreac.cpp:46-76, vdepsreacdef.cpp:194-218): k(V) tabulated at
+ * vmin + i dv (V), i < ntab, interpolated linearly at the triangle potential. */
+int sg_add_vdep_sreac(sg_solver* h, int32_t patch, const uint32_t* slhs, const uint32_t* ilhs,
+                      const int32_t* supd, const int32_t* iupd, double vmin, double dv, int32_t ntab,
+                      const double* ktab, int32_t* out_idx);
+/* OhmicCurr (ohmiccurrdef): g (S per channel) through surface species sspec, erev (V). */
+int sg_add_ohmic(sg_solver* h, int32_t patch, int32_t sspec, double g, double erev, int32_t* out_idx);
+int sg_get_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double* n);   /* TOS:4831 getTriSpecCount */
+int sg_set_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double n);    /* setTriSpecCount */
+int sg_get_patch_count(sg_solver* h, int32_t patch, int32_t sspec, double* n); /* getPatchSpecCount */
+int sg_set_patch_count(sg_solver* h, int32_t patch, int32_t sspec, double n);  /* setPatchSpecCount */
+int sg_get_tri_ohmic_i(sg_solver* h, int32_t tri, double* amps);  /* getTriOhmicI: last EField step */
+
 /* ---- membrane potential (EField; api.hpp:140, 2874-2875; efield.hpp:59) ----------
  * Units at this boundary are the reference API's: V, A, s, F/m^2, ohm m, ohm m^2.
  * Inside, the EField works in um, ms, mV, pA, pF, nS like src/steps/solver/efield. */

@@ -78,6 +78,15 @@ PROTOTYPES = {
     "sg_set_conservation_check": [_P, _i32],
     "sg_set_graphs": [_P, _i32],
     "sg_get_status": [_P, _pu32],
+    "sg_set_surface": [_P, _i32, _i32, _pi32, _pi32, _pf64, _i32],
+    "sg_add_sreac": [_P, _i32, _pu32, _pu32, _pi32, _pi32, _f64, _pi32],
+    "sg_add_vdep_sreac": [_P, _i32, _pu32, _pu32, _pi32, _pi32, _f64, _f64, _i32, _pf64, _pi32],
+    "sg_add_ohmic": [_P, _i32, _i32, _f64, _f64, _pi32],
+    "sg_get_tri_count": [_P, _i32, _i32, _pf64],
+    "sg_set_tri_count": [_P, _i32, _i32, _f64],
+    "sg_get_patch_count": [_P, _i32, _i32, _pf64],
+    "sg_set_patch_count": [_P, _i32, _i32, _f64],
+    "sg_get_tri_ohmic_i": [_P, _i32, _pf64],
     "sg_set_efield_mesh": [_P, _i32, _pf64, _pi32, _i32, _pi32, _i32],
     "sg_set_efield_dt": [_P, _f64],
     "sg_get_efield_dt": [_P, _pf64],

@@ -26,6 +26,28 @@ namespace sg {
 
 static const double AVOGADRO = 6.02214179e23;  // src/steps/math/constants.hpp:45
 
+// Membrane current per triangle over the EField step just taken (Tri::computeI,
+// src/steps/mpi/tetopsplit/tri.cpp:664-694): sum over the patch's ohmic currents of
+// g * (integral of the channel-state count / dt) * (V_tri - E_rev), in pA; the integrals
+// restart at zero for the next step.
+__global__ void ohmic_current_kernel(int M, int nss, int noc, const sg_ohmic* oc, const int32_t* tri_patch,
+                                     double* spec_int, const double* triV, double inv_dt, double* tri_I,
+                                     double* tri_I_last) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        const int p = tri_patch[m];
+        double I = 0.0;
+        for (int k = 0; k < noc; ++k) {
+            if (oc[k].patch != p) continue;
+            double nbar = spec_int[(size_t)oc[k].sspec * M + m] * inv_dt;
+            I += (nbar * oc[k].g) * (triV[m] - oc[k].erev * 1.0e3);  // S * mV
+        }
+        I *= 1.0e9;  // S mV -> pA
+        tri_I[m] = I;
+        tri_I_last[m] = I;
+        for (int s = 0; s < nss; ++s) spec_int[(size_t)s * M + m] = 0.0;
+    }
+}
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
@@ -88,6 +110,117 @@ struct Solver {
     int block = 128;
     int grid = 0;
     bool check = true;
+
+    // ---- membrane triangles and surface reactions ----
+    int nsspec = 0, ntris = 0, npatch = 0;
+    std::vector<int32_t> tri_inner, tri_patch;      // [M]
+    std::vector<double> tri_area;                   // [M] m^2
+    std::vector<sg_sreac> sreacs;                   // grouped by patch at setup
+    std::vector<double> skcst;
+    std::vector<int32_t> sreac_order_user, patch_sb;
+    std::vector<sg_vtab> vtabs;
+    std::vector<double> vtab_vals;
+    std::vector<sg_ohmic> ohmics;
+    int max_sreac_per_patch = 0;
+    bool surf_touches_volume = false;
+    DevBuf<uint32_t> d_tri_counts;
+    DevBuf<int32_t> d_tet_tris, d_tri_patch, d_psb;
+    DevBuf<double> d_tri_area, d_skcst, d_vvals, d_spec_int, d_tri_Iohm;
+    DevBuf<sg_sreac> d_sreacs;
+    DevBuf<sg_vtab> d_vtabs;
+    DevBuf<sg_ohmic> d_ohmics;
+    DevBuf<unsigned long long> d_surf_ext;
+    bool has_surf() const { return ntris > 0 && nsspec > 0; }
+
+    void setup_surface() {
+        if (!has_surf()) return;
+        if (nreal != 1) throw NotImplErr("membrane triangles with batched realizations");
+        // Surface reactions grouped by patch.
+        const int RS = (int)sreacs.size();
+        std::vector<int32_t> order(RS);
+        for (int i = 0; i < RS; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return sreacs[x].patch < sreacs[y].patch; });
+        std::vector<sg_sreac> sorted(RS);
+        std::vector<double> ks(RS);
+        sreac_order_user.assign(RS, 0);
+        for (int i = 0; i < RS; ++i) {
+            sorted[i] = sreacs[order[i]];
+            ks[i] = skcst[order[i]];
+            sreac_order_user[order[i]] = i;
+        }
+        sreacs = sorted;
+        skcst = ks;
+        patch_sb.assign(npatch + 1, 0);
+        for (auto& r : sreacs) patch_sb[r.patch + 1] += 1;
+        for (int p = 0; p < npatch; ++p) patch_sb[p + 1] += patch_sb[p];
+        max_sreac_per_patch = 1;
+        for (int p = 0; p < npatch; ++p) max_sreac_per_patch = std::max(max_sreac_per_patch, patch_sb[p + 1] - patch_sb[p]);
+        surf_touches_volume = false;
+        for (auto& r : sreacs)
+            if (r.niupd > 0) surf_touches_volume = true;
+        // SSA units: each triangle joins the unit of its inner tet.
+        std::vector<int32_t> tt((size_t)ntets * 4, -1);
+        for (int m = 0; m < ntris; ++m) {
+            int t = tri_inner[m];
+            if (t < 0 || t >= ntets) throw ArgErr("membrane triangle without a valid inner tet");
+            int slot = 0;
+            while (slot < 4 && tt[(size_t)t * 4 + slot] >= 0) ++slot;
+            if (slot == 4) throw ArgErr("a tet has more than four membrane triangles");
+            tt[(size_t)t * 4 + slot] = m;
+        }
+        d_tri_counts.alloc((size_t)nsspec * ntris);
+        d_tet_tris.alloc(tt.size());
+        d_tri_patch.alloc(ntris);
+        d_psb.alloc(npatch + 1);
+        d_tri_area.alloc(ntris);
+        d_skcst.alloc(std::max(RS, 1));
+        d_vvals.alloc(std::max<size_t>(vtab_vals.size(), 1));
+        d_spec_int.alloc((size_t)nsspec * ntris);
+        d_tri_Iohm.alloc(ntris);
+        d_sreacs.alloc(std::max(RS, 1));
+        d_vtabs.alloc(std::max<size_t>(vtabs.size(), 1));
+        d_ohmics.alloc(std::max<size_t>(ohmics.size(), 1));
+        d_surf_ext.alloc(1);
+        h2d(d_tet_tris.p, tt.data(), tt.size());
+        h2d(d_tri_patch.p, tri_patch.data(), tri_patch.size());
+        h2d(d_psb.p, patch_sb.data(), patch_sb.size());
+        h2d(d_tri_area.p, tri_area.data(), tri_area.size());
+        if (RS) h2d(d_skcst.p, skcst.data(), skcst.size());
+        if (!vtab_vals.empty()) h2d(d_vvals.p, vtab_vals.data(), vtab_vals.size());
+        if (RS) h2d(d_sreacs.p, sreacs.data(), sreacs.size());
+        if (!vtabs.empty()) h2d(d_vtabs.p, vtabs.data(), vtabs.size());
+        if (!ohmics.empty()) h2d(d_ohmics.p, ohmics.data(), ohmics.size());
+    }
+
+    void reset_surface() {
+        if (!has_surf()) return;
+        SG_CUDA(cudaMemsetAsync(d_tri_counts.p, 0, d_tri_counts.n * 4, stream));
+        SG_CUDA(cudaMemsetAsync(d_spec_int.p, 0, d_spec_int.n * 8, stream));
+        SG_CUDA(cudaMemsetAsync(d_tri_Iohm.p, 0, d_tri_Iohm.n * 8, stream));
+        SG_CUDA(cudaMemsetAsync(d_surf_ext.p, 0, 8, stream));
+    }
+
+    sg_surf_args surf_args() {
+        sg_surf_args s;
+        std::memset(&s, 0, sizeof(s));
+        if (!has_surf()) return s;
+        s.tri_counts = d_tri_counts.p;
+        s.tet_tris = d_tet_tris.p;
+        s.tri_patch = d_tri_patch.p;
+        s.tri_area = d_tri_area.p;
+        s.tri_V = ef_on ? ef.tri_V : nullptr;
+        s.sreacs = d_sreacs.p;
+        s.patch_sreac_begin = d_psb.p;
+        s.skcst = d_skcst.p;
+        s.vtabs = d_vtabs.p;
+        s.vtab_vals = d_vvals.p;
+        s.spec_int = d_spec_int.p;
+        s.nsspec = nsspec;
+        s.ntris = ntris;
+        s.nsreac = (int)sreacs.size();
+        s.max_sreac_per_patch = max_sreac_per_patch;
+        return s;
+    }
 
     // ---- EField (membrane potential) ----
     EFieldSystem ef;
@@ -233,6 +366,7 @@ struct Solver {
         }
         clampm.assign(ntets, 0u);
         is_setup = true;
+        setup_surface();
         set_kernel_smem_limits();
         reset();
     }
@@ -341,6 +475,7 @@ struct Solver {
         }
         pending_host = false;
         niteration = 0;
+        reset_surface();
         upload_params();
         sync();
     }
@@ -376,6 +511,8 @@ struct Solver {
         a.diff_total = d_diff_total.p;
         a.launch_state = d_launch.p;
         a.status = d_status.p;
+        a.surf = surf_args();
+        a.surf_ext = has_surf() ? d_surf_ext.p : nullptr;
         a.ntets = ntets;
         a.nspec = nspec;
         a.ndiff = ndiff;
@@ -386,7 +523,14 @@ struct Solver {
         return a;
     }
 
-    size_t window_smem() const { return smem_bytes(block, nspec, (int)reacs.size()); }
+    // Models with membrane triangles run the SURF kernel (block 128).
+    int eff_block() const { return has_surf() ? 128 : block; }
+    size_t window_smem() const {
+        size_t b = smem_bytes(eff_block(), nspec, (int)reacs.size());
+        if (has_surf()) b = ((b + 15) & ~(size_t)15) + surf_smem_bytes(128, nsspec, max_sreac_per_patch);
+        return b;
+    }
+    int check_flag() const { return (check && !any_clamp && !(has_surf() && surf_touches_volume)) ? 1 : 0; }
 
     void set_kernel_smem_limits() {
         size_t sm = smem_bytes(256, nspec, (int)reacs.size());
@@ -396,32 +540,47 @@ struct Solver {
             SG_CUDA(cudaFuncSetAttribute(window_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             SG_CUDA(cudaFuncSetAttribute(window_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         }
+        if (has_surf()) {
+            size_t ss = window_smem();
+            if (ss > 227 * 1024) throw NotImplErr("too many surface species or reactions for the shared-memory staging");
+            if (ss > 48 * 1024)
+                SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)ss));
+        }
     }
 
     int window_grid() {
         if (grid > 0) return grid;
         size_t sm = window_smem();
         int per_sm = 0;
-        switch (block) {
-            case 64: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<64>, 64, sm)); break;
-            case 128: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<128>, 128, sm)); break;
-            case 256: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<256>, 256, sm)); break;
-            default: throw ArgErr("block size must be 64, 128 or 256");
+        if (has_surf()) {
+            SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<128, true>, 128, sm));
+        } else {
+            switch (block) {
+                case 64: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<64>, 64, sm)); break;
+                case 128: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<128>, 128, sm)); break;
+                case 256: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<256>, 256, sm)); break;
+                default: throw ArgErr("block size must be 64, 128 or 256");
+            }
         }
         if (per_sm < 1) per_sm = 1;
-        long need = ((long)ntets + block - 1) / block;
+        long need = ((long)ntets + eff_block() - 1) / eff_block();
         long cap = (long)per_sm * nsm;
         return (int)std::max(1L, std::min(need, cap));
     }
 
     void launch_window(const sg_window_args& a, int g) {
         size_t sm = window_smem();
-        int chk = (check && !any_clamp) ? 1 : 0;
-        switch (block) {
-            case 64: window_kernel<64><<<g, 64, sm, stream>>>(a, chk); break;
-            case 128: window_kernel<128><<<g, 128, sm, stream>>>(a, chk); break;
-            case 256: window_kernel<256><<<g, 256, sm, stream>>>(a, chk); break;
-            default: throw ArgErr("block size must be 64, 128 or 256");
+        int chk = check_flag();
+        if (has_surf()) {
+            window_kernel<128, true><<<g, 128, sm, stream>>>(a, chk);
+        } else {
+            switch (block) {
+                case 64: window_kernel<64><<<g, 64, sm, stream>>>(a, chk); break;
+                case 128: window_kernel<128><<<g, 128, sm, stream>>>(a, chk); break;
+                case 256: window_kernel<256><<<g, 256, sm, stream>>>(a, chk); break;
+                default: throw ArgErr("block size must be 64, 128 or 256");
+            }
         }
         SG_CUDA(cudaGetLastError());
     }
@@ -439,7 +598,7 @@ struct Solver {
     }
 
     cudaGraphExec_t window_graph(const sg_window_args& a, int g) {
-        int chk = (check && !any_clamp) ? 1 : 0;
+        int chk = check_flag();
         if (graph_exec && g == graph_grid && block == graph_block && chk == graph_check &&
             std::memcmp(&a, &graph_args, sizeof(a)) == 0)
             return graph_exec;
@@ -513,8 +672,18 @@ struct Solver {
             download_reals();
             check_status();
             double real_dt = time() - t0;
-            // Membrane currents of the step (no channel currents on this path: tri_I = 0).
-            SG_CUDA(cudaMemsetAsync(ef.tri_I, 0, std::max(ef.ntris, 1) * 8, stream));
+            // Membrane currents of the step from the channel-state time integrals.
+            if (has_surf() && !ohmics.empty()) {
+                int g = std::max(1, std::min((ntris + 255) / 256, nsm * 4));
+                ohmic_current_kernel<<<g, 256, 0, stream>>>(ntris, nsspec, (int)ohmics.size(), d_ohmics.p,
+                                                            d_tri_patch.p, d_spec_int.p, ef.tri_V, 1.0 / real_dt,
+                                                            ef.tri_I, d_tri_Iohm.p);
+                SG_CUDA(cudaGetLastError());
+                launches += 1;
+            } else {
+                SG_CUDA(cudaMemsetAsync(ef.tri_I, 0, std::max(ef.ntris, 1) * 8, stream));
+                if (has_surf()) SG_CUDA(cudaMemsetAsync(d_spec_int.p, 0, d_spec_int.n * 8, stream));
+            }
             ef.advance(real_dt * 1.0e3, stream);  // efield.cpp:229-234: s -> ms
         }
         sync();
@@ -714,6 +883,12 @@ struct Solver {
     // floor allocation, then the remainder placed by adjusted Pareto order sampling
     // (src/steps/math/sample.hpp:59-200) with the fractional parts as inclusion weights.
     void distribute(double x, const std::vector<int>& tets, std::vector<uint32_t>& v, sg_stream* st) {
+        distribute_w(x, tets, vol, v, st);
+    }
+
+    // Same rule with weights w (tet volumes for compartments, triangle areas for patches).
+    void distribute_w(double x, const std::vector<int>& tets, const std::vector<double>& vol,
+                      std::vector<uint32_t>& v, sg_stream* st) {
         if (tets.empty()) return;
         if (x == 0.0) {
             for (int t : tets) v[t] = 0;
@@ -853,6 +1028,60 @@ struct Solver {
         for (int rr = rb; rr < re; ++rr) dcst[((size_t)rr * ncomp + c) * nspec + s] = d;
         upload_params();
         sync();
+    }
+
+    // ---- membrane triangle counts (TOS:4831 getTriSpecCount, setTriSpecCount; patch
+    //      counts distributed by triangle area as setPatchSpecCount) ----
+    void check_tri(int m, int s) const {
+        if (!has_surf()) throw ProgErr("no membrane triangles in this solver");
+        if (m < 0 || m >= ntris) throw ArgErr("triangle index out of range: " + std::to_string(m));
+        if (s < 0 || s >= nsspec) throw ArgErr("surface species index out of range: " + std::to_string(s));
+    }
+    double get_tri_count(int m, int s) {
+        check_tri(m, s);
+        uint32_t c = 0;
+        d2h(&c, d_tri_counts.p + (size_t)s * ntris + m, 1);
+        sync();
+        return (double)c;
+    }
+    void set_tri_count(int m, int s, double n) {
+        check_tri(m, s);
+        sg_stream st = setup_stream();
+        uint32_t c = round_count(n, &st);
+        h2d(d_tri_counts.p + (size_t)s * ntris + m, &c, 1);
+        sync();
+    }
+    double get_patch_count(int p, int s) {
+        check_tri(0, s);
+        std::vector<uint32_t> v(ntris);
+        d2h(v.data(), d_tri_counts.p + (size_t)s * ntris, ntris);
+        sync();
+        unsigned long long sum = 0;
+        for (int m = 0; m < ntris; ++m)
+            if (tri_patch[m] == p) sum += v[m];
+        return (double)sum;
+    }
+    void set_patch_count(int p, int s, double n) {
+        check_tri(0, s);
+        if (p < 0 || p >= npatch) throw ArgErr("patch index out of range");
+        if (!(n >= 0.0) || n > 4294967295.0) throw ArgErr("count out of range");
+        std::vector<uint32_t> v(ntris);
+        d2h(v.data(), d_tri_counts.p + (size_t)s * ntris, ntris);
+        sync();
+        std::vector<int> tris;
+        for (int m = 0; m < ntris; ++m)
+            if (tri_patch[m] == p) tris.push_back(m);
+        sg_stream st = setup_stream();
+        distribute_w(n, tris, tri_area, v, &st);
+        h2d(d_tri_counts.p + (size_t)s * ntris, v.data(), (size_t)ntris);
+        sync();
+    }
+    double get_tri_ohmic_i(int m) {
+        check_tri(m, 0);
+        double x = 0.0;
+        d2h(&x, d_tri_Iohm.p + m, 1);
+        sync();
+        return x * 1.0e-12;  // pA -> A
     }
 
     unsigned long long reac_extent(int user_reac) {
@@ -1195,11 +1424,157 @@ int sg_set_conservation_check(sg_solver* h, int32_t on) {
     return guarded([&] { S(h)->check = on != 0; });
 }
 
+int sg_set_surface(sg_solver* h, int32_t nsspec, int32_t ntris, const int32_t* tri_inner_tet,
+                   const int32_t* tri_patch, const double* tri_area, int32_t npatch) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (nsspec <= 0 || nsspec > 32) throw sg::ArgErr("surface species count must be in 1..32");
+        if (ntris <= 0 || npatch <= 0) throw sg::ArgErr("need membrane triangles and patches");
+        need(tri_inner_tet, "tri_inner_tet");
+        need(tri_patch, "tri_patch");
+        need(tri_area, "tri_area");
+        s->nsspec = nsspec;
+        s->ntris = ntris;
+        s->npatch = npatch;
+        s->tri_inner.assign(tri_inner_tet, tri_inner_tet + ntris);
+        s->tri_patch.assign(tri_patch, tri_patch + ntris);
+        s->tri_area.assign(tri_area, tri_area + ntris);
+        for (int32_t p : s->tri_patch)
+            if (p < 0 || p >= npatch) throw sg::ArgErr("triangle patch index out of range");
+        for (double a : s->tri_area)
+            if (!(a > 0.0)) throw sg::ArgErr("triangle area must be positive");
+    });
+}
+
+static void build_sreac(Solver* s, int32_t patch, const uint32_t* slhs, const uint32_t* ilhs, const int32_t* supd,
+                        const int32_t* iupd, sg_sreac& r) {
+    s->require_not_setup();
+    if (s->nsspec <= 0) throw sg::ProgErr("call sg_set_surface first");
+    if (patch < 0 || patch >= s->npatch) throw sg::ArgErr("patch index out of range");
+    need(slhs, "slhs");
+    need(ilhs, "ilhs");
+    need(supd, "supd");
+    need(iupd, "iupd");
+    std::memset(&r, 0, sizeof(r));
+    r.patch = patch;
+    r.vdep = -1;
+    for (int i = 0; i < s->nsspec; ++i) {
+        if (!slhs[i]) continue;
+        if (slhs[i] > 4 || r.nslhs == SG_MAX_LHS) throw sg::ArgErr("surface reactant stoichiometry");
+        r.slhs_spec[r.nslhs] = i;
+        r.slhs_ord[r.nslhs++] = (int32_t)slhs[i];
+        r.order += (int32_t)slhs[i];
+    }
+    for (int i = 0; i < s->nspec; ++i) {
+        if (!ilhs[i]) continue;
+        if (ilhs[i] > 4 || r.nilhs == SG_MAX_LHS) throw sg::ArgErr("volume reactant stoichiometry");
+        r.ilhs_spec[r.nilhs] = i;
+        r.ilhs_ord[r.nilhs++] = (int32_t)ilhs[i];
+        r.order += (int32_t)ilhs[i];
+    }
+    if (r.order > 4) throw sg::ArgErr("reaction order above 4 is not supported");
+    r.surf_surf = (r.nilhs == 0) ? 1 : 0;
+    for (int i = 0; i < s->nsspec; ++i) {
+        if (!supd[i]) continue;
+        if (r.nsupd == SG_MAX_UPD) throw sg::ArgErr("too many changed surface species");
+        r.supd_spec[r.nsupd] = i;
+        r.supd_delta[r.nsupd++] = supd[i];
+    }
+    for (int i = 0; i < s->nspec; ++i) {
+        if (!iupd[i]) continue;
+        if (r.niupd == SG_MAX_UPD) throw sg::ArgErr("too many changed volume species");
+        r.iupd_spec[r.niupd] = i;
+        r.iupd_delta[r.niupd++] = iupd[i];
+    }
+}
+
+int sg_add_sreac(sg_solver* h, int32_t patch, const uint32_t* slhs, const uint32_t* ilhs, const int32_t* supd,
+                 const int32_t* iupd, double kcst, int32_t* out_idx) {
+    return guarded([&] {
+        Solver* s = S(h);
+        sg_sreac r;
+        build_sreac(s, patch, slhs, ilhs, supd, iupd, r);
+        if (!(kcst >= 0.0)) throw sg::ArgErr("reaction constant must be non-negative");
+        s->sreacs.push_back(r);
+        s->skcst.push_back(kcst);
+        if (out_idx) *out_idx = (int32_t)s->sreacs.size() - 1;
+    });
+}
+
+int sg_add_vdep_sreac(sg_solver* h, int32_t patch, const uint32_t* slhs, const uint32_t* ilhs,
+                      const int32_t* supd, const int32_t* iupd, double vmin, double dv, int32_t ntab,
+                      const double* ktab, int32_t* out_idx) {
+    return guarded([&] {
+        Solver* s = S(h);
+        sg_sreac r;
+        build_sreac(s, patch, slhs, ilhs, supd, iupd, r);
+        need(ktab, "ktab");
+        if (ntab < 2 || !(dv > 0.0)) throw sg::ArgErr("k(V) table needs >= 2 points and dv > 0");
+        for (int i = 0; i < ntab; ++i)
+            if (!(ktab[i] >= 0.0)) throw sg::ArgErr("k(V) must be non-negative");
+        sg_vtab vt;
+        vt.vmin = vmin;
+        vt.dv = dv;
+        vt.off = (int32_t)s->vtab_vals.size();
+        vt.n = ntab;
+        s->vtab_vals.insert(s->vtab_vals.end(), ktab, ktab + ntab);
+        r.vdep = (int32_t)s->vtabs.size();
+        s->vtabs.push_back(vt);
+        s->sreacs.push_back(r);
+        s->skcst.push_back(0.0);
+        if (out_idx) *out_idx = (int32_t)s->sreacs.size() - 1;
+    });
+}
+
+int sg_add_ohmic(sg_solver* h, int32_t patch, int32_t sspec, double g, double erev, int32_t* out_idx) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (patch < 0 || patch >= s->npatch) throw sg::ArgErr("patch index out of range");
+        if (sspec < 0 || sspec >= s->nsspec) throw sg::ArgErr("surface species index out of range");
+        if (!(g >= 0.0)) throw sg::ArgErr("conductance must be non-negative");
+        s->ohmics.push_back(sg_ohmic{patch, sspec, g, erev});
+        if (out_idx) *out_idx = (int32_t)s->ohmics.size() - 1;
+    });
+}
+
+int sg_get_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double* n) {
+    return guarded([&] {
+        need(n, "n");
+        *n = S(h)->get_tri_count(tri, sspec);
+    });
+}
+
+int sg_set_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double n) {
+    return guarded([&] { S(h)->set_tri_count(tri, sspec, n); });
+}
+
+int sg_get_patch_count(sg_solver* h, int32_t patch, int32_t sspec, double* n) {
+    return guarded([&] {
+        need(n, "n");
+        *n = S(h)->get_patch_count(patch, sspec);
+    });
+}
+
+int sg_set_patch_count(sg_solver* h, int32_t patch, int32_t sspec, double n) {
+    return guarded([&] { S(h)->set_patch_count(patch, sspec, n); });
+}
+
+int sg_get_tri_ohmic_i(sg_solver* h, int32_t tri, double* amps) {
+    return guarded([&] {
+        need(amps, "amps");
+        *amps = S(h)->get_tri_ohmic_i(tri);
+    });
+}
+
 int sg_set_efield_mesh(sg_solver* h, int32_t nverts, const double* verts, const int32_t* tet_verts,
                        int32_t ntris, const int32_t* tri_verts, int32_t method) {
     return guarded([&] {
         Solver* s = S(h);
         s->require_setup();
+        if (s->has_surf() && ntris != s->ntris)
+            throw sg::ArgErr("the EField membrane must be the surface triangles, in the same order");
         need(verts, "verts");
         need(tet_verts, "tet_verts");
         if (ntris > 0) need(tri_verts, "tri_verts");

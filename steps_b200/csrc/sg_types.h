@@ -34,6 +34,57 @@ typedef struct sg_reac {
     uint32_t upd_mask;                 // bit per changed species
 } sg_reac;
 
+// One surface reaction of a patch (Patchdef sreac_lhs_S/I, sreac_upd_S/I,
+// src/steps/solver/patchdef.hpp), optionally with a voltage-dependent constant
+// (VDepSReacdef, src/steps/solver/vdepsreacdef.cpp:194-218).  Reactants and products on
+// the triangle (S) and in its inner tet (I); outer-volume terms are not supported.
+typedef struct sg_sreac {
+    int32_t patch;
+    int32_t order;                     // total lhs stoichiometry (surface + volume)
+    int32_t surf_surf;                 // 1: no volume reactant -> area scaling of the constant
+    int32_t vdep;                      // index of the k(V) table, -1 for a constant kcst
+    int32_t nslhs, nilhs, nsupd, niupd;
+    int32_t slhs_spec[SG_MAX_LHS], slhs_ord[SG_MAX_LHS];
+    int32_t ilhs_spec[SG_MAX_LHS], ilhs_ord[SG_MAX_LHS];
+    int32_t supd_spec[SG_MAX_UPD], supd_delta[SG_MAX_UPD];
+    int32_t iupd_spec[SG_MAX_UPD], iupd_delta[SG_MAX_UPD];
+} sg_sreac;
+
+// k(V) table of a voltage-dependent surface reaction: k at vmin + i dv, i < n (V, /s ...).
+typedef struct sg_vtab {
+    double vmin;
+    double dv;
+    int32_t off;                       // offset into the concatenated table values
+    int32_t n;
+} sg_vtab;
+
+// Ohmic current through one surface species (channel state) of a patch (OhmicCurrdef).
+typedef struct sg_ohmic {
+    int32_t patch;
+    int32_t sspec;
+    double g;                          // S per channel
+    double erev;                       // V
+} sg_ohmic;
+
+// Surface part of the window kernel (null tables when the model has no membrane).
+typedef struct sg_surf_args {
+    uint32_t* tri_counts;              // [SS][M] surface species per membrane triangle
+    const int32_t* tet_tris;           // [T][4] membrane triangles whose SSA unit is the tet, -1
+    const int32_t* tri_patch;          // [M]
+    const double* tri_area;            // [M] m^2
+    const double* tri_V;               // [M] mV (EField), null without EField
+    const sg_sreac* sreacs;            // [RS] grouped by patch
+    const int32_t* patch_sreac_begin;  // [npatch + 1]
+    const double* skcst;               // [RS]
+    const sg_vtab* vtabs;
+    const double* vtab_vals;
+    double* spec_int;                  // [SS][M] time integral of surface counts (s) this EField step
+    int32_t nsspec;
+    int32_t ntris;
+    int32_t nsreac;
+    int32_t max_sreac_per_patch;
+} sg_surf_args;
+
 // Per realization bookkeeping, advanced on the device by the last block of each
 // window launch so that the window kernel can be replayed from a CUDA graph.
 typedef struct sg_real {
@@ -75,6 +126,8 @@ typedef struct sg_window_args {
     unsigned long long* diff_total;    // [1]     diffused molecules since reset
     unsigned long long* launch_state;  // [4]: done blocks, launch parity, active count, prev valid
     uint32_t* status;                  // device error word
+    sg_surf_args surf;                 // membrane triangles (SURF kernels only)
+    unsigned long long* surf_ext;      // [1] surface reaction events since reset
     int32_t ntets;                     // total tets over realizations
     int32_t nspec;
     int32_t ndiff;

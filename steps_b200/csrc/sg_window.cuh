@@ -16,6 +16,7 @@
 // the reverse-face table, so every tet only writes its own counts.
 #pragma once
 #include "sg_rng.cuh"
+#include "sg_surf.cuh"
 #include "sg_types.h"
 
 namespace sg {
@@ -178,13 +179,161 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
     }
 }
 
+// SSA of a unit made of a tet and up to four membrane triangles (inner tet = this tet):
+// volume reactions, then each triangle's surface reactions, in a fixed order.  All
+// propensities are re-evaluated after every event (such units are few).  Triangle counts
+// and their time integrals (ohmic currents) are written back at the end of the window.
+static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const smem_layout& L, const surf_layout& SL,
+                                          int tid, int BLOCK, int rb, int re, const double* K, double ivs,
+                                          uint32_t clampm, double T, sg_stream* st, int4 tris) {
+    const sg_surf_args& sa = a.surf;
+    const int SS = sa.nsspec, RSP = sa.max_sreac_per_patch, M = sa.ntris;
+    uint32_t* sc = L.cnt + tid;
+    double* so = L.occ + tid;
+    double* sl = L.last + tid;
+    const int mm[4] = {tris.x, tris.y, tris.z, tris.w};
+    int pb[4], pe[4];
+    double area[4], vm[4];
+    for (int j = 0; j < 4; ++j) {
+        pb[j] = pe[j] = 0;
+        area[j] = 0.0;
+        vm[j] = 0.0;
+        const int m = mm[j];
+        if (m < 0) continue;
+        const int p = sa.tri_patch[m];
+        pb[j] = sa.patch_sreac_begin[p];
+        pe[j] = sa.patch_sreac_begin[p + 1];
+        area[j] = sa.tri_area[m];
+        vm[j] = sa.tri_V ? sa.tri_V[m] : 0.0;
+        for (int s = 0; s < SS; ++s) {
+            SL.cnt[(j * SS + s) * BLOCK + tid] = sa.tri_counts[(size_t)s * M + m];
+            SL.occ[(j * SS + s) * BLOCK + tid] = 0.0;
+            SL.last[(j * SS + s) * BLOCK + tid] = 0.0;
+        }
+    }
+    double tt = 0.0;
+    for (;;) {
+        double a0 = 0.0;
+        for (int q = rb; q < re; ++q) {
+            const sg_reac* rc = &L.reac[q];
+            double pq = reac_prop(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
+            L.prop[q * BLOCK + tid] = pq;
+            a0 = a0 + pq;
+        }
+        for (int j = 0; j < 4; ++j) {
+            for (int q = pb[j]; q < pe[j]; ++q) {
+                const sg_sreac& r = sa.sreacs[q];
+                double k = (r.vdep >= 0) ? vdep_k(sa, r.vdep, vm[j], a.status) : sa.skcst[q];
+                double h = sreac_h(r, SL.cnt + (size_t)j * SS * BLOCK + tid, sc, BLOCK);
+                double pq = h * sreac_ccst(r, k, ivs, area[j]);
+                SL.prop[(j * RSP + (q - pb[j])) * BLOCK + tid] = pq;
+                a0 = a0 + pq;
+            }
+        }
+        if (!(a0 > 0.0)) break;
+        double dt = -sg_log(sg_u01_oc(sg_next_u32(st))) / a0;
+        if (tt + dt > T) break;
+        tt = tt + dt;
+        double target = sg_u01_co(sg_next_u32(st)) * a0;
+        double cum = 0.0;
+        int sj = -2, sq = -1, lj = -2, lq = -1;  // selected (slot or -1 = volume, index)
+        for (int q = rb; q < re && sj == -2; ++q) {
+            double pq = L.prop[q * BLOCK + tid];
+            if (pq > 0.0) {
+                lj = -1;
+                lq = q;
+                cum = cum + pq;
+                if (target < cum) {
+                    sj = -1;
+                    sq = q;
+                }
+            }
+        }
+        for (int j = 0; j < 4 && sj == -2; ++j) {
+            for (int q = pb[j]; q < pe[j]; ++q) {
+                double pq = SL.prop[(j * RSP + (q - pb[j])) * BLOCK + tid];
+                if (pq > 0.0) {
+                    lj = j;
+                    lq = q;
+                    cum = cum + pq;
+                    if (target < cum) {
+                        sj = j;
+                        sq = q;
+                        break;
+                    }
+                }
+            }
+        }
+        if (sj == -2) {
+            sj = lj;
+            sq = lq;
+        }
+        if (sq < 0) break;
+        if (sj == -1) {
+            const sg_reac* rc = &L.reac[sq];
+            for (int i = 0; i < rc->nupd; ++i) {
+                int s = rc->upd_spec[i];
+                if ((clampm >> s) & 1u) continue;
+                uint32_t old = sc[s * BLOCK];
+                so[s * BLOCK] = so[s * BLOCK] + (double)old * (tt - sl[s * BLOCK]);
+                sl[s * BLOCK] = tt;
+                long long nc = (long long)old + rc->upd_delta[i];
+                if (nc < 0 || nc > 0xFFFFFFFFll) {
+                    atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
+                    nc = nc < 0 ? 0 : 0xFFFFFFFFll;
+                }
+                sc[s * BLOCK] = (uint32_t)nc;
+            }
+            atomicAdd(&L.ext[sq], 1u);
+        } else {
+            const sg_sreac& r = sa.sreacs[sq];
+            for (int i = 0; i < r.nsupd; ++i) {
+                size_t o = (size_t)(sj * SS + r.supd_spec[i]) * BLOCK + tid;
+                uint32_t old = SL.cnt[o];
+                SL.occ[o] = SL.occ[o] + (double)old * (tt - SL.last[o]);
+                SL.last[o] = tt;
+                long long nc = (long long)old + r.supd_delta[i];
+                if (nc < 0 || nc > 0xFFFFFFFFll) {
+                    atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
+                    nc = nc < 0 ? 0 : 0xFFFFFFFFll;
+                }
+                SL.cnt[o] = (uint32_t)nc;
+            }
+            for (int i = 0; i < r.niupd; ++i) {
+                int s = r.iupd_spec[i];
+                if ((clampm >> s) & 1u) continue;
+                uint32_t old = sc[s * BLOCK];
+                so[s * BLOCK] = so[s * BLOCK] + (double)old * (tt - sl[s * BLOCK]);
+                sl[s * BLOCK] = tt;
+                long long nc = (long long)old + r.iupd_delta[i];
+                if (nc < 0 || nc > 0xFFFFFFFFll) {
+                    atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
+                    nc = nc < 0 ? 0 : 0xFFFFFFFFll;
+                }
+                sc[s * BLOCK] = (uint32_t)nc;
+            }
+            atomicAdd(a.surf_ext, 1ull);
+        }
+    }
+    for (int j = 0; j < 4; ++j) {
+        const int m = mm[j];
+        if (m < 0) continue;
+        for (int s = 0; s < SS; ++s) {
+            size_t o = (size_t)(j * SS + s) * BLOCK + tid;
+            uint32_t c = SL.cnt[o];
+            sa.tri_counts[(size_t)s * M + m] = c;
+            sa.spec_int[(size_t)s * M + m] += SL.occ[o] + (double)c * (T - SL.last[o]);
+        }
+    }
+}
+
 // Resident threads per SM the window kernel is compiled for (caps registers per thread).
 #ifndef SG_WINDOW_THREADS_PER_SM
 #define SG_WINDOW_THREADS_PER_SM 1024
 #endif
 
 // Window kernel: gather (if pending) -> totals -> SSA -> diffusion leave -> store.
-template <int BLOCK>
+template <int BLOCK, bool SURF = false>
 __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     window_kernel(sg_window_args a, int check) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -193,6 +342,10 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     const int R = a.nreac;
     const int tid = threadIdx.x;
     smem_layout L = carve(smem_raw, BLOCK, S, R);
+    surf_layout SLy;
+    if (SURF)
+        SLy = surf_carve(smem_raw + ((smem_bytes(BLOCK, S, R) + 15) & ~(size_t)15), BLOCK, a.surf.nsspec,
+                         a.surf.max_sreac_per_patch);
     for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
     for (int i = tid; i < R; i += BLOCK) L.reac[i] = a.reacs[i];
     for (int i = tid; i < S; i += BLOCK) L.tot[i] = 0ull;
@@ -269,8 +422,16 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
         const int rb = __ldg(&a.comp_reac_begin[comp]);
         const int re = __ldg(&a.comp_reac_begin[comp + 1]);
 
-        // Phase 2: reaction SSA over the window.
-        if (re > rb) tet_ssa(a, L, tid, BLOCK, rb, re, K, ivs, clampm, T, &st);
+        // Phase 2: reaction SSA over the window (with the tet's membrane triangles, if any).
+        if (SURF) {
+            const int4 tr = __ldg(reinterpret_cast<const int4*>(a.surf.tet_tris) + t);
+            if ((tr.x & tr.y & tr.z & tr.w) >= 0 || tr.x >= 0 || tr.y >= 0 || tr.z >= 0 || tr.w >= 0)
+                tet_ssa_surf(a, L, SLy, tid, BLOCK, rb, re, K, ivs, clampm, T, &st, tr);
+            else if (re > rb)
+                tet_ssa(a, L, tid, BLOCK, rb, re, K, ivs, clampm, T, &st);
+        } else if (re > rb) {
+            tet_ssa(a, L, tid, BLOCK, rb, re, K, ivs, clampm, T, &st);
+        }
 
         // Phase 3: diffusion leave, one (tet, species) at a time.
         const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);

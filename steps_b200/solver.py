@@ -68,14 +68,97 @@ def flatten(model, geom):
                 reacs.append((ci, rid, lhs, upd, r.kcst))
             for did, d in vs.diffs.items():
                 diffs.append((ci, did, sidx(d.lig), d.dcst))
+    surf = flatten_surface(model, geom, spec_index, comp_index, tet_comp)
     return {
         "spec_names": spec_names, "spec_index": spec_index,
         "comp_names": comp_names, "comp_index": comp_index,
-        "tet_comp": tet_comp, "reacs": reacs, "diffs": diffs,
+        "tet_comp": tet_comp, "reacs": reacs, "diffs": diffs, "surf": surf,
         "vol": np.ascontiguousarray(geom.tet_vol, dtype=np.float64),
         "neighb": np.ascontiguousarray(geom.tet_neighb, dtype=np.int32),
         "area": np.ascontiguousarray(geom.tet_area, dtype=np.float64),
         "dist": np.ascontiguousarray(geom.tet_dist, dtype=np.float64),
+    }
+
+
+def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
+    """Patches -> membrane triangle tables (the role of Patchdef, src/steps/solver/patchdef.hpp):
+    the sorted union of all patch triangles, each with its inner tet (the tet on the side of
+    the patch's inner compartment), patch and area; the surface species; the surface
+    reactions (dense slhs/ilhs/supd/iupd rows), k(V) tables of voltage-dependent ones, and
+    the ohmic currents.  None when the mesh has no patch with a surface system."""
+    patches = [p for p in getattr(geom, "patches", {}).values() if p.surfsys]
+    if not patches:
+        return None
+    tris = np.unique(np.concatenate([p.tris for p in patches]))
+    tri_index = {int(t): i for i, t in enumerate(tris)}
+    tri_patch = np.full(len(tris), -1, dtype=np.int32)
+    inner = np.full(len(tris), -1, dtype=np.int32)
+    for pi, p in enumerate(patches):
+        ci = comp_index[p.icomp.id] if p.icomp is not None else -1
+        for t in p.tris:
+            m = tri_index[int(t)]
+            if tri_patch[m] >= 0:
+                raise ArgErr("a triangle belongs to two patches")
+            tri_patch[m] = pi
+            a, b = geom.tri_tets[t]
+            inner[m] = a if (a >= 0 and tet_comp[a] == ci) else b
+            if inner[m] < 0 or tet_comp[inner[m]] != ci:
+                raise ArgErr(f"triangle {t} has no tet in the inner compartment of patch {p.id}")
+    sspecs = []
+
+    def sid(name):
+        if name not in sspecs:
+            sspecs.append(name)
+        return sspecs.index(name)
+
+    for p in patches:
+        for ssn in p.surfsys:
+            ss = model.surfsys[ssn]
+            for r in list(ss.sreacs.values()) + list(ss.vdepsreacs.values()):
+                if r.olhs or r.orhs:
+                    raise _lib.NotImplErr("surface reactions with outer-volume species")
+                for s in r.slhs + r.srhs:
+                    sid(s)
+            for oc in ss.ohmiccurrs.values():
+                sid(oc.chanstate)
+    S, SS = len(spec_index), max(len(sspecs), 1)
+
+    def rows(r):
+        slhs = np.zeros(SS, np.uint32)
+        ilhs = np.zeros(S, np.uint32)
+        supd = np.zeros(SS, np.int32)
+        iupd = np.zeros(S, np.int32)
+        for s in r.slhs:
+            slhs[sid(s)] += 1
+            supd[sid(s)] -= 1
+        for s in r.srhs:
+            supd[sid(s)] += 1
+        for s in r.ilhs:
+            ilhs[spec_index[s]] += 1
+            iupd[spec_index[s]] -= 1
+        for s in r.irhs:
+            iupd[spec_index[s]] += 1
+        return slhs, ilhs, supd, iupd
+
+    sreacs, ohmics = [], []
+    for pi, p in enumerate(patches):
+        for ssn in p.surfsys:
+            ss = model.surfsys[ssn]
+            for rid, r in ss.sreacs.items():
+                sreacs.append((pi, rid, rows(r), r.kcst, None))
+            for rid, r in ss.vdepsreacs.items():
+                vmin, vmax, dv = r.vrange
+                n = int(round((vmax - vmin) / dv)) + 1
+                tab = np.array([r.kfunc(vmin + i * dv) for i in range(n)], dtype=np.float64)
+                sreacs.append((pi, rid, rows(r), 0.0, (vmin, dv, tab)))
+            for oid, oc in ss.ohmiccurrs.items():
+                ohmics.append((pi, oid, sid(oc.chanstate), oc.g, oc.erev))
+    return {
+        "patch_names": [p.id for p in patches], "tris": tris, "tri_index": tri_index,
+        "tri_patch": tri_patch, "tri_inner": inner,
+        "tri_area": np.ascontiguousarray(geom.tri_area[tris], dtype=np.float64),
+        "sspec_names": sspecs, "sspec_index": {n: i for i, n in enumerate(sspecs)},
+        "sreacs": sreacs, "ohmics": ohmics, "nsspec": SS,
     }
 
 
@@ -129,6 +212,28 @@ class TetOpSplit:
             out = C.c_int32()
             check(L.sg_add_diff(h, ci, s, d, C.byref(out)))
             self.diff_index[(self.comp_names[ci], did)] = s
+        self.surf = F["surf"]
+        if self.surf is not None:
+            sf = self.surf
+            tri_inner = np.ascontiguousarray(sf["tri_inner"], dtype=np.int32)
+            tri_patch = np.ascontiguousarray(sf["tri_patch"], dtype=np.int32)
+            check(L.sg_set_surface(h, sf["nsspec"], len(sf["tris"]), ptr(tri_inner, C.c_int32),
+                                   ptr(tri_patch, C.c_int32), ptr(sf["tri_area"], C.c_double),
+                                   len(sf["patch_names"])))
+            self.sreac_index = {}
+            for (pi, rid, (slhs, ilhs, supd, iupd), k, vdep) in sf["sreacs"]:
+                out = C.c_int32()
+                args = (h, pi, ptr(slhs, C.c_uint32), ptr(ilhs, C.c_uint32), ptr(supd, C.c_int32),
+                        ptr(iupd, C.c_int32))
+                if vdep is None:
+                    check(L.sg_add_sreac(*args, k, C.byref(out)))
+                else:
+                    vmin, dv, tab = vdep
+                    check(L.sg_add_vdep_sreac(*args, vmin, dv, len(tab), ptr(tab, C.c_double), C.byref(out)))
+                self.sreac_index[(sf["patch_names"][pi], rid)] = out.value
+            for (pi, oid, ss, g, erev) in sf["ohmics"]:
+                out = C.c_int32()
+                check(L.sg_add_ohmic(h, pi, ss, g, erev, C.byref(out)))
         if realizations is not None:
             off = np.ascontiguousarray(realizations, dtype=np.int32)
             self.nreal = len(off) - 1
@@ -143,6 +248,8 @@ class TetOpSplit:
         if len(membs) != 1:
             raise ArgErr("the membrane potential needs exactly one Memb on the mesh")
         memb = next(iter(membs.values()))
+        if self.surf is not None and not np.array_equal(memb.tris, self.surf["tris"]):
+            raise ArgErr("the membrane must consist of exactly the patches with surface systems")
         self.memb_tris = memb.tris
         self.memb_index = {int(t): i for i, t in enumerate(memb.tris)}
         verts = np.ascontiguousarray(geom.verts, dtype=np.float64)
@@ -313,6 +420,51 @@ class TetOpSplit:
         except KeyError:
             raise ArgErr(f"diffusion '{d}' undefined in compartment '{c}'") from None
         check(self._L.sg_set_diff_d(self._h, self._comp(c), s, int(realization), float(dcst)))
+
+    # ------------------------------------------------------ triangles / patches
+    def _tri(self, tidx):
+        try:
+            return self.surf["tri_index"][int(tidx)]
+        except (TypeError, KeyError):
+            raise ArgErr(f"triangle {tidx} is not in a patch") from None
+
+    def _sspec(self, name):
+        try:
+            return self.surf["sspec_index"][name]
+        except (TypeError, KeyError):
+            raise ArgErr(f"unknown surface species '{name}'") from None
+
+    def _patch(self, name):
+        try:
+            return self.surf["patch_names"].index(name)
+        except (TypeError, ValueError):
+            raise ArgErr(f"unknown patch '{name}'") from None
+
+    def getTriSpecCount(self, tidx, s):
+        n = C.c_double()
+        check(self._L.sg_get_tri_count(self._h, self._tri(tidx), self._sspec(s), C.byref(n)))
+        return n.value
+
+    def setTriSpecCount(self, tidx, s, n):
+        check(self._L.sg_set_tri_count(self._h, self._tri(tidx), self._sspec(s), float(n)))
+
+    def getPatchSpecCount(self, p, s):
+        n = C.c_double()
+        check(self._L.sg_get_patch_count(self._h, self._patch(p), self._sspec(s), C.byref(n)))
+        return n.value
+
+    def setPatchSpecCount(self, p, s, n):
+        check(self._L.sg_set_patch_count(self._h, self._patch(p), self._sspec(s), float(n)))
+
+    def getTriOhmicI(self, tidx, oc=None):
+        x = C.c_double()
+        check(self._L.sg_get_tri_ohmic_i(self._h, self._tri(tidx), C.byref(x)))
+        return x.value
+
+    getTriCount = getTriSpecCount
+    setTriCount = setTriSpecCount
+    getPatchCount = getPatchSpecCount
+    setPatchCount = setPatchSpecCount
 
     # ------------------------------------------------ membrane potential (EField)
     def setEfieldDT(self, dt):
