@@ -326,17 +326,176 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args):
+    """Batched ensemble: 512 realizations of n^3 Kuhn cubes (n uniform in 8..30) with the
+    8-species network and per-realization log-normal (0.2) rate jitter, in one launch per
+    window; against the same realizations run one after another with the plain path."""
+    import torch
+
+    from steps_b200 import rng as srng
+    from steps_b200 import workloads as W
+    from steps_b200.solver import TetOpSplit
+
+    nreal = args.nreal
+    sizes = W.batched_sizes(nreal, SEED)
+    t0 = time.perf_counter()
+    mesh = W.batched_mesh(sizes)
+    mdl = W.random_network(SEED)
+    r = srng.create("r123", 512)
+    r.initialize(SEED)
+    sim = TetOpSplit(mdl, mesh, r, realizations=mesh.offsets)
+    jit = W.rate_jitter(nreal, 12, SEED)
+    names = [f"r{q}" for q in range(12)]
+    base = [sim.getCompReacK("comp", n, 0) for n in names]
+    for rr in range(nreal):
+        for q, n in enumerate(names):
+            sim.setCompReacK("comp", n, base[q] * jit[rr, q], realization=rr)
+    rows = W.poisson_counts(mesh.ntets, 50.0, SEED, nspec=NSPEC)
+    for i, s in enumerate(sim.spec_names):
+        sim.setSpecCounts(s, rows[i])
+    setup_s = time.perf_counter() - t0
+    ext = torch.cuda.ExternalStream(sim.getStream())
+    t_sim = 0.0
+    for _ in range(args.warmup):
+        t_sim += STEP_SIM_S
+        sim.run(t_sim)
+    torch.cuda.synchronize()
+    it0 = sim.getNIteration()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(args.steps):
+        t_sim += STEP_SIM_S
+        sim.run(t_sim)
+    e1.record(ext)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    windows = sim.getNIteration() - it0
+    batched = mesh.ntets * NSPEC * windows / (ms * 1e-3)
+    del sim
+    # The same realizations with the plain path, one solver per realization (bounded sample).
+    sample = sizes[: args.plain_sample]
+    upd, plain_ms = 0, 0.0
+    for k, n in enumerate(sample):
+        m = W.cube_mesh(n)
+        rk = srng.create("r123", 512)
+        rk.initialize(SEED + k)
+        ps = TetOpSplit(mdl, m, rk)
+        for q, nm in enumerate(names):
+            ps.setCompReacK("comp", nm, base[q] * jit[k, q])
+        pr = W.poisson_counts(m.ntets, 50.0, SEED + k, nspec=NSPEC)
+        for i, s in enumerate(ps.spec_names):
+            ps.setSpecCounts(s, pr[i])
+        es = torch.cuda.ExternalStream(ps.getStream())
+        ps.run(args.warmup * STEP_SIM_S)
+        i0 = ps.getNIteration()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(es)
+        ps.run((args.warmup + args.steps) * STEP_SIM_S)
+        a1.record(es)
+        a1.synchronize()
+        plain_ms += a0.elapsed_time(a1)
+        upd += m.ntets * NSPEC * (ps.getNIteration() - i0)
+        del ps
+    plain = upd / (plain_ms * 1e-3)
+    print(json.dumps({
+        "metric": "tet-species updates/s", "value": batched, "unit": "tet-species updates/s",
+        "config": {"workload": f"batched: {nreal} realizations of n^3 Kuhn cubes, n in 8..30, "
+                               f"{mesh.ntets} tets, 8 species, 12 reactions, rate jitter 0.2",
+                   "sim_ms_per_step": 1.0, "steps": args.steps, "warmup": args.warmup},
+        "windows": windows, "ms": ms, "setup_s": setup_s,
+        "plain_sequential": {"value": plain, "realizations_sampled": len(sample), "ms": plain_ms},
+        "batched_over_plain": batched / plain,
+    }), flush=True)
+    return 0
+
+
+def run_efield(args):
+    """EField configuration: 20x20x200 Kuhn cubes (480,000 tets), every boundary triangle
+    membrane, Cm 1 uF/cm^2, leak 3e-5 S/cm^2 at -65 mV, a two-state voltage-gated channel
+    at 10/um^2 (alpha = 0.1 exp(V/25 mV)/ms, beta = 0.1 exp(-V/25 mV)/ms, 20 pS, +50 mV),
+    1 nA on the z = 0 face, EField dt 1 us; FP64 CG against FP32 CG + FP64 refinement."""
+    import math
+
+    from steps_b200 import geom as sgeom
+    from steps_b200 import model as smodel
+    from steps_b200 import rng as srng
+    from steps_b200.solver import EF_DV_CG_FP64, EF_DV_CG_MIXED, TetOpSplit
+
+    nx, ny, nz = args.ef_dims
+    mesh = sgeom.kuhn_box(nx, ny, nz, 1e-7)
+    cyto = sgeom.TmComp("cyto", mesh, np.arange(mesh.ntets))
+    cyto.addVolsys("vsys")
+    surf = mesh.getSurfTris()
+    patch = sgeom.TmPatch("memb", mesh, surf, cyto)
+    patch.addSurfsys("ssys")
+    sgeom.Memb("membrane", mesh, [patch])
+    mdl = smodel.Model()
+    smodel.Volsys("vsys", mdl)
+    ss = smodel.Surfsys("ssys", mdl)
+    ch = smodel.Chan("Na", mdl)
+    c = smodel.ChanState("C", mdl, ch)
+    o = smodel.ChanState("O", mdl, ch)
+    smodel.VDepSReac("open", ss, slhs=[c], srhs=[o], k=lambda v: 100.0 * math.exp(v / 0.025))
+    smodel.VDepSReac("close", ss, slhs=[o], srhs=[c], k=lambda v: 100.0 * math.exp(-v / 0.025))
+    smodel.OhmicCurr("I", ss, chanstate=o, g=20e-12, erev=0.05)
+    zmin = np.unique(mesh.tris[surf][np.all(mesh.verts[mesh.tris[surf]][:, :, 2] <= 1e-12, axis=1)])
+    out = {}
+    finals = {}
+    for name, method in (("fp64", EF_DV_CG_FP64), ("mixed", EF_DV_CG_MIXED)):
+        r = srng.create("r123", 512)
+        r.initialize(SEED)
+        sim = TetOpSplit(mdl, mesh, r, method)
+        sim.setEfieldTolerance(args.ef_tol, 1e-4)
+        sim.setEfieldDT(1e-6)
+        sim.setMembPotential("membrane", -0.065)
+        sim.setMembCapac("membrane", 0.01)
+        sim.setMembRes("membrane", 1.0 / 0.3, -0.065)
+        sim.setPatchSpecCount("memb", "C", 10.0 * patch.getArea() * 1e12)
+        for v in zmin:
+            sim.setVertIClamp(int(v), 1e-9 / len(zmin))
+        t_end = args.ef_steps * 1e-6
+        w0 = time.perf_counter()
+        sim.run(t_end)
+        wall = time.perf_counter() - w0
+        steps, iters, solve_ms, rr = sim.getEfieldStats()
+        finals[name] = np.array([sim.getVertV(v) for v in range(0, mesh.nverts, 97)])
+        out[name] = {"steps": steps, "cg_iterations_per_step": iters / max(steps, 1),
+                     "solve_ms_per_step": solve_ms / max(steps, 1), "wall_s": wall,
+                     "sim_ms_per_wall_s": t_end * 1e3 / wall}
+        del sim
+    err = float(np.max(np.abs(finals["mixed"] - finals["fp64"]) / np.abs(finals["fp64"])))
+    print(json.dumps({
+        "metric": "EField solve ms per step", "config": {"mesh": f"{nx}x{ny}x{nz} Kuhn cubes",
+                                                         "tets": mesh.ntets, "verts": mesh.nverts,
+                                                         "steps": args.ef_steps, "tol": args.ef_tol},
+        "fp64": out["fp64"], "mixed": out["mixed"],
+        "mixed_speedup_solve": out["fp64"]["solve_ms_per_step"] / out["mixed"]["solve_ms_per_step"],
+        "max_rel_v_diff_mixed_vs_fp64": err,
+    }), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["plain", "batched", "efield"], default="plain")
+    ap.add_argument("--nreal", type=int, default=512)
+    ap.add_argument("--plain-sample", type=int, default=64)
+    ap.add_argument("--ef-dims", type=int, nargs=3, default=[20, 20, 200])
+    ap.add_argument("--ef-steps", type=int, default=5000)
+    ap.add_argument("--ef-tol", type=float, default=1e-10)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "batched":
+        return run_batched(args)
+    if args.config == "efield":
+        return run_efield(args)
     return run_ours(args)
 
 

@@ -410,8 +410,32 @@ __global__ void residual_kernel(int n, int width, const int32_t* col, const doub
         rv[i] = ri;
         r32[i] = (float)ri;
         acc[0] += ri * ri;
+        acc[1] += bv[i] * bv[i];
     }
-    reduce_last<1>(acc, partials, counter, [&](double* tot) { scal[S_RR] = tot[0]; });
+    reduce_last<2>(acc, partials, counter, [&](double* tot) {
+        scal[S_RR] = tot[0];
+        scal[S_BB] = tot[1];
+    });
+}
+
+// Restart of FP64 CG from the residual r = b - A x0 of a warm start x0: z, p, r.z; the
+// tolerance stays relative to |b| (set by residual_kernel).
+__global__ void cg_restart_kernel(int n, const double* diag, const double* rv, double* zv, double* pv,
+                                  double* partials, unsigned int* counter, double* scal, double rel_tol) {
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double zi = rv[i] / diag[i];
+        zv[i] = zi;
+        pv[i] = zi;
+        acc[0] += rv[i] * zi;
+    }
+    reduce_last<1>(acc, partials, counter, [&](double* tot) {
+        scal[S_RZ] = tot[0];
+        scal[S_RZ0] = tot[0];
+        scal[S_TOL2] = rel_tol * rel_tol * scal[S_BB];
+        scal[S_ITER] = 0.0;
+        scal[S_DONE] = (scal[S_RR] <= scal[S_TOL2]) ? 1.0 : 0.0;
+    });
 }
 
 __global__ void add_correction_kernel(int n, double* xv, const float* d) {
@@ -509,7 +533,10 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
     const int chunk = 16;
     double h[10];
     if (method == EF_CG_FP64) {
-        cg_start_kernel<double><<<g, kBlock, 0, stream>>>(n, diag64, b, x, r, z, p, red, red_count, scal, tol);
+        // Warm start from the previous step's dV (x keeps it).
+        residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, red, red_count,
+                                                  scal);
+        cg_restart_kernel<<<g, kBlock, 0, stream>>>(n, diag64, r, z, p, red, red_count, scal, tol);
         for (int it = 0; it < max_iter; it += chunk) {
             for (int c = 0; c < chunk; ++c) {
                 spmv_dot_kernel<double><<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, p, q, red,
@@ -527,14 +554,14 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
         stats.last_rel_residual = h[S_BB] > 0.0 ? std::sqrt(h[S_RR] / h[S_BB]) : 0.0;
         if (h[S_BB] > 0.0 && h[S_RR] > h[S_TOL2]) throw DeviceErr("EField CG did not converge");
     } else {
-        // Mixed precision: FP32 CG on the correction, FP64 residuals and accumulation.
-        SG_CUDA(cudaMemsetAsync(x, 0, n * 8, stream));
+        // Mixed precision: FP32 CG on the correction, FP64 residuals and accumulation,
+        // warm-started from the previous step's dV.
         residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, red, red_count,
                                                   scal);
         SG_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream));
         SG_CUDA(cudaStreamSynchronize(stream));
-        const double bb = h[S_RR];
-        double rr = bb;
+        const double bb = h[S_BB];
+        double rr = h[S_RR];
         int outer = 0;
         while (bb > 0.0 && rr > tol * tol * bb && outer < 50) {
             // Inner FP32 solve of A d = r32: s32 is its residual, q32 = A p32.
