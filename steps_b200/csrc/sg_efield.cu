@@ -398,7 +398,7 @@ __global__ void cg_start_kernel(int n, const double* diag, const T* rhs, T* xv, 
 __global__ void residual_kernel(int n, int width, const int32_t* col, const double* a, const double* diag,
                                 const double* bv, const double* xv, double* rv, float* r32,
                                 double* partials, unsigned int* counter, double* scal) {
-    double acc[1] = {0.0};
+    double acc[2] = {0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = diag[i] * xv[i];
         for (int w = 0; w < width; ++w) {
