@@ -137,6 +137,14 @@ void EFieldSystem::release() {
     dfree(x32);
     dfree(s32);
     dfree(acol_dev);
+    dfree(d_agg);
+    dfree(d_einv64);
+    dfree(d_einv32);
+    dfree(d_c64);
+    dfree(d_y64);
+    dfree(d_c32);
+    dfree(d_y32);
+    nagg = 0;
     dfree(red);
     dfree(scal);
     dfree(red_count);
@@ -154,6 +162,7 @@ void EFieldSystem::setup(int nv, const double* verts_um, int ntet, const int32_t
     nverts = nv;
     ntris = nt;
     efield_couple(nv, verts_um, ntet, tets, nbr_ptr, nbr_idx, geo_cc);
+    this->verts_um.assign(verts_um, verts_um + (size_t)nv * 3);
     tri_verts.assign(tris, tris + (size_t)nt * 3);
     tri_area_um2.assign(nt, 0.0);
     vert_area_um2.assign(nv, 0.0);
@@ -332,30 +341,89 @@ __global__ void spmv_dot_kernel(int n, int width, const int32_t* col, const T* a
     });
 }
 
-// x += alpha p; r -= alpha q; z = r / diag; partial r.z and r.r; last block: beta, convergence.
+// x += alpha p; r -= alpha q; restriction c[agg] += r; partial r.r; last block: convergence.
 template <typename T>
-__global__ void update_kernel(int n, const double* diag, T* xv, T* rv, T* zv, const T* pv, const T* qv,
+__global__ void update_kernel(int n, T* xv, T* rv, const T* pv, const T* qv, const int32_t* agg, T* cvec,
                               double* partials, unsigned int* counter, double* scal, int max_iter) {
     if (scal[S_DONE] != 0.0) return;
     const T alpha = (T)scal[S_ALPHA];
-    double acc[2] = {0.0, 0.0};
+    double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         T xi = xv[i] + alpha * pv[i];
         T ri = rv[i] - alpha * qv[i];
-        T zi = ri / (T)diag[i];
         xv[i] = xi;
         rv[i] = ri;
-        zv[i] = zi;
-        acc[0] += (double)ri * (double)zi;
-        acc[1] += (double)ri * (double)ri;
+        if (agg[i] >= 0) atomicAdd(&cvec[agg[i]], ri);
+        acc[0] += (double)ri * (double)ri;
     }
-    reduce_last<2>(acc, partials, counter, [&](double* tot) {
-        double rz_old = scal[S_RZ];
-        scal[S_BETA] = (rz_old != 0.0) ? tot[0] / rz_old : 0.0;
-        scal[S_RZ] = tot[0];
-        scal[S_RR] = tot[1];
+    reduce_last<1>(acc, partials, counter, [&](double* tot) {
+        scal[S_RR] = tot[0];
         scal[S_ITER] += 1.0;
-        if (tot[1] <= scal[S_TOL2] || scal[S_ITER] >= (double)max_iter) scal[S_DONE] = 1.0;
+        if (tot[0] <= scal[S_TOL2] || scal[S_ITER] >= (double)max_iter) scal[S_DONE] = 1.0;
+    });
+}
+
+// Solve start from x = 0 with right-hand side rhs: r = rhs, restriction, r.r (= rhs.rhs).
+template <typename T>
+__global__ void init_kernel(int n, const T* rhs, T* xv, T* rv, const int32_t* agg, T* cvec, double* partials,
+                            unsigned int* counter, double* scal, double rel_tol) {
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        T ri = rhs[i];
+        xv[i] = (T)0;
+        rv[i] = ri;
+        if (agg[i] >= 0) atomicAdd(&cvec[agg[i]], ri);
+        acc[0] += (double)ri * (double)ri;
+    }
+    reduce_last<1>(acc, partials, counter, [&](double* tot) {
+        scal[S_RR] = tot[0];
+        scal[S_BB] = tot[0];
+        scal[S_TOL2] = rel_tol * rel_tol * tot[0];
+        scal[S_ITER] = 0.0;
+        scal[S_DONE] = (tot[0] <= 0.0) ? 1.0 : 0.0;
+    });
+}
+
+// Coarse solve y = E^-1 c (one warp per coarse row).
+template <typename T>
+__global__ void coarse_kernel(int nagg, const T* einv, const T* cvec, T* yv, const double* scal) {
+    if (scal[S_DONE] != 0.0) return;
+    const int lane = threadIdx.x & 31;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nagg;
+         row += (gridDim.x * blockDim.x) >> 5) {
+        T s = (T)0;
+        for (int k = lane; k < nagg; k += 32) s += einv[(size_t)row * nagg + k] * cvec[k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) yv[row] = s;
+    }
+}
+
+// z = r / diag + y[agg] (two-level preconditioner); zero c for the next restriction;
+// partial r.z; last block: beta = r.z / previous r.z (0 at the start of a solve).
+template <typename T>
+__global__ void precond_kernel(int n, int nagg, const double* diag, const T* rv, T* zv, T* pv, const int32_t* agg,
+                               const T* yv, T* cvec, double* partials, unsigned int* counter, double* scal,
+                               int start) {
+    if (scal[S_DONE] != 0.0 && !start) return;
+    if (blockIdx.x == 0)
+        for (int k = threadIdx.x; k < nagg; k += blockDim.x) cvec[k] = (T)0;
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        T zi = rv[i] / (T)diag[i];
+        if (agg[i] >= 0 && nagg > 0) zi += yv[agg[i]];
+        zv[i] = zi;
+        if (start) pv[i] = zi;  // first search direction
+        acc[0] += (double)rv[i] * (double)zi;
+    }
+    reduce_last<1>(acc, partials, counter, [&](double* tot) {
+        if (start) {
+            scal[S_BETA] = 0.0;
+            if (scal[S_RR] <= scal[S_TOL2]) scal[S_DONE] = 1.0;
+        } else {
+            double rz_old = scal[S_RZ];
+            scal[S_BETA] = (rz_old != 0.0) ? tot[0] / rz_old : 0.0;
+        }
+        scal[S_RZ] = tot[0];
     });
 }
 
@@ -368,36 +436,11 @@ __global__ void direction_kernel(int n, const T* zv, T* pv, const double* scal) 
         pv[i] = zv[i] + beta * pv[i];
 }
 
-// Start of a CG solve of A x = rhs from x = 0: r = rhs, z = r / diag, p = z; r.z, r.r.
-template <typename T>
-__global__ void cg_start_kernel(int n, const double* diag, const T* rhs, T* xv, T* rv, T* zv, T* pv,
-                                double* partials, unsigned int* counter, double* scal, double rel_tol) {
-    double acc[2] = {0.0, 0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        T ri = rhs[i];
-        T zi = ri / (T)diag[i];
-        xv[i] = (T)0;
-        rv[i] = ri;
-        zv[i] = zi;
-        pv[i] = zi;
-        acc[0] += (double)ri * (double)zi;
-        acc[1] += (double)ri * (double)ri;
-    }
-    reduce_last<2>(acc, partials, counter, [&](double* tot) {
-        scal[S_RZ] = tot[0];
-        scal[S_RZ0] = tot[0];
-        scal[S_RR] = tot[1];
-        scal[S_BB] = tot[1];
-        scal[S_TOL2] = rel_tol * rel_tol * tot[1];
-        scal[S_ITER] = 0.0;
-        scal[S_DONE] = (tot[1] <= 0.0) ? 1.0 : 0.0;
-    });
-}
-
-// FP64 residual of the refinement loop: r64 = b - A x64, r32 = (float) r64, partial r.r.
+// FP64 residual r64 = b - A x64 (warm starts and the refinement loop), r32 = (float) r64,
+// optional restriction into cvec; partial r.r and b.b.
 __global__ void residual_kernel(int n, int width, const int32_t* col, const double* a, const double* diag,
-                                const double* bv, const double* xv, double* rv, float* r32,
-                                double* partials, unsigned int* counter, double* scal) {
+                                const double* bv, const double* xv, double* rv, float* r32, const int32_t* agg,
+                                double* cvec, double* partials, unsigned int* counter, double* scal) {
     double acc[2] = {0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = diag[i] * xv[i];
@@ -409,6 +452,7 @@ __global__ void residual_kernel(int n, int width, const int32_t* col, const doub
         double ri = bv[i] - s;
         rv[i] = ri;
         r32[i] = (float)ri;
+        if (cvec && agg[i] >= 0) atomicAdd(&cvec[agg[i]], ri);
         acc[0] += ri * ri;
         acc[1] += bv[i] * bv[i];
     }
@@ -418,24 +462,11 @@ __global__ void residual_kernel(int n, int width, const int32_t* col, const doub
     });
 }
 
-// Restart of FP64 CG from the residual r = b - A x0 of a warm start x0: z, p, r.z; the
-// tolerance stays relative to |b| (set by residual_kernel).
-__global__ void cg_restart_kernel(int n, const double* diag, const double* rv, double* zv, double* pv,
-                                  double* partials, unsigned int* counter, double* scal, double rel_tol) {
-    double acc[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double zi = rv[i] / diag[i];
-        zv[i] = zi;
-        pv[i] = zi;
-        acc[0] += rv[i] * zi;
-    }
-    reduce_last<1>(acc, partials, counter, [&](double* tot) {
-        scal[S_RZ] = tot[0];
-        scal[S_RZ0] = tot[0];
-        scal[S_TOL2] = rel_tol * rel_tol * scal[S_BB];
-        scal[S_ITER] = 0.0;
-        scal[S_DONE] = (scal[S_RR] <= scal[S_TOL2]) ? 1.0 : 0.0;
-    });
+// Tolerance and counters of an FP64 solve warm-started by residual_kernel.
+__global__ void warm_start_kernel(double* scal, double rel_tol) {
+    scal[S_TOL2] = rel_tol * rel_tol * scal[S_BB];
+    scal[S_ITER] = 0.0;
+    scal[S_DONE] = (scal[S_BB] <= 0.0) ? 1.0 : 0.0;
 }
 
 __global__ void add_correction_kernel(int n, double* xv, const float* d) {
@@ -456,6 +487,79 @@ __global__ void tri_v_kernel(int nt, const int32_t* tv, const double* V, double*
 int grid_for(int n, int nsm) { return std::max(1, std::min((n + kBlock - 1) / kBlock, std::min(nsm * 8, 1024))); }
 
 }  // namespace
+
+// In-place inverse of a dense SPD matrix through its Cholesky factor (row-major n x n).
+static void spd_inverse(int n, std::vector<double>& E) {
+    std::vector<double> L((size_t)n * n, 0.0);
+    for (int j = 0; j < n; ++j) {
+        double s = E[(size_t)j * n + j];
+        for (int k = 0; k < j; ++k) s -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
+        if (!(s > 0.0)) throw DeviceErr("EField coarse matrix is not positive definite");
+        double d = std::sqrt(s);
+        L[(size_t)j * n + j] = d;
+        for (int i = j + 1; i < n; ++i) {
+            double t = E[(size_t)i * n + j];
+            const double* li = &L[(size_t)i * n];
+            const double* lj = &L[(size_t)j * n];
+            for (int k = 0; k < j; ++k) t -= li[k] * lj[k];
+            L[(size_t)i * n + j] = t / d;
+        }
+    }
+    // W = L^-1 (lower triangular), then E^-1 = W^T W.
+    std::vector<double> W((size_t)n * n, 0.0);
+    for (int j = 0; j < n; ++j) {
+        W[(size_t)j * n + j] = 1.0 / L[(size_t)j * n + j];
+        for (int i = j + 1; i < n; ++i) {
+            double t = 0.0;
+            for (int k = j; k < i; ++k) t -= L[(size_t)i * n + k] * W[(size_t)k * n + j];
+            W[(size_t)i * n + j] = t / L[(size_t)i * n + i];
+        }
+    }
+    for (int a = 0; a < n; ++a)
+        for (int b = a; b < n; ++b) {
+            double t = 0.0;
+            for (int k = b; k < n; ++k) t += W[(size_t)k * n + a] * W[(size_t)k * n + b];
+            E[(size_t)a * n + b] = t;
+            E[(size_t)b * n + a] = t;
+        }
+}
+
+// Aggregates: the bounding box cut into bins of about `target` vertices (bins per axis in
+// proportion to the box's extent); clamped vertices belong to none.  Returns the count.
+static int make_aggregates(int n, const std::vector<double>& X, const std::vector<uint8_t>& clamped, int target,
+                           std::vector<int32_t>& agg) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) {
+            lo[c] = std::min(lo[c], X[(size_t)i * 3 + c]);
+            hi[c] = std::max(hi[c], X[(size_t)i * 3 + c]);
+        }
+    double ext[3], vol = 1.0;
+    for (int c = 0; c < 3; ++c) {
+        ext[c] = std::max(hi[c] - lo[c], 1e-12);
+        vol *= ext[c];
+    }
+    double k = std::max(1.0, (double)n / target);
+    double s = std::cbrt(vol / k);
+    long nb[3];
+    for (int c = 0; c < 3; ++c) nb[c] = std::max(1L, (long)std::llround(ext[c] / s));
+    std::vector<long> lin(n);
+    for (int i = 0; i < n; ++i) {
+        long id[3];
+        for (int c = 0; c < 3; ++c)
+            id[c] = std::min(nb[c] - 1, (long)((X[(size_t)i * 3 + c] - lo[c]) / ext[c] * nb[c]));
+        lin[i] = id[0] + nb[0] * (id[1] + nb[1] * id[2]);
+    }
+    std::vector<long> keys;
+    for (int i = 0; i < n; ++i)
+        if (!clamped[i]) keys.push_back(lin[i]);
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    agg.assign(n, -1);
+    for (int i = 0; i < n; ++i)
+        if (!clamped[i]) agg[i] = (int32_t)(std::lower_bound(keys.begin(), keys.end(), lin[i]) - keys.begin());
+    return (int)keys.size();
+}
 
 void EFieldSystem::set_potential(double v_mV, cudaStream_t stream) {
     fill_kernel<<<grid_for(nverts, nsm), kBlock, 0, stream>>>(V, nverts, v_mV);
@@ -516,48 +620,104 @@ void EFieldSystem::build_matrix(double dt_ms, cudaStream_t stream) {
     if (ntris)
         SG_CUDA(cudaMemcpyAsync(d_tri_iclamp, tri_iclamp.data(), tri_iclamp.size() * 8, cudaMemcpyHostToDevice,
                                 stream));
+    // Coarse space of the two-level preconditioner: about 1000 aggregates (>= 16 vertices
+    // each), E = Z^T A Z over the unclamped system, inverted densely.
+    std::vector<int32_t> agg;
+    const int target = std::max(16, n / 1000);
+    const int na = make_aggregates(n, verts_um, vclamped, target, agg);
+    std::vector<double> E((size_t)na * na, 0.0);
+    for (int i = 0; i < n; ++i) {
+        if (agg[i] < 0) continue;
+        E[(size_t)agg[i] * na + agg[i]] += diag[i];
+        for (int w = 0; w < width; ++w) {
+            int j = acol[(size_t)w * n + i];
+            if (j < 0) break;
+            E[(size_t)agg[i] * na + agg[j]] += a64[(size_t)w * n + i];
+        }
+    }
+    if (na > 0) spd_inverse(na, E);
+    std::vector<float> E32(E.begin(), E.end());
+    if (na != nagg || !d_agg) {
+        dfree(d_einv64);
+        dfree(d_einv32);
+        dfree(d_c64);
+        dfree(d_y64);
+        dfree(d_c32);
+        dfree(d_y32);
+        size_t m = std::max(na, 1);
+        dalloc(d_einv64, m * m);
+        dalloc(d_einv32, m * m);
+        dalloc(d_c64, m);
+        dalloc(d_y64, m);
+        dalloc(d_c32, m);
+        dalloc(d_y32, m);
+        if (!d_agg) dalloc(d_agg, n);
+        nagg = na;
+    }
+    SG_CUDA(cudaMemcpyAsync(d_agg, agg.data(), agg.size() * 4, cudaMemcpyHostToDevice, stream));
+    if (na) {
+        SG_CUDA(cudaMemcpyAsync(d_einv64, E.data(), E.size() * 8, cudaMemcpyHostToDevice, stream));
+        SG_CUDA(cudaMemcpyAsync(d_einv32, E32.data(), E32.size() * 4, cudaMemcpyHostToDevice, stream));
+    }
     SG_CUDA(cudaStreamSynchronize(stream));  // host vectors above are temporaries
     dt_built = dt_ms;
     dirty = false;
 }
 
-// One EField step: RHS from the current V and currents, CG solve, V update.
+// Two-level PCG iterations from a started state (r, its restriction in c, and the
+// scalars S_RR, S_TOL2, S_ITER, S_DONE set): preconditioned start, then chunks of
+// {q = A p, alpha} -> {x, r, restriction} -> {coarse solve} -> {z, beta} -> {p} until the
+// device flag S_DONE is set; h receives the final scalars.
+template <typename T>
+void EFieldSystem::pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* qv,
+                            const T* einv, T* cvec, T* yv, double* h) {
+    const int gc = std::max(1, std::min((nagg * 32 + kBlock - 1) / kBlock, nsm * 4));
+    coarse_kernel<T><<<gc, kBlock, 0, stream>>>(nagg, einv, cvec, yv, scal);
+    precond_kernel<T><<<g, kBlock, 0, stream>>>(n, nagg, diag64, rv, zv, pv, d_agg, yv, cvec, red, red_count, scal, 1);
+    const int chunk = 8;
+    for (int it = 0; it < max_iter; it += chunk) {
+        for (int c = 0; c < chunk; ++c) {
+            spmv_dot_kernel<T><<<g, kBlock, 0, stream>>>(n, width, acol_dev, a, diag64, pv, qv, red, red_count, scal);
+            update_kernel<T><<<g, kBlock, 0, stream>>>(n, xv, rv, pv, qv, d_agg, cvec, red, red_count, scal, max_iter);
+            coarse_kernel<T><<<gc, kBlock, 0, stream>>>(nagg, einv, cvec, yv, scal);
+            precond_kernel<T><<<g, kBlock, 0, stream>>>(n, nagg, diag64, rv, zv, pv, d_agg, yv, cvec, red, red_count,
+                                                        scal, 0);
+            direction_kernel<T><<<g, kBlock, 0, stream>>>(n, zv, pv, scal);
+        }
+        SG_CUDA(cudaGetLastError());
+        SG_CUDA(cudaMemcpyAsync(h, scal, 10 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        SG_CUDA(cudaStreamSynchronize(stream));
+        if (h[S_DONE] != 0.0) break;
+    }
+}
+
+// One EField step: RHS from the current V and currents, CG solve, V update.  The matrix
+// is rebuilt when the step length changes by more than rounding (the truncated last step
+// of a run), or when clamps or membrane properties change.
 void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
-    if (dirty || dt_ms != dt_built) build_matrix(dt_ms, stream);
+    if (dirty || std::fabs(dt_ms - dt_built) > 1e-9 * dt_built) build_matrix(dt_ms, stream);
     const int n = nverts;
     const int g = grid_for(n, nsm);
     SG_CUDA(cudaEventRecord(ev0, stream));
     rhs_kernel<<<g, kBlock, 0, stream>>>(n, width, V, ell_col, ell_cc, cap_gext, v_leak, d_vert_iclamp, d_vt_ptr,
                                          d_vt_idx, tri_I, d_tri_iclamp, d_vclamped, b);
     SG_CUDA(cudaGetLastError());
-    const int chunk = 16;
     double h[10];
     if (method == EF_CG_FP64) {
-        // Warm start from the previous step's dV (x keeps it).
-        residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, red, red_count,
-                                                  scal);
-        cg_restart_kernel<<<g, kBlock, 0, stream>>>(n, diag64, r, z, p, red, red_count, scal, tol);
-        for (int it = 0; it < max_iter; it += chunk) {
-            for (int c = 0; c < chunk; ++c) {
-                spmv_dot_kernel<double><<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, p, q, red,
-                                                                   red_count, scal);
-                update_kernel<double><<<g, kBlock, 0, stream>>>(n, diag64, x, r, z, p, q, red, red_count, scal,
-                                                                max_iter);
-                direction_kernel<double><<<g, kBlock, 0, stream>>>(n, z, p, scal);
-            }
-            SG_CUDA(cudaGetLastError());
-            SG_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream));
-            SG_CUDA(cudaStreamSynchronize(stream));
-            if (h[S_DONE] != 0.0) break;
-        }
+        // Warm start from the previous step's dV (x keeps it): r = b - A x, restricted.
+        SG_CUDA(cudaMemsetAsync(d_c64, 0, std::max(nagg, 1) * 8, stream));
+        residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, d_agg, d_c64,
+                                                  red, red_count, scal);
+        warm_start_kernel<<<1, 1, 0, stream>>>(scal, tol);
+        pcg_loop<double>(stream, n, g, ell_a64, x, r, z, p, q, d_einv64, d_c64, d_y64, h);
         stats.iterations += (uint64_t)h[S_ITER];
         stats.last_rel_residual = h[S_BB] > 0.0 ? std::sqrt(h[S_RR] / h[S_BB]) : 0.0;
         if (h[S_BB] > 0.0 && h[S_RR] > h[S_TOL2]) throw DeviceErr("EField CG did not converge");
     } else {
-        // Mixed precision: FP32 CG on the correction, FP64 residuals and accumulation,
-        // warm-started from the previous step's dV.
-        residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, red, red_count,
-                                                  scal);
+        // Mixed precision: FP32 two-level PCG on the correction, FP64 residuals and
+        // accumulation, warm-started from the previous step's dV.
+        residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, d_agg, nullptr,
+                                                  red, red_count, scal);
         SG_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream));
         SG_CUDA(cudaStreamSynchronize(stream));
         const double bb = h[S_BB];
@@ -565,25 +725,14 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
         int outer = 0;
         while (bb > 0.0 && rr > tol * tol * bb && outer < 50) {
             // Inner FP32 solve of A d = r32: s32 is its residual, q32 = A p32.
-            cg_start_kernel<float><<<g, kBlock, 0, stream>>>(n, diag64, r32, x32, s32, z32, p32, red, red_count, scal,
-                                                             inner_tol);
-            for (int it = 0; it < max_iter; it += chunk) {
-                for (int c = 0; c < chunk; ++c) {
-                    spmv_dot_kernel<float><<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a32, diag64, p32, q32,
-                                                                     red, red_count, scal);
-                    update_kernel<float><<<g, kBlock, 0, stream>>>(n, diag64, x32, s32, z32, p32, q32, red,
-                                                                   red_count, scal, max_iter);
-                    direction_kernel<float><<<g, kBlock, 0, stream>>>(n, z32, p32, scal);
-                }
-                SG_CUDA(cudaGetLastError());
-                SG_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream));
-                SG_CUDA(cudaStreamSynchronize(stream));
-                if (h[S_DONE] != 0.0) break;
-            }
+            SG_CUDA(cudaMemsetAsync(d_c32, 0, std::max(nagg, 1) * 4, stream));
+            init_kernel<float><<<g, kBlock, 0, stream>>>(n, r32, x32, s32, d_agg, d_c32, red, red_count, scal,
+                                                         inner_tol);
+            pcg_loop<float>(stream, n, g, ell_a32, x32, s32, z32, p32, q32, d_einv32, d_c32, d_y32, h);
             stats.iterations += (uint64_t)h[S_ITER];
             add_correction_kernel<<<g, kBlock, 0, stream>>>(n, x, x32);
-            residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, red,
-                                                      red_count, scal);
+            residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, d_agg,
+                                                      nullptr, red, red_count, scal);
             SG_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream));
             SG_CUDA(cudaStreamSynchronize(stream));
             rr = h[S_RR];

@@ -65,6 +65,17 @@ struct EFieldSystem {
     double* diag64 = nullptr;             // A_ii
     double* cap_gext = nullptr;           // [2][nverts]: C_i (pF), g_i (nS)
     uint8_t* d_vclamped = nullptr;
+    // Two-level preconditioner M^-1 = D^-1 + Z E^-1 Z^T: Z aggregates vertices into spatial
+    // bins (piecewise-constant coarse space), E = Z^T A Z is inverted densely on the host.
+    std::vector<double> verts_um;         // [nverts][3] for the aggregation
+    int nagg = 0;
+    int32_t* d_agg = nullptr;             // [nverts] aggregate of each vertex, -1 for clamped
+    double* d_einv64 = nullptr;           // [nagg][nagg]
+    float* d_einv32 = nullptr;
+    double* d_c64 = nullptr;              // restricted residual [nagg]
+    double* d_y64 = nullptr;              // coarse correction [nagg]
+    float* d_c32 = nullptr;
+    float* d_y32 = nullptr;
     int32_t* acol_dev = nullptr;          // [width][nverts] matrix columns (clamped ones removed)
     double inner_tol = 1.0e-4;            // relative residual of each FP32 inner solve
     double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
@@ -87,6 +98,9 @@ struct EFieldSystem {
     // One EField step of dt_ms with tri_I already set on the device.
     void advance(double dt_ms, cudaStream_t stream);
     void release();
+    template <typename T>
+    void pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* qv, const T* einv,
+                  T* cvec, T* yv, double* h);
 };
 
 // Geometric coupling of a tet mesh: for every edge ij, sum over tets of the linear-FEM
