@@ -139,7 +139,8 @@ int sg_get_tri_ohmic_i(sg_solver* h, int32_t tri, double* amps);  /* getTriOhmic
 
 /* Membrane mesh: all mesh vertices (m, [nverts][3]), every tet's 4 vertices (tets of a
  * compartment conduct; efield.cpp:48-112 initMesh), and the membrane triangles' vertices.
- * method: 0 = FP64 Jacobi-PCG, 1 = FP32 PCG inside FP64 residual refinement.  Replaces
+ * method: 0 = FP64 PCG, 1 = FP32 PCG inside FP64 residual refinement; both precondition
+ * with Jacobi plus a dense coarse solve on spatial vertex aggregates.  Replaces
  * TetOpSplitP::_setupEField (TOS:1092-1279); switches run() to the EField loop (TOS:1851). */
 int sg_set_efield_mesh(sg_solver* h, int32_t nverts, const double* verts, const int32_t* tet_verts,
                        int32_t ntris, const int32_t* tri_verts, int32_t method);
@@ -161,6 +162,12 @@ int sg_get_efield_stats(sg_solver* h, uint64_t* steps, uint64_t* iterations, dou
                         double* last_rel_residual);
 
 /* ---- device options (no reference counterpart) ------------------------------ */
+
+/* Mixed-precision EField accuracy check: after each mixed step also solve the same system
+ * in FP64 from zero to rel_tol (not counted in the solve time) and record the largest
+ * per-vertex |V_mixed - V_fp64| / |V_fp64|; read it with sg_get_efield_check. */
+int sg_set_efield_check(sg_solver* h, int32_t on, double rel_tol);
+int sg_get_efield_check(sg_solver* h, uint64_t* steps, double* max_rel, double* last_rel);
 
 /* Window-kernel launch shape: block in {64,128,256}; grid 0 = occupancy-sized. */
 int sg_set_launch(sg_solver* h, int32_t block, int32_t grid);

@@ -101,6 +101,8 @@ PROTOTYPES = {
     "sg_set_vert_v_clamped": [_P, _i32, _i32],
     "sg_set_vert_iclamp": [_P, _i32, _f64],
     "sg_get_efield_stats": [_P, _pu64, _pu64, _pf64, _pf64],
+    "sg_set_efield_check": [_P, _i32, _f64],
+    "sg_get_efield_check": [_P, _pu64, _pf64, _pf64],
     "sg_get_stream": [_P, C.POINTER(_P)],
     "sg_set_profiling": [_P, _i32],
     "sg_get_profile": [_P, _pf64, _pu64, _pu64],

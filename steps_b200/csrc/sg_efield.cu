@@ -136,8 +136,13 @@ void EFieldSystem::release() {
     dfree(q32);
     dfree(x32);
     dfree(s32);
+    dfree(xchk);
     dfree(acol_dev);
     dfree(d_agg);
+    dfree(d_seg_ptr);
+    dfree(d_seg_idx);
+    dfree(d_seg_agg);
+    nseg = 0;
     dfree(d_einv64);
     dfree(d_einv32);
     dfree(d_c64);
@@ -150,7 +155,9 @@ void EFieldSystem::release() {
     dfree(red_count);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
-    ev0 = ev1 = nullptr;
+    if (evc0) cudaEventDestroy(evc0);
+    if (evc1) cudaEventDestroy(evc1);
+    ev0 = ev1 = evc0 = evc1 = nullptr;
 }
 
 EFieldSystem::~EFieldSystem() { release(); }
@@ -250,7 +257,7 @@ namespace {
 
 constexpr int kBlock = 256;
 // Device scalar slots.
-enum { S_RZ = 0, S_PQ, S_ALPHA, S_BETA, S_RR, S_BB, S_DONE, S_ITER, S_TOL2, S_RZ0 };
+enum { S_RZ = 0, S_PQ, S_ALPHA, S_BETA, S_RR, S_BB, S_DONE, S_ITER, S_TOL2, S_RZ0, S_CHK };
 
 __global__ void fill_kernel(double* v, int n, double x) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = x;
@@ -308,12 +315,29 @@ __device__ void reduce_last(double (&v)[NV], double* partials, unsigned int* cou
     }
     __syncthreads();
     if (!last) return;
+    // The whole last block sums the block partials: thread t takes blocks t, t + kBlock, ...
+    // in order, then a fixed shuffle tree and the warps in order (deterministic).
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (int blk = threadIdx.x; blk < (int)gridDim.x; blk += kBlock)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[(size_t)blk * NV + k]);
+    __syncthreads();  // sh is reused below
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = acc[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[k][wid] = x;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
         double tot[NV];
-        for (int k = 0; k < NV; ++k) tot[k] = 0.0;
-        for (int blk = 0; blk < (int)gridDim.x; ++blk)
-            for (int k = 0; k < NV; ++k) tot[k] += __ldcg(&partials[(size_t)blk * NV + k]);
+        for (int k = 0; k < NV; ++k) {
+            tot[k] = 0.0;
+            for (int w = 0; w < kBlock / 32; ++w) tot[k] += sh[k][w];
+        }
         *counter = 0u;
         fin(tot);
     }
@@ -341,20 +365,44 @@ __global__ void spmv_dot_kernel(int n, int width, const int32_t* col, const T* a
     });
 }
 
-// x += alpha p; r -= alpha q; restriction c[agg] += r; partial r.r; last block: convergence.
+// Vertex segments: segment sg lists the vertices seg_idx[seg_ptr[sg] .. seg_ptr[sg + 1]) of
+// aggregate seg_agg[sg] in ascending order (-1: vertices in no aggregate).  One warp walks
+// a segment and writes its restriction c[agg] = sum of r with a fixed shuffle tree, so the
+// coarse right-hand side is the same in every run (no floating-point atomics).
+struct Segs {
+    int n;
+    const int32_t* ptr;
+    const int32_t* idx;
+    const int32_t* agg;
+};
+
 template <typename T>
-__global__ void update_kernel(int n, T* xv, T* rv, const T* pv, const T* qv, const int32_t* agg, T* cvec,
-                              double* partials, unsigned int* counter, double* scal, int max_iter) {
+__device__ __forceinline__ void seg_store(const Segs& sg, int k, T c, T* cvec) {
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    const int ag = sg.agg[k];
+    if ((threadIdx.x & 31) == 0 && ag >= 0 && cvec) cvec[ag] = c;
+}
+
+// x += alpha p; r -= alpha q; restriction c = Z^T r; partial r.r; last block: convergence.
+template <typename T>
+__global__ void update_kernel(Segs sg, T* xv, T* rv, const T* pv, const T* qv, T* cvec, double* partials,
+                              unsigned int* counter, double* scal, int max_iter) {
     if (scal[S_DONE] != 0.0) return;
     const T alpha = (T)scal[S_ALPHA];
+    const int lane = threadIdx.x & 31;
     double acc[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        T xi = xv[i] + alpha * pv[i];
-        T ri = rv[i] - alpha * qv[i];
-        xv[i] = xi;
-        rv[i] = ri;
-        if (agg[i] >= 0) atomicAdd(&cvec[agg[i]], ri);
-        acc[0] += (double)ri * (double)ri;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < sg.n; k += (gridDim.x * blockDim.x) >> 5) {
+        T c = (T)0;
+        for (int m = sg.ptr[k] + lane; m < sg.ptr[k + 1]; m += 32) {
+            const int i = sg.idx[m];
+            T xi = xv[i] + alpha * pv[i];
+            T ri = rv[i] - alpha * qv[i];
+            xv[i] = xi;
+            rv[i] = ri;
+            c += ri;
+            acc[0] += (double)ri * (double)ri;
+        }
+        seg_store(sg, k, c, cvec);
     }
     reduce_last<1>(acc, partials, counter, [&](double* tot) {
         scal[S_RR] = tot[0];
@@ -365,15 +413,21 @@ __global__ void update_kernel(int n, T* xv, T* rv, const T* pv, const T* qv, con
 
 // Solve start from x = 0 with right-hand side rhs: r = rhs, restriction, r.r (= rhs.rhs).
 template <typename T>
-__global__ void init_kernel(int n, const T* rhs, T* xv, T* rv, const int32_t* agg, T* cvec, double* partials,
-                            unsigned int* counter, double* scal, double rel_tol) {
+__global__ void init_kernel(Segs sg, const T* rhs, T* xv, T* rv, T* cvec, double* partials, unsigned int* counter,
+                            double* scal, double rel_tol) {
+    const int lane = threadIdx.x & 31;
     double acc[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        T ri = rhs[i];
-        xv[i] = (T)0;
-        rv[i] = ri;
-        if (agg[i] >= 0) atomicAdd(&cvec[agg[i]], ri);
-        acc[0] += (double)ri * (double)ri;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < sg.n; k += (gridDim.x * blockDim.x) >> 5) {
+        T c = (T)0;
+        for (int m = sg.ptr[k] + lane; m < sg.ptr[k + 1]; m += 32) {
+            const int i = sg.idx[m];
+            T ri = rhs[i];
+            xv[i] = (T)0;
+            rv[i] = ri;
+            c += ri;
+            acc[0] += (double)ri * (double)ri;
+        }
+        seg_store(sg, k, c, cvec);
     }
     reduce_last<1>(acc, partials, counter, [&](double* tot) {
         scal[S_RR] = tot[0];
@@ -398,15 +452,11 @@ __global__ void coarse_kernel(int nagg, const T* einv, const T* cvec, T* yv, con
     }
 }
 
-// z = r / diag + y[agg] (two-level preconditioner); zero c for the next restriction;
-// partial r.z; last block: beta = r.z / previous r.z (0 at the start of a solve).
+// z = r / diag + y[agg] (two-level preconditioner); partial r.z; last block: beta = r.z / previous r.z (0 at the start of a solve).
 template <typename T>
 __global__ void precond_kernel(int n, int nagg, const double* diag, const T* rv, T* zv, T* pv, const int32_t* agg,
-                               const T* yv, T* cvec, double* partials, unsigned int* counter, double* scal,
-                               int start) {
+                               const T* yv, double* partials, unsigned int* counter, double* scal, int start) {
     if (scal[S_DONE] != 0.0 && !start) return;
-    if (blockIdx.x == 0)
-        for (int k = threadIdx.x; k < nagg; k += blockDim.x) cvec[k] = (T)0;
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         T zi = rv[i] / (T)diag[i];
@@ -439,22 +489,28 @@ __global__ void direction_kernel(int n, const T* zv, T* pv, const double* scal) 
 // FP64 residual r64 = b - A x64 (warm starts and the refinement loop), r32 = (float) r64,
 // optional restriction into cvec; partial r.r and b.b.
 __global__ void residual_kernel(int n, int width, const int32_t* col, const double* a, const double* diag,
-                                const double* bv, const double* xv, double* rv, float* r32, const int32_t* agg,
-                                double* cvec, double* partials, unsigned int* counter, double* scal) {
+                                const double* bv, const double* xv, double* rv, float* r32, Segs sg, double* cvec,
+                                double* partials, unsigned int* counter, double* scal) {
+    const int lane = threadIdx.x & 31;
     double acc[2] = {0.0, 0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double s = diag[i] * xv[i];
-        for (int w = 0; w < width; ++w) {
-            int j = col[(size_t)w * n + i];
-            if (j < 0) break;
-            s += a[(size_t)w * n + i] * xv[j];
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < sg.n; k += (gridDim.x * blockDim.x) >> 5) {
+        double c = 0.0;
+        for (int m = sg.ptr[k] + lane; m < sg.ptr[k + 1]; m += 32) {
+            const int i = sg.idx[m];
+            double s = diag[i] * xv[i];
+            for (int w = 0; w < width; ++w) {
+                int j = col[(size_t)w * n + i];
+                if (j < 0) break;
+                s += a[(size_t)w * n + i] * xv[j];
+            }
+            double ri = bv[i] - s;
+            rv[i] = ri;
+            r32[i] = (float)ri;
+            c += ri;
+            acc[0] += ri * ri;
+            acc[1] += bv[i] * bv[i];
         }
-        double ri = bv[i] - s;
-        rv[i] = ri;
-        r32[i] = (float)ri;
-        if (cvec && agg[i] >= 0) atomicAdd(&cvec[agg[i]], ri);
-        acc[0] += ri * ri;
-        acc[1] += bv[i] * bv[i];
+        seg_store(sg, k, c, cvec);
     }
     reduce_last<2>(acc, partials, counter, [&](double* tot) {
         scal[S_RR] = tot[0];
@@ -471,6 +527,27 @@ __global__ void warm_start_kernel(double* scal, double rel_tol) {
 
 __global__ void add_correction_kernel(int n, double* xv, const float* d) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) xv[i] += (double)d[i];
+}
+
+// Check of a mixed-precision step: max over unclamped vertices of |dV - dV64| / |V + dV64|
+// into scal[S_CHK] (non-negative doubles order like their bit patterns, so the max is an
+// integer atomic and independent of thread order).
+__global__ void check_kernel(int n, const double* V, const double* dv, const double* dv64, const uint8_t* clamped,
+                             double* scal) {
+    double m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (clamped[i]) continue;
+        double ref = fabs(V[i] + dv64[i]);
+        double e = fabs(dv[i] - dv64[i]);
+        double rel = ref > 0.0 ? e / ref : e;
+        m = rel > m ? rel : m;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        double y = __shfl_down_sync(0xffffffffu, m, o);
+        m = y > m ? y : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long*>(&scal[S_CHK]), (unsigned long long)__double_as_longlong(m));
 }
 
 // V += dV on unclamped vertices; then triangle potentials (mean of the 3 vertices).
@@ -655,6 +732,45 @@ void EFieldSystem::build_matrix(double dt_ms, cudaStream_t stream) {
         nagg = na;
     }
     SG_CUDA(cudaMemcpyAsync(d_agg, agg.data(), agg.size() * 4, cudaMemcpyHostToDevice, stream));
+    // Segments: each aggregate's vertices in ascending order, then the vertices of no
+    // aggregate (clamped) in chunks of 256.
+    std::vector<int32_t> sptr(1, 0), sidx, sagg;
+    {
+        std::vector<int32_t> cnt(na + 1, 0);
+        for (int i = 0; i < n; ++i)
+            if (agg[i] >= 0) cnt[agg[i] + 1]++;
+        for (int a = 0; a < na; ++a) cnt[a + 1] += cnt[a];
+        sidx.assign(n, 0);
+        std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
+        int nfree = 0;
+        for (int i = 0; i < n; ++i)
+            if (agg[i] >= 0) sidx[fill[agg[i]]++] = i;
+        for (int a = 0; a < na; ++a) {
+            sptr.push_back(cnt[a + 1]);
+            sagg.push_back(a);
+        }
+        int pos = cnt[na];
+        for (int i = 0; i < n; ++i)
+            if (agg[i] < 0) {
+                sidx[pos++] = i;
+                if (++nfree == 256) {
+                    sptr.push_back(pos);
+                    sagg.push_back(-1);
+                    nfree = 0;
+                }
+            }
+        if (nfree) {
+            sptr.push_back(pos);
+            sagg.push_back(-1);
+        }
+    }
+    nseg = (int)sagg.size();
+    dalloc(d_seg_ptr, sptr.size());
+    dalloc(d_seg_idx, std::max<size_t>(sidx.size(), 1));
+    dalloc(d_seg_agg, std::max<size_t>(sagg.size(), 1));
+    SG_CUDA(cudaMemcpyAsync(d_seg_ptr, sptr.data(), sptr.size() * 4, cudaMemcpyHostToDevice, stream));
+    SG_CUDA(cudaMemcpyAsync(d_seg_idx, sidx.data(), sidx.size() * 4, cudaMemcpyHostToDevice, stream));
+    if (nseg) SG_CUDA(cudaMemcpyAsync(d_seg_agg, sagg.data(), sagg.size() * 4, cudaMemcpyHostToDevice, stream));
     if (na) {
         SG_CUDA(cudaMemcpyAsync(d_einv64, E.data(), E.size() * 8, cudaMemcpyHostToDevice, stream));
         SG_CUDA(cudaMemcpyAsync(d_einv32, E32.data(), E32.size() * 4, cudaMemcpyHostToDevice, stream));
@@ -672,16 +788,18 @@ template <typename T>
 void EFieldSystem::pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* qv,
                             const T* einv, T* cvec, T* yv, double* h) {
     const int gc = std::max(1, std::min((nagg * 32 + kBlock - 1) / kBlock, nsm * 4));
+    const Segs sg{nseg, d_seg_ptr, d_seg_idx, d_seg_agg};
+    const int gs = seg_grid();
     coarse_kernel<T><<<gc, kBlock, 0, stream>>>(nagg, einv, cvec, yv, scal);
-    precond_kernel<T><<<g, kBlock, 0, stream>>>(n, nagg, diag64, rv, zv, pv, d_agg, yv, cvec, red, red_count, scal, 1);
+    precond_kernel<T><<<g, kBlock, 0, stream>>>(n, nagg, diag64, rv, zv, pv, d_agg, yv, red, red_count, scal, 1);
     const int chunk = 8;
     for (int it = 0; it < max_iter; it += chunk) {
         for (int c = 0; c < chunk; ++c) {
             spmv_dot_kernel<T><<<g, kBlock, 0, stream>>>(n, width, acol_dev, a, diag64, pv, qv, red, red_count, scal);
-            update_kernel<T><<<g, kBlock, 0, stream>>>(n, xv, rv, pv, qv, d_agg, cvec, red, red_count, scal, max_iter);
+            update_kernel<T><<<gs, kBlock, 0, stream>>>(sg, xv, rv, pv, qv, cvec, red, red_count, scal, max_iter);
             coarse_kernel<T><<<gc, kBlock, 0, stream>>>(nagg, einv, cvec, yv, scal);
-            precond_kernel<T><<<g, kBlock, 0, stream>>>(n, nagg, diag64, rv, zv, pv, d_agg, yv, cvec, red, red_count,
-                                                        scal, 0);
+            precond_kernel<T><<<g, kBlock, 0, stream>>>(n, nagg, diag64, rv, zv, pv, d_agg, yv, red, red_count, scal,
+                                                        0);
             direction_kernel<T><<<g, kBlock, 0, stream>>>(n, zv, pv, scal);
         }
         SG_CUDA(cudaGetLastError());
@@ -698,16 +816,18 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
     if (dirty || std::fabs(dt_ms - dt_built) > 1e-9 * dt_built) build_matrix(dt_ms, stream);
     const int n = nverts;
     const int g = grid_for(n, nsm);
+    const Segs sg{nseg, d_seg_ptr, d_seg_idx, d_seg_agg};
+    const int gs = seg_grid();
     SG_CUDA(cudaEventRecord(ev0, stream));
     rhs_kernel<<<g, kBlock, 0, stream>>>(n, width, V, ell_col, ell_cc, cap_gext, v_leak, d_vert_iclamp, d_vt_ptr,
                                          d_vt_idx, tri_I, d_tri_iclamp, d_vclamped, b);
     SG_CUDA(cudaGetLastError());
     double h[10];
+    double check_ms = 0.0;
     if (method == EF_CG_FP64) {
         // Warm start from the previous step's dV (x keeps it): r = b - A x, restricted.
-        SG_CUDA(cudaMemsetAsync(d_c64, 0, std::max(nagg, 1) * 8, stream));
-        residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, d_agg, d_c64,
-                                                  red, red_count, scal);
+        residual_kernel<<<gs, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, sg, d_c64, red,
+                                                   red_count, scal);
         warm_start_kernel<<<1, 1, 0, stream>>>(scal, tol);
         pcg_loop<double>(stream, n, g, ell_a64, x, r, z, p, q, d_einv64, d_c64, d_y64, h);
         stats.iterations += (uint64_t)h[S_ITER];
@@ -716,8 +836,8 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
     } else {
         // Mixed precision: FP32 two-level PCG on the correction, FP64 residuals and
         // accumulation, warm-started from the previous step's dV.
-        residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, d_agg, nullptr,
-                                                  red, red_count, scal);
+        residual_kernel<<<gs, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, sg, nullptr,
+                                                   red, red_count, scal);
         SG_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream));
         SG_CUDA(cudaStreamSynchronize(stream));
         const double bb = h[S_BB];
@@ -725,14 +845,12 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
         int outer = 0;
         while (bb > 0.0 && rr > tol * tol * bb && outer < 50) {
             // Inner FP32 solve of A d = r32: s32 is its residual, q32 = A p32.
-            SG_CUDA(cudaMemsetAsync(d_c32, 0, std::max(nagg, 1) * 4, stream));
-            init_kernel<float><<<g, kBlock, 0, stream>>>(n, r32, x32, s32, d_agg, d_c32, red, red_count, scal,
-                                                         inner_tol);
+            init_kernel<float><<<gs, kBlock, 0, stream>>>(sg, r32, x32, s32, d_c32, red, red_count, scal, inner_tol);
             pcg_loop<float>(stream, n, g, ell_a32, x32, s32, z32, p32, q32, d_einv32, d_c32, d_y32, h);
             stats.iterations += (uint64_t)h[S_ITER];
             add_correction_kernel<<<g, kBlock, 0, stream>>>(n, x, x32);
-            residual_kernel<<<g, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, d_agg,
-                                                      nullptr, red, red_count, scal);
+            residual_kernel<<<gs, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, sg, nullptr,
+                                                       red, red_count, scal);
             SG_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream));
             SG_CUDA(cudaStreamSynchronize(stream));
             rr = h[S_RR];
@@ -741,6 +859,29 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
         }
         stats.last_rel_residual = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
         if (bb > 0.0 && rr > tol * tol * bb) throw DeviceErr("EField refinement did not converge");
+        if (check) {
+            // FP64 solve of the same system from zero, then the per-vertex comparison.
+            if (!xchk) dalloc(xchk, n);
+            if (!evc0) {
+                SG_CUDA(cudaEventCreate(&evc0));
+                SG_CUDA(cudaEventCreate(&evc1));
+            }
+            SG_CUDA(cudaEventRecord(evc0, stream));
+            init_kernel<double><<<gs, kBlock, 0, stream>>>(sg, b, xchk, r, d_c64, red, red_count, scal, check_tol);
+            pcg_loop<double>(stream, n, g, ell_a64, xchk, r, z, p, q, d_einv64, d_c64, d_y64, h);
+            SG_CUDA(cudaMemsetAsync(scal + S_CHK, 0, sizeof(double), stream));
+            check_kernel<<<g, kBlock, 0, stream>>>(n, V, x, xchk, d_vclamped, scal);
+            double e = 0.0;
+            SG_CUDA(cudaMemcpyAsync(&e, scal + S_CHK, sizeof(double), cudaMemcpyDeviceToHost, stream));
+            SG_CUDA(cudaEventRecord(evc1, stream));
+            SG_CUDA(cudaEventSynchronize(evc1));
+            float cms = 0.0f;
+            SG_CUDA(cudaEventElapsedTime(&cms, evc0, evc1));
+            check_ms = cms;
+            stats.check_steps += 1;
+            stats.check_last_rel = e;
+            stats.check_max_rel = std::max(stats.check_max_rel, e);
+        }
     }
     apply_kernel<<<g, kBlock, 0, stream>>>(n, V, x, d_vclamped);
     if (ntris) tri_v_kernel<<<grid_for(ntris, nsm), kBlock, 0, stream>>>(ntris, d_tri_verts, V, tri_V);
@@ -749,7 +890,7 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
     SG_CUDA(cudaEventSynchronize(ev1));
     float ms = 0.0f;
     SG_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-    stats.solve_ms += ms;
+    stats.solve_ms += ms - check_ms;  // the check solve is not part of the step's cost
     stats.steps += 1;
 }
 

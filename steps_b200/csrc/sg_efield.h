@@ -7,12 +7,14 @@
 // Each EField step assembles the backward-Euler system of dVsolver.hpp:126-180,
 //     A_ii = C_i/dt + g_i + sum_j cc_ij,   A_ij = -cc_ij,
 //     b_i  = I_i + g_i (V_ext - V_i) + sum_j cc_ij (V_j - V_i),
-// solves A dV = b with Jacobi-preconditioned CG (FP64, or FP32 CG inside an FP64
-// residual-refinement loop) and updates V += dV on unclamped vertices.  Clamped rows
+// solves A dV = b with CG preconditioned by Jacobi plus a coarse solve on spatial vertex
+// aggregates (FP64, or FP32 CG inside an FP64 residual-refinement loop), warm-started
+// from the previous step's dV, and updates V += dV on unclamped vertices.  Clamped rows
 // are identity rows with b = 0, so their columns drop out and A stays SPD.
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <vector>
 
@@ -26,6 +28,10 @@ struct EFieldStats {
     uint64_t refinements = 0;       // FP64 residual evaluations
     double last_rel_residual = 0.0;
     double solve_ms = 0.0;          // device time of the solves (CUDA events)
+    // Per-step check of the mixed solve against an FP64 solve of the same system.
+    uint64_t check_steps = 0;
+    double check_max_rel = 0.0;     // max over steps and vertices of |V_mixed - V_fp64| / |V_fp64|
+    double check_last_rel = 0.0;
 };
 
 struct EFieldSystem {
@@ -70,6 +76,12 @@ struct EFieldSystem {
     std::vector<double> verts_um;         // [nverts][3] for the aggregation
     int nagg = 0;
     int32_t* d_agg = nullptr;             // [nverts] aggregate of each vertex, -1 for clamped
+    // Vertex segments for the restriction Z^T r: one per aggregate (its vertices in
+    // ascending order), then chunks of the vertices in no aggregate.
+    int nseg = 0;
+    int32_t* d_seg_ptr = nullptr;         // [nseg + 1]
+    int32_t* d_seg_idx = nullptr;         // [nverts]
+    int32_t* d_seg_agg = nullptr;         // [nseg], -1 = no aggregate
     double* d_einv64 = nullptr;           // [nagg][nagg]
     float* d_einv32 = nullptr;
     double* d_c64 = nullptr;              // restricted residual [nagg]
@@ -78,6 +90,9 @@ struct EFieldSystem {
     float* d_y32 = nullptr;
     int32_t* acol_dev = nullptr;          // [width][nverts] matrix columns (clamped ones removed)
     double inner_tol = 1.0e-4;            // relative residual of each FP32 inner solve
+    bool check = false;                   // mixed method: also solve in FP64 and compare
+    double check_tol = 1.0e-12;           // relative residual of the FP64 check solve
+    double* xchk = nullptr;               // [nverts] dV of the FP64 check solve
     double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
     float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr, *x32 = nullptr, *s32 = nullptr;
     double* red = nullptr;                // reduction partials
@@ -85,7 +100,7 @@ struct EFieldSystem {
     unsigned int* red_count = nullptr;
     double dt_built = -1.0;
     bool dirty = true;                    // clamps / membrane properties changed
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc0 = nullptr, evc1 = nullptr;
     EFieldStats stats;
     int nsm = 148;
 
@@ -98,6 +113,9 @@ struct EFieldSystem {
     // One EField step of dt_ms with tri_I already set on the device.
     void advance(double dt_ms, cudaStream_t stream);
     void release();
+    // Grid of the warp-per-segment kernels: 8 segments per block, at most 1024 blocks (the
+    // reduction partials hold 2 x 1024 values); warps stride over the rest.
+    int seg_grid() const { return nseg > 0 ? std::min((nseg + 7) / 8, 1024) : 1; }
     template <typename T>
     void pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* qv, const T* einv,
                   T* cvec, T* yv, double* h);

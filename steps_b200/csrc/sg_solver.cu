@@ -1707,6 +1707,26 @@ int sg_get_efield_stats(sg_solver* h, uint64_t* steps, uint64_t* iterations, dou
     });
 }
 
+int sg_set_efield_check(sg_solver* h, int32_t on, double rel_tol) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        if (on && !(rel_tol > 0.0)) throw sg::ArgErr("bad check tolerance");
+        s->ef.check = on != 0;
+        if (on) s->ef.check_tol = rel_tol;
+    });
+}
+
+int sg_get_efield_check(sg_solver* h, uint64_t* steps, double* max_rel, double* last_rel) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        if (steps) *steps = s->ef.stats.check_steps;
+        if (max_rel) *max_rel = s->ef.stats.check_max_rel;
+        if (last_rel) *last_rel = s->ef.stats.check_last_rel;
+    });
+}
+
 int sg_get_stream(sg_solver* h, void** stream) {
     return guarded([&] {
         need(stream, "stream");

@@ -519,6 +519,17 @@ class TetOpSplit:
         check(self._L.sg_get_efield_stats(self._h, C.byref(s), C.byref(it), C.byref(ms), C.byref(rr)))
         return s.value, it.value, ms.value, rr.value
 
+    def setEfieldCheck(self, on, rel_tol=1e-12):
+        """Mixed-precision EField: after every step also solve the same system in FP64 (not
+        timed) and record the largest per-vertex relative voltage difference."""
+        check(self._L.sg_set_efield_check(self._h, 1 if on else 0, float(rel_tol)))
+
+    def getEfieldCheck(self):
+        """(checked steps, max over steps of max_v |V_mixed - V_fp64| / |V_fp64|, last step's)."""
+        s, mx, last = C.c_uint64(), C.c_double(), C.c_double()
+        check(self._L.sg_get_efield_check(self._h, C.byref(s), C.byref(mx), C.byref(last)))
+        return s.value, mx.value, last.value
+
     # --------------------------------------------------------- device knobs
     def setLaunch(self, block, grid=0):
         check(self._L.sg_set_launch(self._h, int(block), int(grid)))

@@ -116,3 +116,33 @@ def test_rallpack1_membres(steps_lib, method):
     steps, iters, ms, rr = sim.getEfieldStats()
     assert steps == 25000
     assert rms0 < 1.0e-3 and rmsx < 1.0e-3, (rms0, rmsx, iters / steps)
+
+
+def test_mixed_step_check_against_fp64(steps_lib):
+    """The mixed method's per-step check: every step's V from the FP32-inner solve is within
+    1e-6 relative of an FP64 solve of the same system; an FP64-method solver refuses nothing
+    and records no check steps."""
+    mesh = sgeom.kuhn_box(6, 6, 30, 1e-7)
+    sgeom.TmComp("cyto", mesh, np.arange(mesh.ntets))
+    surf = mesh.getSurfTris()
+    patch = sgeom.TmPatch("memb", mesh, surf, mesh.comps["cyto"])
+    sgeom.Memb("membrane", mesh, [patch])
+    mdl = smodel.Model()
+    smodel.Volsys("vsys", mdl)
+    sim = TetOpSplit(mdl, mesh, make_rng(4), EF_DV_CG_MIXED)
+    sim.setEfieldTolerance(1e-10, 1e-4)
+    sim.setEfieldCheck(True, 1e-12)
+    sim.setEfieldDT(1e-6)
+    sim.setMembPotential("membrane", -0.065)
+    sim.setMembCapac("membrane", 0.01)
+    sim.setMembRes("membrane", 1.0 / 0.3, -0.065)
+    zmin = np.unique(mesh.tris[surf][np.all(mesh.verts[mesh.tris[surf]][:, :, 2] <= 1e-12, axis=1)])
+    for v in zmin:
+        sim.setVertIClamp(int(v), 1e-10 / len(zmin))
+    sim.run(50e-6)
+    n, mx, last = sim.getEfieldCheck()
+    assert n == 50
+    assert 0.0 < mx < 1e-6, mx
+    assert last <= mx
+    v = np.array([sim.getVertV(i) for i in range(mesh.nverts)])
+    assert np.ptp(v) > 1e-6  # the injection moved V
