@@ -86,6 +86,12 @@ int sg_get_niteration(sg_solver* h, uint64_t* n); /* TetOpSplitP::getNIteration 
 int sg_get_reac_extent(sg_solver* h, int32_t reac, uint64_t* n); /* getReacExtent TOS:8302 */
 int sg_get_diff_extent(sg_solver* h, uint64_t* n);               /* getDiffExtent TOS:8314 */
 int sg_set_diff_apply_threshold(sg_solver* h, int32_t threshold); /* TOS:8296 */
+/* API::checkpoint / API::restore (TOS:217-451): the complete simulation state (counts,
+ * time and window indices, constants, clamps, extents, membrane and EField state) in this
+ * library's own binary format.  restore needs a solver built from the same mesh and
+ * model; the continuation is identical to the uninterrupted run. */
+int sg_checkpoint(sg_solver* h, const char* file_name);
+int sg_restore(sg_solver* h, const char* file_name);
 
 /* ---- counts (api.hpp:2324-2325, 2582-2583) --------------------------------- */
 
@@ -168,9 +174,21 @@ int sg_get_efield_stats(sg_solver* h, uint64_t* steps, uint64_t* iterations, dou
  * per-vertex |V_mixed - V_fp64| / |V_fp64|; read it with sg_get_efield_check. */
 int sg_set_efield_check(sg_solver* h, int32_t on, double rel_tol);
 int sg_get_efield_check(sg_solver* h, uint64_t* steps, double* max_rel, double* last_rel);
+/* EField solve form: 1 = every CG iteration inside one cooperative launch (grid barriers
+ * between the phases), 0 = three kernel launches per iteration. */
+int sg_set_efield_persistent(sg_solver* h, int32_t on);
 
-/* Window-kernel launch shape: block in {64,128,256}; grid 0 = occupancy-sized. */
+/* Window-kernel launch shape: block in {64,128,256}; grid > 0 blocks, 0 = occupancy-sized
+ * (blocks stride over the tets), -1 = one tet per thread. */
 int sg_set_launch(sg_solver* h, int32_t block, int32_t grid);
+int sg_get_launch(sg_solver* h, int32_t* block, int32_t* grid);
+/* Autotune the launch shape at the next run() with more than 13 windows: after one
+ * untimed window, 12 windows are timed two each under block {64,128,256} x grid
+ * {occupancy-sized (0), one tet per thread (-1)}, and the fastest shape is kept (the
+ * sample path does not depend on the shape).  The six timings (ms, in that order) are read
+ * back with sg_get_autotune_ms. */
+int sg_set_autotune(sg_solver* h, int32_t on);
+int sg_get_autotune_ms(sg_solver* h, float* ms, int32_t cap, int32_t* count);
 /* Replay window launches from a captured CUDA graph of 16 windows (on by default). */
 int sg_set_graphs(sg_solver* h, int32_t on);
 /* Per-window bit-exact molecule-conservation check (on by default). */

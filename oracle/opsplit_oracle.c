@@ -145,13 +145,14 @@ static uint32_t or_binv(or_stream* st, uint32_t n, double p) {
     double r = or_powu(q, n);
     double u = u_co(or_u32(st));
     uint32_t x = 0;
-    while (u >= r && x < n) {
+    /* Unbounded search, clamped: the factor turns negative from x = n + 2. */
+    while (u >= r) {
         u = u - r;
         x += 1;
-        r = r * (a * (1.0 / (double)x) - s);
+        r = r * fma(a, 1.0 / (double)x, -s);
         if (!(r > 0.0)) break;
     }
-    return x;
+    return x < n ? x : n;
 }
 
 static double or_fc(uint32_t k) {
@@ -481,11 +482,13 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
     const int S = s->nspec;
     const int c = s->tcomp[t];
     uint32_t cnt[OR_MAXS];
-    double occ[OR_MAXS], last[OR_MAXS];
+    /* Occupancy (tet.cpp:318-340 keeps the running integral and the last update time):
+     * the integral of a count over [0, T) is c_end T - sum_k (change_k) t_k, so tdel keeps
+     * sum_k (change_k) t_k. */
+    double tdel[OR_MAXS];
     for (int i = 0; i < S; ++i) {
         cnt[i] = s->counts[(size_t)i * s->ntets + t];
-        occ[i] = 0.0;
-        last[i] = 0.0;
+        tdel[i] = 0.0;
     }
     const uint32_t clampm = s->clamp[t];
     or_stream st;
@@ -529,8 +532,7 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
             for (int i = 0; i < S; ++i) {
                 int32_t d = s->reac[sel].upd[i];
                 if (d == 0 || ((clampm >> i) & 1u)) continue;
-                occ[i] = occ[i] + (double)cnt[i] * (tt - last[i]);
-                last[i] = tt;
+                tdel[i] = tdel[i] + (double)d * tt;
                 cnt[i] = (uint32_t)((int64_t)cnt[i] + d);
             }
 #pragma omp atomic
@@ -553,8 +555,8 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
         double t1 = T * (D * G);
         if (t1 >= 1.0) t1 = 1.0;
         uint32_t mean_n = pop;
-        if (occ[i] != 0.0 || last[i] != 0.0) {
-            double nbar = (occ[i] + (double)pop * (T - last[i])) / T;
+        if (tdel[i] != 0.0) {
+            double nbar = (double)pop - tdel[i] * (1.0 / T);
             if (nbar > (double)pop) nbar = (double)pop;
             double nint = floor(nbar);
             double frc = nbar - nint;

@@ -74,7 +74,12 @@ PROTOTYPES = {
     "sg_set_reac_k": [_P, _i32, _i32, _f64],
     "sg_get_reac_k": [_P, _i32, _i32, _pf64],
     "sg_set_diff_d": [_P, _i32, _i32, _i32, _f64],
+    "sg_checkpoint": [_P, C.c_char_p],
+    "sg_restore": [_P, C.c_char_p],
     "sg_set_launch": [_P, _i32, _i32],
+    "sg_get_launch": [_P, _pi32, _pi32],
+    "sg_set_autotune": [_P, _i32],
+    "sg_get_autotune_ms": [_P, C.POINTER(C.c_float), _i32, _pi32],
     "sg_set_conservation_check": [_P, _i32],
     "sg_set_graphs": [_P, _i32],
     "sg_get_status": [_P, _pu32],
@@ -102,6 +107,7 @@ PROTOTYPES = {
     "sg_set_vert_iclamp": [_P, _i32, _f64],
     "sg_get_efield_stats": [_P, _pu64, _pu64, _pf64, _pf64],
     "sg_set_efield_check": [_P, _i32, _f64],
+    "sg_set_efield_persistent": [_P, _i32],
     "sg_get_efield_check": [_P, _pu64, _pf64, _pf64],
     "sg_get_stream": [_P, C.POINTER(_P)],
     "sg_set_profiling": [_P, _i32],

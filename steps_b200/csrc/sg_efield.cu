@@ -129,10 +129,12 @@ void EFieldSystem::release() {
     dfree(r);
     dfree(z);
     dfree(p);
+    dfree(p2);
     dfree(q);
     dfree(r32);
     dfree(z32);
     dfree(p32);
+    dfree(p2_32);
     dfree(q32);
     dfree(x32);
     dfree(s32);
@@ -146,13 +148,12 @@ void EFieldSystem::release() {
     dfree(d_einv64);
     dfree(d_einv32);
     dfree(d_c64);
-    dfree(d_y64);
     dfree(d_c32);
-    dfree(d_y32);
     nagg = 0;
     dfree(red);
     dfree(scal);
     dfree(red_count);
+    dfree(d_bar);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evc0) cudaEventDestroy(evc0);
@@ -226,16 +227,19 @@ void EFieldSystem::setup(int nv, const double* verts_um, int ntet, const int32_t
     dalloc(r, nv);
     dalloc(z, nv);
     dalloc(p, nv);
+    dalloc(p2, nv);
     dalloc(q, nv);
     dalloc(r32, nv);
     dalloc(z32, nv);
     dalloc(p32, nv);
+    dalloc(p2_32, nv);
     dalloc(q32, nv);
     dalloc(x32, nv);
     dalloc(s32, nv);
     dalloc(red, 4096);
     dalloc(scal, 32);
     dalloc(red_count, 4);
+    dalloc(d_bar, 4);
     if (nt) SG_CUDA(cudaMemcpyAsync(d_tri_verts, tris, (size_t)nt * 3 * 4, cudaMemcpyHostToDevice, stream));
     SG_CUDA(cudaMemcpyAsync(d_vt_ptr, vt_ptr.data(), vt_ptr.size() * 4, cudaMemcpyHostToDevice, stream));
     if (nt) SG_CUDA(cudaMemcpyAsync(d_vt_idx, vt_idx.data(), vt_idx.size() * 4, cudaMemcpyHostToDevice, stream));
@@ -343,21 +347,28 @@ __device__ void reduce_last(double (&v)[NV], double* partials, unsigned int* cou
     }
 }
 
-// q = A p (A = diag + off-diagonal ELL), partial p.q; last block: alpha = rz / pq.
+// Direction and product in one pass: p' = z + beta p (computed for the row and for every
+// neighbour it reads, so no separate direction kernel), q = A p' with A = diag + ELL,
+// partial p'.q; last block: alpha = rz / pq.  p' goes to pout (p is double-buffered).
 template <typename T>
-__global__ void spmv_dot_kernel(int n, int width, const int32_t* col, const T* a, const double* diag, const T* pv,
-                                T* qv, double* partials, unsigned int* counter, double* scal) {
+__global__ void spmv_kernel(int n, int width, const int32_t* col, const T* a, const double* diag, const T* zv,
+                            const T* pin, T* pout, T* qv, double* partials, unsigned int* counter, double* scal) {
     if (scal[S_DONE] != 0.0) return;
+    const T beta = (T)scal[S_BETA];
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        T s = (T)diag[i] * pv[i];
+        const T pi = zv[i] + beta * pin[i];
+        T s = (T)diag[i] * pi;
+        // Padding (-1) is skipped per entry rather than ending the loop, so the unrolled
+        // column and neighbour loads are all in flight together.
+#pragma unroll 4
         for (int w = 0; w < width; ++w) {
-            int j = col[(size_t)w * n + i];
-            if (j < 0) break;
-            s += a[(size_t)w * n + i] * pv[j];
+            const int j = col[(size_t)w * n + i];
+            if (j >= 0) s += a[(size_t)w * n + i] * (zv[j] + beta * pin[j]);
         }
+        pout[i] = pi;
         qv[i] = s;
-        acc[0] += (double)pv[i] * (double)s;
+        acc[0] += (double)pi * (double)s;
     }
     reduce_last<1>(acc, partials, counter, [&](double* tot) {
         scal[S_PQ] = tot[0];
@@ -438,32 +449,35 @@ __global__ void init_kernel(Segs sg, const T* rhs, T* xv, T* rv, T* cvec, double
     });
 }
 
-// Coarse solve y = E^-1 c (one warp per coarse row).
+// Two-level preconditioner, one warp per vertex segment: the warp of aggregate a forms
+// y_a = (E^-1 c)_a (row a of the dense coarse inverse times the restricted residual) and
+// sets z = r / diag + y_a on the aggregate's vertices; vertices in no aggregate get
+// z = r / diag.  Partial r.z; last block: beta = r.z / previous r.z (0 at the start of a
+// solve, where p = z is also written as the first direction).
 template <typename T>
-__global__ void coarse_kernel(int nagg, const T* einv, const T* cvec, T* yv, const double* scal) {
-    if (scal[S_DONE] != 0.0) return;
-    const int lane = threadIdx.x & 31;
-    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nagg;
-         row += (gridDim.x * blockDim.x) >> 5) {
-        T s = (T)0;
-        for (int k = lane; k < nagg; k += 32) s += einv[(size_t)row * nagg + k] * cvec[k];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) yv[row] = s;
-    }
-}
-
-// z = r / diag + y[agg] (two-level preconditioner); partial r.z; last block: beta = r.z / previous r.z (0 at the start of a solve).
-template <typename T>
-__global__ void precond_kernel(int n, int nagg, const double* diag, const T* rv, T* zv, T* pv, const int32_t* agg,
-                               const T* yv, double* partials, unsigned int* counter, double* scal, int start) {
+__global__ void precond_kernel(Segs sg, int nagg, const double* diag, const T* rv, T* zv, T* pv, const T* einv,
+                               const T* cvec, double* partials, unsigned int* counter, double* scal, int start) {
     if (scal[S_DONE] != 0.0 && !start) return;
+    const int lane = threadIdx.x & 31;
     double acc[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        T zi = rv[i] / (T)diag[i];
-        if (agg[i] >= 0 && nagg > 0) zi += yv[agg[i]];
-        zv[i] = zi;
-        if (start) pv[i] = zi;  // first search direction
-        acc[0] += (double)rv[i] * (double)zi;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < sg.n; k += (gridDim.x * blockDim.x) >> 5) {
+        const int ag = sg.agg[k];
+        T y = (T)0;
+        if (ag >= 0) {
+            const T* row = einv + (size_t)ag * nagg;
+#pragma unroll 4
+            for (int j = lane; j < nagg; j += 32) y += row[j] * cvec[j];
+            for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
+            y = __shfl_sync(0xffffffffu, y, 0);
+        }
+        for (int m = sg.ptr[k] + lane; m < sg.ptr[k + 1]; m += 32) {
+            const int i = sg.idx[m];
+            const T ri = rv[i];
+            const T zi = ri / (T)diag[i] + y;
+            zv[i] = zi;
+            if (start) pv[i] = zi;
+            acc[0] += (double)ri * (double)zi;
+        }
     }
     reduce_last<1>(acc, partials, counter, [&](double* tot) {
         if (start) {
@@ -477,13 +491,195 @@ __global__ void precond_kernel(int n, int nagg, const double* diag, const T* rv,
     });
 }
 
-// p = z + beta p
+// ---------------------------------------------------------------------------
+// The whole PCG solve in one cooperative launch (all blocks co-resident): the three
+// phases of an iteration are separated by grid barriers instead of kernel boundaries,
+// and each scalar (p.q, r.r, r.z) is reduced by every block from the same block
+// partials in the same order, so all blocks take identical decisions without a second
+// barrier.  Vectors written by other blocks inside the launch are read with __ldcg (L2),
+// never from a stale L1 line.  The barrier waits are bounded: a block that waits longer
+// than kSpinLimit polls sets bar[2] and every block leaves at its next barrier.
+// ---------------------------------------------------------------------------
+constexpr unsigned int kSpinLimit = 1u << 22;  // x ~100 ns polls: about half a second
+
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, unsigned int& gen) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int g = gen;
+        if (atomicAdd(&bar[0], 1u) == nblocks - 1u) {
+            bar[0] = 0u;  // nobody arrives at the next barrier before the release below
+            __threadfence();
+            atomicExch(&bar[1], g + 1u);
+        } else {
+            unsigned int spins = 0;
+            while (*(volatile unsigned int*)&bar[1] == g) {
+                if (++spins > kSpinLimit) {
+                    atomicOr(&bar[2], 1u);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    gen += 1u;
+    return *(volatile unsigned int*)&bar[2] == 0u;
+}
+
+// Block partial of v -> partials[blockIdx]; barrier; the sum over all blocks in block
+// order (thread-strided, fixed shuffle tree, warps in order), the same in every block.
+__device__ __forceinline__ bool grid_sum(double v, double* partials, unsigned int* bar, unsigned int& gen,
+                                         double* out) {
+    __shared__ double sh[kBlock / 32];
+    __shared__ double tot;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) s += sh[w];
+        partials[blockIdx.x] = s;
+    }
+    if (!grid_barrier(bar, gridDim.x, gen)) return false;
+    double a = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += kBlock) a += __ldcg(&partials[b]);
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0) sh[wid] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) s += sh[w];
+        tot = s;
+    }
+    __syncthreads();
+    *out = tot;
+    __syncthreads();  // sh and tot are reused by the next call
+    return true;
+}
+
 template <typename T>
-__global__ void direction_kernel(int n, const T* zv, T* pv, const double* scal) {
-    if (scal[S_DONE] != 0.0) return;
-    const T beta = (T)scal[S_BETA];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        pv[i] = zv[i] + beta * pv[i];
+struct PcgArgs {
+    int n, width, nagg, max_iter;
+    const int32_t* col;
+    const T* a;
+    const double* diag;
+    const T* einv;
+    Segs sg;
+    T *x, *r, *z, *p, *p2, *q, *c;
+    double* partials;  // [3][gridDim]
+    double* scal;
+    unsigned int* bar;  // count, generation, error
+};
+
+// Two-level PCG from a started state (r and its restriction c set, scal[S_RR], scal[S_TOL2]
+// set).  The same arithmetic as the multi-kernel loop: z = r / d + y, p' = z + beta p,
+// q = A p', x += alpha p', r -= alpha q.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) pcg_persistent_kernel(PcgArgs<T> P) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    const unsigned int G = gridDim.x;
+    unsigned int gen = *(volatile unsigned int*)&P.bar[1];
+    double* part0 = P.partials;
+    double* part1 = P.partials + G;
+    double* part2 = P.partials + 2 * G;
+    const double tol2 = __ldcg(&P.scal[S_TOL2]);
+    double rr = __ldcg(&P.scal[S_RR]);
+    double rz = 0.0, beta = 0.0;
+    int iter = 0;
+    bool ok = true;
+
+    // Phase C at the start: z = M^-1 r, p = z, r.z.
+    auto precond = [&](bool start) -> double {
+        double acc = 0.0;
+        for (int k = gw; k < P.sg.n; k += nw) {
+            const int ag = __ldg(&P.sg.agg[k]);
+            T y = (T)0;
+            if (ag >= 0) {
+                const T* row = P.einv + (size_t)ag * P.nagg;
+#pragma unroll 4
+                for (int j = lane; j < P.nagg; j += 32) y += __ldg(&row[j]) * __ldcg(&P.c[j]);
+                for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
+                y = __shfl_sync(0xffffffffu, y, 0);
+            }
+            const int m1 = __ldg(&P.sg.ptr[k + 1]);
+            for (int m = __ldg(&P.sg.ptr[k]) + lane; m < m1; m += 32) {
+                const int i = __ldg(&P.sg.idx[m]);
+                const T ri = __ldcg(&P.r[i]);
+                const T zi = ri / (T)__ldg(&P.diag[i]) + y;
+                P.z[i] = zi;
+                if (start) P.p[i] = zi;
+                acc += (double)ri * (double)zi;
+            }
+        }
+        return acc;
+    };
+
+    if (rr > tol2) {
+        double v = precond(true);
+        ok = grid_sum(v, part0, P.bar, gen, &rz);
+        T* pin = P.p;
+        T* pout = P.p2;
+        while (ok) {
+            // Phase A: p' = z + beta p, q = A p', p'.q.
+            const T bt = (T)beta;
+            double acc = 0.0;
+            for (int i = gt; i < P.n; i += nt) {
+                const T pi = __ldcg(&P.z[i]) + bt * __ldcg(&pin[i]);
+                T s = (T)__ldg(&P.diag[i]) * pi;
+#pragma unroll 4
+                for (int w = 0; w < P.width; ++w) {
+                    const int j = __ldg(&P.col[(size_t)w * P.n + i]);
+                    if (j >= 0) s += __ldg(&P.a[(size_t)w * P.n + i]) * (__ldcg(&P.z[j]) + bt * __ldcg(&pin[j]));
+                }
+                pout[i] = pi;
+                P.q[i] = s;
+                acc += (double)pi * (double)s;
+            }
+            double pq = 0.0;
+            if (!(ok = grid_sum(acc, part1, P.bar, gen, &pq))) break;
+            const T alpha = (T)((pq != 0.0) ? rz / pq : 0.0);
+            // Phase B: x += alpha p', r -= alpha q, restriction c, r.r.
+            acc = 0.0;
+            for (int k = gw; k < P.sg.n; k += nw) {
+                T cs = (T)0;
+                const int m1 = __ldg(&P.sg.ptr[k + 1]);
+                for (int m = __ldg(&P.sg.ptr[k]) + lane; m < m1; m += 32) {
+                    const int i = __ldg(&P.sg.idx[m]);
+                    const T xi = __ldcg(&P.x[i]) + alpha * __ldcg(&pout[i]);
+                    const T ri = __ldcg(&P.r[i]) - alpha * __ldcg(&P.q[i]);
+                    P.x[i] = xi;
+                    P.r[i] = ri;
+                    cs += ri;
+                    acc += (double)ri * (double)ri;
+                }
+                for (int o = 16; o > 0; o >>= 1) cs += __shfl_down_sync(0xffffffffu, cs, o);
+                const int ag = __ldg(&P.sg.agg[k]);
+                if (lane == 0 && ag >= 0) P.c[ag] = cs;
+            }
+            if (!(ok = grid_sum(acc, part2, P.bar, gen, &rr))) break;
+            ++iter;
+            if (rr <= tol2 || iter >= P.max_iter) break;
+            // Phase C: z = M^-1 r, r.z, beta.
+            double rzn = 0.0;
+            if (!(ok = grid_sum(precond(false), part0, P.bar, gen, &rzn))) break;
+            beta = (rz != 0.0) ? rzn / rz : 0.0;
+            rz = rzn;
+            T* tp = pin;
+            pin = pout;
+            pout = tp;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.scal[S_RR] = rr;
+        P.scal[S_ITER] = (double)iter;
+        P.scal[S_RZ] = rz;
+        P.scal[S_DONE] = 1.0;
+    }
 }
 
 // FP64 residual r64 = b - A x64 (warm starts and the refinement loop), r32 = (float) r64,
@@ -498,10 +694,10 @@ __global__ void residual_kernel(int n, int width, const int32_t* col, const doub
         for (int m = sg.ptr[k] + lane; m < sg.ptr[k + 1]; m += 32) {
             const int i = sg.idx[m];
             double s = diag[i] * xv[i];
+#pragma unroll 4
             for (int w = 0; w < width; ++w) {
-                int j = col[(size_t)w * n + i];
-                if (j < 0) break;
-                s += a[(size_t)w * n + i] * xv[j];
+                const int j = col[(size_t)w * n + i];
+                if (j >= 0) s += a[(size_t)w * n + i] * xv[j];
             }
             double ri = bv[i] - s;
             rv[i] = ri;
@@ -718,16 +914,12 @@ void EFieldSystem::build_matrix(double dt_ms, cudaStream_t stream) {
         dfree(d_einv64);
         dfree(d_einv32);
         dfree(d_c64);
-        dfree(d_y64);
         dfree(d_c32);
-        dfree(d_y32);
         size_t m = std::max(na, 1);
         dalloc(d_einv64, m * m);
         dalloc(d_einv32, m * m);
         dalloc(d_c64, m);
-        dalloc(d_y64, m);
         dalloc(d_c32, m);
-        dalloc(d_y32, m);
         if (!d_agg) dalloc(d_agg, n);
         nagg = na;
     }
@@ -781,32 +973,80 @@ void EFieldSystem::build_matrix(double dt_ms, cudaStream_t stream) {
 }
 
 // Two-level PCG iterations from a started state (r, its restriction in c, and the
-// scalars S_RR, S_TOL2, S_ITER, S_DONE set): preconditioned start, then chunks of
-// {q = A p, alpha} -> {x, r, restriction} -> {coarse solve} -> {z, beta} -> {p} until the
-// device flag S_DONE is set; h receives the final scalars.
+// scalars S_RR, S_TOL2, S_ITER, S_DONE set): preconditioned start, then chunks of three
+// kernels per iteration, {p = z + beta p, q = A p, alpha} -> {x, r, restriction c} ->
+// {coarse solve, z, beta}, until the device flag S_DONE is set; h receives the final
+// scalars.  pv and pv2 alternate as the direction buffer.
 template <typename T>
-void EFieldSystem::pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* qv,
-                            const T* einv, T* cvec, T* yv, double* h) {
-    const int gc = std::max(1, std::min((nagg * 32 + kBlock - 1) / kBlock, nsm * 4));
+void EFieldSystem::pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* pv2,
+                            T* qv, const T* einv, T* cvec, double* h) {
     const Segs sg{nseg, d_seg_ptr, d_seg_idx, d_seg_agg};
     const int gs = seg_grid();
-    coarse_kernel<T><<<gc, kBlock, 0, stream>>>(nagg, einv, cvec, yv, scal);
-    precond_kernel<T><<<g, kBlock, 0, stream>>>(n, nagg, diag64, rv, zv, pv, d_agg, yv, red, red_count, scal, 1);
+    precond_kernel<T><<<gs, kBlock, 0, stream>>>(sg, nagg, diag64, rv, zv, pv, einv, cvec, red, red_count, scal, 1);
+    T* pin = pv;
+    T* pout = pv2;
     const int chunk = 8;
     for (int it = 0; it < max_iter; it += chunk) {
         for (int c = 0; c < chunk; ++c) {
-            spmv_dot_kernel<T><<<g, kBlock, 0, stream>>>(n, width, acol_dev, a, diag64, pv, qv, red, red_count, scal);
-            update_kernel<T><<<gs, kBlock, 0, stream>>>(sg, xv, rv, pv, qv, cvec, red, red_count, scal, max_iter);
-            coarse_kernel<T><<<gc, kBlock, 0, stream>>>(nagg, einv, cvec, yv, scal);
-            precond_kernel<T><<<g, kBlock, 0, stream>>>(n, nagg, diag64, rv, zv, pv, d_agg, yv, red, red_count, scal,
-                                                        0);
-            direction_kernel<T><<<g, kBlock, 0, stream>>>(n, zv, pv, scal);
+            spmv_kernel<T><<<g, kBlock, 0, stream>>>(n, width, acol_dev, a, diag64, zv, pin, pout, qv, red, red_count,
+                                                     scal);
+            update_kernel<T><<<gs, kBlock, 0, stream>>>(sg, xv, rv, pout, qv, cvec, red, red_count, scal, max_iter);
+            precond_kernel<T><<<gs, kBlock, 0, stream>>>(sg, nagg, diag64, rv, zv, nullptr, einv, cvec, red,
+                                                         red_count, scal, 0);
+            std::swap(pin, pout);
         }
         SG_CUDA(cudaGetLastError());
         SG_CUDA(cudaMemcpyAsync(h, scal, 10 * sizeof(double), cudaMemcpyDeviceToHost, stream));
         SG_CUDA(cudaStreamSynchronize(stream));
         if (h[S_DONE] != 0.0) break;
     }
+}
+
+// The persistent form of pcg_loop: one cooperative launch runs every iteration.
+template <typename T>
+void EFieldSystem::pcg_persistent(cudaStream_t stream, int n, const T* a, T* xv, T* rv, T* zv, T* pv, T* pv2,
+                                  T* qv, const T* einv, T* cvec, double* h) {
+    int per_sm = 0;
+    SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_persistent_kernel<T>, kBlock, 0));
+    const int want = std::max((n + kBlock - 1) / kBlock, (nseg + 7) / 8);
+    const int G = std::max(1, std::min(std::min(want, std::max(per_sm, 1) * nsm), 1024));
+    PcgArgs<T> P;
+    P.n = n;
+    P.width = width;
+    P.nagg = nagg;
+    P.max_iter = max_iter;
+    P.col = acol_dev;
+    P.a = a;
+    P.diag = diag64;
+    P.einv = einv;
+    P.sg = Segs{nseg, d_seg_ptr, d_seg_idx, d_seg_agg};
+    P.x = xv;
+    P.r = rv;
+    P.z = zv;
+    P.p = pv;
+    P.p2 = pv2;
+    P.q = qv;
+    P.c = cvec;
+    P.partials = red;
+    P.scal = scal;
+    P.bar = d_bar;
+    SG_CUDA(cudaMemsetAsync(d_bar, 0, 4 * sizeof(unsigned int), stream));
+    void* args[] = {&P};
+    SG_CUDA(cudaLaunchCooperativeKernel((const void*)pcg_persistent_kernel<T>, dim3(G), dim3(kBlock), args, 0, stream));
+    unsigned int err = 0;
+    SG_CUDA(cudaMemcpyAsync(h, scal, 10 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SG_CUDA(cudaMemcpyAsync(&err, d_bar + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
+    SG_CUDA(cudaStreamSynchronize(stream));
+    if (err) throw DeviceErr("EField solve: a grid barrier wait timed out");
+}
+
+template <typename T>
+void EFieldSystem::pcg(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* pv2, T* qv,
+                       const T* einv, T* cvec, double* h) {
+    if (persistent)
+        pcg_persistent<T>(stream, n, a, xv, rv, zv, pv, pv2, qv, einv, cvec, h);
+    else
+        pcg_loop<T>(stream, n, g, a, xv, rv, zv, pv, pv2, qv, einv, cvec, h);
 }
 
 // One EField step: RHS from the current V and currents, CG solve, V update.  The matrix
@@ -829,7 +1069,7 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
         residual_kernel<<<gs, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, sg, d_c64, red,
                                                    red_count, scal);
         warm_start_kernel<<<1, 1, 0, stream>>>(scal, tol);
-        pcg_loop<double>(stream, n, g, ell_a64, x, r, z, p, q, d_einv64, d_c64, d_y64, h);
+        pcg<double>(stream, n, g, ell_a64, x, r, z, p, p2, q, d_einv64, d_c64, h);
         stats.iterations += (uint64_t)h[S_ITER];
         stats.last_rel_residual = h[S_BB] > 0.0 ? std::sqrt(h[S_RR] / h[S_BB]) : 0.0;
         if (h[S_BB] > 0.0 && h[S_RR] > h[S_TOL2]) throw DeviceErr("EField CG did not converge");
@@ -846,7 +1086,7 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
         while (bb > 0.0 && rr > tol * tol * bb && outer < 50) {
             // Inner FP32 solve of A d = r32: s32 is its residual, q32 = A p32.
             init_kernel<float><<<gs, kBlock, 0, stream>>>(sg, r32, x32, s32, d_c32, red, red_count, scal, inner_tol);
-            pcg_loop<float>(stream, n, g, ell_a32, x32, s32, z32, p32, q32, d_einv32, d_c32, d_y32, h);
+            pcg<float>(stream, n, g, ell_a32, x32, s32, z32, p32, p2_32, q32, d_einv32, d_c32, h);
             stats.iterations += (uint64_t)h[S_ITER];
             add_correction_kernel<<<g, kBlock, 0, stream>>>(n, x, x32);
             residual_kernel<<<gs, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, sg, nullptr,
@@ -868,7 +1108,7 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
             }
             SG_CUDA(cudaEventRecord(evc0, stream));
             init_kernel<double><<<gs, kBlock, 0, stream>>>(sg, b, xchk, r, d_c64, red, red_count, scal, check_tol);
-            pcg_loop<double>(stream, n, g, ell_a64, xchk, r, z, p, q, d_einv64, d_c64, d_y64, h);
+            pcg<double>(stream, n, g, ell_a64, xchk, r, z, p, p2, q, d_einv64, d_c64, h);
             SG_CUDA(cudaMemsetAsync(scal + S_CHK, 0, sizeof(double), stream));
             check_kernel<<<g, kBlock, 0, stream>>>(n, V, x, xchk, d_vclamped, scal);
             double e = 0.0;

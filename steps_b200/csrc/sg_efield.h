@@ -85,19 +85,20 @@ struct EFieldSystem {
     double* d_einv64 = nullptr;           // [nagg][nagg]
     float* d_einv32 = nullptr;
     double* d_c64 = nullptr;              // restricted residual [nagg]
-    double* d_y64 = nullptr;              // coarse correction [nagg]
     float* d_c32 = nullptr;
-    float* d_y32 = nullptr;
     int32_t* acol_dev = nullptr;          // [width][nverts] matrix columns (clamped ones removed)
     double inner_tol = 1.0e-4;            // relative residual of each FP32 inner solve
     bool check = false;                   // mixed method: also solve in FP64 and compare
     double check_tol = 1.0e-12;           // relative residual of the FP64 check solve
     double* xchk = nullptr;               // [nverts] dV of the FP64 check solve
-    double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
-    float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr, *x32 = nullptr, *s32 = nullptr;
+    double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *p2 = nullptr, *q = nullptr;
+    float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *p2_32 = nullptr, *q32 = nullptr, *x32 = nullptr,
+          *s32 = nullptr;
     double* red = nullptr;                // reduction partials
     double* scal = nullptr;               // device scalars
     unsigned int* red_count = nullptr;
+    unsigned int* d_bar = nullptr;        // grid barrier of the persistent solve: count, generation, error
+    bool persistent = false;              // whole solve in one cooperative launch (else a launch per phase)
     double dt_built = -1.0;
     bool dirty = true;                    // clamps / membrane properties changed
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc0 = nullptr, evc1 = nullptr;
@@ -117,8 +118,14 @@ struct EFieldSystem {
     // reduction partials hold 2 x 1024 values); warps stride over the rest.
     int seg_grid() const { return nseg > 0 ? std::min((nseg + 7) / 8, 1024) : 1; }
     template <typename T>
-    void pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* qv, const T* einv,
-                  T* cvec, T* yv, double* h);
+    void pcg(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* pv2, T* qv,
+             const T* einv, T* cvec, double* h);
+    template <typename T>
+    void pcg_persistent(cudaStream_t stream, int n, const T* a, T* xv, T* rv, T* zv, T* pv, T* pv2, T* qv,
+                        const T* einv, T* cvec, double* h);
+    template <typename T>
+    void pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv, T* rv, T* zv, T* pv, T* pv2, T* qv,
+                  const T* einv, T* cvec, double* h);
 };
 
 // Geometric coupling of a tet mesh: for every edge ij, sum over tets of the linear-FEM

@@ -305,6 +305,7 @@ void run_noalloc(int32_t ntets, int32_t nspec, int32_t nreac, uint32_t* counts, 
     if (sm > 48 * 1024)
         SG_CUDA(cudaFuncSetAttribute(sg::window_kernel<kBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
+    SG_CUDA(cudaFuncSetAttribute(sg::window_kernel<kBlock>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     int per_sm = 0;
     SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sg::window_kernel<kBlock>, kBlock, sm));
     long need = ((long)ntets + kBlock - 1) / kBlock;

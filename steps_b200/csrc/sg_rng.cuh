@@ -252,20 +252,36 @@ SG_HD double sg_rcp(const double* tab, uint32_t x) {
 }
 
 // Sequential search from 0: pmf recurrence f(x) = f(x-1) * ((n+1) s / x - s), s = p/q,
-// with 1/x from the reciprocal table (one multiply instead of a division per step).
+// the factor as one fma with 1/x from the reciprocal table.  The search runs on without
+// an x < n test: past x = n the factor is rounding-small, and negative from x = n + 2, so
+// the loop ends by x = n + 2 at the latest and the result is clamped to n (the value the
+// bounded search returns).  With n + 3 < SG_RCP_TABLE the next reciprocal is loaded one
+// step ahead, off the multiply chain.
 SG_HD uint32_t sg_binv(sg_stream* st, uint32_t n, double p, const double* rcp, double s) {
     double q = 1.0 - p;
     double a = ((double)n + 1.0) * s;
     double r = sg_pow_u(q, n);
     double u = sg_u01_co(sg_next_u32(st));
     uint32_t x = 0;
-    while (u >= r && x < n) {
-        u = u - r;
-        x += 1;
-        r = r * (a * sg_rcp(rcp, x) - s);
-        if (!(r > 0.0)) break;  // pmf underflowed past the mass: stop at x
+    if (rcp && n + 3u < (uint32_t)SG_RCP_TABLE) {
+        double rc = rcp[1];
+        while (u >= r) {
+            u = u - r;
+            x += 1;
+            double m = fma(a, rc, -s);
+            rc = rcp[x + 1];
+            r = r * m;
+            if (!(r > 0.0)) break;  // pmf underflowed past the mass (or x > n)
+        }
+    } else {
+        while (u >= r) {
+            u = u - r;
+            x += 1;
+            r = r * fma(a, sg_rcp(rcp, x), -s);
+            if (!(r > 0.0)) break;
+        }
     }
-    return x;
+    return x < n ? x : n;
 }
 
 // Stirling-series remainder fc(k) = ln k! - ((k + 1/2) ln(k + 1) - (k + 1) + ln(2 pi)/2),

@@ -533,6 +533,11 @@ struct Solver {
     int check_flag() const { return (check && !any_clamp && !(has_surf() && surf_touches_volume)) ? 1 : 0; }
 
     void set_kernel_smem_limits() {
+        // Window kernels are occupancy-bound on shared memory: ask for the largest carveout.
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<64>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<128>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<256>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         size_t sm = smem_bytes(256, nspec, (int)reacs.size());
         if (sm > 227 * 1024) throw NotImplErr("too many species for the shared-memory staging");
         if (sm > 48 * 1024) {
@@ -549,8 +554,11 @@ struct Solver {
         }
     }
 
+    // grid > 0: that many blocks; 0: occupancy-sized (blocks stride over the tets);
+    // -1: one tet per thread (the hardware schedules new blocks as old ones finish).
     int window_grid() {
         if (grid > 0) return grid;
+        if (grid == -1) return (int)std::max(1L, ((long)ntets + eff_block() - 1) / eff_block());
         size_t sm = window_smem();
         int per_sm = 0;
         if (has_surf()) {
@@ -719,6 +727,52 @@ struct Solver {
         return x * 1.0e-3;
     }
 
+    // ---- launch-shape autotuning ----
+    // The sample path does not depend on the launch shape (every tet draws from its own
+    // counter stream), so tuning runs real windows: after one untimed window, the next
+    // windows of a run are timed under each candidate {block 64, 128, 256} x {occupancy-
+    // sized grid, one tet per thread} and the fastest shape is kept.
+    static constexpr int kTuneWindows = 2;
+    static constexpr int kTuneCands = 6;
+    bool tune_pending = false;
+    std::vector<float> tune_ms;
+
+    uint64_t autotune(const sg_window_args& a) {
+        const int blocks[3] = {64, 128, 256};
+        int best_block = block, best_grid = grid;
+        float best = 0.0f;
+        tune_ms.clear();
+        cudaEvent_t e0, e1;
+        SG_CUDA(cudaEventCreate(&e0));
+        SG_CUDA(cudaEventCreate(&e1));
+        launch_window(a, window_grid());  // untimed: first-launch costs
+        for (int bi = 0; bi < 3; ++bi) {
+            block = blocks[bi];
+            for (int mode = 0; mode < 2; ++mode) {
+                grid = mode ? -1 : 0;
+                const int g = window_grid();
+                SG_CUDA(cudaEventRecord(e0, stream));
+                for (int i = 0; i < kTuneWindows; ++i) launch_window(a, g);
+                SG_CUDA(cudaEventRecord(e1, stream));
+                SG_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.0f;
+                SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                tune_ms.push_back(ms);
+                if (tune_ms.size() == 1 || ms < best) {
+                    best = ms;
+                    best_block = block;
+                    best_grid = grid;
+                }
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        block = best_block;
+        grid = best_grid;
+        tune_pending = false;
+        return (uint64_t)kTuneWindows * kTuneCands + 1;
+    }
+
     // Enqueue every window up to endtime for all realizations (no host sync).
     uint64_t enqueue_windows(double endtime) {
         uint64_t n = 0;
@@ -731,12 +785,13 @@ struct Solver {
         upload_reals();
         if (n == 0) return 0;
         sg_window_args a = window_args();
+        uint64_t done = 0;
+        if (tune_pending && !has_surf() && n > (uint64_t)kTuneWindows * kTuneCands + 1) done = autotune(a);
         int g = window_grid();
         if (profiling) SG_CUDA(cudaEventRecord(ev_begin, stream));
         // Windows advance their own time on the device, so a captured chunk of window
         // launches replays unchanged; the remainder is launched directly.
-        uint64_t done = 0;
-        if (use_graphs && n >= (uint64_t)kGraphChunk) {
+        if (use_graphs && n - done >= (uint64_t)kGraphChunk) {
             cudaGraphExec_t ge = window_graph(a, g);
             for (; done + kGraphChunk <= n; done += kGraphChunk) SG_CUDA(cudaGraphLaunch(ge, stream));
         }
@@ -1104,6 +1159,180 @@ struct Solver {
         for (int i = 0; i < (int)reacs.size(); ++i) v += reac_extent(i);
         return v;
     }
+
+    // ---- checkpoint / restore (TOS:217-451 checkpoint, restore) ----
+    // Binary file: a header of sizes (checked on restore against this solver's mesh and
+    // model), then every state array, each preceded by its element count and size.  The
+    // pending inflow is applied first, so counts are complete.  Random streams are keyed by
+    // (seed, realization, tet, window), so restoring the window indices and the seed makes
+    // the continuation identical to the uninterrupted run.
+    struct CkptHeader {
+        char magic[8];
+        uint32_t version;
+        int32_t ntets, nspec, nreal, ncomp, nreac, ntris, nsspec, nverts, nsreac;
+        uint64_t seed, niteration, setup_calls;
+        double efdt;
+    };
+
+    template <typename T>
+    static void put(FILE* f, const T* p, size_t n) {
+        uint64_t hd[2] = {(uint64_t)n, (uint64_t)sizeof(T)};
+        if (std::fwrite(hd, sizeof(hd), 1, f) != 1 || (n && std::fwrite(p, sizeof(T), n, f) != n))
+            throw ProgErr("checkpoint: write failed");
+    }
+    template <typename T>
+    static void get(FILE* f, T* p, size_t n, const char* what) {
+        uint64_t hd[2] = {0, 0};
+        if (std::fread(hd, sizeof(hd), 1, f) != 1 || hd[0] != n || hd[1] != sizeof(T))
+            throw ArgErr(std::string("checkpoint does not match this solver (") + what + ")");
+        if (n && std::fread(p, sizeof(T), n, f) != n) throw ArgErr("checkpoint: truncated file");
+    }
+    template <typename T>
+    void put_dev(FILE* f, const T* dp, size_t n) {
+        std::vector<T> h(n);
+        if (n) d2h(h.data(), dp, n);
+        sync();
+        put(f, h.data(), n);
+    }
+    template <typename T>
+    void get_dev(FILE* f, T* dp, size_t n, const char* what) {
+        std::vector<T> h(n);
+        get(f, h.data(), n, what);
+        if (n) h2d(dp, h.data(), n);
+        sync();
+    }
+
+    CkptHeader ckpt_header() const {
+        CkptHeader hd{};
+        std::memcpy(hd.magic, "SGB2CKPT", 8);
+        hd.version = 1;
+        hd.ntets = ntets;
+        hd.nspec = nspec;
+        hd.nreal = nreal;
+        hd.ncomp = ncomp;
+        hd.nreac = (int32_t)reacs.size();
+        hd.ntris = ntris;
+        hd.nsspec = nsspec;
+        hd.nverts = ef_on ? ef.nverts : 0;
+        hd.nsreac = (int32_t)sreacs.size();
+        hd.seed = seed;
+        hd.niteration = niteration;
+        hd.setup_calls = setup_calls;
+        hd.efdt = efdt;
+        return hd;
+    }
+
+    void checkpoint(const std::string& path) {
+        require_setup();
+        flush();
+        download_reals();
+        FILE* f = std::fopen(path.c_str(), "wb");
+        if (!f) throw ArgErr("cannot open checkpoint file for writing: " + path);
+        try {
+            CkptHeader hd = ckpt_header();
+            put(f, &hd, 1);
+            put(f, reals.data(), reals.size());
+            put(f, kcst.data(), kcst.size());
+            put(f, dcst.data(), dcst.size());
+            put(f, clampm.data(), clampm.size());
+            put_dev(f, d_counts.p, d_counts.n);
+            put_dev(f, d_totals.p, d_totals.n);
+            put_dev(f, d_ext.p, d_ext.n);
+            put_dev(f, d_ext_total.p, d_ext_total.n);
+            put_dev(f, d_diff_total.p, d_diff_total.n);
+            put_dev(f, d_launch.p, d_launch.n);
+            if (has_surf()) {
+                put(f, skcst.data(), skcst.size());
+                put_dev(f, d_tri_counts.p, d_tri_counts.n);
+                put_dev(f, d_spec_int.p, d_spec_int.n);
+                put_dev(f, d_tri_Iohm.p, d_tri_Iohm.n);
+                put_dev(f, d_surf_ext.p, d_surf_ext.n);
+            }
+            if (ef_on) {
+                const int nv = ef.nverts;
+                double mp[4] = {ef.cm, ef.sigma, ef.g_leak, ef.v_leak};
+                put(f, mp, 4);
+                put(f, ef.vclamped.data(), ef.vclamped.size());
+                put(f, ef.vert_iclamp.data(), ef.vert_iclamp.size());
+                put(f, ef.tri_iclamp.data(), ef.tri_iclamp.size());
+                put_dev(f, ef.V, (size_t)nv);
+                put_dev(f, ef.x, (size_t)nv);  // warm start of the next solve
+                put_dev(f, ef.tri_V, (size_t)ef.ntris);
+            }
+        } catch (...) {
+            std::fclose(f);
+            throw;
+        }
+        if (std::fclose(f) != 0) throw ProgErr("checkpoint: close failed");
+    }
+
+    void restore(const std::string& path) {
+        require_setup();
+        flush();
+        FILE* f = std::fopen(path.c_str(), "rb");
+        if (!f) throw ArgErr("cannot open checkpoint file: " + path);
+        try {
+            CkptHeader hd{};
+            get(f, &hd, 1, "header");
+            CkptHeader me = ckpt_header();
+            if (std::memcmp(hd.magic, me.magic, 8) != 0 || hd.version != 1) throw ArgErr("not a checkpoint file");
+            if (hd.ntets != me.ntets || hd.nspec != me.nspec || hd.nreal != me.nreal || hd.ncomp != me.ncomp ||
+                hd.nreac != me.nreac || hd.ntris != me.ntris || hd.nsspec != me.nsspec || hd.nverts != me.nverts ||
+                hd.nsreac != me.nsreac)
+                throw ArgErr("checkpoint was written by a solver with another mesh or model");
+            get(f, reals.data(), reals.size(), "realizations");
+            get(f, kcst.data(), kcst.size(), "reaction constants");
+            get(f, dcst.data(), dcst.size(), "diffusion constants");
+            get(f, clampm.data(), clampm.size(), "clamps");
+            any_clamp = false;
+            for (uint32_t m : clampm)
+                if (m) any_clamp = true;
+            h2d(d_clamp.p, clampm.data(), clampm.size());
+            h2d(d_kcst.p, kcst.data(), kcst.size());
+            h2d(d_dcst.p, dcst.data(), dcst.size());
+            upload_reals();
+            get_dev(f, d_counts.p, d_counts.n, "counts");
+            get_dev(f, d_totals.p, d_totals.n, "totals");
+            get_dev(f, d_ext.p, d_ext.n, "extents");
+            get_dev(f, d_ext_total.p, d_ext_total.n, "extents");
+            get_dev(f, d_diff_total.p, d_diff_total.n, "diffusion extent");
+            get_dev(f, d_launch.p, d_launch.n, "launch state");
+            if (has_surf()) {
+                get(f, skcst.data(), skcst.size(), "surface constants");
+                h2d(d_skcst.p, skcst.data(), skcst.size());
+                get_dev(f, d_tri_counts.p, d_tri_counts.n, "triangle counts");
+                get_dev(f, d_spec_int.p, d_spec_int.n, "channel integrals");
+                get_dev(f, d_tri_Iohm.p, d_tri_Iohm.n, "ohmic currents");
+                get_dev(f, d_surf_ext.p, d_surf_ext.n, "surface extents");
+            }
+            if (ef_on) {
+                const int nv = ef.nverts;
+                double mp[4];
+                get(f, mp, 4, "membrane");
+                ef.cm = mp[0];
+                ef.sigma = mp[1];
+                ef.g_leak = mp[2];
+                ef.v_leak = mp[3];
+                get(f, ef.vclamped.data(), ef.vclamped.size(), "vertex clamps");
+                get(f, ef.vert_iclamp.data(), ef.vert_iclamp.size(), "vertex current clamps");
+                get(f, ef.tri_iclamp.data(), ef.tri_iclamp.size(), "triangle current clamps");
+                get_dev(f, ef.V, (size_t)nv, "potentials");
+                get_dev(f, ef.x, (size_t)nv, "EField warm start");
+                get_dev(f, ef.tri_V, (size_t)ef.ntris, "triangle potentials");
+                ef.dirty = true;
+            }
+            niteration = hd.niteration;
+            setup_calls = hd.setup_calls;
+            efdt = hd.efdt;
+            pending_host = false;
+        } catch (...) {
+            std::fclose(f);
+            throw;
+        }
+        std::fclose(f);
+        drop_graph();
+        sync();
+    }
 };
 
 }  // namespace sg
@@ -1390,6 +1619,20 @@ int sg_get_diff_extent(sg_solver* h, uint64_t* n) {
     });
 }
 
+int sg_checkpoint(sg_solver* h, const char* file_name) {
+    return guarded([&] {
+        need(file_name, "file_name");
+        S(h)->checkpoint(file_name);
+    });
+}
+
+int sg_restore(sg_solver* h, const char* file_name) {
+    return guarded([&] {
+        need(file_name, "file_name");
+        S(h)->restore(file_name);
+    });
+}
+
 int sg_get_nsteps(sg_solver* h, uint64_t* n) {
     return guarded([&] {
         need(n, "n");
@@ -1407,9 +1650,28 @@ int sg_get_niteration(sg_solver* h, uint64_t* n) {
 int sg_set_launch(sg_solver* h, int32_t block, int32_t grid) {
     return guarded([&] {
         if (block != 64 && block != 128 && block != 256) throw sg::ArgErr("block must be 64, 128 or 256");
-        if (grid < 0) throw sg::ArgErr("grid must be >= 0 (0 = occupancy-sized)");
+        if (grid < -1) throw sg::ArgErr("grid must be >= -1 (0 = occupancy-sized, -1 = one tet per thread)");
         S(h)->block = block;
         S(h)->grid = grid;
+    });
+}
+
+int sg_get_launch(sg_solver* h, int32_t* block, int32_t* grid) {
+    return guarded([&] {
+        if (block) *block = S(h)->block;
+        if (grid) *grid = S(h)->grid;
+    });
+}
+
+int sg_set_autotune(sg_solver* h, int32_t on) {
+    return guarded([&] { S(h)->tune_pending = on != 0; });
+}
+
+int sg_get_autotune_ms(sg_solver* h, float* ms, int32_t cap, int32_t* count) {
+    return guarded([&] {
+        const auto& v = S(h)->tune_ms;
+        if (count) *count = (int32_t)v.size();
+        for (int i = 0; i < (int)v.size() && i < cap; ++i) ms[i] = v[i];
     });
 }
 
@@ -1714,6 +1976,14 @@ int sg_set_efield_check(sg_solver* h, int32_t on, double rel_tol) {
         if (on && !(rel_tol > 0.0)) throw sg::ArgErr("bad check tolerance");
         s->ef.check = on != 0;
         if (on) s->ef.check_tol = rel_tol;
+    });
+}
+
+int sg_set_efield_persistent(sg_solver* h, int32_t on) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        s->ef.persistent = on != 0;
     });
 }
 

@@ -68,8 +68,7 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 // Shared-memory carve-up for a block of BLOCK threads.
 struct smem_layout {
     uint32_t* cnt;             // [S][BLOCK]
-    double* occ;               // [S][BLOCK]
-    double* last;              // [S][BLOCK]
+    double* tdel;              // [S][BLOCK] sum over count changes of (change) x (time of change)
     double* prop;              // [R][BLOCK] propensities of this thread's tet
     sg_reac* reac;             // [R] copy of the reaction table
     unsigned long long* tot;   // [S]
@@ -81,7 +80,7 @@ struct smem_layout {
 __host__ __device__ inline size_t smem_bytes(int block, int nspec, int nreac) {
     size_t b = (size_t)block * nspec * 4;
     b = (b + 15) & ~(size_t)15;
-    b += (size_t)block * nspec * 16;
+    b += (size_t)block * nspec * 8;
     b += (size_t)block * nreac * 8;
     b += (size_t)nreac * sizeof(sg_reac);
     b = (b + 7) & ~(size_t)7;
@@ -97,9 +96,7 @@ __device__ inline smem_layout carve(unsigned char* base, int block, int nspec, i
     size_t b = (size_t)block * nspec * 4;
     L.cnt = (uint32_t*)base;
     b = (b + 15) & ~(size_t)15;
-    L.occ = (double*)(base + b);
-    b += (size_t)block * nspec * 8;
-    L.last = (double*)(base + b);
+    L.tdel = (double*)(base + b);
     b += (size_t)block * nspec * 8;
     L.prop = (double*)(base + b);
     b += (size_t)block * nreac * 8;
@@ -118,13 +115,15 @@ __device__ inline smem_layout carve(unsigned char* base, int block, int nspec, i
 }
 
 // SSA for one tet over [0, T): direct method with FP64 propensities, waiting
-// times -log(U)/a0, occupancy integration per changed species.
+// times -log(U)/a0.  Occupancy: the time integral of a count over the window is
+// c_end T - sum_k (change_k) t_k, so only sum_k (change_k) t_k is kept per species
+// (tdel); the reference keeps the running integral and the last update time instead
+// (tet.cpp:318-340), the same quantity up to rounding.
 __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layout& L, int tid,
                                         int BLOCK, int rb, int re, const double* K, double ivs,
                                         uint32_t clampm, double T, sg_stream* st) {
     uint32_t* sc = L.cnt + tid;
-    double* so = L.occ + tid;
-    double* sl = L.last + tid;
+    double* sd = L.tdel + tid;
     double* sp = L.prop + tid;  // sp[q * BLOCK]: propensity of reaction q in this tet
     double tt = 0.0;
     // Propensities are kept per reaction and only the ones whose reactants changed are
@@ -166,13 +165,12 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
             int s = rc->upd_spec[i];
             if ((clampm >> s) & 1u) continue;
             uint32_t old = sc[s * BLOCK];
-            so[s * BLOCK] = so[s * BLOCK] + (double)old * (tt - sl[s * BLOCK]);
-            sl[s * BLOCK] = tt;
             long long nc = (long long)old + rc->upd_delta[i];
             if (nc < 0 || nc > 0xFFFFFFFFll) {
                 atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
                 nc = nc < 0 ? 0 : 0xFFFFFFFFll;
             }
+            sd[s * BLOCK] = sd[s * BLOCK] + (double)(nc - (long long)old) * tt;
             sc[s * BLOCK] = (uint32_t)nc;
         }
         atomicAdd(&L.ext[sel], 1u);
@@ -189,8 +187,7 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
     const sg_surf_args& sa = a.surf;
     const int SS = sa.nsspec, RSP = sa.max_sreac_per_patch, M = sa.ntris;
     uint32_t* sc = L.cnt + tid;
-    double* so = L.occ + tid;
-    double* sl = L.last + tid;
+    double* sd = L.tdel + tid;
     const int mm[4] = {tris.x, tris.y, tris.z, tris.w};
     int pb[4], pe[4];
     double area[4], vm[4];
@@ -275,13 +272,12 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
                 int s = rc->upd_spec[i];
                 if ((clampm >> s) & 1u) continue;
                 uint32_t old = sc[s * BLOCK];
-                so[s * BLOCK] = so[s * BLOCK] + (double)old * (tt - sl[s * BLOCK]);
-                sl[s * BLOCK] = tt;
                 long long nc = (long long)old + rc->upd_delta[i];
                 if (nc < 0 || nc > 0xFFFFFFFFll) {
                     atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
                     nc = nc < 0 ? 0 : 0xFFFFFFFFll;
                 }
+                sd[s * BLOCK] = sd[s * BLOCK] + (double)(nc - (long long)old) * tt;
                 sc[s * BLOCK] = (uint32_t)nc;
             }
             atomicAdd(&L.ext[sq], 1u);
@@ -303,13 +299,12 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
                 int s = r.iupd_spec[i];
                 if ((clampm >> s) & 1u) continue;
                 uint32_t old = sc[s * BLOCK];
-                so[s * BLOCK] = so[s * BLOCK] + (double)old * (tt - sl[s * BLOCK]);
-                sl[s * BLOCK] = tt;
                 long long nc = (long long)old + r.iupd_delta[i];
                 if (nc < 0 || nc > 0xFFFFFFFFll) {
                     atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
                     nc = nc < 0 ? 0 : 0xFFFFFFFFll;
                 }
+                sd[s * BLOCK] = sd[s * BLOCK] + (double)(nc - (long long)old) * tt;
                 sc[s * BLOCK] = (uint32_t)nc;
             }
             atomicAdd(a.surf_ext, 1ull);
@@ -406,8 +401,7 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
                     }
                     c = (uint32_t)sum;
                 }
-                L.occ[s * BLOCK + tid] = 0.0;
-                L.last[s * BLOCK + tid] = 0.0;
+                L.tdel[s * BLOCK + tid] = 0.0;
             }
             L.cnt[s * BLOCK + tid] = c;
             unsigned long long v = warp_sum_u64((unsigned long long)c);
@@ -441,6 +435,7 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
         const double odd2 = sg_binom_odds((double)g.y);
         const double odd3 = sg_binom_odds((double)g.z);
         uint32_t* out = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane;
+        const double invT = 1.0 / T;  // one division per tet for the occupancy means
         for (int s = 0; s < S; ++s) {
             int ds = __ldg(&a.diff_slot[s]);
             if (ds < 0) continue;
@@ -451,10 +446,11 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             if (pop > 0u) {
                 double t1 = T * (D * G);
                 if (t1 >= 1.0) t1 = 1.0;
-                double so = L.occ[s * BLOCK + tid], sl = L.last[s * BLOCK + tid];
+                const double sd = L.tdel[s * BLOCK + tid];
                 uint32_t mean_n = pop;
-                if (so != 0.0 || sl != 0.0) {
-                    double nbar = (so + (double)pop * (T - sl)) / T;
+                if (sd != 0.0) {
+                    // Occupancy mean over the window: c_end - sum_k (change_k) t_k / T.
+                    double nbar = (double)pop - sd * invT;
                     if (nbar > (double)pop) nbar = (double)pop;
                     double nint = floor(nbar);
                     double frc = nbar - nint;

@@ -10,6 +10,7 @@ wm_hosts) are accepted and ignored: the whole mesh lives on one GPU.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -20,7 +21,7 @@ EF_NONE = 0
 EF_DEFAULT = 1
 EF_DV_BDSYS = 2
 EF_DV_PETSC = 3
-# GPU membrane-potential solvers: Jacobi-preconditioned CG in FP64, or FP32 CG inside an
+# GPU membrane-potential solvers: two-level preconditioned CG in FP64, or FP32 CG inside an
 # FP64 residual-refinement loop.  The reference's direct/PETSc choices map to FP64 CG.
 EF_DV_CG_FP64 = 10
 EF_DV_CG_MIXED = 11
@@ -299,6 +300,15 @@ class TetOpSplit:
     def advance(self, adv):
         check(self._L.sg_advance(self._h, float(adv)))
 
+    def checkpoint(self, file_name):
+        """Write the complete simulation state to file_name (API::checkpoint)."""
+        check(self._L.sg_checkpoint(self._h, os.fsencode(file_name)))
+
+    def restore(self, file_name):
+        """Load a state written by checkpoint() of a solver on the same mesh and model
+        (API::restore); the run continues exactly as the checkpointed one would have."""
+        check(self._L.sg_restore(self._h, os.fsencode(file_name)))
+
     def step(self):
         raise _lib.NotImplErr("step() is not implemented for operator-split solvers")
 
@@ -524,6 +534,11 @@ class TetOpSplit:
         timed) and record the largest per-vertex relative voltage difference."""
         check(self._L.sg_set_efield_check(self._h, 1 if on else 0, float(rel_tol)))
 
+    def setEfieldPersistent(self, on):
+        """Run each EField solve as one cooperative launch (True) or as three kernel
+        launches per CG iteration (False)."""
+        check(self._L.sg_set_efield_persistent(self._h, 1 if on else 0))
+
     def getEfieldCheck(self):
         """(checked steps, max over steps of max_v |V_mixed - V_fp64| / |V_fp64|, last step's)."""
         s, mx, last = C.c_uint64(), C.c_double(), C.c_double()
@@ -533,6 +548,26 @@ class TetOpSplit:
     # --------------------------------------------------------- device knobs
     def setLaunch(self, block, grid=0):
         check(self._L.sg_set_launch(self._h, int(block), int(grid)))
+
+    def getLaunch(self):
+        """(block, grid) of the window kernel; grid 0 = occupancy-sized, -1 = one tet per
+        thread."""
+        b, g = C.c_int32(), C.c_int32()
+        check(self._L.sg_get_launch(self._h, C.byref(b), C.byref(g)))
+        return b.value, g.value
+
+    def setAutotune(self, on=True):
+        """Time 12 windows of the next run (after one untimed window) under six launch
+        shapes and keep the fastest (results do not depend on the shape)."""
+        check(self._L.sg_set_autotune(self._h, 1 if on else 0))
+
+    def getAutotuneTimes(self):
+        """ms of the two timed windows under each candidate shape, in the order block
+        64, 128, 256 x grid {occupancy-sized, one tet per thread}; empty before tuning."""
+        buf = (C.c_float * 8)()
+        n = C.c_int32()
+        check(self._L.sg_get_autotune_ms(self._h, buf, 8, C.byref(n)))
+        return list(buf)[: n.value]
 
     def setConservationCheck(self, on):
         check(self._L.sg_set_conservation_check(self._h, 1 if on else 0))

@@ -156,3 +156,26 @@ def test_launch_shapes_agree(steps_lib, block):
         sim.run(k * 1.0e-3)
         ora.run(k * 1.0e-3)
         assert_same(sim, ora, f"block {block} step {k}")
+
+
+def test_autotuned_run_matches_oracle(steps_lib):
+    """Autotuning times 12 windows (after an untimed one) under six launch shapes; the
+    counts after the run still equal the oracle's, and the kept shape is a candidate."""
+    mesh = W.cube_mesh(9)
+    sim, ora = pair(W.random_network(3), mesh, seed=6)
+    rows = W.poisson_counts(mesh.ntets, 30.0, 6, nspec=8)
+    for i, s in enumerate(sim.spec_names):
+        sim.setSpecCounts(s, rows[i])
+    sync_counts(sim, ora)
+    sim.setAutotune(True)
+    t = 40 * sim.getUpdPeriod()
+    sim.run(t)
+    ora.run(t)
+    assert_same(sim, ora, "autotuned run")
+    times = sim.getAutotuneTimes()
+    assert len(times) == 6 and all(x > 0.0 for x in times)
+    block, grid = sim.getLaunch()
+    assert block in (64, 128, 256) and grid in (0, -1)
+    sim.run(2 * t)
+    ora.run(2 * t)
+    assert_same(sim, ora, "after tuning")
