@@ -72,7 +72,7 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "50",
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "20",
                  "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -289,11 +289,14 @@ def run_ours(args):
     bytes_per_window = mesh.ntets * (BYTES_PER_TET_SPEC * NSPEC + BYTES_PER_TET)
     avg_win_s = (win_ms * 1e-3) / max(nwin, 1)
     achieved = bytes_per_window / avg_win_s / 1e9
+    # DRAM bytes per window-kernel launch on this workload from the committed ncu summary.
     traffic = None
-    prof_path = os.path.join(ROOT, "profiles", "traffic_window_kernel.json")
+    prof_path = os.path.join(ROOT, "profiles", "window_kernel_plain_384k.md")
     if os.path.exists(prof_path):
         with open(prof_path) as f:
-            traffic = json.load(f).get("bytes_per_launch_scaled_to_384k")
+            for ln in f:
+                if ln.startswith("dram_bytes_per_launch:"):
+                    traffic = int(ln.split(":")[1])
 
     if rank == 0:
         mdl_cpu, mesh_cpu, rows_cpu = (mdl, mesh, rows)
@@ -305,6 +308,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "u32+f64", "data": "synthetic",
             "config": dict(config_dict(mesh), parallelism=f"replicas{world}",
                            launch={"block": sim.getLaunch()[0], "grid": sim.getLaunch()[1],
+                                   "smem_carveout_pct": sim.getCarveout(),
                                    "autotune_ms": sim.getAutotuneTimes()}),
             "sim_ms_per_wall_s": (STEP_SIM_S * 1e3 * args.steps) / (t_max * 1e-3),
             "windows_per_step": windows / args.steps,
@@ -455,7 +459,8 @@ def run_efield(args):
         r = srng.create("r123", 512)
         r.initialize(SEED)
         sim = TetOpSplit(mdl, mesh, r, method)
-        sim.setEfieldTolerance(args.ef_tol, 1e-4)
+        sim.setEfieldTolerance(args.ef_tol, args.ef_inner_tol)
+        sim.setEfieldPersistent(bool(args.ef_persistent))
         if method == EF_DV_CG_MIXED:
             sim.setEfieldCheck(True, 1e-12)  # untimed FP64 solve of every step's system
         sim.setEfieldDT(1e-6)
@@ -483,12 +488,109 @@ def run_efield(args):
     print(json.dumps({
         "metric": "EField solve ms per step", "config": {"mesh": f"{nx}x{ny}x{nz} Kuhn cubes",
                                                          "tets": mesh.ntets, "verts": mesh.nverts,
-                                                         "steps": args.ef_steps, "tol": args.ef_tol},
+                                                         "steps": args.ef_steps, "tol": args.ef_tol,
+                                                         "persistent_solve": bool(args.ef_persistent)},
         "fp64": out["fp64"], "mixed": out["mixed"],
         "mixed_speedup_solve": out["fp64"]["solve_ms_per_step"] / out["mixed"]["solve_ms_per_step"],
         "max_rel_v_err_per_step": out["mixed"]["check_vs_fp64_solve"]["max_rel_v_err"],
         "max_rel_v_diff_end_of_run": err,
     }), flush=True)
+    return 0
+
+
+def run_coupled(args):
+    """Full coupled batched configuration: 16 realizations of a 5x5x8 um box (50x50x80 Kuhn
+    cubes, 1.2 M tets each) in one launch per window.  Volume: Ca + CB <-> CaCB (kf 1e8 /M/s,
+    kb 100 /s), D_Ca 2.2e-10, D_CB = D_CaCB = 2e-11 m^2/s, CB 50 uM, Ca 50 nM.  Membrane (every
+    boundary triangle): Cm 1 uF/cm^2, leak 3e-5 S/cm^2 at -65 mV, the two-state channel of the
+    EField configuration (10/um^2, 20 pS, +50 mV) and a voltage-gated Ca channel (3/um^2, the
+    same kinetics with the exponent's sign flipped) whose open state emits Ca into its tet at
+    0.1 pA per channel (0.1e-12 / 2e per second).  Mixed-precision EField, dt 1 us; the split
+    window is shorter than the EField step only when D_Ca G < 1e6 /s, so each EField step runs
+    one truncated window."""
+    import math
+
+    from steps_b200 import geom as sgeom
+    from steps_b200 import model as smodel
+    from steps_b200 import rng as srng
+    from steps_b200.solver import EF_DV_CG_FP64, EF_DV_CG_MIXED, TetOpSplit
+
+    t0 = time.perf_counter()
+    nx, ny, nz = args.cp_dims
+    base = sgeom.kuhn_box(nx, ny, nz, 1e-7)
+    mesh = sgeom.replicate(base, args.cp_nreal)
+    cyto = sgeom.TmComp("cyto", mesh, np.arange(mesh.ntets))
+    cyto.addVolsys("vsys")
+    patch = sgeom.TmPatch("memb", mesh, mesh.getSurfTris(), cyto)
+    patch.addSurfsys("ssys")
+    sgeom.Memb("membrane", mesh, [patch])
+    mdl = smodel.Model()
+    ca, cb, cacb = smodel.Spec("Ca", mdl), smodel.Spec("CB", mdl), smodel.Spec("CaCB", mdl)
+    vs = smodel.Volsys("vsys", mdl)
+    smodel.Reac("bind", vs, lhs=[ca, cb], rhs=[cacb], kcst=1e8)
+    smodel.Reac("unbind", vs, lhs=[cacb], rhs=[ca, cb], kcst=100.0)
+    smodel.Diff("dCa", vs, ca, 2.2e-10)
+    smodel.Diff("dCB", vs, cb, 2e-11)
+    smodel.Diff("dCaCB", vs, cacb, 2e-11)
+    ss = smodel.Surfsys("ssys", mdl)
+    vr = (-150.0e-3, 200.0e-3, 1.0e-4)
+    na = smodel.Chan("Na", mdl)
+    c, o = smodel.ChanState("C", mdl, na), smodel.ChanState("O", mdl, na)
+    smodel.VDepSReac("open", ss, slhs=[c], srhs=[o], k=lambda v: 100.0 * math.exp(v / 0.025), vrange=vr)
+    smodel.VDepSReac("close", ss, slhs=[o], srhs=[c], k=lambda v: 100.0 * math.exp(-v / 0.025), vrange=vr)
+    smodel.OhmicCurr("I", ss, chanstate=o, g=20e-12, erev=0.05)
+    cach = smodel.Chan("CaCh", mdl)
+    cc, co = smodel.ChanState("CaC", mdl, cach), smodel.ChanState("CaO", mdl, cach)
+    smodel.VDepSReac("caopen", ss, slhs=[cc], srhs=[co], k=lambda v: 100.0 * math.exp(-v / 0.025), vrange=vr)
+    smodel.VDepSReac("caclose", ss, slhs=[co], srhs=[cc], k=lambda v: 100.0 * math.exp(v / 0.025), vrange=vr)
+    smodel.SReac("caflux", ss, slhs=[co], srhs=[co], irhs=[ca], kcst=0.1e-12 / (2.0 * 1.602176487e-19))
+    method = EF_DV_CG_MIXED if args.cp_method == "mixed" else EF_DV_CG_FP64
+    r = srng.create("r123", 512)
+    r.initialize(SEED)
+    sim = TetOpSplit(mdl, mesh, r, method, realizations=mesh.offsets)
+    sim.setEfieldDT(1e-6)
+    sim.setMembPotential("membrane", -0.065)
+    sim.setMembCapac("membrane", 0.01)
+    sim.setMembRes("membrane", 1.0 / 0.3, -0.065)
+    sim.setCompSpecConc("cyto", "CB", 50e-6)
+    sim.setCompSpecConc("cyto", "Ca", 50e-9)
+    area_r = patch.getArea() / args.cp_nreal * 1e12  # um^2 per realization
+    for q in range(args.cp_nreal):
+        sim.setPatchSpecCount("memb", "C", 10.0 * area_r, realization=q)
+        sim.setPatchSpecCount("memb", "CaC", 3.0 * area_r, realization=q)
+    setup_s = time.perf_counter() - t0
+    import torch
+
+    ext = torch.cuda.ExternalStream(sim.getStream())
+    sim.run(args.cp_warmup_ms * 1e-3)
+    torch.cuda.synchronize()
+    it0 = sim.getNIteration()
+    s0, _, ms0, _ = sim.getEfieldStats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record(ext)
+    sim.run((args.cp_warmup_ms + args.cp_ms) * 1e-3)
+    e1.record(ext)
+    e1.synchronize()
+    wall = time.perf_counter() - w0
+    ms = e0.elapsed_time(e1)
+    windows = sim.getNIteration() - it0
+    s1, iters, ms1, rr = sim.getEfieldStats()
+    upd = mesh.ntets * 3 * windows
+    print(json.dumps({
+        "metric": "tet-species updates/s; sim-ms per wall-s", "value": upd / (ms * 1e-3),
+        "unit": "tet-species updates/s",
+        "config": {"workload": f"coupled batched: {args.cp_nreal} realizations of {nx}x{ny}x{nz} Kuhn cubes "
+                               f"({base.ntets} tets, {base.nverts} vertices each), Ca/CB/CaCB + membrane "
+                               f"channels + {args.cp_method} EField",
+                   "tets": mesh.ntets, "verts": mesh.nverts, "membrane_tris": int(len(mesh.getSurfTris())),
+                   "timed_sim_ms": args.cp_ms, "warmup_sim_ms": args.cp_warmup_ms},
+        "windows": windows, "efield_steps": s1 - s0, "ms": ms, "wall_s": wall, "setup_s": setup_s,
+        "sim_ms_per_wall_s": args.cp_ms / wall,
+        "efield_solve_ms_per_step": (ms1 - ms0) / max(s1 - s0, 1),
+        "cg_iterations_per_step_overall": iters / max(s1, 1),
+    }), flush=True)
+    del sim
     return 0
 
 
@@ -498,12 +600,19 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["plain", "batched", "efield"], default="plain")
+    ap.add_argument("--config", choices=["plain", "batched", "efield", "coupled"], default="plain")
+    ap.add_argument("--cp-dims", type=int, nargs=3, default=[50, 50, 80])
+    ap.add_argument("--cp-nreal", type=int, default=16)
+    ap.add_argument("--cp-ms", type=float, default=0.5, help="timed simulated ms (the configuration runs 20)")
+    ap.add_argument("--cp-warmup-ms", type=float, default=0.02)
+    ap.add_argument("--cp-method", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--ef-inner-tol", type=float, default=1e-4)
     ap.add_argument("--nreal", type=int, default=512)
     ap.add_argument("--plain-sample", type=int, default=64)
     ap.add_argument("--ef-dims", type=int, nargs=3, default=[20, 20, 200])
     ap.add_argument("--ef-steps", type=int, default=5000)
     ap.add_argument("--ef-tol", type=float, default=1e-10)
+    ap.add_argument("--ef-persistent", type=int, default=1, help="1: each EField solve in one cooperative launch")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -513,6 +622,8 @@ def main():
         return run_batched(args)
     if args.config == "efield":
         return run_efield(args)
+    if args.config == "coupled":
+        return run_coupled(args)
     return run_ours(args)
 
 

@@ -135,8 +135,10 @@ int sg_add_vdep_sreac(sg_solver* h, int32_t patch, const uint32_t* slhs, const u
 int sg_add_ohmic(sg_solver* h, int32_t patch, int32_t sspec, double g, double erev, int32_t* out_idx);
 int sg_get_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double* n);   /* TOS:4831 getTriSpecCount */
 int sg_set_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double n);    /* setTriSpecCount */
-int sg_get_patch_count(sg_solver* h, int32_t patch, int32_t sspec, double* n); /* getPatchSpecCount */
-int sg_set_patch_count(sg_solver* h, int32_t patch, int32_t sspec, double n);  /* setPatchSpecCount */
+/* getPatchSpecCount / setPatchSpecCount; real selects the triangles whose inner tet is in
+ * that realization, -1 all of them (counts are distributed by triangle area). */
+int sg_get_patch_count(sg_solver* h, int32_t patch, int32_t sspec, int32_t real, double* n);
+int sg_set_patch_count(sg_solver* h, int32_t patch, int32_t sspec, int32_t real, double n);
 int sg_get_tri_ohmic_i(sg_solver* h, int32_t tri, double* amps);  /* getTriOhmicI: last EField step */
 
 /* ---- membrane potential (EField; api.hpp:140, 2874-2875; efield.hpp:59) ----------
@@ -182,12 +184,14 @@ int sg_set_efield_persistent(sg_solver* h, int32_t on);
  * (blocks stride over the tets), -1 = one tet per thread. */
 int sg_set_launch(sg_solver* h, int32_t block, int32_t grid);
 int sg_get_launch(sg_solver* h, int32_t* block, int32_t* grid);
-/* Autotune the launch shape at the next run() with more than 13 windows: after one
- * untimed window, 12 windows are timed two each under block {64,128,256} x grid
- * {occupancy-sized (0), one tet per thread (-1)}, and the fastest shape is kept (the
- * sample path does not depend on the shape).  The six timings (ms, in that order) are read
- * back with sg_get_autotune_ms. */
+/* Autotune the launch shape at the next run() with more than 17 windows: after one
+ * untimed window, two windows each are timed under block {64,128,256} x grid
+ * {occupancy-sized (0), one tet per thread (-1)} with the full shared-memory carveout, then
+ * the best of those with carveouts 75% and 50%; the fastest is kept (the sample path does
+ * not depend on the shape).  The eight timings (ms, in that order) are read back with
+ * sg_get_autotune_ms, the kept carveout with sg_get_carveout. */
 int sg_set_autotune(sg_solver* h, int32_t on);
+int sg_get_carveout(sg_solver* h, int32_t* percent);
 int sg_get_autotune_ms(sg_solver* h, float* ms, int32_t cap, int32_t* count);
 /* Replay window launches from a captured CUDA graph of 16 windows (on by default). */
 int sg_set_graphs(sg_solver* h, int32_t on);

@@ -552,6 +552,8 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
         o[0] = o[1] = o[2] = o[3] = 0;
         uint32_t pop = cnt[i];
         if (pop == 0) continue;
+        /* Each (tet, species) leaves on its own stream (purpose 16 + species). */
+        or_stream_init(&st, s->seed, (uint32_t)r, (uint32_t)(t - s->real_begin[r]), w, 16u + (uint32_t)i);
         double t1 = T * (D * G);
         if (t1 >= 1.0) t1 = 1.0;
         uint32_t mean_n = pop;

@@ -79,6 +79,7 @@ PROTOTYPES = {
     "sg_set_launch": [_P, _i32, _i32],
     "sg_get_launch": [_P, _pi32, _pi32],
     "sg_set_autotune": [_P, _i32],
+    "sg_get_carveout": [_P, _pi32],
     "sg_get_autotune_ms": [_P, C.POINTER(C.c_float), _i32, _pi32],
     "sg_set_conservation_check": [_P, _i32],
     "sg_set_graphs": [_P, _i32],
@@ -89,8 +90,8 @@ PROTOTYPES = {
     "sg_add_ohmic": [_P, _i32, _i32, _f64, _f64, _pi32],
     "sg_get_tri_count": [_P, _i32, _i32, _pf64],
     "sg_set_tri_count": [_P, _i32, _i32, _f64],
-    "sg_get_patch_count": [_P, _i32, _i32, _pf64],
-    "sg_set_patch_count": [_P, _i32, _i32, _f64],
+    "sg_get_patch_count": [_P, _i32, _i32, _i32, _pf64],
+    "sg_set_patch_count": [_P, _i32, _i32, _i32, _f64],
     "sg_get_tri_ohmic_i": [_P, _i32, _pf64],
     "sg_set_efield_mesh": [_P, _i32, _pf64, _pi32, _i32, _pi32, _i32],
     "sg_set_efield_dt": [_P, _f64],

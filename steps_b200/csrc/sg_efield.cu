@@ -141,6 +141,10 @@ void EFieldSystem::release() {
     dfree(xchk);
     dfree(acol_dev);
     dfree(d_agg);
+    dfree(d_agg_base);
+    dfree(d_agg_len);
+    dfree(d_agg_row);
+    einv_len = 0;
     dfree(d_seg_ptr);
     dfree(d_seg_idx);
     dfree(d_seg_agg);
@@ -191,6 +195,30 @@ void EFieldSystem::setup(int nv, const double* verts_um, int ntet, const int32_t
     }
     width = 0;
     for (int i = 0; i < nv; ++i) width = std::max(width, nbr_ptr[i + 1] - nbr_ptr[i]);
+    // Connected components of the vertex graph (batched realizations are disjoint copies).
+    {
+        std::vector<int32_t> comp(nv, -1), stack;
+        comp_verts.clear();
+        for (int s0 = 0; s0 < nv; ++s0) {
+            if (comp[s0] >= 0) continue;
+            const int c = (int)comp_verts.size();
+            comp_verts.emplace_back();
+            comp[s0] = c;
+            stack.assign(1, s0);
+            while (!stack.empty()) {
+                const int v = stack.back();
+                stack.pop_back();
+                comp_verts[c].push_back(v);
+                for (int k = nbr_ptr[v]; k < nbr_ptr[v + 1]; ++k)
+                    if (comp[nbr_idx[k]] < 0) {
+                        comp[nbr_idx[k]] = c;
+                        stack.push_back(nbr_idx[k]);
+                    }
+            }
+            std::sort(comp_verts[c].begin(), comp_verts[c].end());
+        }
+        ncomp_v = (int)comp_verts.size();
+    }
     vclamped.assign(nv, 0);
     vert_iclamp.assign(nv, 0.0);
     tri_iclamp.assign(nt, 0.0);
@@ -449,13 +477,22 @@ __global__ void init_kernel(Segs sg, const T* rhs, T* xv, T* rv, T* cvec, double
     });
 }
 
+// Coarse inverse layout: one dense block per connected component; aggregate a's row
+// starts at row[a] and spans the len[a] aggregates of its component, base[a] the first.
+struct Coarse {
+    const int32_t* base;
+    const int32_t* len;
+    const long long* row;
+};
+
 // Two-level preconditioner, one warp per vertex segment: the warp of aggregate a forms
-// y_a = (E^-1 c)_a (row a of the dense coarse inverse times the restricted residual) and
+// y_a = (E^-1 c)_a (row a of the component's dense coarse inverse times the restricted
+// residual of that component) and
 // sets z = r / diag + y_a on the aggregate's vertices; vertices in no aggregate get
 // z = r / diag.  Partial r.z; last block: beta = r.z / previous r.z (0 at the start of a
 // solve, where p = z is also written as the first direction).
 template <typename T>
-__global__ void precond_kernel(Segs sg, int nagg, const double* diag, const T* rv, T* zv, T* pv, const T* einv,
+__global__ void precond_kernel(Segs sg, Coarse cs, const double* diag, const T* rv, T* zv, T* pv, const T* einv,
                                const T* cvec, double* partials, unsigned int* counter, double* scal, int start) {
     if (scal[S_DONE] != 0.0 && !start) return;
     const int lane = threadIdx.x & 31;
@@ -464,9 +501,11 @@ __global__ void precond_kernel(Segs sg, int nagg, const double* diag, const T* r
         const int ag = sg.agg[k];
         T y = (T)0;
         if (ag >= 0) {
-            const T* row = einv + (size_t)ag * nagg;
+            const T* row = einv + cs.row[ag];
+            const T* cb = cvec + cs.base[ag];
+            const int len = cs.len[ag];
 #pragma unroll 4
-            for (int j = lane; j < nagg; j += 32) y += row[j] * cvec[j];
+            for (int j = lane; j < len; j += 32) y += row[j] * cb[j];
             for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
             y = __shfl_sync(0xffffffffu, y, 0);
         }
@@ -562,7 +601,8 @@ __device__ __forceinline__ bool grid_sum(double v, double* partials, unsigned in
 
 template <typename T>
 struct PcgArgs {
-    int n, width, nagg, max_iter;
+    int n, width, max_iter;
+    Coarse cs;
     const int32_t* col;
     const T* a;
     const double* diag;
@@ -600,9 +640,11 @@ __global__ void __launch_bounds__(kBlock) pcg_persistent_kernel(PcgArgs<T> P) {
             const int ag = __ldg(&P.sg.agg[k]);
             T y = (T)0;
             if (ag >= 0) {
-                const T* row = P.einv + (size_t)ag * P.nagg;
+                const T* row = P.einv + __ldg(&P.cs.row[ag]);
+                const T* cb = P.c + __ldg(&P.cs.base[ag]);
+                const int len = __ldg(&P.cs.len[ag]);
 #pragma unroll 4
-                for (int j = lane; j < P.nagg; j += 32) y += __ldg(&row[j]) * __ldcg(&P.c[j]);
+                for (int j = lane; j < len; j += 32) y += __ldg(&row[j]) * __ldcg(&cb[j]);
                 for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
                 y = __shfl_sync(0xffffffffu, y, 0);
             }
@@ -797,12 +839,13 @@ static void spd_inverse(int n, std::vector<double>& E) {
         }
 }
 
-// Aggregates: the bounding box cut into bins of about `target` vertices (bins per axis in
-// proportion to the box's extent); clamped vertices belong to none.  Returns the count.
-static int make_aggregates(int n, const std::vector<double>& X, const std::vector<uint8_t>& clamped, int target,
-                           std::vector<int32_t>& agg) {
+// Aggregates of one connected component: its bounding box cut into bins of about `target`
+// vertices (bins per axis in proportion to the box's extent); clamped vertices belong to
+// none.  Aggregate ids start at `base`; returns how many this component has.
+static int make_aggregates(const std::vector<int32_t>& verts, const std::vector<double>& X,
+                           const std::vector<uint8_t>& clamped, int target, int base, std::vector<int32_t>& agg) {
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int i = 0; i < n; ++i)
+    for (int i : verts)
         for (int c = 0; c < 3; ++c) {
             lo[c] = std::min(lo[c], X[(size_t)i * 3 + c]);
             hi[c] = std::max(hi[c], X[(size_t)i * 3 + c]);
@@ -812,25 +855,26 @@ static int make_aggregates(int n, const std::vector<double>& X, const std::vecto
         ext[c] = std::max(hi[c] - lo[c], 1e-12);
         vol *= ext[c];
     }
-    double k = std::max(1.0, (double)n / target);
+    double k = std::max(1.0, (double)verts.size() / target);
     double s = std::cbrt(vol / k);
     long nb[3];
     for (int c = 0; c < 3; ++c) nb[c] = std::max(1L, (long)std::llround(ext[c] / s));
-    std::vector<long> lin(n);
-    for (int i = 0; i < n; ++i) {
+    std::vector<long> lin(verts.size()), keys;
+    for (size_t q = 0; q < verts.size(); ++q) {
+        const int i = verts[q];
         long id[3];
         for (int c = 0; c < 3; ++c)
             id[c] = std::min(nb[c] - 1, (long)((X[(size_t)i * 3 + c] - lo[c]) / ext[c] * nb[c]));
-        lin[i] = id[0] + nb[0] * (id[1] + nb[1] * id[2]);
+        lin[q] = id[0] + nb[0] * (id[1] + nb[1] * id[2]);
+        if (!clamped[i]) keys.push_back(lin[q]);
     }
-    std::vector<long> keys;
-    for (int i = 0; i < n; ++i)
-        if (!clamped[i]) keys.push_back(lin[i]);
     std::sort(keys.begin(), keys.end());
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
-    agg.assign(n, -1);
-    for (int i = 0; i < n; ++i)
-        if (!clamped[i]) agg[i] = (int32_t)(std::lower_bound(keys.begin(), keys.end(), lin[i]) - keys.begin());
+    for (size_t q = 0; q < verts.size(); ++q) {
+        const int i = verts[q];
+        agg[i] = clamped[i] ? -1
+                            : base + (int32_t)(std::lower_bound(keys.begin(), keys.end(), lin[q]) - keys.begin());
+    }
     return (int)keys.size();
 }
 
@@ -893,37 +937,73 @@ void EFieldSystem::build_matrix(double dt_ms, cudaStream_t stream) {
     if (ntris)
         SG_CUDA(cudaMemcpyAsync(d_tri_iclamp, tri_iclamp.data(), tri_iclamp.size() * 8, cudaMemcpyHostToDevice,
                                 stream));
-    // Coarse space of the two-level preconditioner: about 1000 aggregates (>= 16 vertices
-    // each), E = Z^T A Z over the unclamped system, inverted densely.
-    std::vector<int32_t> agg;
-    const int target = std::max(16, n / 1000);
-    const int na = make_aggregates(n, verts_um, vclamped, target, agg);
-    std::vector<double> E((size_t)na * na, 0.0);
+    // Coarse space of the two-level preconditioner, per connected component of the vertex
+    // graph (no edge joins two components, so E = Z^T A Z is block diagonal): about 1000
+    // aggregates (>= 16 vertices each) per component, each block inverted densely and
+    // stored row-major one after another.
+    std::vector<int32_t> agg(n, -1);
+    std::vector<int32_t> cbase(ncomp_v + 1, 0);
+    for (int c = 0; c < ncomp_v; ++c) {
+        const int target = std::max(16, (int)comp_verts[c].size() / 1000);
+        cbase[c + 1] = cbase[c] + make_aggregates(comp_verts[c], verts_um, vclamped, target, cbase[c], agg);
+    }
+    const int na = cbase[ncomp_v];
+    std::vector<int32_t> h_agg_base(std::max(na, 1), 0), h_agg_len(std::max(na, 1), 0);
+    std::vector<long long> h_agg_row(std::max(na, 1), 0), boff(ncomp_v + 1, 0);
+    for (int c = 0; c < ncomp_v; ++c) {
+        const long long m = cbase[c + 1] - cbase[c];
+        boff[c + 1] = boff[c] + m * m;
+        for (int a = cbase[c]; a < cbase[c + 1]; ++a) {
+            h_agg_base[a] = cbase[c];
+            h_agg_len[a] = (int32_t)m;
+            h_agg_row[a] = boff[c] + (long long)(a - cbase[c]) * m;
+        }
+    }
+    std::vector<double> E((size_t)boff[ncomp_v], 0.0);
     for (int i = 0; i < n; ++i) {
-        if (agg[i] < 0) continue;
-        E[(size_t)agg[i] * na + agg[i]] += diag[i];
+        const int ai = agg[i];
+        if (ai < 0) continue;
+        double* row = &E[(size_t)h_agg_row[ai]];
+        const int b0 = h_agg_base[ai];
+        row[ai - b0] += diag[i];
         for (int w = 0; w < width; ++w) {
             int j = acol[(size_t)w * n + i];
             if (j < 0) break;
-            E[(size_t)agg[i] * na + agg[j]] += a64[(size_t)w * n + i];
+            row[agg[j] - b0] += a64[(size_t)w * n + i];
         }
     }
-    if (na > 0) spd_inverse(na, E);
+    for (int c = 0; c < ncomp_v; ++c) {
+        const int m = cbase[c + 1] - cbase[c];
+        if (m == 0) continue;
+        std::vector<double> blk(E.begin() + boff[c], E.begin() + boff[c + 1]);
+        spd_inverse(m, blk);
+        std::copy(blk.begin(), blk.end(), E.begin() + boff[c]);
+    }
     std::vector<float> E32(E.begin(), E.end());
-    if (na != nagg || !d_agg) {
+    if (na != nagg || (size_t)boff[ncomp_v] != einv_len || !d_agg) {
         dfree(d_einv64);
         dfree(d_einv32);
         dfree(d_c64);
         dfree(d_c32);
+        dfree(d_agg_base);
+        dfree(d_agg_len);
+        dfree(d_agg_row);
         size_t m = std::max(na, 1);
-        dalloc(d_einv64, m * m);
-        dalloc(d_einv32, m * m);
+        einv_len = (size_t)boff[ncomp_v];
+        dalloc(d_einv64, std::max<size_t>(einv_len, 1));
+        dalloc(d_einv32, std::max<size_t>(einv_len, 1));
         dalloc(d_c64, m);
         dalloc(d_c32, m);
+        dalloc(d_agg_base, m);
+        dalloc(d_agg_len, m);
+        dalloc(d_agg_row, m);
         if (!d_agg) dalloc(d_agg, n);
         nagg = na;
     }
     SG_CUDA(cudaMemcpyAsync(d_agg, agg.data(), agg.size() * 4, cudaMemcpyHostToDevice, stream));
+    SG_CUDA(cudaMemcpyAsync(d_agg_base, h_agg_base.data(), h_agg_base.size() * 4, cudaMemcpyHostToDevice, stream));
+    SG_CUDA(cudaMemcpyAsync(d_agg_len, h_agg_len.data(), h_agg_len.size() * 4, cudaMemcpyHostToDevice, stream));
+    SG_CUDA(cudaMemcpyAsync(d_agg_row, h_agg_row.data(), h_agg_row.size() * 8, cudaMemcpyHostToDevice, stream));
     // Segments: each aggregate's vertices in ascending order, then the vertices of no
     // aggregate (clamped) in chunks of 256.
     std::vector<int32_t> sptr(1, 0), sidx, sagg;
@@ -963,7 +1043,7 @@ void EFieldSystem::build_matrix(double dt_ms, cudaStream_t stream) {
     SG_CUDA(cudaMemcpyAsync(d_seg_ptr, sptr.data(), sptr.size() * 4, cudaMemcpyHostToDevice, stream));
     SG_CUDA(cudaMemcpyAsync(d_seg_idx, sidx.data(), sidx.size() * 4, cudaMemcpyHostToDevice, stream));
     if (nseg) SG_CUDA(cudaMemcpyAsync(d_seg_agg, sagg.data(), sagg.size() * 4, cudaMemcpyHostToDevice, stream));
-    if (na) {
+    if (!E.empty()) {
         SG_CUDA(cudaMemcpyAsync(d_einv64, E.data(), E.size() * 8, cudaMemcpyHostToDevice, stream));
         SG_CUDA(cudaMemcpyAsync(d_einv32, E32.data(), E32.size() * 4, cudaMemcpyHostToDevice, stream));
     }
@@ -982,7 +1062,8 @@ void EFieldSystem::pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv
                             T* qv, const T* einv, T* cvec, double* h) {
     const Segs sg{nseg, d_seg_ptr, d_seg_idx, d_seg_agg};
     const int gs = seg_grid();
-    precond_kernel<T><<<gs, kBlock, 0, stream>>>(sg, nagg, diag64, rv, zv, pv, einv, cvec, red, red_count, scal, 1);
+    const Coarse cs{d_agg_base, d_agg_len, d_agg_row};
+    precond_kernel<T><<<gs, kBlock, 0, stream>>>(sg, cs, diag64, rv, zv, pv, einv, cvec, red, red_count, scal, 1);
     T* pin = pv;
     T* pout = pv2;
     const int chunk = 8;
@@ -991,7 +1072,7 @@ void EFieldSystem::pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv
             spmv_kernel<T><<<g, kBlock, 0, stream>>>(n, width, acol_dev, a, diag64, zv, pin, pout, qv, red, red_count,
                                                      scal);
             update_kernel<T><<<gs, kBlock, 0, stream>>>(sg, xv, rv, pout, qv, cvec, red, red_count, scal, max_iter);
-            precond_kernel<T><<<gs, kBlock, 0, stream>>>(sg, nagg, diag64, rv, zv, nullptr, einv, cvec, red,
+            precond_kernel<T><<<gs, kBlock, 0, stream>>>(sg, cs, diag64, rv, zv, nullptr, einv, cvec, red,
                                                          red_count, scal, 0);
             std::swap(pin, pout);
         }
@@ -1013,7 +1094,7 @@ void EFieldSystem::pcg_persistent(cudaStream_t stream, int n, const T* a, T* xv,
     PcgArgs<T> P;
     P.n = n;
     P.width = width;
-    P.nagg = nagg;
+    P.cs = Coarse{d_agg_base, d_agg_len, d_agg_row};
     P.max_iter = max_iter;
     P.col = acol_dev;
     P.a = a;

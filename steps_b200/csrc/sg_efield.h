@@ -75,6 +75,12 @@ struct EFieldSystem {
     // bins (piecewise-constant coarse space), E = Z^T A Z is inverted densely on the host.
     std::vector<double> verts_um;         // [nverts][3] for the aggregation
     int nagg = 0;
+    int ncomp_v = 0;                      // connected components of the vertex graph
+    std::vector<std::vector<int32_t>> comp_verts;  // their vertices, ascending
+    size_t einv_len = 0;                  // sum over components of (aggregates)^2
+    int32_t* d_agg_base = nullptr;        // [nagg] first aggregate of the aggregate's component
+    int32_t* d_agg_len = nullptr;         // [nagg] aggregates in that component
+    long long* d_agg_row = nullptr;       // [nagg] offset of the aggregate's row in the coarse inverse
     int32_t* d_agg = nullptr;             // [nverts] aggregate of each vertex, -1 for clamped
     // Vertex segments for the restriction Z^T r: one per aggregate (its vertices in
     // ascending order), then chunks of the vertices in no aggregate.
@@ -82,7 +88,7 @@ struct EFieldSystem {
     int32_t* d_seg_ptr = nullptr;         // [nseg + 1]
     int32_t* d_seg_idx = nullptr;         // [nverts]
     int32_t* d_seg_agg = nullptr;         // [nseg], -1 = no aggregate
-    double* d_einv64 = nullptr;           // [nagg][nagg]
+    double* d_einv64 = nullptr;           // per component a dense [m][m] block, m its aggregates
     float* d_einv32 = nullptr;
     double* d_c64 = nullptr;              // restricted residual [nagg]
     float* d_c32 = nullptr;
@@ -98,7 +104,7 @@ struct EFieldSystem {
     double* scal = nullptr;               // device scalars
     unsigned int* red_count = nullptr;
     unsigned int* d_bar = nullptr;        // grid barrier of the persistent solve: count, generation, error
-    bool persistent = false;              // whole solve in one cooperative launch (else a launch per phase)
+    bool persistent = true;               // whole solve in one cooperative launch (else a launch per phase)
     double dt_built = -1.0;
     bool dirty = true;                    // clamps / membrane properties changed
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc0 = nullptr, evc1 = nullptr;

@@ -74,9 +74,10 @@ SG_HD sg_u32x4 sg_philox4x32(sg_u32x4 c, uint32_t k0, uint32_t k1) {
 }
 
 // Stream purposes (top byte of counter word w).
-#define SG_PURPOSE_WINDOW 0u   // SSA + diffusion of one unit in one split window
+#define SG_PURPOSE_WINDOW 0u   // reaction SSA of one unit in one split window
 #define SG_PURPOSE_SETUP 1u    // host-side placement of molecules (setters)
 #define SG_PURPOSE_EFIELD 2u   // reserved
+#define SG_PURPOSE_DIFF 16u    // + species: diffusion leave of one (unit, species) in one window
 
 // One independent stream: counter = (block, unit, window_lo, purpose<<24 | window_hi24),
 // key = (seed_lo, seed_hi + realization * W0).  Draw j of the stream is word

@@ -134,7 +134,6 @@ struct Solver {
 
     void setup_surface() {
         if (!has_surf()) return;
-        if (nreal != 1) throw NotImplErr("membrane triangles with batched realizations");
         // Surface reactions grouped by patch.
         const int RS = (int)sreacs.size();
         std::vector<int32_t> order(RS);
@@ -533,11 +532,9 @@ struct Solver {
     int check_flag() const { return (check && !any_clamp && !(has_surf() && surf_touches_volume)) ? 1 : 0; }
 
     void set_kernel_smem_limits() {
-        // Window kernels are occupancy-bound on shared memory: ask for the largest carveout.
-        SG_CUDA(cudaFuncSetAttribute(window_kernel<64>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        SG_CUDA(cudaFuncSetAttribute(window_kernel<128>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        SG_CUDA(cudaFuncSetAttribute(window_kernel<256>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        // Window kernels are occupancy-bound on shared memory: the largest carveout unless
+        // the autotuner picked another.
+        set_carveout(carveout);
         size_t sm = smem_bytes(256, nspec, (int)reacs.size());
         if (sm > 227 * 1024) throw NotImplErr("too many species for the shared-memory staging");
         if (sm > 48 * 1024) {
@@ -666,7 +663,11 @@ struct Solver {
     // min(t + efdt, endtime), then the membrane currents and the EField solve over the
     // step actually taken; the new triangle potentials feed the next windows.
     void run_with_efield(double endtime) {
-        if (nreal != 1) throw NotImplErr("EField with batched realizations");
+        // Batched realizations share the EField steps: their vertex systems are disjoint
+        // blocks of one system, so every realization must advance on the same windows.
+        for (int r = 1; r < nreal; ++r)
+            if (reals[r].t != reals[0].t || reals[r].period != reals[0].period)
+                throw NotImplErr("EField with batched realizations of different times or update periods");
         while (time() < endtime) {
             double t0 = time();
             double t1 = std::min(t0 + efdt, endtime);
@@ -731,44 +732,62 @@ struct Solver {
     // The sample path does not depend on the launch shape (every tet draws from its own
     // counter stream), so tuning runs real windows: after one untimed window, the next
     // windows of a run are timed under each candidate {block 64, 128, 256} x {occupancy-
-    // sized grid, one tet per thread} and the fastest shape is kept.
+    // sized grid, one tet per thread} with the largest shared-memory carveout, then the best
+    // of those with carveouts of 75% and 50% (fewer resident blocks, more L1 for the
+    // kernel's local memory), and the fastest is kept.
     static constexpr int kTuneWindows = 2;
-    static constexpr int kTuneCands = 6;
+    static constexpr int kTuneCands = 8;
     bool tune_pending = false;
     std::vector<float> tune_ms;
+    int carveout = 100;  // preferred shared-memory carveout of the window kernels, percent
+
+    void set_carveout(int pct) {
+        carveout = pct;
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<64>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<128>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<256>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    }
 
     uint64_t autotune(const sg_window_args& a) {
         const int blocks[3] = {64, 128, 256};
-        int best_block = block, best_grid = grid;
+        int best_block = block, best_grid = grid, best_carve = 100;
         float best = 0.0f;
         tune_ms.clear();
         cudaEvent_t e0, e1;
         SG_CUDA(cudaEventCreate(&e0));
         SG_CUDA(cudaEventCreate(&e1));
-        launch_window(a, window_grid());  // untimed: first-launch costs
-        for (int bi = 0; bi < 3; ++bi) {
-            block = blocks[bi];
-            for (int mode = 0; mode < 2; ++mode) {
-                grid = mode ? -1 : 0;
-                const int g = window_grid();
-                SG_CUDA(cudaEventRecord(e0, stream));
-                for (int i = 0; i < kTuneWindows; ++i) launch_window(a, g);
-                SG_CUDA(cudaEventRecord(e1, stream));
-                SG_CUDA(cudaEventSynchronize(e1));
-                float ms = 0.0f;
-                SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                tune_ms.push_back(ms);
-                if (tune_ms.size() == 1 || ms < best) {
-                    best = ms;
-                    best_block = block;
-                    best_grid = grid;
-                }
+        auto timed = [&](int b, int gm, int cv) {
+            block = b;
+            grid = gm;
+            set_carveout(cv);
+            const int g = window_grid();
+            SG_CUDA(cudaEventRecord(e0, stream));
+            for (int i = 0; i < kTuneWindows; ++i) launch_window(a, g);
+            SG_CUDA(cudaEventRecord(e1, stream));
+            SG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            tune_ms.push_back(ms);
+            if (tune_ms.size() == 1 || ms < best) {
+                best = ms;
+                best_block = b;
+                best_grid = gm;
+                best_carve = cv;
             }
-        }
+        };
+        set_carveout(100);
+        launch_window(a, window_grid());  // untimed: first-launch costs
+        for (int bi = 0; bi < 3; ++bi)
+            for (int mode = 0; mode < 2; ++mode) timed(blocks[bi], mode ? -1 : 0, 100);
+        const int bb = best_block, bg = best_grid;
+        timed(bb, bg, 75);
+        timed(bb, bg, 50);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         block = best_block;
         grid = best_grid;
+        set_carveout(best_carve);
         tune_pending = false;
         return (uint64_t)kTuneWindows * kTuneCands + 1;
     }
@@ -1106,26 +1125,34 @@ struct Solver {
         h2d(d_tri_counts.p + (size_t)s * ntris + m, &c, 1);
         sync();
     }
-    double get_patch_count(int p, int s) {
+    // A triangle belongs to the realization of its inner tet; real = -1 selects all.
+    bool tri_in(int m, int p, int real) const {
+        if (tri_patch[m] != p) return false;
+        if (real < 0) return true;
+        return tri_inner[m] >= real_begin[real] && tri_inner[m] < real_begin[real + 1];
+    }
+    double get_patch_count(int p, int s, int real) {
         check_tri(0, s);
+        if (real >= 0) check_real(real);
         std::vector<uint32_t> v(ntris);
         d2h(v.data(), d_tri_counts.p + (size_t)s * ntris, ntris);
         sync();
         unsigned long long sum = 0;
         for (int m = 0; m < ntris; ++m)
-            if (tri_patch[m] == p) sum += v[m];
+            if (tri_in(m, p, real)) sum += v[m];
         return (double)sum;
     }
-    void set_patch_count(int p, int s, double n) {
+    void set_patch_count(int p, int s, int real, double n) {
         check_tri(0, s);
         if (p < 0 || p >= npatch) throw ArgErr("patch index out of range");
+        if (real >= 0) check_real(real);
         if (!(n >= 0.0) || n > 4294967295.0) throw ArgErr("count out of range");
         std::vector<uint32_t> v(ntris);
         d2h(v.data(), d_tri_counts.p + (size_t)s * ntris, ntris);
         sync();
         std::vector<int> tris;
         for (int m = 0; m < ntris; ++m)
-            if (tri_patch[m] == p) tris.push_back(m);
+            if (tri_in(m, p, real)) tris.push_back(m);
         sg_stream st = setup_stream();
         distribute_w(n, tris, tri_area, v, &st);
         h2d(d_tri_counts.p + (size_t)s * ntris, v.data(), (size_t)ntris);
@@ -1663,6 +1690,13 @@ int sg_get_launch(sg_solver* h, int32_t* block, int32_t* grid) {
     });
 }
 
+int sg_get_carveout(sg_solver* h, int32_t* percent) {
+    return guarded([&] {
+        need(percent, "percent");
+        *percent = S(h)->carveout;
+    });
+}
+
 int sg_set_autotune(sg_solver* h, int32_t on) {
     return guarded([&] { S(h)->tune_pending = on != 0; });
 }
@@ -1812,15 +1846,15 @@ int sg_set_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double n) {
     return guarded([&] { S(h)->set_tri_count(tri, sspec, n); });
 }
 
-int sg_get_patch_count(sg_solver* h, int32_t patch, int32_t sspec, double* n) {
+int sg_get_patch_count(sg_solver* h, int32_t patch, int32_t sspec, int32_t real, double* n) {
     return guarded([&] {
         need(n, "n");
-        *n = S(h)->get_patch_count(patch, sspec);
+        *n = S(h)->get_patch_count(patch, sspec, real);
     });
 }
 
-int sg_set_patch_count(sg_solver* h, int32_t patch, int32_t sspec, double n) {
-    return guarded([&] { S(h)->set_patch_count(patch, sspec, n); });
+int sg_set_patch_count(sg_solver* h, int32_t patch, int32_t sspec, int32_t real, double n) {
+    return guarded([&] { S(h)->set_patch_count(patch, sspec, real, n); });
 }
 
 int sg_get_tri_ohmic_i(sg_solver* h, int32_t tri, double* amps) {

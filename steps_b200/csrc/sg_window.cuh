@@ -444,6 +444,9 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             uint32_t pop = L.cnt[s * BLOCK + tid];
             uint4 k = make_uint4(0u, 0u, 0u, 0u);
             if (pop > 0u) {
+                // Each (tet, species) leaves on its own stream, so the leave of a species
+                // does not depend on how many draws the SSA or another species took.
+                sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)tlocal, w, SG_PURPOSE_DIFF + (uint32_t)s);
                 double t1 = T * (D * G);
                 if (t1 >= 1.0) t1 = 1.0;
                 const double sd = L.tdel[s * BLOCK + tid];

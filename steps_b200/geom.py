@@ -186,6 +186,43 @@ class Memb:
         mesh.membs[id] = self
 
 
+def replicate(mesh, n, gap=None):
+    """n disjoint copies of mesh in one Tetmesh (batched realizations of one geometry): copy r
+    is shifted along x by r * (extent + gap) and owns tets [r T, (r + 1) T); every derived
+    array is tiled from the original instead of recomputed.  offsets holds the
+    realization tet ranges."""
+    T, V, M = mesh.ntets, mesh.nverts, mesh.ntris
+    lo, hi = mesh.verts.min(axis=0), mesh.verts.max(axis=0)
+    step = (hi[0] - lo[0]) + (gap if gap is not None else 0.25 * (hi[0] - lo[0]))
+    shift = np.zeros((n, 1, 3))
+    shift[:, 0, 0] = step * np.arange(n)
+
+    def tile_idx(a, per):
+        r = np.arange(n).reshape((n,) + (1,) * a.ndim) * per
+        out = np.where(a[None] >= 0, a[None] + r, a[None])
+        return out.reshape((-1,) + a.shape[1:])
+
+    m = object.__new__(Tetmesh)
+    m.verts = np.ascontiguousarray((mesh.verts[None] + shift).reshape(-1, 3))
+    m.tets = np.ascontiguousarray(tile_idx(mesh.tets, V))
+    m.ntets, m.nverts = n * T, n * V
+    m.comps, m.patches = {}, {}
+    m.tet_vol = np.tile(mesh.tet_vol, n)
+    m.tet_bary = (mesh.tet_bary[None] + shift).reshape(-1, 3)
+    m.tet_area = np.tile(mesh.tet_area, (n, 1))
+    m.tet_neighb = tile_idx(mesh.tet_neighb, T)
+    m.face_key = tile_idx(mesh.face_key, V)
+    m.tet_dist = np.tile(mesh.tet_dist, (n, 1))
+    m.tris = tile_idx(mesh.tris, V)
+    m.ntris = n * M
+    m.tet_tri = tile_idx(mesh.tet_tri, M)
+    m.tri_tets = tile_idx(mesh.tri_tets, T)
+    m.tri_area = np.tile(mesh.tri_area, n)
+    m.tri_bary = (mesh.tri_bary[None] + shift).reshape(-1, 3)
+    m.offsets = np.arange(n + 1, dtype=np.int32) * T
+    return m
+
+
 def kuhn_box(nx, ny, nz, h=1.0e-7, origin=(0.0, 0.0, 0.0)):
     """Box of nx*ny*nz cubes of side h, each cut into 6 tets along its main diagonal
     (Kuhn / Freudenthal triangulation; conforming across cubes).

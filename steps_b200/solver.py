@@ -458,13 +458,15 @@ class TetOpSplit:
     def setTriSpecCount(self, tidx, s, n):
         check(self._L.sg_set_tri_count(self._h, self._tri(tidx), self._sspec(s), float(n)))
 
-    def getPatchSpecCount(self, p, s):
+    def getPatchSpecCount(self, p, s, realization=-1):
         n = C.c_double()
-        check(self._L.sg_get_patch_count(self._h, self._patch(p), self._sspec(s), C.byref(n)))
+        check(self._L.sg_get_patch_count(self._h, self._patch(p), self._sspec(s), int(realization), C.byref(n)))
         return n.value
 
-    def setPatchSpecCount(self, p, s, n):
-        check(self._L.sg_set_patch_count(self._h, self._patch(p), self._sspec(s), float(n)))
+    def setPatchSpecCount(self, p, s, n, realization=-1):
+        """Distribute n molecules over the patch's triangles by area (of one realization, or
+        of all with realization=-1)."""
+        check(self._L.sg_set_patch_count(self._h, self._patch(p), self._sspec(s), int(realization), float(n)))
 
     def getTriOhmicI(self, tidx, oc=None):
         x = C.c_double()
@@ -549,6 +551,12 @@ class TetOpSplit:
     def setLaunch(self, block, grid=0):
         check(self._L.sg_set_launch(self._h, int(block), int(grid)))
 
+    def getCarveout(self):
+        """Preferred shared-memory carveout (percent) of the window kernels."""
+        x = C.c_int32()
+        check(self._L.sg_get_carveout(self._h, C.byref(x)))
+        return x.value
+
     def getLaunch(self):
         """(block, grid) of the window kernel; grid 0 = occupancy-sized, -1 = one tet per
         thread."""
@@ -557,13 +565,14 @@ class TetOpSplit:
         return b.value, g.value
 
     def setAutotune(self, on=True):
-        """Time 12 windows of the next run (after one untimed window) under six launch
+        """Time 16 windows of the next run (after one untimed window) under eight launch
         shapes and keep the fastest (results do not depend on the shape)."""
         check(self._L.sg_set_autotune(self._h, 1 if on else 0))
 
     def getAutotuneTimes(self):
         """ms of the two timed windows under each candidate shape, in the order block
-        64, 128, 256 x grid {occupancy-sized, one tet per thread}; empty before tuning."""
+        64, 128, 256 x grid {occupancy-sized, one tet per thread} at the full shared-memory
+        carveout, then the best of those at carveouts 75% and 50%; empty before tuning."""
         buf = (C.c_float * 8)()
         n = C.c_int32()
         check(self._L.sg_get_autotune_ms(self._h, buf, 8, C.byref(n)))

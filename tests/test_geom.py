@@ -66,3 +66,21 @@ def test_two_compartments_exclusive():
     sgeom.TmComp("a", m, range(10))
     with pytest.raises(ValueError):
         sgeom.TmComp("b", m, range(5, 20))
+
+
+def test_replicate_matches_full_construction():
+    """geom.replicate tiles a mesh's derived arrays; they equal a Tetmesh built from the
+    concatenated vertices and tets."""
+    import numpy as np
+
+    from steps_b200 import geom as G
+
+    m = G.kuhn_box(3, 2, 4, 1e-7)
+    r = G.replicate(m, 3)
+    t = G.Tetmesh(r.verts, r.tets)
+    for k in ["tet_vol", "tet_area", "tet_neighb", "tet_dist", "tris", "tet_tri", "tri_tets", "tri_area",
+              "tri_bary", "tet_bary"]:
+        a, b = getattr(r, k), getattr(t, k)
+        assert a.shape == b.shape and np.allclose(a, b), k
+    assert list(r.offsets) == [0, m.ntets, 2 * m.ntets, 3 * m.ntets]
+    assert len(r.getSurfTris()) == 3 * len(m.getSurfTris())

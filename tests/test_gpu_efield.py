@@ -59,8 +59,9 @@ def rallpack1_sim(method):
     return sim, extrema(zmin_v), extrema(zmax_v), d["v0"], d["vx"]
 
 
+@pytest.mark.parametrize("persistent", [False, True])
 @pytest.mark.parametrize("method,rtol", [(EF_DV_CG_FP64, 1e-9), (EF_DV_CG_MIXED, 1e-7)])
-def test_efield_steps_match_fp64_direct_solve(steps_lib, method, rtol):
+def test_efield_steps_match_fp64_direct_solve(steps_lib, method, rtol, persistent):
     """20 EField steps on a 4x4x10 Kuhn box (membrane = every boundary triangle, leak,
     a current clamp, one voltage-clamped vertex) against the FP64 direct-solve oracle."""
     from oracle.efield_oracle import EFieldOracle
@@ -73,6 +74,7 @@ def test_efield_steps_match_fp64_direct_solve(steps_lib, method, rtol):
     mdl = smodel.Model()
     smodel.Volsys("vsys", mdl)
     sim = TetOpSplit(mdl, mesh, make_rng(3), method)
+    sim.setEfieldPersistent(persistent)
     sim.setEfieldTolerance(1e-12, 1e-4)
     sim.setEfieldDT(1e-6)
     sim.setMembPotential("membrane", -0.065)
@@ -118,7 +120,8 @@ def test_rallpack1_membres(steps_lib, method):
     assert rms0 < 1.0e-3 and rmsx < 1.0e-3, (rms0, rmsx, iters / steps)
 
 
-def test_mixed_step_check_against_fp64(steps_lib):
+@pytest.mark.parametrize("persistent", [False, True])
+def test_mixed_step_check_against_fp64(steps_lib, persistent):
     """The mixed method's per-step check: every step's V from the FP32-inner solve is within
     1e-6 relative of an FP64 solve of the same system; an FP64-method solver refuses nothing
     and records no check steps."""
@@ -130,6 +133,7 @@ def test_mixed_step_check_against_fp64(steps_lib):
     mdl = smodel.Model()
     smodel.Volsys("vsys", mdl)
     sim = TetOpSplit(mdl, mesh, make_rng(4), EF_DV_CG_MIXED)
+    sim.setEfieldPersistent(persistent)
     sim.setEfieldTolerance(1e-10, 1e-4)
     sim.setEfieldCheck(True, 1e-12)
     sim.setEfieldDT(1e-6)

@@ -159,7 +159,7 @@ def test_launch_shapes_agree(steps_lib, block):
 
 
 def test_autotuned_run_matches_oracle(steps_lib):
-    """Autotuning times 12 windows (after an untimed one) under six launch shapes; the
+    """Autotuning times 16 windows (after an untimed one) under eight launch shapes; the
     counts after the run still equal the oracle's, and the kept shape is a candidate."""
     mesh = W.cube_mesh(9)
     sim, ora = pair(W.random_network(3), mesh, seed=6)
@@ -168,12 +168,13 @@ def test_autotuned_run_matches_oracle(steps_lib):
         sim.setSpecCounts(s, rows[i])
     sync_counts(sim, ora)
     sim.setAutotune(True)
-    t = 40 * sim.getUpdPeriod()
+    t = 48 * sim.getUpdPeriod()
     sim.run(t)
     ora.run(t)
     assert_same(sim, ora, "autotuned run")
     times = sim.getAutotuneTimes()
-    assert len(times) == 6 and all(x > 0.0 for x in times)
+    assert len(times) == 8 and all(x > 0.0 for x in times)
+    assert sim.getCarveout() in (100, 75, 50)
     block, grid = sim.getLaunch()
     assert block in (64, 128, 256) and grid in (0, -1)
     sim.run(2 * t)
