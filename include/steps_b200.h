@@ -184,14 +184,20 @@ int sg_set_efield_persistent(sg_solver* h, int32_t on);
  * (blocks stride over the tets), -1 = one tet per thread. */
 int sg_set_launch(sg_solver* h, int32_t block, int32_t grid);
 int sg_get_launch(sg_solver* h, int32_t* block, int32_t* grid);
-/* Autotune the launch shape at the next run() with more than 17 windows: after one
+/* Autotune the launch shape at the next run() with more than 19 windows: after one
  * untimed window, two windows each are timed under block {64,128,256} x grid
  * {occupancy-sized (0), one tet per thread (-1)} with the full shared-memory carveout, then
- * the best of those with carveouts 75% and 50%; the fastest is kept (the sample path does
- * not depend on the shape).  The eight timings (ms, in that order) are read back with
- * sg_get_autotune_ms, the kept carveout with sg_get_carveout. */
+ * the best of those with carveouts 75% and 50% and as a split window; the fastest is kept
+ * (the sample path does not depend on the shape).  The nine timings (ms, in that order)
+ * are read back with sg_get_autotune_ms, the kept carveout with sg_get_carveout. */
 int sg_set_autotune(sg_solver* h, int32_t on);
 int sg_get_carveout(sg_solver* h, int32_t* percent);
+/* Window as two kernels: reactions (gather, SSA) with one thread per tet, then the
+ * diffusion leave with one thread per (diffusing species, tet); the same results as the
+ * fused kernel.  Models with membrane triangles always run fused.  The autotuner also
+ * tries it (after the carveouts: a ninth candidate). */
+int sg_set_split(sg_solver* h, int32_t on);
+int sg_get_split(sg_solver* h, int32_t* on);
 int sg_get_autotune_ms(sg_solver* h, float* ms, int32_t cap, int32_t* count);
 /* Replay window launches from a captured CUDA graph of 16 windows (on by default). */
 int sg_set_graphs(sg_solver* h, int32_t on);

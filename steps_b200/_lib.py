@@ -80,6 +80,8 @@ PROTOTYPES = {
     "sg_get_launch": [_P, _pi32, _pi32],
     "sg_set_autotune": [_P, _i32],
     "sg_get_carveout": [_P, _pi32],
+    "sg_set_split": [_P, _i32],
+    "sg_get_split": [_P, _pi32],
     "sg_get_autotune_ms": [_P, C.POINTER(C.c_float), _i32, _pi32],
     "sg_set_conservation_check": [_P, _i32],
     "sg_set_graphs": [_P, _i32],

@@ -97,7 +97,9 @@ struct Solver {
 
     // ---- device state ----
     DevBuf<uint32_t> d_counts, d_outflow, d_clamp, d_status;
-    DevBuf<int32_t> d_nbr, d_comp, d_crb, d_dslot;
+    DevBuf<int32_t> d_nbr, d_comp, d_crb, d_dslot, d_dspec;
+    DevBuf<double> d_tdel;                      // [D][T] split mode only
+    bool split = false;                         // window as two kernels (reactions, diffusion)
     DevBuf<float> d_geo;
     DevBuf<double> d_ivs, d_kcst, d_dcst;
     DevBuf<sg_reac> d_reacs;
@@ -358,6 +360,13 @@ struct Solver {
         if (R) h2d(d_reacs.p, reacs.data(), reacs.size());
         h2d(d_crb.p, comp_reac_begin.data(), comp_reac_begin.size());
         h2d(d_dslot.p, diff_slot.data(), diff_slot.size());
+        {
+            std::vector<int32_t> dspec(std::max(ndiff, 1), 0);
+            for (int s = 0; s < nspec; ++s)
+                if (diff_slot[s] >= 0) dspec[diff_slot[s]] = s;
+            d_dspec.alloc(dspec.size());
+            h2d(d_dspec.p, dspec.data(), dspec.size());
+        }
         reals.assign(nreal, sg_real{});
         for (int r = 0; r < nreal; ++r) {
             reals[r].tet_begin = real_begin[r];
@@ -512,6 +521,8 @@ struct Solver {
         a.status = d_status.p;
         a.surf = surf_args();
         a.surf_ext = has_surf() ? d_surf_ext.p : nullptr;
+        a.tdel = d_tdel.p;
+        a.diff_spec = d_dspec.p;
         a.ntets = ntets;
         a.nspec = nspec;
         a.ndiff = ndiff;
@@ -541,6 +552,9 @@ struct Solver {
             SG_CUDA(cudaFuncSetAttribute(window_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             SG_CUDA(cudaFuncSetAttribute(window_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             SG_CUDA(cudaFuncSetAttribute(window_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            SG_CUDA(cudaFuncSetAttribute(window_kernel<64, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            SG_CUDA(cudaFuncSetAttribute(window_kernel<128, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            SG_CUDA(cudaFuncSetAttribute(window_kernel<256, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         }
         if (has_surf()) {
             size_t ss = window_smem();
@@ -574,11 +588,28 @@ struct Solver {
         return (int)std::max(1L, std::min(need, cap));
     }
 
+    bool use_split() const { return split && !has_surf(); }
+    void ensure_split_buffers() {
+        if (!d_tdel.p && ndiff > 0) d_tdel.alloc((size_t)ndiff * ntets);
+    }
+
     void launch_window(const sg_window_args& a, int g) {
         size_t sm = window_smem();
         int chk = check_flag();
         if (has_surf()) {
             window_kernel<128, true><<<g, 128, sm, stream>>>(a, chk);
+        } else if (use_split()) {
+            if (ndiff > 0 && !a.tdel) throw ProgErr("split window without its buffers");
+            switch (block) {
+                case 64: window_kernel<64, false, true><<<g, 64, sm, stream>>>(a, chk); break;
+                case 128: window_kernel<128, false, true><<<g, 128, sm, stream>>>(a, chk); break;
+                case 256: window_kernel<256, false, true><<<g, 256, sm, stream>>>(a, chk); break;
+                default: throw ArgErr("block size must be 64, 128 or 256");
+            }
+            SG_CUDA(cudaGetLastError());
+            const long long pairs = (long long)ndiff * ntets;
+            const int gd = (int)std::max(1LL, std::min((pairs + 255) / 256, (long long)nsm * 64));
+            diffuse_kernel<256><<<gd, 256, 0, stream>>>(a, chk);
         } else {
             switch (block) {
                 case 64: window_kernel<64><<<g, 64, sm, stream>>>(a, chk); break;
@@ -595,7 +626,7 @@ struct Solver {
     bool use_graphs = true;
     cudaGraphExec_t graph_exec = nullptr;
     sg_window_args graph_args{};
-    int graph_grid = -1, graph_block = -1, graph_check = -1;
+    int graph_grid = -1, graph_block = -1, graph_check = -1, graph_split = -1;
 
     void drop_graph() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -605,7 +636,7 @@ struct Solver {
     cudaGraphExec_t window_graph(const sg_window_args& a, int g) {
         int chk = check_flag();
         if (graph_exec && g == graph_grid && block == graph_block && chk == graph_check &&
-            std::memcmp(&a, &graph_args, sizeof(a)) == 0)
+            (int)use_split() == graph_split && std::memcmp(&a, &graph_args, sizeof(a)) == 0)
             return graph_exec;
         drop_graph();
         cudaGraph_t graph = nullptr;
@@ -625,6 +656,7 @@ struct Solver {
         graph_grid = g;
         graph_block = block;
         graph_check = chk;
+        graph_split = (int)use_split();
         return graph_exec;
     }
 
@@ -736,7 +768,7 @@ struct Solver {
     // of those with carveouts of 75% and 50% (fewer resident blocks, more L1 for the
     // kernel's local memory), and the fastest is kept.
     static constexpr int kTuneWindows = 2;
-    static constexpr int kTuneCands = 8;
+    static constexpr int kTuneCands = 9;
     bool tune_pending = false;
     std::vector<float> tune_ms;
     int carveout = 100;  // preferred shared-memory carveout of the window kernels, percent
@@ -746,6 +778,9 @@ struct Solver {
         SG_CUDA(cudaFuncSetAttribute(window_kernel<64>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         SG_CUDA(cudaFuncSetAttribute(window_kernel<128>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         SG_CUDA(cudaFuncSetAttribute(window_kernel<256>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<64, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<128, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<256, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
     }
 
@@ -757,13 +792,17 @@ struct Solver {
         cudaEvent_t e0, e1;
         SG_CUDA(cudaEventCreate(&e0));
         SG_CUDA(cudaEventCreate(&e1));
-        auto timed = [&](int b, int gm, int cv) {
+        bool best_split = false;
+        ensure_split_buffers();
+        const sg_window_args as = window_args();  // with the split buffers
+        auto timed = [&](int b, int gm, int cv, bool sp) {
             block = b;
             grid = gm;
+            split = sp;
             set_carveout(cv);
             const int g = window_grid();
             SG_CUDA(cudaEventRecord(e0, stream));
-            for (int i = 0; i < kTuneWindows; ++i) launch_window(a, g);
+            for (int i = 0; i < kTuneWindows; ++i) launch_window(as, g);
             SG_CUDA(cudaEventRecord(e1, stream));
             SG_CUDA(cudaEventSynchronize(e1));
             float ms = 0.0f;
@@ -774,19 +813,23 @@ struct Solver {
                 best_block = b;
                 best_grid = gm;
                 best_carve = cv;
+                best_split = sp;
             }
         };
         set_carveout(100);
-        launch_window(a, window_grid());  // untimed: first-launch costs
+        split = false;
+        launch_window(as, window_grid());  // untimed: first-launch costs
         for (int bi = 0; bi < 3; ++bi)
-            for (int mode = 0; mode < 2; ++mode) timed(blocks[bi], mode ? -1 : 0, 100);
+            for (int mode = 0; mode < 2; ++mode) timed(blocks[bi], mode ? -1 : 0, 100, false);
         const int bb = best_block, bg = best_grid;
-        timed(bb, bg, 75);
-        timed(bb, bg, 50);
+        timed(bb, bg, 75, false);
+        timed(bb, bg, 50, false);
+        timed(bb, bg, 100, true);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         block = best_block;
         grid = best_grid;
+        split = best_split;
         set_carveout(best_carve);
         tune_pending = false;
         return (uint64_t)kTuneWindows * kTuneCands + 1;
@@ -805,7 +848,14 @@ struct Solver {
         if (n == 0) return 0;
         sg_window_args a = window_args();
         uint64_t done = 0;
-        if (tune_pending && !has_surf() && n > (uint64_t)kTuneWindows * kTuneCands + 1) done = autotune(a);
+        if (tune_pending && !has_surf() && n > (uint64_t)kTuneWindows * kTuneCands + 1) {
+            done = autotune(a);
+            a = window_args();  // the tuner may have allocated the split buffers
+        }
+        if (use_split()) {
+            ensure_split_buffers();
+            a = window_args();
+        }
         int g = window_grid();
         if (profiling) SG_CUDA(cudaEventRecord(ev_begin, stream));
         // Windows advance their own time on the device, so a captured chunk of window
@@ -1687,6 +1737,17 @@ int sg_get_launch(sg_solver* h, int32_t* block, int32_t* grid) {
     return guarded([&] {
         if (block) *block = S(h)->block;
         if (grid) *grid = S(h)->grid;
+    });
+}
+
+int sg_set_split(sg_solver* h, int32_t on) {
+    return guarded([&] { S(h)->split = on != 0; });
+}
+
+int sg_get_split(sg_solver* h, int32_t* on) {
+    return guarded([&] {
+        need(on, "on");
+        *on = S(h)->use_split() ? 1 : 0;
     });
 }
 

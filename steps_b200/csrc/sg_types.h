@@ -128,6 +128,8 @@ typedef struct sg_window_args {
     uint32_t* status;                  // device error word
     sg_surf_args surf;                 // membrane triangles (SURF kernels only)
     unsigned long long* surf_ext;      // [1] surface reaction events since reset
+    double* tdel;                      // [D][T] change-time sums handed to the diffusion kernel (split mode)
+    const int32_t* diff_spec;          // [D]: species of each diffusing index
     int32_t ntets;                     // total tets over realizations
     int32_t nspec;
     int32_t ndiff;

@@ -322,17 +322,142 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
     }
 }
 
+// Diffusion leave of one (tet, species) with pop > 0 molecules (TOS:1633-1712,
+// diff.cpp:473-585): the occupancy mean n = c_end - sd / T with a Bernoulli on its
+// fraction, Binomial(n, min(1, T D G)) leaving, split over the faces by conditional
+// binomials on the selectors c0..c2 (the last face takes the rest).  Each (tet, species)
+// draws from its own stream (purpose SG_PURPOSE_DIFF + species), so the result does not
+// depend on the SSA's draws, on the other species or on which kernel runs it.
+__device__ __forceinline__ uint4 leave_species(uint64_t seed, uint32_t real, uint32_t unit, unsigned long long w,
+                                               uint32_t s, uint32_t pop, double sd, double T, double invT, double D,
+                                               float4 g, double odd1, double odd2, double odd3, const float* rcp,
+                                               sg_stream* st, uint32_t* out_kn) {
+    sg_stream_init(st, seed, real, unit, w, SG_PURPOSE_DIFF + s);
+    double t1 = T * (D * (double)g.w);
+    if (t1 >= 1.0) t1 = 1.0;
+    uint32_t mean_n = pop;
+    if (sd != 0.0) {
+        double nbar = (double)pop - sd * invT;
+        if (nbar > (double)pop) nbar = (double)pop;
+        double nint = floor(nbar);
+        double frc = nbar - nint;
+        mean_n = (uint32_t)nint;
+        if (frc > 0.0) {
+            if (sg_u01_co(sg_next_u32(st)) < frc) mean_n += 1u;
+        }
+    }
+    // Stage 0: molecules leaving; stages 1-3: the face split.  One sampler call site.
+    uint4 k = make_uint4(0u, 0u, 0u, 0u);
+    uint32_t n = mean_n, Kn = 0u;
+    double pst = t1;
+    double ost = (t1 > 0.0 && t1 < 1.0) ? sg_binom_odds(t1) : 0.0;
+#pragma unroll 1
+    for (int stage = 0; stage < 4; ++stage) {
+        uint32_t v = sg_binom_leave(st, n, pst, ost, rcp);
+        if (stage == 0) {
+            Kn = v;
+            n = v;
+            pst = (double)g.x;
+            ost = odd1;
+        } else if (stage == 1) {
+            k.x = v;
+            n -= v;
+            pst = (double)g.y;
+            ost = odd2;
+        } else if (stage == 2) {
+            k.y = v;
+            n -= v;
+            pst = (double)g.z;
+            ost = odd3;
+        } else {
+            k.z = v;
+            n -= v;
+        }
+    }
+    k.w = n;
+    *out_kn = Kn;
+    return k;
+}
+
+// Last block of a window: conservation check, counters, device-side time advance.
+// flag is a 2-int shared scratch; parity is the launch parity read at kernel start.
+__device__ __forceinline__ void window_last_block(const sg_window_args& a, int check, unsigned long long parity,
+                                                  int* flag, int BLOCK) {
+    const int S = a.nspec, R = a.nreac, tid = threadIdx.x, lane = tid & 31;
+    const unsigned long long p = parity, q = parity ^ 1ull;
+    int nact = 0;
+    for (int i = tid; i < a.nreal; i += BLOCK) {
+        const sg_real* rl = &a.reals[i];
+        if (__ldcg(&rl->t) < __ldcg(&rl->t_end)) nact += 1;
+    }
+    for (int o = 16; o > 0; o >>= 1) nact += __shfl_down_sync(0xffffffffu, nact, o);
+    if (lane == 0) atomicAdd(&flag[1], nact);
+    __syncthreads();
+    nact = flag[1];
+    const bool do_check = check && __ldcg(&a.launch_state[3]) != 0ull &&
+                          (unsigned long long)nact == __ldcg(&a.launch_state[2]);
+    for (int s = tid; s < S && do_check; s += BLOCK) {
+        long long expect = (long long)__ldcg(&a.totals[q * S + s]);
+        for (int rr = 0; rr < R; ++rr) {
+            const sg_reac* rc = &a.reacs[rr];
+            for (int i = 0; i < rc->nupd; ++i)
+                if (rc->upd_spec[i] == s)
+                    expect += (long long)rc->upd_delta[i] * (long long)__ldcg(&a.ext[q * R + rr]);
+        }
+        if ((unsigned long long)expect != __ldcg(&a.totals[p * S + s]))
+            atomicOr(a.status, SG_ERR_CONSERVATION);
+    }
+    __syncthreads();
+    for (int rr = tid; rr < R; rr += BLOCK) {
+        a.ext_total[rr] += __ldcg(&a.ext[p * R + rr]);
+        a.ext[q * R + rr] = 0ull;
+    }
+    for (int s = tid; s < S; s += BLOCK) a.totals[q * S + s] = 0ull;
+    for (int i = tid; i < a.nreal; i += BLOCK) {
+        sg_real* rl = &a.reals[i];
+        double rt = __ldcg(&rl->t), rend = __ldcg(&rl->t_end), per = __ldcg(&rl->period);
+        if (rt < rend) {
+            rl->t = (rt + per > rend) ? rend : rt + per;
+            rl->window = __ldcg(&rl->window) + 1ull;
+            rl->pending = 1;
+        }
+    }
+    if (tid == 0) {
+        a.launch_state[2] = (unsigned long long)nact;
+        a.launch_state[3] = 1ull;
+        a.launch_state[1] = p + 1ull;
+        a.launch_state[0] = 0ull;
+    }
+}
+
+// Count this block as finished; true in the last block of the launch (flag: 2 ints).
+__device__ __forceinline__ bool window_block_done(const sg_window_args& a, int* flag) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long prev = atomicAdd(&a.launch_state[0], 1ull);
+        flag[0] = (prev == (unsigned long long)(gridDim.x - 1)) ? 1 : 0;
+        flag[1] = 0;
+    }
+    __syncthreads();
+    if (!flag[0]) return false;
+    __threadfence();
+    return true;
+}
+
 // Resident threads per SM the window kernel is compiled for (caps registers per thread).
 #ifndef SG_WINDOW_THREADS_PER_SM
 #define SG_WINDOW_THREADS_PER_SM 1024
 #endif
 
 // Window kernel: gather (if pending) -> totals -> SSA -> diffusion leave -> store.
-template <int BLOCK, bool SURF = false>
+// SPLIT: reactions only (gather, SSA, counts and change-time sums to global memory); the
+// diffusion leave and the end of the window run in diffuse_kernel.
+template <int BLOCK, bool SURF = false, bool SPLIT = false>
 __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     window_kernel(sg_window_args a, int check) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double s_rcp[SG_RCP_TABLE];
+    __shared__ float s_rcp[SG_RCP_TABLE];
     const int S = a.nspec;
     const int R = a.nreac;
     const int tid = threadIdx.x;
@@ -341,7 +466,7 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     if (SURF)
         SLy = surf_carve(smem_raw + ((smem_bytes(BLOCK, S, R) + 15) & ~(size_t)15), BLOCK, a.surf.nsspec,
                          a.surf.max_sreac_per_patch);
-    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
+    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0f : 1.0f / (float)i;
     for (int i = tid; i < R; i += BLOCK) L.reac[i] = a.reacs[i];
     for (int i = tid; i < S; i += BLOCK) L.tot[i] = 0ull;
     for (int i = tid; i < R; i += BLOCK) L.ext[i] = 0u;
@@ -427,9 +552,16 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             tet_ssa(a, L, tid, BLOCK, rb, re, K, ivs, clampm, T, &st);
         }
 
+        if (SPLIT) {
+            for (int s = 0; s < S; ++s) {
+                const int ds = __ldg(&a.diff_slot[s]);
+                if (ds >= 0) a.tdel[(size_t)ds * a.ntets + t] = L.tdel[s * BLOCK + tid];
+                a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
+            }
+            continue;
+        }
         // Phase 3: diffusion leave, one (tet, species) at a time.
         const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
-        const double G = (double)g.w;
         // Odds ratios of the three face selectors, once per tet instead of once per draw.
         const double odd1 = sg_binom_odds((double)g.x);
         const double odd2 = sg_binom_odds((double)g.y);
@@ -444,53 +576,9 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             uint32_t pop = L.cnt[s * BLOCK + tid];
             uint4 k = make_uint4(0u, 0u, 0u, 0u);
             if (pop > 0u) {
-                // Each (tet, species) leaves on its own stream, so the leave of a species
-                // does not depend on how many draws the SSA or another species took.
-                sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)tlocal, w, SG_PURPOSE_DIFF + (uint32_t)s);
-                double t1 = T * (D * G);
-                if (t1 >= 1.0) t1 = 1.0;
-                const double sd = L.tdel[s * BLOCK + tid];
-                uint32_t mean_n = pop;
-                if (sd != 0.0) {
-                    // Occupancy mean over the window: c_end - sum_k (change_k) t_k / T.
-                    double nbar = (double)pop - sd * invT;
-                    if (nbar > (double)pop) nbar = (double)pop;
-                    double nint = floor(nbar);
-                    double frc = nbar - nint;
-                    mean_n = (uint32_t)nint;
-                    if (frc > 0.0) {
-                        if (sg_u01_co(sg_next_u32(&st)) < frc) mean_n += 1u;
-                    }
-                }
-                // Stage 0: molecules leaving, Binomial(mean_n, t1); stages 1-3: conditional
-                // face split of them; the last face takes the rest.  One sampler call site.
-                uint32_t n = mean_n, Kn = 0u;
-                double pst = t1;
-                double ost = (t1 > 0.0 && t1 < 1.0) ? sg_binom_odds(t1) : 0.0;
-#pragma unroll 1
-                for (int stage = 0; stage < 4; ++stage) {
-                    uint32_t v = sg_binom_o(&st, n, pst, ost, s_rcp);
-                    if (stage == 0) {
-                        Kn = v;
-                        n = v;
-                        pst = (double)g.x;
-                        ost = odd1;
-                    } else if (stage == 1) {
-                        k.x = v;
-                        n -= v;
-                        pst = (double)g.y;
-                        ost = odd2;
-                    } else if (stage == 2) {
-                        k.y = v;
-                        n -= v;
-                        pst = (double)g.z;
-                        ost = odd3;
-                    } else {
-                        k.z = v;
-                        n -= v;
-                    }
-                }
-                k.w = n;
+                uint32_t Kn = 0u;
+                k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop,
+                                  L.tdel[s * BLOCK + tid], T, invT, D, g, odd1, odd2, odd3, s_rcp, &st, &Kn);
                 if (Kn > 0u) {
                     if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
                     moved += Kn;
@@ -517,62 +605,70 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     for (int i = tid; i < R; i += BLOCK)
         if (L.ext[i]) atomicAdd(&a.ext[parity * R + i], (unsigned long long)L.ext[i]);
     if (tid == 0 && L.moved[0]) atomicAdd(a.diff_total, L.moved[0]);
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-        unsigned long long prev = atomicAdd(&a.launch_state[0], 1ull);
-        L.flag[0] = (prev == (unsigned long long)(gridDim.x - 1)) ? 1 : 0;
-        L.flag[1] = 0;
-    }
-    __syncthreads();
-    if (!L.flag[0]) return;
-    __threadfence();
+    if (SPLIT) return;  // diffuse_kernel ends the window
+    if (!window_block_done(a, L.flag)) return;
+    window_last_block(a, check, parity, L.flag, BLOCK);
+}
 
-    // Last block: conservation check, counters, device-side time advance.
-    const unsigned long long p = parity, q = parity ^ 1ull;
-    int nact = 0;
-    for (int i = tid; i < a.nreal; i += BLOCK) {
-        const sg_real* rl = &a.reals[i];
-        if (__ldcg(&rl->t) < __ldcg(&rl->t_end)) nact += 1;
-    }
-    for (int o = 16; o > 0; o >>= 1) nact += __shfl_down_sync(0xffffffffu, nact, o);
-    if (lane == 0) atomicAdd(&L.flag[1], nact);
+// Split window, second kernel: the diffusion leave with one thread per (diffusing
+// species, tet), species-major so that a warp reads 32 consecutive tets of one species;
+// then the end of the window (last block).  Identical results to the fused kernel.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 4) diffuse_kernel(sg_window_args a, int check) {
+    __shared__ float s_rcp[SG_RCP_TABLE];
+    __shared__ int flag[2];
+    __shared__ unsigned long long s_moved;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0f : 1.0f / (float)i;
+    if (tid == 0) s_moved = 0ull;
     __syncthreads();
-    nact = L.flag[1];
-    const bool do_check = check && __ldcg(&a.launch_state[3]) != 0ull &&
-                          (unsigned long long)nact == __ldcg(&a.launch_state[2]);
-    for (int s = tid; s < S && do_check; s += BLOCK) {
-        long long expect = (long long)__ldcg(&a.totals[q * S + s]);
-        for (int rr = 0; rr < R; ++rr) {
-            const sg_reac* rc = &a.reacs[rr];
-            for (int i = 0; i < rc->nupd; ++i)
-                if (rc->upd_spec[i] == s)
-                    expect += (long long)rc->upd_delta[i] * (long long)__ldcg(&a.ext[q * R + rr]);
+    const unsigned long long parity = __ldcg(&a.launch_state[1]) & 1ull;
+    const size_t plane = (size_t)a.ntets * 4;
+    const long long total = (long long)a.ndiff * a.ntets;
+    unsigned long long moved = 0ull;
+    for (long long idx = (long long)blockIdx.x * BLOCK + tid; idx < total; idx += (long long)gridDim.x * BLOCK) {
+        const int ds = (int)(idx / a.ntets);
+        const int t = (int)(idx - (long long)ds * a.ntets);
+        const int r = find_real(a.reals, a.nreal, t);
+        const sg_real* rl = &a.reals[r];
+        const double rt = rl->t, rend = rl->t_end, per = rl->period;
+        if (!(rt < rend)) continue;
+        const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
+        if (comp < 0) continue;
+        const int s = __ldg(&a.diff_spec[ds]);
+        const double D = __ldg(&a.dcst[((size_t)r * a.ncomp + comp) * a.nspec + s]);
+        if (!(D > 0.0)) continue;
+        const double T = (rt + per > rend) ? rend - rt : per;
+        const unsigned long long w = rl->window;
+        const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
+        const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
+        const size_t ci = (size_t)s * a.ntets + t;
+        const uint32_t pop = a.counts[ci];
+        uint4 k = make_uint4(0u, 0u, 0u, 0u);
+        if (pop > 0u) {
+            const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
+            sg_stream st;
+            uint32_t Kn = 0u;
+            k = leave_species(a.seed, (uint32_t)r, (uint32_t)(t - rl->tet_begin), w, (uint32_t)s, pop,
+                              a.tdel[(size_t)ds * a.ntets + t], T, 1.0 / T, D, g, sg_binom_odds((double)g.x),
+                              sg_binom_odds((double)g.y), sg_binom_odds((double)g.z), s_rcp, &st, &Kn);
+            if (Kn > 0u) {
+                if (!((clampm >> s) & 1u)) a.counts[ci] = pop - Kn;
+                moved += Kn;
+            }
         }
-        if ((unsigned long long)expect != __ldcg(&a.totals[p * S + s]))
-            atomicOr(a.status, SG_ERR_CONSERVATION);
+        uint32_t* po = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane + (size_t)ds * plane;
+        if (nb.x >= 0) po[nb.x] = k.x;
+        if (nb.y >= 0) po[nb.y] = k.y;
+        if (nb.z >= 0) po[nb.z] = k.z;
+        if (nb.w >= 0) po[nb.w] = k.w;
     }
+    moved = warp_sum_u64(moved);
+    if (lane == 0 && moved) atomicAdd(&s_moved, moved);
     __syncthreads();
-    for (int rr = tid; rr < R; rr += BLOCK) {
-        a.ext_total[rr] += __ldcg(&a.ext[p * R + rr]);
-        a.ext[q * R + rr] = 0ull;
-    }
-    for (int s = tid; s < S; s += BLOCK) a.totals[q * S + s] = 0ull;
-    for (int i = tid; i < a.nreal; i += BLOCK) {
-        sg_real* rl = &a.reals[i];
-        double rt = __ldcg(&rl->t), rend = __ldcg(&rl->t_end), per = __ldcg(&rl->period);
-        if (rt < rend) {
-            rl->t = (rt + per > rend) ? rend : rt + per;
-            rl->window = __ldcg(&rl->window) + 1ull;
-            rl->pending = 1;
-        }
-    }
-    if (tid == 0) {
-        a.launch_state[2] = (unsigned long long)nact;
-        a.launch_state[3] = 1ull;
-        a.launch_state[1] = p + 1ull;
-        a.launch_state[0] = 0ull;
-    }
+    if (tid == 0 && s_moved) atomicAdd(a.diff_total, s_moved);
+    if (!window_block_done(a, flag)) return;
+    window_last_block(a, check, parity, flag, BLOCK);
 }
 
 // Apply the pending inflow of the last window to the counts (enter phase only).

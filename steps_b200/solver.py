@@ -551,6 +551,16 @@ class TetOpSplit:
     def setLaunch(self, block, grid=0):
         check(self._L.sg_set_launch(self._h, int(block), int(grid)))
 
+    def setSplit(self, on):
+        """Run each window as two kernels (reactions per tet, diffusion per (species, tet));
+        results are identical to the fused kernel."""
+        check(self._L.sg_set_split(self._h, 1 if on else 0))
+
+    def getSplit(self):
+        x = C.c_int32()
+        check(self._L.sg_get_split(self._h, C.byref(x)))
+        return bool(x.value)
+
     def getCarveout(self):
         """Preferred shared-memory carveout (percent) of the window kernels."""
         x = C.c_int32()
@@ -565,17 +575,18 @@ class TetOpSplit:
         return b.value, g.value
 
     def setAutotune(self, on=True):
-        """Time 16 windows of the next run (after one untimed window) under eight launch
+        """Time 18 windows of the next run (after one untimed window) under nine launch
         shapes and keep the fastest (results do not depend on the shape)."""
         check(self._L.sg_set_autotune(self._h, 1 if on else 0))
 
     def getAutotuneTimes(self):
         """ms of the two timed windows under each candidate shape, in the order block
         64, 128, 256 x grid {occupancy-sized, one tet per thread} at the full shared-memory
-        carveout, then the best of those at carveouts 75% and 50%; empty before tuning."""
-        buf = (C.c_float * 8)()
+        carveout, then the best of those at carveouts 75% and 50% and split; empty before
+        tuning."""
+        buf = (C.c_float * 16)()
         n = C.c_int32()
-        check(self._L.sg_get_autotune_ms(self._h, buf, 8, C.byref(n)))
+        check(self._L.sg_get_autotune_ms(self._h, buf, 16, C.byref(n)))
         return list(buf)[: n.value]
 
     def setConservationCheck(self, on):

@@ -53,10 +53,13 @@ def test_diffusion_only_large_counts(steps_lib):
         assert int(sim.getSpecCounts("A").sum(dtype=np.uint64)) == total
 
 
-def test_random_network_poisson(steps_lib):
-    """8 species, 12 reactions (zeroth, first, second order) on 6^3 cubes, Poisson(50) counts."""
+@pytest.mark.parametrize("split", [False, True])
+def test_random_network_poisson(steps_lib, split):
+    """8 species, 12 reactions (zeroth, first, second order) on 6^3 cubes, Poisson(50) counts;
+    fused and split windows."""
     mdl = W.random_network(2025)
     sim, ora = pair(mdl, W.cube_mesh(6), seed=2025)
+    sim.setSplit(split)
     rows = W.poisson_counts(sim.geom.ntets, 50.0, 2025)
     for i, s in enumerate(sim.spec_names):
         sim.setSpecCounts(s, rows[i])
@@ -71,9 +74,11 @@ def test_random_network_poisson(steps_lib):
         assert sim.getCompReacExtent("comp", f"r{r}") == ora.reac_extent(r)
 
 
-def test_two_compartments(steps_lib):
+@pytest.mark.parametrize("split", [False, True])
+def test_two_compartments(steps_lib, split):
     """Different reactions and diffusion rules per compartment; no diffusion across."""
     sim, ora = pair(two_comp_model(), two_comp_mesh(6), seed=5)
+    sim.setSplit(split)
     for c in ("left", "right"):
         for s in ("A", "B"):
             sim.setCompSpecCount(c, s, 2500.5)
@@ -85,8 +90,10 @@ def test_two_compartments(steps_lib):
         assert_same(sim, ora, f"t={t}")
 
 
-def test_clamped_species(steps_lib):
+@pytest.mark.parametrize("split", [False, True])
+def test_clamped_species(steps_lib, split):
     sim, ora = pair(W.ab_c_model(), W.cube_mesh(5), seed=11)
+    sim.setSplit(split)
     sim.setCompSpecCount("comp", "A", 5000)
     sim.setCompSpecCount("comp", "B", 5000)
     for t in (0, 17, 400):
@@ -102,12 +109,14 @@ def test_clamped_species(steps_lib):
     assert [sim.getTetSpecCount(t, "A") for t in (0, 17, 400)] == clamped_before
 
 
-def test_batched_realizations_with_jitter(steps_lib):
+@pytest.mark.parametrize("split", [False, True])
+def test_batched_realizations_with_jitter(steps_lib, split):
     """Realizations of different sizes in one launch, per-realization rate constants."""
     sizes = [3, 5, 4, 6]
     mesh = W.batched_mesh(sizes)
     mdl = W.random_network(7)
     sim, ora = pair(mdl, mesh, seed=3, realizations=mesh.offsets)
+    sim.setSplit(split)
     jit = W.rate_jitter(len(sizes), 12, 3)
     for r in range(len(sizes)):
         for q in range(12):
@@ -145,10 +154,12 @@ def test_long_runs_graph_replay(steps_lib, graphs):
     assert sim.getNIteration() == ora.window() >= 80
 
 
-@pytest.mark.parametrize("block", [64, 256])
-def test_launch_shapes_agree(steps_lib, block):
-    """The result does not depend on the block size (counter-based streams)."""
+@pytest.mark.parametrize("block,split", [(64, False), (256, False), (128, True), (256, True)])
+def test_launch_shapes_agree(steps_lib, block, split):
+    """The result does not depend on the block size or on the split window (counter-based
+    streams)."""
     sim, ora = pair(W.ab_c_model(), W.cube_mesh(7), seed=4, block=block)
+    sim.setSplit(split)
     sim.setCompSpecCount("comp", "A", 7000)
     sim.setCompSpecCount("comp", "B", 3000)
     sync_counts(sim, ora)
@@ -159,7 +170,7 @@ def test_launch_shapes_agree(steps_lib, block):
 
 
 def test_autotuned_run_matches_oracle(steps_lib):
-    """Autotuning times 16 windows (after an untimed one) under eight launch shapes; the
+    """Autotuning times 18 windows (after an untimed one) under nine launch shapes; the
     counts after the run still equal the oracle's, and the kept shape is a candidate."""
     mesh = W.cube_mesh(9)
     sim, ora = pair(W.random_network(3), mesh, seed=6)
@@ -173,7 +184,7 @@ def test_autotuned_run_matches_oracle(steps_lib):
     ora.run(t)
     assert_same(sim, ora, "autotuned run")
     times = sim.getAutotuneTimes()
-    assert len(times) == 8 and all(x > 0.0 for x in times)
+    assert len(times) == 9 and all(x > 0.0 for x in times)
     assert sim.getCarveout() in (100, 75, 50)
     block, grid = sim.getLaunch()
     assert block in (64, 128, 256) and grid in (0, -1)
