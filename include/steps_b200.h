@@ -108,6 +108,9 @@ int sg_set_comp_count(sg_solver* h, int32_t comp, int32_t spec, int32_t real, do
  * and its setter counterpart.  out/in hold ntets uint32 values. */
 int sg_get_spec_counts(sg_solver* h, int32_t spec, uint32_t* out);
 int sg_set_spec_counts(sg_solver* h, int32_t spec, const uint32_t* in);
+/* getBatchTetSpecCountsNP (TOS:5715): out[i] = count of spec in tets[i], gathered on the
+ * device so that only the n selected values cross to the host. */
+int sg_get_batch_tet_counts(sg_solver* h, int32_t spec, const int32_t* tets, int32_t n, double* out);
 
 /* API::setTetSpecClamped (TOS setTetSpecClamped). */
 int sg_set_tet_clamped(sg_solver* h, int32_t tet, int32_t spec, int32_t clamped);
@@ -140,6 +143,14 @@ int sg_set_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double n);    /* 
 int sg_get_patch_count(sg_solver* h, int32_t patch, int32_t sspec, int32_t real, double* n);
 int sg_set_patch_count(sg_solver* h, int32_t patch, int32_t sspec, int32_t real, double n);
 int sg_get_tri_ohmic_i(sg_solver* h, int32_t tri, double* amps);  /* getTriOhmicI: last EField step */
+/* Surface diffusion (SDiff, sdiff.cpp:62-83, 498-560; TOS:585-630 triangle neighbours):
+ * for membrane triangle m and edge e, nbr[3m+e] is the membrane triangle across that edge
+ * (-1 = none), nbr_edge its edge index, len the edge length (m) and dist the distance of
+ * the two barycentres (m).  Diffusion runs towards neighbours of the same patch. */
+int sg_set_tri_neighbours(sg_solver* h, const int32_t* nbr, const int32_t* nbr_edge, const double* len,
+                          const double* dist);
+/* One surface diffusion rule: surface species sspec diffuses on patch with dcst (m^2/s). */
+int sg_add_sdiff(sg_solver* h, int32_t patch, int32_t sspec, double dcst, int32_t* out_idx);
 
 /* ---- membrane potential (EField; api.hpp:140, 2874-2875; efield.hpp:59) ----------
  * Units at this boundary are the reference API's: V, A, s, F/m^2, ohm m, ohm m^2.

@@ -234,55 +234,6 @@ static uint32_t or_binom(or_stream* st, uint32_t n, double p) {
     return flip ? n - k : k;
 }
 
-/* Diffusion-leave binomial: BINV in single precision (24-bit uniform, float pmf
- * recurrence with correctly rounded float reciprocals, one fmaf per step) below the cut for
- * n < 125, BINV in double for larger n, BTRD in double above the cut. */
-static float or_powuf(float q, uint32_t n) {
-    float r = 1.0f, b = q;
-    while (n) {
-        if (n & 1u) r = r * b;
-        b = b * b;
-        n >>= 1;
-    }
-    return r;
-}
-
-static uint32_t or_binv_f(or_stream* st, uint32_t n, double pp) {
-    const float p = (float)pp;
-    const float s = (float)(pp / (1.0 - pp));
-    const float q = 1.0f - p;
-    const float a = ((float)n + 1.0f) * s;
-    float r = or_powuf(q, n);
-    float u = (float)(or_u32(st) >> 8) * 5.9604644775390625e-8f;
-    uint32_t x = 0;
-    while (u >= r) {
-        u = u - r;
-        x += 1;
-        r = r * fmaf(a, 1.0f / (float)x, -s);
-        if (!(r > 0.0f)) break;
-    }
-    return x < n ? x : n;
-}
-
-static uint32_t or_binom_leave(or_stream* st, uint32_t n, double p) {
-    if (n == 0 || !(p > 0.0)) return 0;
-    if (p >= 1.0) return n;
-    int flip = p > 0.5;
-    double pp = flip ? 1.0 - p : p;
-    uint32_t k;
-    if ((double)n * pp < 24.0)
-        k = (n + 3u < 128u) ? or_binv_f(st, n, pp) : or_binv(st, n, pp);
-    else
-        k = or_btrd(st, n, pp);
-    return flip ? n - k : k;
-}
-
-void or_binom_leave_many(uint64_t seed, uint32_t unit, uint32_t n, double p, uint32_t count, uint32_t* out) {
-    or_stream st;
-    or_stream_init(&st, seed, 0, unit, 0, 0);
-    for (uint32_t i = 0; i < count; ++i) out[i] = or_binom_leave(&st, n, p);
-}
-
 /* Draw count binomials from one stream (sampler tests): out[i] = Binom(n, p). */
 void or_binom_many(uint64_t seed, uint32_t unit, uint32_t n, double p, uint32_t count, uint32_t* out) {
     or_stream st;
@@ -614,11 +565,11 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
             mean_n = (uint32_t)nint;
             if (frc > 0.0 && u_co(or_u32(&st)) < frc) mean_n += 1;
         }
-        uint32_t Kn = or_binom_leave(&st, mean_n, t1);
+        uint32_t Kn = or_binom(&st, mean_n, t1);
         if (Kn == 0) continue;
         uint32_t rem = Kn;
         for (int f = 0; f < 3; ++f) {
-            o[f] = or_binom_leave(&st, rem, (double)g[f]);
+            o[f] = or_binom(&st, rem, (double)g[f]);
             rem -= o[f];
         }
         o[3] = rem;

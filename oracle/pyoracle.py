@@ -50,7 +50,6 @@ def load():
         lib.or_log_export.argtypes = [C.c_double]
         lib.or_log_export.restype = C.c_double
         lib.or_binom_many.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, pu]
-        lib.or_binom_leave_many.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, pu]
         _lib = lib
     return _lib
 
@@ -146,11 +145,4 @@ def log(x):
 def binom_many(seed, unit, n, p, count):
     out = np.empty(count, dtype=np.uint32)
     load().or_binom_many(seed, unit, n, p, count, _p(out, C.c_uint32))
-    return out
-
-
-def binom_leave_many(seed, unit, n, p, count):
-    """The diffusion-leave sampler (single-precision BINV below the cut, BTRD above)."""
-    out = np.empty(count, dtype=np.uint32)
-    load().or_binom_leave_many(seed, unit, n, p, count, _p(out, C.c_uint32))
     return out

@@ -69,6 +69,7 @@ PROTOTYPES = {
     "sg_get_comp_count": [_P, _i32, _i32, _i32, _pf64],
     "sg_set_comp_count": [_P, _i32, _i32, _i32, _f64],
     "sg_get_spec_counts": [_P, _i32, _pu32],
+    "sg_get_batch_tet_counts": [_P, _i32, _pi32, _i32, _pf64],
     "sg_set_spec_counts": [_P, _i32, _pu32],
     "sg_set_tet_clamped": [_P, _i32, _i32, _i32],
     "sg_set_reac_k": [_P, _i32, _i32, _f64],
@@ -89,6 +90,8 @@ PROTOTYPES = {
     "sg_set_surface": [_P, _i32, _i32, _pi32, _pi32, _pf64, _i32],
     "sg_add_sreac": [_P, _i32, _pu32, _pu32, _pi32, _pi32, _f64, _pi32],
     "sg_add_vdep_sreac": [_P, _i32, _pu32, _pu32, _pi32, _pi32, _f64, _f64, _i32, _pf64, _pi32],
+    "sg_set_tri_neighbours": [_P, _pi32, _pi32, _pf64, _pf64],
+    "sg_add_sdiff": [_P, _i32, _i32, _f64, _pi32],
     "sg_add_ohmic": [_P, _i32, _i32, _f64, _f64, _pi32],
     "sg_get_tri_count": [_P, _i32, _i32, _pf64],
     "sg_set_tri_count": [_P, _i32, _i32, _f64],

@@ -23,7 +23,6 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
-    "-DSG_NOINLINE_REFILL",
     "-shared",
 ]
 

@@ -78,6 +78,7 @@ SG_HD sg_u32x4 sg_philox4x32(sg_u32x4 c, uint32_t k0, uint32_t k1) {
 #define SG_PURPOSE_SETUP 1u    // host-side placement of molecules (setters)
 #define SG_PURPOSE_EFIELD 2u   // reserved
 #define SG_PURPOSE_DIFF 16u    // + species: diffusion leave of one (unit, species) in one window
+#define SG_PURPOSE_SDIFF 80u   // + surface species: surface diffusion leave of one (triangle, species)
 
 // One independent stream: counter = (block, unit, window_lo, purpose<<24 | window_hi24),
 // key = (seed_lo, seed_hi + realization * W0).  Draw j of the stream is word
@@ -285,51 +286,6 @@ SG_HD uint32_t sg_binv(sg_stream* st, uint32_t n, double p, const double* rcp, d
     return x < n ? x : n;
 }
 
-// FP32 form of the same search for the diffusion leave (the binomials of molecules leaving
-// a tet), used for n + 3 < SG_RCP_TABLE: the uniform is the top 24 bits of one draw (exact
-// in float), the pmf recurrence r *= fma(a, 1/x, -s) runs in float with a table of
-// correctly rounded float reciprocals.  With n < 125 the rounding of q = 1 - p and of the
-// recurrence stays below about n * 2^-24 relative (< 1e-5), so the sampled law differs from
-// the exact binomial by about 1e-6 in the CDF; q^n stays above 3e-15 in this regime
-// (n p < SG_BINV_CUT, p <= 1/2), far inside float's range.  Larger n use the FP64 search.
-SG_HD float sg_pow_uf(float q, uint32_t n) {
-    float r = 1.0f;
-    float b = q;
-    while (n) {
-        if (n & 1u) r = r * b;
-        b = b * b;
-        n >>= 1;
-    }
-    return r;
-}
-
-SG_HD uint32_t sg_binv_f(sg_stream* st, uint32_t n, float p, const float* rcp, float s) {
-    const float q = 1.0f - p;
-    const float a = ((float)n + 1.0f) * s;
-    float r = sg_pow_uf(q, n);
-    float u = (float)(sg_next_u32(st) >> 8) * 5.9604644775390625e-8f;  // [0,1) in steps of 2^-24
-    uint32_t x = 0;
-    if (rcp && n + 3u < (uint32_t)SG_RCP_TABLE) {
-        float rc = rcp[1];
-        while (u >= r) {
-            u = u - r;
-            x += 1;
-            const float m = fmaf(a, rc, -s);
-            rc = rcp[x + 1];
-            r = r * m;
-            if (!(r > 0.0f)) break;
-        }
-    } else {
-        while (u >= r) {
-            u = u - r;
-            x += 1;
-            r = r * fmaf(a, 1.0f / (float)x, -s);
-            if (!(r > 0.0f)) break;
-        }
-    }
-    return x < n ? x : n;
-}
-
 // Stirling-series remainder fc(k) = ln k! - ((k + 1/2) ln(k + 1) - (k + 1) + ln(2 pi)/2),
 // tabulated for k < 10 (values computed from the definition), series beyond.
 SG_HD double sg_stirling_fc(uint32_t k) {
@@ -435,22 +391,6 @@ SG_HD uint32_t sg_binom_o(sg_stream* st, uint32_t n, double p, double odds, cons
     bool flip = p > 0.5;
     double pp = flip ? 1.0 - p : p;
     uint32_t k = ((double)n * pp < SG_BINV_CUT) ? sg_binv(st, n, pp, rcp, odds) : sg_btrd(st, n, pp);
-    return flip ? n - k : k;
-}
-
-// The diffusion-leave binomial: FP32 BINV below the cut for n < 125, FP64 BINV for larger
-// n, FP64 BTRD above the cut.
-SG_HD uint32_t sg_binom_leave(sg_stream* st, uint32_t n, double p, double odds, const float* rcpf) {
-    if (n == 0 || !(p > 0.0)) return 0;
-    if (p >= 1.0) return n;
-    bool flip = p > 0.5;
-    double pp = flip ? 1.0 - p : p;
-    uint32_t k;
-    if ((double)n * pp < SG_BINV_CUT)
-        k = (n + 3u < (uint32_t)SG_RCP_TABLE) ? sg_binv_f(st, n, (float)pp, rcpf, (float)odds)
-                                              : sg_binv(st, n, pp, nullptr, odds);
-    else
-        k = sg_btrd(st, n, pp);
     return flip ? n - k : k;
 }
 

@@ -30,6 +30,13 @@ static const double AVOGADRO = 6.02214179e23;  // src/steps/math/constants.hpp:4
 // src/steps/mpi/tetopsplit/tri.cpp:664-694): sum over the patch's ohmic currents of
 // g * (integral of the channel-state count / dt) * (V_tri - E_rev), in pA; the integrals
 // restart at zero for the next step.
+// out[i] = count of species row `row` in tet idx[i] (device-side gather for the batch
+// getters, so a recording step moves only the selected tets).
+__global__ void gather_counts_kernel(int n, const uint32_t* row, const int32_t* idx, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = (double)row[idx[i]];
+}
+
 __global__ void ohmic_current_kernel(int M, int nss, int noc, const sg_ohmic* oc, const int32_t* tri_patch,
                                      double* spec_int, const double* triV, double inv_dt, double* tri_I,
                                      double* tri_I_last) {
@@ -132,7 +139,78 @@ struct Solver {
     DevBuf<sg_vtab> d_vtabs;
     DevBuf<sg_ohmic> d_ohmics;
     DevBuf<unsigned long long> d_surf_ext;
+    DevBuf<int32_t> d_memb_tets;                    // tets with membrane triangles
+    int nmemb_tets = 0;
+    // Surface diffusion (sdiff.cpp): edge neighbours, rules, device state.
+    std::vector<int32_t> tri_nbr, tri_nbr_edge;     // [M*3] membrane neighbour across edge e, its edge
+    std::vector<double> tri_len, tri_dist;          // [M*3] edge length, barycentre distance (m)
+    std::vector<double> sdcst;                      // [npatch][SS] m^2/s, 0 = no rule
+    std::vector<int32_t> sdiff_slot;                // [SS] compact index or -1
+    std::vector<float> sgeo;                        // [M*4] c0, c1, 1, G (1/m^2)
+    int nsdiff = 0;
+    DevBuf<uint32_t> d_tri_out;
+    DevBuf<double> d_tri_occ, d_sdcst;
+    DevBuf<int32_t> d_sdslot, d_sdspec, d_snbr, d_tri_inner;
+    DevBuf<float> d_sgeo;
     bool has_surf() const { return ntris > 0 && nsspec > 0; }
+
+    // Surface diffusion tables (sdiff.cpp:62-83): per triangle the edge coefficients
+    // g_e = l_e / (A d_e) towards same-patch neighbours, G = sum g_e, and the conditional
+    // selectors c0 = g0 / G, c1 = g1 / (g1 + g2); the scaled constant is D G.
+    void setup_sdiff() {
+        sdiff_slot.assign(nsspec, -1);
+        nsdiff = 0;
+        bool any = false;
+        for (double d : sdcst)
+            if (d > 0.0) any = true;
+        if (!any) return;
+        if (tri_nbr.size() != (size_t)ntris * 3) throw ArgErr("surface diffusion needs the triangle neighbours");
+        std::vector<int32_t> sdspec;
+        for (int s = 0; s < nsspec; ++s) {
+            bool has = false;
+            for (int p = 0; p < npatch; ++p)
+                if (sdcst[(size_t)p * nsspec + s] > 0.0) has = true;
+            if (has) {
+                sdiff_slot[s] = (int32_t)sdspec.size();
+                sdspec.push_back(s);
+            }
+        }
+        nsdiff = (int)sdspec.size();
+        sgeo.assign((size_t)ntris * 4, 0.0f);
+        std::vector<int32_t> snbr((size_t)ntris * 4, -1);
+        for (int m = 0; m < ntris; ++m) {
+            double g[3] = {0.0, 0.0, 0.0};
+            for (int e = 0; e < 3; ++e) {
+                const int q = tri_nbr[(size_t)m * 3 + e];
+                if (q < 0 || tri_patch[q] != tri_patch[m]) continue;
+                const double d = tri_dist[(size_t)m * 3 + e];
+                if (!(d > 0.0)) continue;
+                g[e] = tri_len[(size_t)m * 3 + e] / (tri_area[m] * d);
+                snbr[(size_t)m * 4 + e] = (q << 2) | tri_nbr_edge[(size_t)m * 3 + e];
+            }
+            const double G = g[0] + g[1] + g[2];
+            const double r12 = g[1] + g[2];
+            sgeo[(size_t)m * 4 + 0] = G > 0.0 ? (float)(g[0] / G) : 0.0f;
+            sgeo[(size_t)m * 4 + 1] = r12 > 0.0 ? (float)(g[1] / r12) : 0.0f;
+            sgeo[(size_t)m * 4 + 2] = 1.0f;
+            sgeo[(size_t)m * 4 + 3] = (float)G;
+        }
+        d_tri_out.alloc((size_t)2 * nsdiff * ntris * 4);
+        SG_CUDA(cudaMemsetAsync(d_tri_out.p, 0, d_tri_out.n * 4, stream));
+        d_tri_occ.alloc((size_t)nsdiff * ntris);
+        d_sdcst.alloc(sdcst.size());
+        d_sdslot.alloc(nsspec);
+        d_sdspec.alloc(nsdiff);
+        d_snbr.alloc(snbr.size());
+        d_sgeo.alloc(sgeo.size());
+        d_tri_inner.alloc(ntris);
+        h2d(d_sdcst.p, sdcst.data(), sdcst.size());
+        h2d(d_sdslot.p, sdiff_slot.data(), sdiff_slot.size());
+        h2d(d_sdspec.p, sdspec.data(), sdspec.size());
+        h2d(d_snbr.p, snbr.data(), snbr.size());
+        h2d(d_sgeo.p, sgeo.data(), sgeo.size());
+        h2d(d_tri_inner.p, tri_inner.data(), tri_inner.size());
+    }
 
     void setup_surface() {
         if (!has_surf()) return;
@@ -183,6 +261,15 @@ struct Solver {
         d_ohmics.alloc(std::max<size_t>(ohmics.size(), 1));
         d_surf_ext.alloc(1);
         h2d(d_tet_tris.p, tt.data(), tt.size());
+        // Tets with membrane triangles, ascending: the SURF launch of a split window.
+        std::vector<int32_t> mt;
+        for (int t = 0; t < ntets; ++t)
+            if (tt[(size_t)t * 4] >= 0) mt.push_back(t);
+        nmemb_tets = (int)mt.size();
+        d_memb_tets.alloc(std::max<size_t>(mt.size(), 1));
+        if (!mt.empty()) h2d(d_memb_tets.p, mt.data(), mt.size());
+        split = true;  // membrane models run the split window by default (see launch_window)
+        setup_sdiff();
         h2d(d_tri_patch.p, tri_patch.data(), tri_patch.size());
         h2d(d_psb.p, patch_sb.data(), patch_sb.size());
         h2d(d_tri_area.p, tri_area.data(), tri_area.size());
@@ -216,6 +303,17 @@ struct Solver {
         s.vtabs = d_vtabs.p;
         s.vtab_vals = d_vvals.p;
         s.spec_int = d_spec_int.p;
+        if (nsdiff > 0) {
+            s.tri_outflow = d_tri_out.p;
+            s.tri_occ = d_tri_occ.p;
+            s.sdiff_slot = d_sdslot.p;
+            s.sdiff_spec = d_sdspec.p;
+            s.sdcst = d_sdcst.p;
+            s.snbr = d_snbr.p;
+            s.sgeo = d_sgeo.p;
+            s.tri_inner = d_tri_inner.p;
+            s.nsdiff = nsdiff;
+        }
         s.nsspec = nsspec;
         s.ntris = ntris;
         s.nsreac = (int)sreacs.size();
@@ -438,6 +536,16 @@ struct Solver {
                     if (sd > mx) mx = sd;
                 }
             }
+            // Surface diffusion rules count too (TOS:5373-5411 takes the max over both).
+            for (int m = 0; nsdiff > 0 && m < ntris; ++m) {
+                const int t = tri_inner[m];
+                if (t < real_begin[r] || t >= real_begin[r + 1]) continue;
+                const double G = (double)sgeo[(size_t)m * 4 + 3];
+                for (int s = 0; s < nsspec; ++s) {
+                    const double sd = sdcst[(size_t)tri_patch[m] * nsspec + s] * G;
+                    if (sd > mx) mx = sd;
+                }
+            }
             reals[r].period = (mx > 0.0) ? 1.0 / mx : std::numeric_limits<double>::infinity();
         }
     }
@@ -559,9 +667,12 @@ struct Solver {
         if (has_surf()) {
             size_t ss = window_smem();
             if (ss > 227 * 1024) throw NotImplErr("too many surface species or reactions for the shared-memory staging");
-            if (ss > 48 * 1024)
+            if (ss > 48 * 1024) {
                 SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)ss));
+                SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+            }
         }
     }
 
@@ -588,7 +699,7 @@ struct Solver {
         return (int)std::max(1L, std::min(need, cap));
     }
 
-    bool use_split() const { return split && !has_surf(); }
+    bool use_split() const { return split || nsdiff > 0; }
     void ensure_split_buffers() {
         if (!d_tdel.p && ndiff > 0) d_tdel.alloc((size_t)ndiff * ntets);
     }
@@ -596,7 +707,36 @@ struct Solver {
     void launch_window(const sg_window_args& a, int g) {
         size_t sm = window_smem();
         int chk = check_flag();
-        if (has_surf()) {
+        if (has_surf() && use_split()) {
+            // Membrane models: the volume-only SSA for every other tet at the volume kernel's
+            // occupancy, the SURF SSA over the membrane tet list, then the diffusion leave.
+            if (ndiff > 0 && !a.tdel) throw ProgErr("split window without its buffers");
+            const size_t smv = smem_bytes(block, nspec, (int)reacs.size());
+            const int gv = (int)std::max(1L, ((long)ntets + block - 1) / block);
+            switch (block) {
+                case 64: window_kernel<64, false, true><<<gv, 64, smv, stream>>>(a, chk); break;
+                case 128: window_kernel<128, false, true><<<gv, 128, smv, stream>>>(a, chk); break;
+                case 256: window_kernel<256, false, true><<<gv, 256, smv, stream>>>(a, chk); break;
+                default: throw ArgErr("block size must be 64, 128 or 256");
+            }
+            SG_CUDA(cudaGetLastError());
+            if (nmemb_tets > 0) {
+                sg_window_args am = a;
+                am.tet_list = d_memb_tets.p;
+                am.nlist = nmemb_tets;
+                window_kernel<128, true, true><<<(nmemb_tets + 127) / 128, 128, sm, stream>>>(am, chk);
+                SG_CUDA(cudaGetLastError());
+            }
+            if (nsdiff > 0) {
+                const long long sp = (long long)nsdiff * ntris;
+                const int gsd = (int)std::max(1LL, std::min((sp + 255) / 256, (long long)nsm * 64));
+                sdiffuse_kernel<256><<<gsd, 256, 0, stream>>>(a);
+                SG_CUDA(cudaGetLastError());
+            }
+            const long long pairs = (long long)ndiff * ntets;
+            const int gd = (int)std::max(1LL, std::min((pairs + 255) / 256, (long long)nsm * 64));
+            diffuse_kernel<256><<<gd, 256, 0, stream>>>(a, chk);
+        } else if (has_surf()) {
             window_kernel<128, true><<<g, 128, sm, stream>>>(a, chk);
         } else if (use_split()) {
             if (ndiff > 0 && !a.tdel) throw ProgErr("split window without its buffers");
@@ -782,6 +922,7 @@ struct Solver {
         SG_CUDA(cudaFuncSetAttribute(window_kernel<128, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         SG_CUDA(cudaFuncSetAttribute(window_kernel<256, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
     }
 
     uint64_t autotune(const sg_window_args& a) {
@@ -908,6 +1049,12 @@ struct Solver {
         int g = std::min((ntets + 255) / 256, nsm * 8);
         flush_kernel<<<std::max(g, 1), 256, 0, stream>>>(a);
         SG_CUDA(cudaGetLastError());
+        if (nsdiff > 0) {
+            const int gs = std::max(1, std::min((int)(((long long)nsdiff * ntris + 255) / 256), nsm * 8));
+            sflush_kernel<<<gs, 256, 0, stream>>>(a);
+            SG_CUDA(cudaGetLastError());
+            launches += 1;
+        }
         clear_pending_kernel<<<(nreal + 255) / 256, 256, 0, stream>>>(d_reals.p, nreal);
         SG_CUDA(cudaGetLastError());
         launches += 2;
@@ -1083,6 +1230,29 @@ struct Solver {
         put_row(s, v);
     }
 
+    // getBatchTetSpecCountsNP (TOS:5715) without moving the whole row.
+    DevBuf<int32_t> d_gidx;
+    DevBuf<double> d_gout;
+    void get_batch_tet_counts(int s, const int32_t* tets, int n, double* out) {
+        require_setup();
+        check_spec(s);
+        if (n < 0) throw ArgErr("negative count of tets");
+        if (n == 0) return;
+        for (int i = 0; i < n; ++i) check_tet(tets[i]);
+        flush();
+        if (d_gidx.n < (size_t)n) {
+            d_gidx.alloc(n);
+            d_gout.alloc(n);
+        }
+        h2d(d_gidx.p, tets, (size_t)n);
+        const int g = std::max(1, std::min((n + 255) / 256, nsm * 8));
+        gather_counts_kernel<<<g, 256, 0, stream>>>(n, d_counts.p + (size_t)s * ntets, d_gidx.p, d_gout.p);
+        SG_CUDA(cudaGetLastError());
+        launches += 1;
+        d2h(out, d_gout.p, (size_t)n);
+        sync();
+    }
+
     void get_spec_row(int s, uint32_t* out) {
         require_setup();
         check_spec(s);
@@ -1163,6 +1333,7 @@ struct Solver {
     }
     double get_tri_count(int m, int s) {
         check_tri(m, s);
+        flush();
         uint32_t c = 0;
         d2h(&c, d_tri_counts.p + (size_t)s * ntris + m, 1);
         sync();
@@ -1170,6 +1341,7 @@ struct Solver {
     }
     void set_tri_count(int m, int s, double n) {
         check_tri(m, s);
+        flush();
         sg_stream st = setup_stream();
         uint32_t c = round_count(n, &st);
         h2d(d_tri_counts.p + (size_t)s * ntris + m, &c, 1);
@@ -1184,6 +1356,7 @@ struct Solver {
     double get_patch_count(int p, int s, int real) {
         check_tri(0, s);
         if (real >= 0) check_real(real);
+        flush();
         std::vector<uint32_t> v(ntris);
         d2h(v.data(), d_tri_counts.p + (size_t)s * ntris, ntris);
         sync();
@@ -1196,6 +1369,7 @@ struct Solver {
         check_tri(0, s);
         if (p < 0 || p >= npatch) throw ArgErr("patch index out of range");
         if (real >= 0) check_real(real);
+        flush();
         if (!(n >= 0.0) || n > 4294967295.0) throw ArgErr("count out of range");
         std::vector<uint32_t> v(ntris);
         d2h(v.data(), d_tri_counts.p + (size_t)s * ntris, ntris);
@@ -1649,6 +1823,16 @@ int sg_get_spec_counts(sg_solver* h, int32_t spec, uint32_t* out) {
     });
 }
 
+int sg_get_batch_tet_counts(sg_solver* h, int32_t spec, const int32_t* tets, int32_t n, double* out) {
+    return guarded([&] {
+        if (n > 0) {
+            need(tets, "tets");
+            need(out, "out");
+        }
+        S(h)->get_batch_tet_counts(spec, tets, n, out);
+    });
+}
+
 int sg_set_spec_counts(sg_solver* h, int32_t spec, const uint32_t* in) {
     return guarded([&] {
         need(in, "in");
@@ -1801,6 +1985,46 @@ int sg_set_surface(sg_solver* h, int32_t nsspec, int32_t ntris, const int32_t* t
             if (p < 0 || p >= npatch) throw sg::ArgErr("triangle patch index out of range");
         for (double a : s->tri_area)
             if (!(a > 0.0)) throw sg::ArgErr("triangle area must be positive");
+    });
+}
+
+int sg_set_tri_neighbours(sg_solver* h, const int32_t* nbr, const int32_t* nbr_edge, const double* len,
+                          const double* dist) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (s->ntris <= 0) throw sg::ProgErr("call sg_set_surface first");
+        need(nbr, "nbr");
+        need(nbr_edge, "nbr_edge");
+        need(len, "len");
+        need(dist, "dist");
+        const size_t n = (size_t)s->ntris * 3;
+        s->tri_nbr.assign(nbr, nbr + n);
+        s->tri_nbr_edge.assign(nbr_edge, nbr_edge + n);
+        s->tri_len.assign(len, len + n);
+        s->tri_dist.assign(dist, dist + n);
+        for (size_t i = 0; i < n; ++i) {
+            const int q = s->tri_nbr[i];
+            if (q < -1 || q >= s->ntris) throw sg::ArgErr("triangle neighbour out of range");
+            if (q >= 0 && (s->tri_nbr_edge[i] < 0 || s->tri_nbr_edge[i] > 2))
+                throw sg::ArgErr("triangle neighbour edge out of range");
+            if (q >= 0 && s->tri_nbr[(size_t)q * 3 + s->tri_nbr_edge[i]] != (int)(i / 3))
+                throw sg::ArgErr("triangle neighbours are not reciprocal");
+        }
+    });
+}
+
+int sg_add_sdiff(sg_solver* h, int32_t patch, int32_t sspec, double dcst, int32_t* out_idx) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (s->nsspec <= 0) throw sg::ProgErr("call sg_set_surface first");
+        if (patch < 0 || patch >= s->npatch) throw sg::ArgErr("patch index out of range");
+        if (sspec < 0 || sspec >= s->nsspec) throw sg::ArgErr("surface species index out of range");
+        if (!(dcst >= 0.0)) throw sg::ArgErr("diffusion constant must be non-negative");
+        s->sdcst.resize((size_t)s->npatch * s->nsspec, 0.0);
+        s->sdcst[(size_t)patch * s->nsspec + sspec] = dcst;
+        if (out_idx) *out_idx = patch * s->nsspec + sspec;
     });
 }
 

@@ -79,6 +79,16 @@ typedef struct sg_surf_args {
     const sg_vtab* vtabs;
     const double* vtab_vals;
     double* spec_int;                  // [SS][M] time integral of surface counts (s) this EField step
+    // Surface diffusion (sdiff.cpp): two-phase like the volume, 4 uint32 slots per (tri, species).
+    uint32_t* tri_outflow;             // [2][SD][M][4] or null without surface diffusion
+    double* tri_occ;                   // [SD][M] window integral of the count, written by the SSA
+    const int32_t* sdiff_slot;         // [SS]: compact surface-diffusing index or -1
+    const int32_t* sdiff_spec;         // [SD]
+    const double* sdcst;               // [npatch][SS] surface diffusion constants (m^2/s), 0 = none
+    const int32_t* snbr;               // [M][4]: (neighbour << 2) | its edge, -1 = none
+    const float* sgeo;                 // [M][4]: conditional selectors c0, c1, 1, G = sum l/(A d)
+    const int32_t* tri_inner;          // [M] inner tet (its realization owns the triangle)
+    int32_t nsdiff;
     int32_t nsspec;
     int32_t ntris;
     int32_t nsreac;
@@ -130,6 +140,8 @@ typedef struct sg_window_args {
     unsigned long long* surf_ext;      // [1] surface reaction events since reset
     double* tdel;                      // [D][T] change-time sums handed to the diffusion kernel (split mode)
     const int32_t* diff_spec;          // [D]: species of each diffusing index
+    const int32_t* tet_list;           // [nlist] tets of this launch, or null for all tets
+    int32_t nlist;
     int32_t ntets;                     // total tets over realizations
     int32_t nspec;
     int32_t ndiff;

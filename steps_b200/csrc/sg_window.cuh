@@ -183,7 +183,8 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
 // and their time integrals (ohmic currents) are written back at the end of the window.
 static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const smem_layout& L, const surf_layout& SL,
                                           int tid, int BLOCK, int rb, int re, const double* K, double ivs,
-                                          uint32_t clampm, double T, sg_stream* st, int4 tris) {
+                                          uint32_t clampm, double T, sg_stream* st, int4 tris,
+                                          unsigned long long w, int pending) {
     const sg_surf_args& sa = a.surf;
     const int SS = sa.nsspec, RSP = sa.max_sreac_per_patch, M = sa.ntris;
     uint32_t* sc = L.cnt + tid;
@@ -203,7 +204,27 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
         area[j] = sa.tri_area[m];
         vm[j] = sa.tri_V ? sa.tri_V[m] : 0.0;
         for (int s = 0; s < SS; ++s) {
-            SL.cnt[(j * SS + s) * BLOCK + tid] = sa.tri_counts[(size_t)s * M + m];
+            uint32_t c = sa.tri_counts[(size_t)s * M + m];
+            if (pending && sa.tri_outflow) {
+                // Gather last window's surface-diffusion inflow (slot e: from the neighbour
+                // across edge e).
+                const int sd = sa.sdiff_slot[s];
+                if (sd >= 0 && sa.sdcst[(size_t)p * SS + s] > 0.0) {
+                    const uint4 v = reinterpret_cast<const uint4*>(
+                        sa.tri_outflow + (size_t)((w + 1) & 1ull) * sa.nsdiff * M * 4)[(size_t)sd * M + m];
+                    const int4 nb = reinterpret_cast<const int4*>(sa.snbr)[m];
+                    unsigned long long sum = c;
+                    if (nb.x >= 0) sum += v.x;
+                    if (nb.y >= 0) sum += v.y;
+                    if (nb.z >= 0) sum += v.z;
+                    if (sum > 0xFFFFFFFFull) {
+                        atomicOr(a.status, SG_ERR_OVERFLOW);
+                        sum = 0xFFFFFFFFull;
+                    }
+                    c = (uint32_t)sum;
+                }
+            }
+            SL.cnt[(j * SS + s) * BLOCK + tid] = c;
             SL.occ[(j * SS + s) * BLOCK + tid] = 0.0;
             SL.last[(j * SS + s) * BLOCK + tid] = 0.0;
         }
@@ -317,10 +338,18 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
             size_t o = (size_t)(j * SS + s) * BLOCK + tid;
             uint32_t c = SL.cnt[o];
             sa.tri_counts[(size_t)s * M + m] = c;
-            sa.spec_int[(size_t)s * M + m] += SL.occ[o] + (double)c * (T - SL.last[o]);
+            const double occ = SL.occ[o] + (double)c * (T - SL.last[o]);
+            sa.spec_int[(size_t)s * M + m] += occ;
+            if (sa.tri_occ) {
+                const int sd = sa.sdiff_slot[s];
+                if (sd >= 0) sa.tri_occ[(size_t)sd * M + m] = occ;
+            }
         }
     }
 }
+
+__device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, double t1, float4 g, double odd1,
+                                             double odd2, double odd3, const double* rcp, uint32_t* out_kn);
 
 // Diffusion leave of one (tet, species) with pop > 0 molecules (TOS:1633-1712,
 // diff.cpp:473-585): the occupancy mean n = c_end - sd / T with a Bernoulli on its
@@ -330,7 +359,7 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
 // depend on the SSA's draws, on the other species or on which kernel runs it.
 __device__ __forceinline__ uint4 leave_species(uint64_t seed, uint32_t real, uint32_t unit, unsigned long long w,
                                                uint32_t s, uint32_t pop, double sd, double T, double invT, double D,
-                                               float4 g, double odd1, double odd2, double odd3, const float* rcp,
+                                               float4 g, double odd1, double odd2, double odd3, const double* rcp,
                                                sg_stream* st, uint32_t* out_kn) {
     sg_stream_init(st, seed, real, unit, w, SG_PURPOSE_DIFF + s);
     double t1 = T * (D * (double)g.w);
@@ -346,14 +375,21 @@ __device__ __forceinline__ uint4 leave_species(uint64_t seed, uint32_t real, uin
             if (sg_u01_co(sg_next_u32(st)) < frc) mean_n += 1u;
         }
     }
-    // Stage 0: molecules leaving; stages 1-3: the face split.  One sampler call site.
+    return leave_split(st, mean_n, t1, g, odd1, odd2, odd3, rcp, out_kn);
+}
+
+// Binomial(mean_n, t1) molecules leave, split over the directions by conditional
+// binomials on the selectors g.x, g.y, g.z; the last direction takes the rest.
+__device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, double t1, float4 g, double odd1,
+                                             double odd2, double odd3, const double* rcp, uint32_t* out_kn) {
+    // Stage 0: molecules leaving; stages 1-3: the split.  One sampler call site.
     uint4 k = make_uint4(0u, 0u, 0u, 0u);
     uint32_t n = mean_n, Kn = 0u;
     double pst = t1;
     double ost = (t1 > 0.0 && t1 < 1.0) ? sg_binom_odds(t1) : 0.0;
 #pragma unroll 1
     for (int stage = 0; stage < 4; ++stage) {
-        uint32_t v = sg_binom_leave(st, n, pst, ost, rcp);
+        uint32_t v = sg_binom_o(st, n, pst, ost, rcp);
         if (stage == 0) {
             Kn = v;
             n = v;
@@ -457,7 +493,7 @@ template <int BLOCK, bool SURF = false, bool SPLIT = false>
 __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     window_kernel(sg_window_args a, int check) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ float s_rcp[SG_RCP_TABLE];
+    __shared__ double s_rcp[SG_RCP_TABLE];
     const int S = a.nspec;
     const int R = a.nreac;
     const int tid = threadIdx.x;
@@ -466,7 +502,7 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     if (SURF)
         SLy = surf_carve(smem_raw + ((smem_bytes(BLOCK, S, R) + 15) & ~(size_t)15), BLOCK, a.surf.nsspec,
                          a.surf.max_sreac_per_patch);
-    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0f : 1.0f / (float)i;
+    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
     for (int i = tid; i < R; i += BLOCK) L.reac[i] = a.reacs[i];
     for (int i = tid; i < S; i += BLOCK) L.tot[i] = 0ull;
     for (int i = tid; i < R; i += BLOCK) L.ext[i] = 0u;
@@ -478,9 +514,11 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     const size_t plane = (size_t)a.ntets * 4;  // uint32 words per diffusing species
     unsigned long long moved = 0ull;
 
-    for (int base = blockIdx.x * BLOCK; base < a.ntets; base += gridDim.x * BLOCK) {
-        const int t = base + tid;
-        bool active = t < a.ntets;
+    // A tet list (split windows of membrane models) restricts the launch to those tets.
+    const int nit = a.tet_list ? a.nlist : a.ntets;
+    for (int base = blockIdx.x * BLOCK; base < nit; base += gridDim.x * BLOCK) {
+        bool active = base + tid < nit;
+        const int t = !active ? 0 : (a.tet_list ? __ldg(&a.tet_list[base + tid]) : base + tid);
         int r = 0, comp = 0, tlocal = 0;
         double T = 0.0;
         unsigned long long w = 0;
@@ -496,6 +534,11 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             tlocal = t - rl->tet_begin;
             if (a.comp) comp = __ldg(&a.comp[t]);
             if (comp < 0) active = false;
+            if (SPLIT && !SURF && a.surf.tet_tris) {
+                // Membrane tets run in the SURF launch over the membrane tet list.
+                const int4 tr = __ldg(reinterpret_cast<const int4*>(a.surf.tet_tris) + t);
+                if (tr.x >= 0 || tr.y >= 0 || tr.z >= 0 || tr.w >= 0) active = false;
+            }
         }
         int4 nb = make_int4(-1, -1, -1, -1);
         uint32_t clampm = 0u;
@@ -545,7 +588,7 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
         if (SURF) {
             const int4 tr = __ldg(reinterpret_cast<const int4*>(a.surf.tet_tris) + t);
             if ((tr.x & tr.y & tr.z & tr.w) >= 0 || tr.x >= 0 || tr.y >= 0 || tr.z >= 0 || tr.w >= 0)
-                tet_ssa_surf(a, L, SLy, tid, BLOCK, rb, re, K, ivs, clampm, T, &st, tr);
+                tet_ssa_surf(a, L, SLy, tid, BLOCK, rb, re, K, ivs, clampm, T, &st, tr, w, pending);
             else if (re > rb)
                 tet_ssa(a, L, tid, BLOCK, rb, re, K, ivs, clampm, T, &st);
         } else if (re > rb) {
@@ -615,11 +658,11 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
 // then the end of the window (last block).  Identical results to the fused kernel.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 4) diffuse_kernel(sg_window_args a, int check) {
-    __shared__ float s_rcp[SG_RCP_TABLE];
+    __shared__ double s_rcp[SG_RCP_TABLE];
     __shared__ int flag[2];
     __shared__ unsigned long long s_moved;
     const int tid = threadIdx.x, lane = tid & 31;
-    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0f : 1.0f / (float)i;
+    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
     if (tid == 0) s_moved = 0ull;
     __syncthreads();
     const unsigned long long parity = __ldcg(&a.launch_state[1]) & 1ull;
@@ -669,6 +712,100 @@ __global__ void __launch_bounds__(BLOCK, 4) diffuse_kernel(sg_window_args a, int
     if (tid == 0 && s_moved) atomicAdd(a.diff_total, s_moved);
     if (!window_block_done(a, flag)) return;
     window_last_block(a, check, parity, flag, BLOCK);
+}
+
+// Surface diffusion leave (TOS:1716-1793, sdiff.cpp:498-560), one thread per (surface-
+// diffusing species, membrane triangle), between the SSA and diffuse_kernel of a split
+// window: n = min(pop, window integral / T) with a Bernoulli on its fraction,
+// Binomial(n, min(1, T D G)) leaving, conditional binomials over the three edges.  Each
+// (triangle, species) draws from its own stream (purpose SG_PURPOSE_SDIFF + species).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) sdiffuse_kernel(sg_window_args a) {
+    __shared__ double s_rcp[SG_RCP_TABLE];
+    __shared__ unsigned long long s_moved;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
+    if (tid == 0) s_moved = 0ull;
+    __syncthreads();
+    const sg_surf_args& sa = a.surf;
+    const int M = sa.ntris, SS = sa.nsspec;
+    const long long total = (long long)sa.nsdiff * M;
+    unsigned long long moved = 0ull;
+    for (long long idx = (long long)blockIdx.x * BLOCK + tid; idx < total; idx += (long long)gridDim.x * BLOCK) {
+        const int sd = (int)(idx / M);
+        const int m = (int)(idx - (long long)sd * M);
+        const int r = find_real(a.reals, a.nreal, __ldg(&sa.tri_inner[m]));
+        const sg_real* rl = &a.reals[r];
+        const double rt = rl->t, rend = rl->t_end, per = rl->period;
+        if (!(rt < rend)) continue;
+        const int s = __ldg(&sa.sdiff_spec[sd]);
+        const double D = __ldg(&sa.sdcst[(size_t)__ldg(&sa.tri_patch[m]) * SS + s]);
+        if (!(D > 0.0)) continue;
+        const double T = (rt + per > rend) ? rend - rt : per;
+        const unsigned long long w = rl->window;
+        const size_t ci = (size_t)s * M + m;
+        const uint32_t pop = sa.tri_counts[ci];
+        uint4 k = make_uint4(0u, 0u, 0u, 0u);
+        if (pop > 0u) {
+            const float4 g = __ldg(reinterpret_cast<const float4*>(sa.sgeo) + m);
+            double t1 = T * (D * (double)g.w);
+            if (t1 >= 1.0) t1 = 1.0;
+            double nd = sa.tri_occ[(size_t)sd * M + m] / T;
+            if (nd > (double)pop) nd = (double)pop;
+            const double nint = floor(nd);
+            const double frc = nd - nint;
+            uint32_t mean_n = (uint32_t)nint;
+            sg_stream st;
+            sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)m, w, SG_PURPOSE_SDIFF + (uint32_t)s);
+            if (frc > 0.0) {
+                if (sg_u01_co(sg_next_u32(&st)) < frc) mean_n += 1u;
+            }
+            uint32_t Kn = 0u;
+            k = leave_split(&st, mean_n, t1, g, sg_binom_odds((double)g.x), sg_binom_odds((double)g.y), 0.0, s_rcp,
+                            &Kn);
+            if (Kn > 0u) {
+                sa.tri_counts[ci] = pop - Kn;
+                moved += Kn;
+            }
+        }
+        const int4 nb = __ldg(reinterpret_cast<const int4*>(sa.snbr) + m);
+        uint32_t* po = sa.tri_outflow + (size_t)(w & 1ull) * sa.nsdiff * M * 4 + (size_t)sd * M * 4;
+        if (nb.x >= 0) po[nb.x] = k.x;
+        if (nb.y >= 0) po[nb.y] = k.y;
+        if (nb.z >= 0) po[nb.z] = k.z;
+    }
+    moved = warp_sum_u64(moved);
+    if (lane == 0 && moved) atomicAdd(&s_moved, moved);
+    __syncthreads();
+    if (tid == 0 && s_moved) atomicAdd(a.diff_total, s_moved);
+}
+
+// Apply the pending surface-diffusion inflow to the triangle counts (before host reads).
+static __global__ void sflush_kernel(sg_window_args a) {
+    const sg_surf_args& sa = a.surf;
+    const int M = sa.ntris, SS = sa.nsspec;
+    const long long total = (long long)sa.nsdiff * M;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int sd = (int)(idx / M);
+        const int m = (int)(idx - (long long)sd * M);
+        const sg_real* rl = &a.reals[find_real(a.reals, a.nreal, sa.tri_inner[m])];
+        if (!rl->pending) continue;
+        const int s = sa.sdiff_spec[sd];
+        if (!(sa.sdcst[(size_t)sa.tri_patch[m] * SS + s] > 0.0)) continue;
+        const uint4 v = reinterpret_cast<const uint4*>(sa.tri_outflow + (size_t)((rl->window + 1) & 1ull) *
+                                                                            sa.nsdiff * M * 4)[(size_t)sd * M + m];
+        const int4 nb = reinterpret_cast<const int4*>(sa.snbr)[m];
+        unsigned long long sum = sa.tri_counts[(size_t)s * M + m];
+        if (nb.x >= 0) sum += v.x;
+        if (nb.y >= 0) sum += v.y;
+        if (nb.z >= 0) sum += v.z;
+        if (sum > 0xFFFFFFFFull) {
+            atomicOr(a.status, SG_ERR_OVERFLOW);
+            sum = 0xFFFFFFFFull;
+        }
+        sa.tri_counts[(size_t)s * M + m] = (uint32_t)sum;
+    }
 }
 
 // Apply the pending inflow of the last window to the counts (enter phase only).

@@ -141,10 +141,12 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
             iupd[spec_index[s]] += 1
         return slhs, ilhs, supd, iupd
 
-    sreacs, ohmics = [], []
+    sreacs, ohmics, sdiffs = [], [], []
     for pi, p in enumerate(patches):
         for ssn in p.surfsys:
             ss = model.surfsys[ssn]
+            for did, d in ss.diffs.items():
+                sdiffs.append((pi, did, sid(d.lig), d.dcst))
             for rid, r in ss.sreacs.items():
                 sreacs.append((pi, rid, rows(r), r.kcst, None))
             for rid, r in ss.vdepsreacs.items():
@@ -154,7 +156,35 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
                 sreacs.append((pi, rid, rows(r), 0.0, (vmin, dv, tab)))
             for oid, oc in ss.ohmiccurrs.items():
                 ohmics.append((pi, oid, sid(oc.chanstate), oc.g, oc.erev))
+    # Edge neighbours of every membrane triangle (sdiff.cpp:62-83, TOS:585-630): across edge j
+    # = (v_j, v_j+1) the other membrane triangle on that edge, its edge index, the edge length
+    # and the distance between the two barycentres.
+    tv = np.asarray(geom.tris)[tris]                       # (M, 3) vertex ids
+    M = len(tris)
+    e = np.stack([tv, np.roll(tv, -1, axis=1)], axis=2)   # (M, 3, 2)
+    ek = np.sort(e, axis=2).reshape(-1, 2)
+    order = np.lexsort((ek[:, 1], ek[:, 0]))
+    eks = ek[order]
+    same = np.all(eks[1:] == eks[:-1], axis=1)
+    tri_nbr = np.full(M * 3, -1, dtype=np.int32)
+    tri_nbr_edge = np.full(M * 3, -1, dtype=np.int32)
+    for i in np.nonzero(same)[0]:
+        a, b = order[i], order[i + 1]
+        if i + 2 < len(order) and same[i + 1]:
+            continue  # an edge of three membrane triangles: no surface diffusion across it
+        if i > 0 and same[i - 1]:
+            continue
+        tri_nbr[a], tri_nbr_edge[a] = b // 3, b % 3
+        tri_nbr[b], tri_nbr_edge[b] = a // 3, a % 3
+    pv = np.asarray(geom.verts)
+    tri_len = np.linalg.norm(pv[e[:, :, 1]] - pv[e[:, :, 0]], axis=2).reshape(-1)
+    bary = pv[tv].mean(axis=1)
+    nb = np.where(tri_nbr >= 0, tri_nbr, 0)
+    tri_dist = np.where(tri_nbr >= 0, np.linalg.norm(bary[nb] - np.repeat(bary, 3, axis=0), axis=1), 0.0)
     return {
+        "sdiffs": sdiffs, "tri_nbr": tri_nbr, "tri_nbr_edge": tri_nbr_edge,
+        "tri_len": np.ascontiguousarray(tri_len, dtype=np.float64),
+        "tri_dist": np.ascontiguousarray(tri_dist, dtype=np.float64),
         "patch_names": [p.id for p in patches], "tris": tris, "tri_index": tri_index,
         "tri_patch": tri_patch, "tri_inner": inner,
         "tri_area": np.ascontiguousarray(geom.tri_area[tris], dtype=np.float64),
@@ -235,6 +265,14 @@ class TetOpSplit:
             for (pi, oid, ss, g, erev) in sf["ohmics"]:
                 out = C.c_int32()
                 check(L.sg_add_ohmic(h, pi, ss, g, erev, C.byref(out)))
+            if sf["sdiffs"]:
+                check(L.sg_set_tri_neighbours(h, ptr(sf["tri_nbr"], C.c_int32), ptr(sf["tri_nbr_edge"], C.c_int32),
+                                              ptr(sf["tri_len"], C.c_double), ptr(sf["tri_dist"], C.c_double)))
+                self.sdiff_index = {}
+                for (pi, did, ss, d) in sf["sdiffs"]:
+                    out = C.c_int32()
+                    check(L.sg_add_sdiff(h, pi, ss, float(d), C.byref(out)))
+                    self.sdiff_index[(sf["patch_names"][pi], did)] = out.value
         if realizations is not None:
             off = np.ascontiguousarray(realizations, dtype=np.int32)
             self.nreal = len(off) - 1
@@ -406,9 +444,20 @@ class TetOpSplit:
         check(self._L.sg_set_spec_counts(self._h, self._spec(s), ptr(a, C.c_uint32)))
 
     def getBatchTetSpecCountsNP(self, tets, s, counts):
-        """Reference getBatchTetSpecCountsNP (TOS:5715): counts[i] = count of s in tets[i]."""
-        row = self.getSpecCounts(s)
-        counts[:] = row[np.asarray(tets, dtype=np.int64)]
+        """Reference getBatchTetSpecCountsNP (TOS:5715): counts[i] = count of s in tets[i],
+        gathered on the device."""
+        idx = np.ascontiguousarray(tets, dtype=np.int32)
+        out = np.empty(len(idx), dtype=np.float64)
+        check(self._L.sg_get_batch_tet_counts(self._h, self._spec(s), ptr(idx, C.c_int32), len(idx),
+                                               ptr(out, C.c_double)))
+        counts[:] = out
+
+    def getBatchTetSpecConcsNP(self, tets, s, concs):
+        """Reference getBatchTetSpecConcsNP: molar concentrations of s in tets[i]."""
+        idx = np.ascontiguousarray(tets, dtype=np.int64)
+        c = np.empty(len(idx), dtype=np.float64)
+        self.getBatchTetSpecCountsNP(idx, s, c)
+        concs[:] = c / (AVOGADRO * self.geom.tet_vol[idx] * 1.0e3)
 
     def getBatchTetSpecCounts(self, tets, s):
         out = np.empty(len(tets), dtype=np.float64)

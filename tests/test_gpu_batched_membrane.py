@@ -84,3 +84,60 @@ def test_patch_counts_per_realization_and_channels(steps_lib):
     assert sim.getPatchSpecCount("memb", "Ko", 1) > 0
     assert sim.getCompSpecCount("cyto", "Ca", 1) > 0
     assert sim.getCompSpecCount("cyto", "Ca", 0) == 0 and sim.getCompSpecCount("cyto", "Ca", 2) == 0
+
+
+@pytest.mark.parametrize("batched", [False, True])
+def test_split_window_equals_fused_with_membrane(steps_lib, batched):
+    """Membrane models run the split window by default (volume SSA for the other tets,
+    SURF SSA over the membrane tet list, diffusion leave per species); the fused SURF
+    kernel gives bit-identical counts, channel states and potentials."""
+    def build(split):
+        base = sgeom.kuhn_box(4, 4, 6, W.H)
+        mesh = sgeom.replicate(base, 2) if batched else base
+        cyto = sgeom.TmComp("cyto", mesh, np.arange(mesh.ntets))
+        cyto.addVolsys("vsys")
+        patch = sgeom.TmPatch("memb", mesh, mesh.getSurfTris(), cyto)
+        patch.addSurfsys("ssys")
+        sgeom.Memb("membrane", mesh, [patch])
+        mdl = smodel.Model()
+        ca, cb, cacb = smodel.Spec("Ca", mdl), smodel.Spec("CB", mdl), smodel.Spec("CaCB", mdl)
+        vs = smodel.Volsys("vsys", mdl)
+        smodel.Reac("bind", vs, lhs=[ca, cb], rhs=[cacb], kcst=1e8)
+        smodel.Reac("unbind", vs, lhs=[cacb], rhs=[ca, cb], kcst=100.0)
+        smodel.Diff("dCa", vs, ca, 2.2e-10)
+        smodel.Diff("dCB", vs, cb, 2e-11)
+        ss = smodel.Surfsys("ssys", mdl)
+        ch = smodel.Chan("CaCh", mdl)
+        c, o = smodel.ChanState("C", mdl, ch), smodel.ChanState("O", mdl, ch)
+        smodel.VDepSReac("open", ss, slhs=[c], srhs=[o], k=lambda v: 3000.0 * math.exp(v / 0.025))
+        smodel.VDepSReac("close", ss, slhs=[o], srhs=[c], k=lambda v: 3000.0 * math.exp(-v / 0.025))
+        smodel.SReac("flux", ss, slhs=[o], srhs=[o], irhs=[ca], kcst=2e6)
+        smodel.OhmicCurr("I", ss, chanstate=o, g=20e-12, erev=0.05)
+        sim = TetOpSplit(mdl, mesh, make_rng(31), EF_DV_CG_FP64,
+                         realizations=mesh.offsets if batched else None)
+        sim.setSplit(split)
+        sim.setEfieldDT(2e-6)
+        sim.setMembPotential("membrane", -0.065)
+        sim.setMembCapac("membrane", 0.01)
+        sim.setMembRes("membrane", 1.0 / 0.3, -0.065)
+        sim.setCompSpecConc("cyto", "CB", 50e-6)
+        # 50 channels of 20 pS: the explicit channel current stays stable at dt = 2 us
+        # (membrane time constant C / g ~ 13 us on this 1.28 um^2 box).
+        sim.setPatchSpecCount("memb", "C", 50)
+        sim.setVertIClamp(0, 5e-12)
+        return mesh, patch, sim
+
+    mesh, patch, fused = build(False)
+    _, _, split = build(True)
+    assert split.getSplit() and not fused.getSplit()
+    for k in range(1, 6):
+        fused.run(k * 20e-6)
+        split.run(k * 20e-6)
+        for s in ("Ca", "CB", "CaCB"):
+            assert np.array_equal(fused.getSpecCounts(s), split.getSpecCounts(s)), (k, s)
+        for s in ("C", "O"):
+            assert fused.getPatchSpecCount("memb", s) == split.getPatchSpecCount("memb", s), (k, s)
+    vf = np.array([fused.getVertV(v) for v in range(mesh.nverts)])
+    vsp = np.array([split.getVertV(v) for v in range(mesh.nverts)])
+    assert np.array_equal(vf, vsp)
+    assert fused.getCompSpecCount("cyto", "Ca") > 0

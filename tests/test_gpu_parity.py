@@ -191,3 +191,26 @@ def test_autotuned_run_matches_oracle(steps_lib):
     sim.run(2 * t)
     ora.run(2 * t)
     assert_same(sim, ora, "after tuning")
+
+
+def test_batch_tet_counts_gather(steps_lib):
+    """getBatchTetSpecCountsNP gathers on the device: the values equal the full row at the
+    requested tets (after the pending inflow is applied), concentrations follow, and an
+    index outside the mesh is an ArgErr."""
+    from steps_b200._lib import ArgErr
+
+    mesh = W.cube_mesh(6)
+    sim, ora = pair(W.ab_c_model(), mesh, seed=8)
+    sim.setCompSpecCount("comp", "A", 9000)
+    sim.setCompSpecCount("comp", "B", 9000)
+    sim.run(2e-3)
+    rng = np.random.default_rng(3)
+    tets = rng.integers(0, mesh.ntets, size=777)
+    got = np.empty(len(tets))
+    sim.getBatchTetSpecCountsNP(tets, "A", got)
+    assert np.array_equal(got, sim.getSpecCounts("A")[tets].astype(np.float64))
+    conc = np.empty(len(tets))
+    sim.getBatchTetSpecConcsNP(tets, "A", conc)
+    assert np.allclose(conc, got / (6.02214179e23 * mesh.tet_vol[tets] * 1e3), rtol=1e-15)
+    with pytest.raises(ArgErr):
+        sim.getBatchTetSpecCountsNP(np.array([0, mesh.ntets]), "A", np.empty(2))

@@ -67,16 +67,13 @@ def test_binomial_reference_grid_rejects_wrong(t_test, p_test):
     assert _ref_style_pvalue(sample, 10, p_test, t_test) <= 0.9
 
 
-@pytest.mark.parametrize("leave", [False, True])
 @pytest.mark.parametrize("n,p", [(10, 0.3), (40, 0.2), (1000, 0.3), (200, 0.93), (5000, 0.5),
                                  (1 << 20, 3e-6), (60, 0.999), (4000000000, 2e-9), (25, 0.4),
                                  (47, 0.5), (120, 0.19)])
-def test_binomial_goodness_of_fit(n, p, leave):
-    """Both samplers (FP64 BINV and the diffusion leave's FP32 BINV, BTRD above the cut)
-    against the exact binomial pmf."""
+def test_binomial_goodness_of_fit(n, p):
+    """BINV below the cut, BTRD above it, against the exact binomial pmf."""
     m = 200000
-    draw = pyoracle.binom_leave_many if leave else pyoracle.binom_many
-    x = draw(777, n % 1000, n, p, m).astype(np.int64)
+    x = pyoracle.binom_many(777, n % 1000, n, p, m).astype(np.int64)
     mean, var = n * p, n * p * (1 - p)
     assert abs(x.mean() - mean) < 5 * math.sqrt(var / m) + 1e-12
     lo, hi = stats.binom.ppf(1e-6, n, p), stats.binom.ppf(1 - 1e-6, n, p)
@@ -96,11 +93,11 @@ def test_binomial_goodness_of_fit(n, p, leave):
 
 
 @pytest.mark.parametrize("n,p", [(12, 0.25), (37, 0.33), (25, 0.5)])
-def test_leave_sampler_large_sample(n, p):
-    """The FP32 search at the face-split sizes of the benchmark, 4 M draws: chi-squared
-    over every outcome with expectation >= 5."""
+def test_binv_large_sample(n, p):
+    """The BINV search at the face-split sizes of the benchmark, 4 M draws: chi-squared over
+    every outcome with expectation >= 5."""
     m = 1 << 22
-    x = pyoracle.binom_leave_many(99, n, n, p, m).astype(np.int64)
+    x = pyoracle.binom_many(99, n, n, p, m).astype(np.int64)
     obs = np.bincount(x, minlength=n + 1)[: n + 1]
     pmf = stats.binom.pmf(np.arange(n + 1), n, p)
     keep = pmf * m >= 5
@@ -109,11 +106,6 @@ def test_leave_sampler_large_sample(n, p):
 
 
 def test_binomial_edges():
-    for draw in (pyoracle.binom_many, pyoracle.binom_leave_many):
-        assert (draw(1, 0, 0, 0.5, 10) == 0).all()
-        assert (draw(1, 0, 17, 0.0, 10) == 0).all()
-        assert (draw(1, 0, 17, 1.0, 10) == 17).all()
-        assert draw(1, 0, 3, 0.9999999, 1000).max() <= 3
     assert (pyoracle.binom_many(1, 0, 0, 0.5, 10) == 0).all()
     assert (pyoracle.binom_many(1, 0, 17, 0.0, 10) == 0).all()
     assert (pyoracle.binom_many(1, 0, 17, 1.0, 10) == 17).all()
