@@ -58,6 +58,20 @@ int sg_set_nspecs(sg_solver* h, int32_t nspec);
 int sg_set_mesh(sg_solver* h, int32_t ntets, const double* vol, const int32_t* neighb,
                 const double* area, const double* dist, const int32_t* tet_comp, int32_t ncomp);
 
+/* Diffusion boundaries (diffboundary.cpp): before sg_setup, face_bnd[4t+f] is the boundary
+ * of face f of tet t (-1 none; both tets of a face name the same boundary) and
+ * bnd_comps[2b], bnd_comps[2b+1] the two compartments boundary b joins.  All start closed. */
+int sg_set_diff_boundaries(sg_solver* h, int32_t nbnd, const int32_t* face_bnd, const int32_t* bnd_comps);
+/* setDiffBoundarySpecDiffusionActive (TOS:2745): open or close species spec across the
+ * boundary in both directions, each side diffusing at its own compartment's constant. */
+int sg_set_diff_boundary_active(sg_solver* h, int32_t bnd, int32_t spec, int32_t active);
+int sg_get_diff_boundary_active(sg_solver* h, int32_t bnd, int32_t spec, int32_t* active);
+/* setDiffBoundarySpecDcst (TOS:2865): constant across the boundary, for the direction into
+ * direction_comp only (or both with -1); opens that direction.  A side whose compartment
+ * has no positive constant for the species sends nothing (as the reference, whose boundary
+ * directions belong to the source tet's diffusion rule). */
+int sg_set_diff_boundary_dcst(sg_solver* h, int32_t bnd, int32_t spec, double dcst, int32_t direction_comp);
+
 /* One volume reaction of a compartment: dense lhs/upd rows over nspec species as in
  * Compdef::reac_lhs / reac_upd (compdef.hpp:252-266); kcst as Reacdef kcst. */
 int sg_add_reac(sg_solver* h, int32_t comp, const uint32_t* lhs, const int32_t* upd, double kcst,

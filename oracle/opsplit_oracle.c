@@ -280,6 +280,17 @@ typedef struct {
     uint64_t* window;          /* [nreal] */
     uint64_t ext[OR_MAXR];
     uint64_t diff_moved;
+    /* Diffusion boundaries (diffboundary.cpp; Diff::setDiffBndActive diff.cpp:307 and
+     * setDirectionDcst :394): boundary of each face, the two compartments of each boundary,
+     * the rate table [nbnd][S][side] (-1 closed, -2 at the source's own constant, >= 0 at
+     * that constant), face coefficients A/(V d) of tets with a boundary face (float), and
+     * the face of the neighbour behind each boundary face. */
+    int nbnd;
+    const int32_t* face_bnd;
+    const int32_t* bnd_comps;
+    double* btab;
+    float* bcoef;
+    int32_t* bnbr;
 } or_solver;
 
 or_solver* or_create(uint64_t seed, int ntets, int nspec, int ncomp, const double* vol,
@@ -322,7 +333,62 @@ void or_destroy(or_solver* s) {
     free(s->t);
     free(s->period);
     free(s->window);
+    free(s->btab);
+    free(s->bcoef);
+    free(s->bnbr);
     free(s);
+}
+
+/* Before or_setup: the boundary tables (the arrays are kept by reference). */
+void or_set_boundaries(or_solver* s, int nbnd, const int32_t* face_bnd, const int32_t* bnd_comps) {
+    s->nbnd = nbnd;
+    s->face_bnd = face_bnd;
+    s->bnd_comps = bnd_comps;
+    s->btab = (double*)malloc(sizeof(double) * (size_t)nbnd * s->nspec * 2);
+    for (size_t i = 0; i < (size_t)nbnd * s->nspec * 2; ++i) s->btab[i] = -1.0;
+}
+
+static int or_has_bnd(const or_solver* s, int t) {
+    if (!s->nbnd) return 0;
+    for (int f = 0; f < 4; ++f)
+        if (s->face_bnd[(size_t)t * 4 + f] >= 0) return 1;
+    return 0;
+}
+
+/* Face rates of tet t for species sp at constant D when it has boundary faces; returns the
+ * total and the float conditional selectors (last open face takes the rest). */
+static double or_bnd_split(const or_solver* s, int t, int sp, double D, float cs[3]) {
+    double r[4];
+    const int c = s->tcomp[t];
+    for (int f = 0; f < 4; ++f) {
+        r[f] = 0.0;
+        const double cf = (double)s->bcoef[(size_t)t * 4 + f];
+        if (s->nbr[(size_t)t * 4 + f] >= 0) {
+            r[f] = cf * D;
+            continue;
+        }
+        const int b = s->face_bnd[(size_t)t * 4 + f];
+        if (b < 0) continue;
+        const int side = (c == s->bnd_comps[(size_t)b * 2]) ? 0 : 1;
+        const double v = s->btab[((size_t)b * s->nspec + sp) * 2 + side];
+        if (v < -1.5) r[f] = cf * D;
+        else if (v >= 0.0) r[f] = cf * v;
+    }
+    const double tot = r[0] + r[1] + r[2] + r[3];
+    int lastf = -1;
+    for (int f = 0; f < 4; ++f)
+        if (r[f] > 0.0) lastf = f;
+    double rem = tot;
+    for (int f = 0; f < 3; ++f) {
+        double q = 0.0;
+        if (r[f] > 0.0) {
+            q = (f == lastf) ? 1.0 : r[f] / rem;
+            if (q > 1.0) q = 1.0;
+            rem -= r[f];
+        }
+        cs[f] = (float)q;
+    }
+    return tot;
 }
 
 /* Reactions are appended per compartment in the order given (the caller passes them
@@ -367,7 +433,12 @@ static void or_periods(or_solver* s) {
             double G = (double)s->geo[(size_t)t * 4 + 3];
             for (int sp = 0; sp < s->nspec; ++sp) {
                 if (!s->has_rule[sp]) continue;
-                double sd = s->dcst[((size_t)r * s->ncomp + c) * s->nspec + sp] * G;
+                const double D = s->dcst[((size_t)r * s->ncomp + c) * s->nspec + sp];
+                double sd = D * G;
+                if (or_has_bnd(s, t)) {
+                    float cs[3];
+                    sd = or_bnd_split(s, t, sp, D, cs);
+                }
                 if (sd > mx) mx = sd;
             }
         }
@@ -421,8 +492,39 @@ int or_setup(or_solver* s) {
         }
         s->geo[(size_t)t * 4 + 3] = (float)G;
     }
+    if (s->nbnd) {
+        s->bcoef = (float*)calloc((size_t)T * 4, sizeof(float));
+        s->bnbr = (int32_t*)malloc((size_t)T * 4 * 4);
+        for (int t = 0; t < T; ++t)
+            for (int f = 0; f < 4; ++f) {
+                s->bnbr[(size_t)t * 4 + f] = -1;
+                int n = s->neighb[(size_t)t * 4 + f];
+                if (n < 0) continue;
+                if (s->face_bnd[(size_t)t * 4 + f] >= 0) {
+                    int rf = -1;
+                    for (int j = 0; j < 4; ++j)
+                        if (s->neighb[(size_t)n * 4 + j] == t) rf = j;
+                    s->bnbr[(size_t)t * 4 + f] = n * 4 + rf;
+                }
+            }
+        for (int t = 0; t < T; ++t) {
+            if (!or_has_bnd(s, t)) continue;
+            for (int f = 0; f < 4; ++f) {
+                const int n = s->neighb[(size_t)t * 4 + f];
+                const double d = s->dist[(size_t)t * 4 + f];
+                if (n >= 0 && d > 0.0)
+                    s->bcoef[(size_t)t * 4 + f] = (float)(s->area[(size_t)t * 4 + f] / (s->vol[t] * d));
+            }
+        }
+    }
     or_periods(s);
     return 0;
+}
+
+/* setDiffBoundarySpecDiffusionActive / setDiffBoundarySpecDcst outcome: the rate table. */
+void or_set_btab(or_solver* s, const double* btab) {
+    memcpy(s->btab, btab, sizeof(double) * (size_t)s->nbnd * s->nspec * 2);
+    or_periods(s);
 }
 
 void or_set_counts(or_solver* s, int spec, const uint32_t* row) {
@@ -555,6 +657,8 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
         /* Each (tet, species) leaves on its own stream (purpose 16 + species). */
         or_stream_init(&st, s->seed, (uint32_t)r, (uint32_t)(t - s->real_begin[r]), w, 16u + (uint32_t)i);
         double t1 = T * (D * G);
+        float gs[3] = {g[0], g[1], g[2]};
+        if (or_has_bnd(s, t)) t1 = T * or_bnd_split(s, t, i, D, gs);
         if (t1 >= 1.0) t1 = 1.0;
         uint32_t mean_n = pop;
         if (tdel[i] != 0.0) {
@@ -569,7 +673,7 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
         if (Kn == 0) continue;
         uint32_t rem = Kn;
         for (int f = 0; f < 3; ++f) {
-            o[f] = or_binom(&st, rem, (double)g[f]);
+            o[f] = or_binom(&st, rem, (double)gs[f]);
             rem -= o[f];
         }
         o[3] = rem;
@@ -592,6 +696,14 @@ static void or_tet_enter(or_solver* s, int r, int t) {
             int n = s->nbr[(size_t)t * 4 + f];
             if (n < 0) continue;
             sum += s->outflow[((size_t)i * s->ntets + n) * 4 + s->rface[(size_t)t * 4 + f]];
+        }
+        /* Boundary faces: what the tet behind sent, when it diffuses species i. */
+        for (int f = 0; s->nbnd && f < 4; ++f) {
+            const int nb = s->bnbr[(size_t)t * 4 + f];
+            if (nb < 0) continue;
+            const int n = nb / 4, cn = s->tcomp[n];
+            if (cn >= 0 && s->has_rule[i] && s->dcst[((size_t)r * s->ncomp + cn) * s->nspec + i] > 0.0)
+                sum += s->outflow[((size_t)i * s->ntets + n) * 4 + nb % 4];
         }
         s->counts[(size_t)i * s->ntets + t] = (uint32_t)sum;
     }

@@ -50,6 +50,8 @@ def load():
         lib.or_log_export.argtypes = [C.c_double]
         lib.or_log_export.restype = C.c_double
         lib.or_binom_many.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, pu]
+        lib.or_set_boundaries.argtypes = [P, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        lib.or_set_btab.argtypes = [P, C.POINTER(C.c_double)]
         _lib = lib
     return _lib
 
@@ -84,6 +86,12 @@ class Oracle:
             self.L.or_add_reac(self.h, ci, _p(lhs, C.c_uint32), _p(upd, C.c_int32), k)
         for (ci, _did, s, d) in F["diffs"]:
             self.L.or_add_diff(self.h, ci, s, d)
+        self.nbnd = len(F.get("diffbound_names", []))
+        if self.nbnd:
+            self._keep += [F["face_bnd"], F["bnd_comps"]]
+            self.L.or_set_boundaries(self.h, self.nbnd, _p(F["face_bnd"], C.c_int32), _p(F["bnd_comps"], C.c_int32))
+            self.bact = np.zeros((self.nbnd, self.nspec, 2), dtype=bool)
+            self.bdcst = np.full((self.nbnd, self.nspec, 2), -1.0)
         if self.L.or_setup(self.h) != 0:
             raise ValueError("neighbour table is not symmetric")
 
@@ -91,6 +99,26 @@ class Oracle:
         if getattr(self, "h", None):
             self.L.or_destroy(self.h)
             self.h = None
+
+    def _push_btab(self):
+        tab = np.where(self.bact, np.where(self.bdcst >= 0.0, self.bdcst, -2.0), -1.0)
+        self._btab = np.ascontiguousarray(tab.reshape(-1), dtype=np.float64)
+        self.L.or_set_btab(self.h, _p(self._btab, C.c_double))
+
+    def set_bnd_active(self, b, s, on):
+        """Same rule as the solver's setDiffBoundarySpecDiffusionActive."""
+        self.bact[b, s, :] = on
+        self._push_btab()
+
+    def set_bnd_dcst(self, b, s, d, direction_comp=-1):
+        """Same rule as the solver's setDiffBoundarySpecDcst (direction_comp index, -1 both)."""
+        comps = self.F["bnd_comps"].reshape(-1, 2)[b]
+        for side in range(2):
+            if direction_comp >= 0 and comps[side] == direction_comp:
+                continue
+            self.bact[b, s, side] = True
+            self.bdcst[b, s, side] = d
+        self._push_btab()
 
     def set_counts(self, s, row):
         a = np.ascontiguousarray(row, dtype=np.uint32)

@@ -50,6 +50,10 @@ PROTOTYPES = {
     "sg_destroy": [_P],
     "sg_set_nspecs": [_P, _i32],
     "sg_set_mesh": [_P, _i32, _pf64, _pi32, _pf64, _pf64, _pi32, _i32],
+    "sg_set_diff_boundaries": [_P, _i32, _pi32, _pi32],
+    "sg_set_diff_boundary_active": [_P, _i32, _i32, _i32],
+    "sg_get_diff_boundary_active": [_P, _i32, _i32, _pi32],
+    "sg_set_diff_boundary_dcst": [_P, _i32, _i32, _f64, _i32],
     "sg_add_reac": [_P, _i32, _pu32, _pi32, _f64, _pi32],
     "sg_add_diff": [_P, _i32, _i32, _f64, _pi32],
     "sg_set_realizations": [_P, _i32, _pi32],

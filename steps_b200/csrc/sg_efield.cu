@@ -122,6 +122,10 @@ void EFieldSystem::release() {
     dfree(ell_a64);
     dfree(ell_a32);
     dfree(diag64);
+    dfree(alt_diag64);
+    dfree(alt_einv64);
+    dfree(alt_einv32);
+    alt_dt = -1.0;
     dfree(cap_gext);
     dfree(d_vclamped);
     dfree(b);
@@ -972,17 +976,31 @@ void EFieldSystem::build_matrix(double dt_ms, cudaStream_t stream) {
             row[agg[j] - b0] += a64[(size_t)w * n + i];
         }
     }
+    // The components' blocks are independent: invert them on all host cores.
+    bool spd_ok = true;
+#pragma omp parallel for schedule(dynamic, 1)
     for (int c = 0; c < ncomp_v; ++c) {
         const int m = cbase[c + 1] - cbase[c];
         if (m == 0) continue;
         std::vector<double> blk(E.begin() + boff[c], E.begin() + boff[c + 1]);
-        spd_inverse(m, blk);
+        try {
+            spd_inverse(m, blk);
+        } catch (...) {
+#pragma omp atomic write
+            spd_ok = false;
+            continue;
+        }
         std::copy(blk.begin(), blk.end(), E.begin() + boff[c]);
     }
+    if (!spd_ok) throw DeviceErr("EField coarse matrix is not positive definite");
     std::vector<float> E32(E.begin(), E.end());
     if (na != nagg || (size_t)boff[ncomp_v] != einv_len || !d_agg) {
         dfree(d_einv64);
         dfree(d_einv32);
+        dfree(alt_diag64);
+        dfree(alt_einv64);
+        dfree(alt_einv32);
+        alt_dt = -1.0;
         dfree(d_c64);
         dfree(d_c32);
         dfree(d_agg_base);
@@ -1134,7 +1152,33 @@ void EFieldSystem::pcg(cudaStream_t stream, int n, int g, const T* a, T* xv, T* 
 // is rebuilt when the step length changes by more than rounding (the truncated last step
 // of a run), or when clamps or membrane properties change.
 void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
-    if (dirty || std::fabs(dt_ms - dt_built) > 1e-9 * dt_built) build_matrix(dt_ms, stream);
+    if (dirty || std::fabs(dt_ms - dt_built) > 1e-9 * dt_built) {
+        // The diagonal and the coarse inverses depend on dt; the previous step length's
+        // are kept, so a run that ends on a short step and resumes at the regular one (or
+        // alternates two lengths) swaps instead of rebuilding on the host.
+        const bool keep = !dirty && dt_built > 0.0 && d_einv64;
+        if (keep && alt_dt > 0.0 && std::fabs(dt_ms - alt_dt) <= 1e-9 * alt_dt) {
+            std::swap(diag64, alt_diag64);
+            std::swap(d_einv64, alt_einv64);
+            std::swap(d_einv32, alt_einv32);
+            std::swap(dt_built, alt_dt);
+        } else {
+            if (keep) {
+                if (!alt_diag64) {
+                    dalloc(alt_diag64, nverts);
+                    dalloc(alt_einv64, std::max<size_t>(einv_len, 1));
+                    dalloc(alt_einv32, std::max<size_t>(einv_len, 1));
+                }
+                std::swap(diag64, alt_diag64);
+                std::swap(d_einv64, alt_einv64);
+                std::swap(d_einv32, alt_einv32);
+                alt_dt = dt_built;
+            } else {
+                alt_dt = -1.0;
+            }
+            build_matrix(dt_ms, stream);
+        }
+    }
     const int n = nverts;
     const int g = grid_for(n, nsm);
     const Segs sg{nseg, d_seg_ptr, d_seg_idx, d_seg_agg};

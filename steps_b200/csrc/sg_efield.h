@@ -69,6 +69,12 @@ struct EFieldSystem {
     double* ell_a64 = nullptr;            // [width][nverts] -cc_ij, clamped columns removed
     float* ell_a32 = nullptr;
     double* diag64 = nullptr;             // A_ii
+    // The previous step length's diagonal and coarse inverses (swapped back in when dt
+    // returns to it without a rebuild); alt_dt < 0: none.
+    double alt_dt = -1.0;
+    double* alt_diag64 = nullptr;
+    double* alt_einv64 = nullptr;
+    float* alt_einv32 = nullptr;
     double* cap_gext = nullptr;           // [2][nverts]: C_i (pF), g_i (nS)
     uint8_t* d_vclamped = nullptr;
     // Two-level preconditioner M^-1 = D^-1 + Z E^-1 Z^T: Z aggregates vertices into spatial

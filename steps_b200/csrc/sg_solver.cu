@@ -106,6 +106,19 @@ struct Solver {
     DevBuf<uint32_t> d_counts, d_outflow, d_clamp, d_status;
     DevBuf<int32_t> d_nbr, d_comp, d_crb, d_dslot, d_dspec;
     DevBuf<double> d_tdel;                      // [D][T] split mode only
+    // Diffusion boundaries.
+    int nbnd = 0;
+    std::vector<int32_t> face_bnd, bnd_comps;   // [T*4] boundary of each face or -1; [nbnd*2]
+    std::vector<double> btab;                   // [nbnd][S][2] -1 closed, -2 own constant, >= 0 constant
+    std::vector<uint8_t> bact;                  // [nbnd][S][2] direction open (side = source compartment)
+    std::vector<double> bdcst;                  // [nbnd][S][2] direction constant, -1 = the source's own
+    std::vector<uint32_t> bface;                // [T] bytes per face, 0xFF = none
+    std::vector<int32_t> bnbr;                  // [T*4]
+    std::vector<float> bcoef;                   // [T*4]
+    DevBuf<uint32_t> d_bface;
+    DevBuf<int32_t> d_bnbr, d_bcomps;
+    DevBuf<float> d_bcoef;
+    DevBuf<double> d_btab;
     bool split = false;                         // window as two kernels (reactions, diffusion)
     DevBuf<float> d_geo;
     DevBuf<double> d_ivs, d_kcst, d_dcst;
@@ -458,6 +471,21 @@ struct Solver {
         if (R) h2d(d_reacs.p, reacs.data(), reacs.size());
         h2d(d_crb.p, comp_reac_begin.data(), comp_reac_begin.size());
         h2d(d_dslot.p, diff_slot.data(), diff_slot.size());
+        if (nbnd > 0) {
+            bact.assign((size_t)nbnd * nspec * 2, 0);
+            bdcst.assign((size_t)nbnd * nspec * 2, -1.0);
+            btab.assign((size_t)nbnd * nspec * 2, -1.0);
+            d_bface.alloc(bface.size());
+            d_bnbr.alloc(bnbr.size());
+            d_bcoef.alloc(bcoef.size());
+            d_bcomps.alloc(bnd_comps.size());
+            d_btab.alloc(btab.size());
+            h2d(d_bface.p, bface.data(), bface.size());
+            h2d(d_bnbr.p, bnbr.data(), bnbr.size());
+            h2d(d_bcoef.p, bcoef.data(), bcoef.size());
+            h2d(d_bcomps.p, bnd_comps.data(), bnd_comps.size());
+            h2d(d_btab.p, btab.data(), btab.size());
+        }
         {
             std::vector<int32_t> dspec(std::max(ndiff, 1), 0);
             for (int s = 0; s < nspec; ++s)
@@ -519,6 +547,107 @@ struct Solver {
             }
             geo[(size_t)t * 4 + 3] = (float)G;
         }
+        build_boundaries();
+    }
+
+    // Boundary faces: the two tets of a face must be in the boundary's two compartments.
+    void build_boundaries() {
+        if (nbnd == 0) return;
+        bface.assign(ntets, 0xFFFFFFFFu);
+        bnbr.assign((size_t)ntets * 4, -1);
+        bcoef.assign((size_t)ntets * 4, 0.0f);
+        for (int t = 0; t < ntets; ++t)
+            for (int f = 0; f < 4; ++f) {
+                const int b = face_bnd[(size_t)t * 4 + f];
+                if (b < 0) continue;
+                if (b >= nbnd) throw ArgErr("diffusion boundary index out of range");
+                const int n = neighb[(size_t)t * 4 + f];
+                if (n < 0) throw ArgErr("diffusion boundary face without a second tet");
+                const int ca = bnd_comps[(size_t)b * 2], cb = bnd_comps[(size_t)b * 2 + 1];
+                const int c = tet_comp[t], cn = tet_comp[n];
+                if (!((c == ca && cn == cb) || (c == cb && cn == ca)))
+                    throw ArgErr("diffusion boundary face does not join the boundary's compartments");
+                int rf = -1;
+                for (int j = 0; j < 4; ++j)
+                    if (neighb[(size_t)n * 4 + j] == t) rf = j;
+                if (face_bnd[(size_t)n * 4 + rf] != b) throw ArgErr("diffusion boundary faces are not symmetric");
+                bface[t] = (bface[t] & ~(0xFFu << (8 * f))) | ((uint32_t)b << (8 * f));
+                bnbr[(size_t)t * 4 + f] = (n << 2) | rf;
+                const double d = dist[(size_t)t * 4 + f];
+                if (!(d > 0.0)) throw ArgErr("diffusion boundary face with zero distance");
+            }
+        // Face coefficients of every tet that has a boundary face (all its faces).
+        for (int t = 0; t < ntets; ++t) {
+            if (bface[t] == 0xFFFFFFFFu) continue;
+            for (int f = 0; f < 4; ++f) {
+                const int n = neighb[(size_t)t * 4 + f];
+                const double d = dist[(size_t)t * 4 + f];
+                if (n >= 0 && d > 0.0) bcoef[(size_t)t * 4 + f] = (float)(area[(size_t)t * 4 + f] / (vol[t] * d));
+            }
+        }
+    }
+
+    // setDiffBoundarySpecDiffusionActive / setDiffBoundarySpecDcst (TOS:2745-2800, 2865-2930).
+    void check_bnd(int b, int s) const {
+        if (b < 0 || b >= nbnd) throw ArgErr("diffusion boundary index out of range");
+        check_spec(s);
+        if (diff_slot[s] < 0) throw ArgErr("species has no diffusion rule");
+    }
+    void upload_btab() {
+        for (size_t i = 0; i < btab.size(); ++i) btab[i] = bact[i] ? (bdcst[i] >= 0.0 ? bdcst[i] : -2.0) : -1.0;
+        h2d(d_btab.p, btab.data(), btab.size());
+        recompute_periods();
+        upload_reals();
+        sync();
+    }
+    void set_bnd_active(int b, int s, bool on) {
+        require_setup();
+        check_bnd(b, s);
+        flush();
+        for (int side = 0; side < 2; ++side) bact[((size_t)b * nspec + s) * 2 + side] = on ? 1 : 0;
+        upload_btab();
+    }
+    bool get_bnd_active(int b, int s) const {
+        check_bnd(b, s);
+        return bact[((size_t)b * nspec + s) * 2] || bact[((size_t)b * nspec + s) * 2 + 1];
+    }
+    // direction_comp >= 0: only diffusion into that compartment takes dcst (and opens).
+    void set_bnd_dcst(int b, int s, double d, int direction_comp) {
+        require_setup();
+        check_bnd(b, s);
+        if (!(d >= 0.0)) throw ArgErr("diffusion constant must be non-negative");
+        if (direction_comp >= 0 && direction_comp != bnd_comps[(size_t)b * 2] &&
+            direction_comp != bnd_comps[(size_t)b * 2 + 1])
+            throw ArgErr("direction compartment is not joined by this boundary");
+        flush();
+        for (int side = 0; side < 2; ++side) {
+            const int src = bnd_comps[(size_t)b * 2 + side];
+            if (direction_comp >= 0 && src == direction_comp) continue;
+            bact[((size_t)b * nspec + s) * 2 + side] = 1;
+            bdcst[((size_t)b * nspec + s) * 2 + side] = d;
+        }
+        upload_btab();
+    }
+
+    // Scaled diffusion constant of tet t for species s at constant D (TOS:5373 with the
+    // boundary directions of diff.cpp:340-398).
+    double tet_scaled_dcst(int t, int s, double D) const {
+        if (nbnd == 0 || bface[t] == 0xFFFFFFFFu) return D * (double)geo[(size_t)t * 4 + 3];
+        double tot = 0.0;
+        for (int f = 0; f < 4; ++f) {
+            const double cf = (double)bcoef[(size_t)t * 4 + f];
+            if (nbrp[(size_t)t * 4 + f] >= 0) {
+                tot += cf * D;
+                continue;
+            }
+            const uint32_t b = (bface[t] >> (8 * f)) & 0xFFu;
+            if (b == 0xFFu) continue;
+            const int side = (tet_comp[t] == bnd_comps[(size_t)b * 2]) ? 0 : 1;
+            const double v = btab[((size_t)b * nspec + s) * 2 + side];
+            if (v < -1.5) tot += cf * D;
+            else if (v >= 0.0) tot += cf * v;
+        }
+        return tot;
     }
 
     // Largest scaled diffusion constant per realization -> update period
@@ -532,7 +661,8 @@ struct Solver {
                 double G = (double)geo[(size_t)t * 4 + 3];
                 for (int s = 0; s < nspec; ++s) {
                     if (diff_slot[s] < 0) continue;
-                    double sd = dcst[((size_t)r * ncomp + c) * nspec + s] * G;
+                    const double D = dcst[((size_t)r * ncomp + c) * nspec + s];
+                    double sd = (nbnd > 0) ? tet_scaled_dcst(t, s, D) : D * G;
                     if (sd > mx) mx = sd;
                 }
             }
@@ -631,6 +761,14 @@ struct Solver {
         a.surf_ext = has_surf() ? d_surf_ext.p : nullptr;
         a.tdel = d_tdel.p;
         a.diff_spec = d_dspec.p;
+        if (nbnd > 0) {
+            a.bface = d_bface.p;
+            a.bnbr = d_bnbr.p;
+            a.bcoef = d_bcoef.p;
+            a.bcomps = d_bcomps.p;
+            a.btab = d_btab.p;
+            a.nbnd = nbnd;
+        }
         a.ntets = ntets;
         a.nspec = nspec;
         a.ndiff = ndiff;
@@ -1420,7 +1558,7 @@ struct Solver {
     struct CkptHeader {
         char magic[8];
         uint32_t version;
-        int32_t ntets, nspec, nreal, ncomp, nreac, ntris, nsspec, nverts, nsreac;
+        int32_t ntets, nspec, nreal, ncomp, nreac, ntris, nsspec, nverts, nsreac, nbnd;
         uint64_t seed, niteration, setup_calls;
         double efdt;
     };
@@ -1466,6 +1604,7 @@ struct Solver {
         hd.nsspec = nsspec;
         hd.nverts = ef_on ? ef.nverts : 0;
         hd.nsreac = (int32_t)sreacs.size();
+        hd.nbnd = nbnd;
         hd.seed = seed;
         hd.niteration = niteration;
         hd.setup_calls = setup_calls;
@@ -1492,6 +1631,10 @@ struct Solver {
             put_dev(f, d_ext_total.p, d_ext_total.n);
             put_dev(f, d_diff_total.p, d_diff_total.n);
             put_dev(f, d_launch.p, d_launch.n);
+            if (nbnd > 0) {
+                put(f, bact.data(), bact.size());
+                put(f, bdcst.data(), bdcst.size());
+            }
             if (has_surf()) {
                 put(f, skcst.data(), skcst.size());
                 put_dev(f, d_tri_counts.p, d_tri_counts.n);
@@ -1529,7 +1672,7 @@ struct Solver {
             if (std::memcmp(hd.magic, me.magic, 8) != 0 || hd.version != 1) throw ArgErr("not a checkpoint file");
             if (hd.ntets != me.ntets || hd.nspec != me.nspec || hd.nreal != me.nreal || hd.ncomp != me.ncomp ||
                 hd.nreac != me.nreac || hd.ntris != me.ntris || hd.nsspec != me.nsspec || hd.nverts != me.nverts ||
-                hd.nsreac != me.nsreac)
+                hd.nsreac != me.nsreac || hd.nbnd != me.nbnd)
                 throw ArgErr("checkpoint was written by a solver with another mesh or model");
             get(f, reals.data(), reals.size(), "realizations");
             get(f, kcst.data(), kcst.size(), "reaction constants");
@@ -1548,6 +1691,13 @@ struct Solver {
             get_dev(f, d_ext_total.p, d_ext_total.n, "extents");
             get_dev(f, d_diff_total.p, d_diff_total.n, "diffusion extent");
             get_dev(f, d_launch.p, d_launch.n, "launch state");
+            if (nbnd > 0) {
+                get(f, bact.data(), bact.size(), "diffusion boundaries");
+                get(f, bdcst.data(), bdcst.size(), "diffusion boundary constants");
+                for (size_t i = 0; i < btab.size(); ++i)
+                    btab[i] = bact[i] ? (bdcst[i] >= 0.0 ? bdcst[i] : -2.0) : -1.0;
+                h2d(d_btab.p, btab.data(), btab.size());
+            }
             if (has_surf()) {
                 get(f, skcst.data(), skcst.size(), "surface constants");
                 h2d(d_skcst.p, skcst.data(), skcst.size());
@@ -1688,6 +1838,41 @@ int sg_set_mesh(sg_solver* h, int32_t ntets, const double* vol, const int32_t* n
         s->nreal = 1;
         s->dcst_def.assign((size_t)ncomp * std::max(s->nspec, 0), 0.0);
     });
+}
+
+int sg_set_diff_boundaries(sg_solver* h, int32_t nbnd, const int32_t* face_bnd, const int32_t* bnd_comps) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (s->ntets <= 0) throw sg::ProgErr("set the mesh first");
+        if (nbnd < 0 || nbnd > 254) throw sg::ArgErr("at most 254 diffusion boundaries");
+        if (nbnd == 0) {
+            s->nbnd = 0;
+            return;
+        }
+        need(face_bnd, "face_bnd");
+        need(bnd_comps, "bnd_comps");
+        s->nbnd = nbnd;
+        s->face_bnd.assign(face_bnd, face_bnd + (size_t)s->ntets * 4);
+        s->bnd_comps.assign(bnd_comps, bnd_comps + (size_t)nbnd * 2);
+        for (int32_t c : s->bnd_comps)
+            if (c < 0 || c >= s->ncomp) throw sg::ArgErr("boundary compartment out of range");
+    });
+}
+
+int sg_set_diff_boundary_active(sg_solver* h, int32_t bnd, int32_t spec, int32_t active) {
+    return guarded([&] { S(h)->set_bnd_active(bnd, spec, active != 0); });
+}
+
+int sg_get_diff_boundary_active(sg_solver* h, int32_t bnd, int32_t spec, int32_t* active) {
+    return guarded([&] {
+        need(active, "active");
+        *active = S(h)->get_bnd_active(bnd, spec) ? 1 : 0;
+    });
+}
+
+int sg_set_diff_boundary_dcst(sg_solver* h, int32_t bnd, int32_t spec, double dcst, int32_t direction_comp) {
+    return guarded([&] { S(h)->set_bnd_dcst(bnd, spec, dcst, direction_comp); });
 }
 
 int sg_add_reac(sg_solver* h, int32_t comp, const uint32_t* lhs, const int32_t* upd, double kcst,

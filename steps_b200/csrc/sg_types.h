@@ -142,6 +142,17 @@ typedef struct sg_window_args {
     const int32_t* diff_spec;          // [D]: species of each diffusing index
     const int32_t* tet_list;           // [nlist] tets of this launch, or null for all tets
     int32_t nlist;
+    // Diffusion boundaries (diffboundary.cpp, diff.cpp:307-398), null without any: per tet
+    // the boundary of each face (byte f, 0xFF = none), the neighbour behind boundary faces
+    // ((n << 2) | its face, -1), the face coefficients A / (V d), the two compartments of
+    // each boundary and the rate table [nbnd][S][side]: -1 closed, -2 open at the source
+    // compartment's constant, >= 0 open at that constant (m^2/s).
+    const uint32_t* bface;
+    const int32_t* bnbr;
+    const float* bcoef;
+    const int32_t* bcomps;
+    const double* btab;
+    int32_t nbnd;
     int32_t ntets;                     // total tets over realizations
     int32_t nspec;
     int32_t ndiff;

@@ -351,18 +351,93 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
 __device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, double t1, float4 g, double odd1,
                                              double odd2, double odd3, const double* rcp, uint32_t* out_kn);
 
+// Inflow of species s through the diffusion-boundary faces of tet t (slots v.f of the tet's
+// own inflow): counted when the tet behind face f diffuses s, because that tet then wrote
+// the slot this window (0 while the boundary is closed in its direction).
+__device__ __forceinline__ unsigned long long bnd_inflow(const sg_window_args& a, int t, int r, int s, uint4 v) {
+    const uint32_t bf = __ldg(&a.bface[t]);
+    if (bf == 0xFFFFFFFFu) return 0ull;
+    const uint32_t vv[4] = {v.x, v.y, v.z, v.w};
+    unsigned long long sum = 0ull;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        if (((bf >> (8 * f)) & 0xFFu) == 0xFFu) continue;
+        const int n = __ldg(&a.bnbr[(size_t)t * 4 + f]) >> 2;
+        const int cn = a.comp ? __ldg(&a.comp[n]) : 0;
+        if (cn >= 0 && __ldg(&a.dcst[((size_t)r * a.ncomp + cn) * a.nspec + s]) > 0.0) sum += vv[f];
+    }
+    return sum;
+}
+
+// Rates of tet t for species s through its faces when some face is a diffusion boundary:
+// same-compartment faces at D, boundary faces at the boundary's rate for the tet's side
+// (closed: 0), each times the face coefficient A / (V d).  Returns the total and the
+// conditional selectors in g (the last open face takes the rest), as the host builds them
+// for tets without boundary faces.
+__device__ __forceinline__ double bnd_split(const sg_window_args& a, int t, int comp, int s, double D, int4 nb,
+                                            float4* g) {
+    const uint32_t bf = __ldg(&a.bface[t]);
+    const float4 cf = __ldg(reinterpret_cast<const float4*>(a.bcoef) + t);
+    const float c4[4] = {cf.x, cf.y, cf.z, cf.w};
+    const int n4[4] = {nb.x, nb.y, nb.z, nb.w};
+    double r[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        r[f] = 0.0;
+        if (n4[f] >= 0) {
+            r[f] = (double)c4[f] * D;
+        } else {
+            const uint32_t b = (bf >> (8 * f)) & 0xFFu;
+            if (b != 0xFFu) {
+                const int side = (comp == __ldg(&a.bcomps[b * 2])) ? 0 : 1;
+                const double v = __ldg(&a.btab[((size_t)b * a.nspec + s) * 2 + side]);
+                if (v < -1.5) r[f] = (double)c4[f] * D;
+                else if (v >= 0.0) r[f] = (double)c4[f] * v;
+            }
+        }
+    }
+    const double tot = r[0] + r[1] + r[2] + r[3];
+    int lastf = -1;
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+        if (r[f] > 0.0) lastf = f;
+    double rem = tot;
+    float cs[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        double c = 0.0;
+        if (r[f] > 0.0) {
+            c = (f == lastf) ? 1.0 : r[f] / rem;
+            if (c > 1.0) c = 1.0;
+            rem -= r[f];
+        }
+        cs[f] = (float)c;
+    }
+    *g = make_float4(cs[0], cs[1], cs[2], 0.0f);
+    return tot;
+}
+
+// Scatter of the boundary faces' leavers into the neighbours' slots.
+__device__ __forceinline__ void bnd_scatter(const sg_window_args& a, int t, uint32_t* po, uint4 k) {
+    const uint32_t bf = __ldg(&a.bface[t]);
+    const uint32_t kk[4] = {k.x, k.y, k.z, k.w};
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+        if (((bf >> (8 * f)) & 0xFFu) != 0xFFu) po[__ldg(&a.bnbr[(size_t)t * 4 + f])] = kk[f];
+}
+
 // Diffusion leave of one (tet, species) with pop > 0 molecules (TOS:1633-1712,
 // diff.cpp:473-585): the occupancy mean n = c_end - sd / T with a Bernoulli on its
-// fraction, Binomial(n, min(1, T D G)) leaving, split over the faces by conditional
+// fraction, Binomial(n, min(1, t1)) leaving (t1 = T D G, or T times the summed face rates
+// at a diffusion boundary), split over the faces by conditional
 // binomials on the selectors c0..c2 (the last face takes the rest).  Each (tet, species)
 // draws from its own stream (purpose SG_PURPOSE_DIFF + species), so the result does not
 // depend on the SSA's draws, on the other species or on which kernel runs it.
 __device__ __forceinline__ uint4 leave_species(uint64_t seed, uint32_t real, uint32_t unit, unsigned long long w,
-                                               uint32_t s, uint32_t pop, double sd, double T, double invT, double D,
+                                               uint32_t s, uint32_t pop, double sd, double invT, double t1,
                                                float4 g, double odd1, double odd2, double odd3, const double* rcp,
                                                sg_stream* st, uint32_t* out_kn) {
     sg_stream_init(st, seed, real, unit, w, SG_PURPOSE_DIFF + s);
-    double t1 = T * (D * (double)g.w);
     if (t1 >= 1.0) t1 = 1.0;
     uint32_t mean_n = pop;
     if (sd != 0.0) {
@@ -563,6 +638,7 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
                     if (nb.y >= 0) sum += v.y;
                     if (nb.z >= 0) sum += v.z;
                     if (nb.w >= 0) sum += v.w;
+                    if (a.bface) sum += bnd_inflow(a, t, r, s, v);
                     if (sum > 0xFFFFFFFFull) {
                         atomicOr(a.status, SG_ERR_OVERFLOW);
                         sum = 0xFFFFFFFFull;
@@ -618,10 +694,19 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             if (!(D > 0.0)) continue;
             uint32_t pop = L.cnt[s * BLOCK + tid];
             uint4 k = make_uint4(0u, 0u, 0u, 0u);
+            const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
             if (pop > 0u) {
                 uint32_t Kn = 0u;
-                k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop,
-                                  L.tdel[s * BLOCK + tid], T, invT, D, g, odd1, odd2, odd3, s_rcp, &st, &Kn);
+                if (bt) {
+                    float4 gb;
+                    const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
+                    k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
+                                      invT, T * tot, gb, sg_binom_odds((double)gb.x), sg_binom_odds((double)gb.y),
+                                      sg_binom_odds((double)gb.z), s_rcp, &st, &Kn);
+                } else {
+                    k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
+                                      invT, T * (D * (double)g.w), g, odd1, odd2, odd3, s_rcp, &st, &Kn);
+                }
                 if (Kn > 0u) {
                     if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
                     moved += Kn;
@@ -634,6 +719,7 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             if (nb.y >= 0) po[nb.y] = k.y;
             if (nb.z >= 0) po[nb.z] = k.z;
             if (nb.w >= 0) po[nb.w] = k.w;
+            if (bt) bnd_scatter(a, t, po, k);
         }
         // Phase 4: store counts.
         for (int s = 0; s < S; ++s) a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
@@ -688,12 +774,15 @@ __global__ void __launch_bounds__(BLOCK, 4) diffuse_kernel(sg_window_args a, int
         const size_t ci = (size_t)s * a.ntets + t;
         const uint32_t pop = a.counts[ci];
         uint4 k = make_uint4(0u, 0u, 0u, 0u);
+        const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
         if (pop > 0u) {
-            const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
+            float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
+            double t1 = T * (D * (double)g.w);
+            if (bt) t1 = T * bnd_split(a, t, comp, s, D, nb, &g);
             sg_stream st;
             uint32_t Kn = 0u;
             k = leave_species(a.seed, (uint32_t)r, (uint32_t)(t - rl->tet_begin), w, (uint32_t)s, pop,
-                              a.tdel[(size_t)ds * a.ntets + t], T, 1.0 / T, D, g, sg_binom_odds((double)g.x),
+                              a.tdel[(size_t)ds * a.ntets + t], 1.0 / T, t1, g, sg_binom_odds((double)g.x),
                               sg_binom_odds((double)g.y), sg_binom_odds((double)g.z), s_rcp, &st, &Kn);
             if (Kn > 0u) {
                 if (!((clampm >> s) & 1u)) a.counts[ci] = pop - Kn;
@@ -705,6 +794,7 @@ __global__ void __launch_bounds__(BLOCK, 4) diffuse_kernel(sg_window_args a, int
         if (nb.y >= 0) po[nb.y] = k.y;
         if (nb.z >= 0) po[nb.z] = k.z;
         if (nb.w >= 0) po[nb.w] = k.w;
+        if (bt) bnd_scatter(a, t, po, k);
     }
     moved = warp_sum_u64(moved);
     if (lane == 0 && moved) atomicAdd(&s_moved, moved);
@@ -830,6 +920,7 @@ static __global__ void flush_kernel(sg_window_args a) {
             if (nb.y >= 0) sum += v.y;
             if (nb.z >= 0) sum += v.z;
             if (nb.w >= 0) sum += v.w;
+            if (a.bface) sum += bnd_inflow(a, t, r, s, v);
             if (sum > 0xFFFFFFFFull) {
                 atomicOr(a.status, SG_ERR_OVERFLOW);
                 sum = 0xFFFFFFFFull;

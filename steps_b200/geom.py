@@ -186,6 +186,36 @@ class Memb:
         mesh.membs[id] = self
 
 
+class DiffBoundary:
+    """Triangles between two compartments across which chosen species may diffuse
+    (src/steps/geom/diffboundary.hpp; activated per species on the solver)."""
+
+    def __init__(self, id, mesh, tris):
+        self.id = id
+        self.mesh = mesh
+        self.tris = np.asarray(tris, dtype=np.int64)
+        owner = {}
+        for name, c in mesh.comps.items():
+            for t in c.tets:
+                owner[int(t)] = name
+        comps = set()
+        for t in self.tris:
+            a, b = mesh.tri_tets[t]
+            if a < 0 or b < 0:
+                raise ValueError(f"diffusion boundary triangle {t} is on the mesh surface")
+            ca = owner.get(int(a))
+            cb = owner.get(int(b))
+            if ca is None or cb is None or ca == cb:
+                raise ValueError(f"diffusion boundary triangle {t} does not join two compartments")
+            comps.add(tuple(sorted((ca, cb))))
+        if len(comps) != 1:
+            raise ValueError("a diffusion boundary joins exactly two compartments")
+        self.comps = next(iter(comps))
+        if not hasattr(mesh, "diffbounds"):
+            mesh.diffbounds = {}
+        mesh.diffbounds[id] = self
+
+
 def replicate(mesh, n, gap=None):
     """n disjoint copies of mesh in one Tetmesh (batched realizations of one geometry): copy r
     is shifted along x by r * (extent + gap) and owns tets [r T, (r + 1) T); every derived

@@ -70,7 +70,20 @@ def flatten(model, geom):
             for did, d in vs.diffs.items():
                 diffs.append((ci, did, sidx(d.lig), d.dcst))
     surf = flatten_surface(model, geom, spec_index, comp_index, tet_comp)
+    # Diffusion boundaries: the boundary of every tet face (-1 none) and the boundary's
+    # two compartments (diffboundary.cpp).
+    dbs = list(getattr(geom, "diffbounds", {}).values())
+    face_bnd = np.full((geom.ntets, 4), -1, dtype=np.int32)
+    bnd_comps = np.zeros((len(dbs), 2), dtype=np.int32)
+    for bi, db in enumerate(dbs):
+        bnd_comps[bi] = [comp_index[db.comps[0]], comp_index[db.comps[1]]]
+        for tri in db.tris:
+            for tet in geom.tri_tets[tri]:
+                f = int(np.nonzero(geom.tet_tri[tet] == tri)[0][0])
+                face_bnd[tet, f] = bi
     return {
+        "diffbound_names": [db.id for db in dbs], "face_bnd": np.ascontiguousarray(face_bnd.reshape(-1)),
+        "bnd_comps": np.ascontiguousarray(bnd_comps.reshape(-1)),
         "spec_names": spec_names, "spec_index": spec_index,
         "comp_names": comp_names, "comp_index": comp_index,
         "tet_comp": tet_comp, "reacs": reacs, "diffs": diffs, "surf": surf,
@@ -233,6 +246,10 @@ class TetOpSplit:
         check(L.sg_set_mesh(h, geom.ntets, ptr(F["vol"], C.c_double), ptr(F["neighb"], C.c_int32),
                             ptr(F["area"], C.c_double), ptr(F["dist"], C.c_double),
                             ptr(F["tet_comp"], C.c_int32), max(len(self.comp_names), 1)))
+        self.diffbound_index = {n: i for i, n in enumerate(F["diffbound_names"])}
+        if F["diffbound_names"]:
+            check(L.sg_set_diff_boundaries(h, len(F["diffbound_names"]), ptr(F["face_bnd"], C.c_int32),
+                                           ptr(F["bnd_comps"], C.c_int32)))
         self.reac_index = {}   # (comp, reac id) -> ABI reaction index
         self.diff_index = {}   # (comp, diff id) -> species index
         for (ci, rid, lhs, upd, k) in F["reacs"]:
@@ -465,6 +482,33 @@ class TetOpSplit:
         return list(out)
 
     # ------------------------------------------------------------- constants
+    # ------------------------------------------------- diffusion boundaries
+    def _db(self, db):
+        try:
+            return self.diffbound_index[db]
+        except KeyError:
+            raise ArgErr(f"unknown diffusion boundary '{db}'") from None
+
+    def setDiffBoundarySpecDiffusionActive(self, db, s, act):
+        """Open (or close) diffusion of s across the boundary in both directions at each
+        side's own constant (TOS:2745-2800)."""
+        check(self._L.sg_set_diff_boundary_active(self._h, self._db(db), self._spec(s), 1 if act else 0))
+
+    def getDiffBoundarySpecDiffusionActive(self, db, s):
+        x = C.c_int32()
+        check(self._L.sg_get_diff_boundary_active(self._h, self._db(db), self._spec(s), C.byref(x)))
+        return bool(x.value)
+
+    def setDiffBoundarySpecDcst(self, db, s, dcst, direction_comp=None):
+        """Diffusion constant across the boundary (TOS:2865-2930); with direction_comp only
+        the diffusion into that compartment takes it.  Opens the direction(s)."""
+        dc = -1 if direction_comp is None else self.comp_index[direction_comp]
+        check(self._L.sg_set_diff_boundary_dcst(self._h, self._db(db), self._spec(s), float(dcst), dc))
+
+    setDiffBoundaryDiffusionActive = setDiffBoundarySpecDiffusionActive
+    getDiffBoundaryDiffusionActive = getDiffBoundarySpecDiffusionActive
+    setDiffBoundaryDcst = setDiffBoundarySpecDcst
+
     def setCompReacK(self, c, r, k, realization=-1):
         check(self._L.sg_set_reac_k(self._h, self._reac(c, r), int(realization), float(k)))
 

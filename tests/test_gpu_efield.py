@@ -101,6 +101,42 @@ def test_efield_steps_match_fp64_direct_solve(steps_lib, method, rtol, persisten
     assert np.ptp(got) > 1e-3  # the clamp and the injection actually moved V
 
 
+def test_step_length_changes_match_direct_solve(steps_lib):
+    """Runs whose end is not a whole number of EField steps end on a short step; the next
+    run resumes at the regular length (the previous length's matrices are swapped back in).
+    Every step still equals the FP64 direct solve of its own length."""
+    from oracle.efield_oracle import EFieldOracle
+
+    mesh = sgeom.kuhn_box(4, 4, 8, 1e-7)
+    sgeom.TmComp("cyto", mesh, np.arange(mesh.ntets))
+    surf = mesh.getSurfTris()
+    patch = sgeom.TmPatch("memb", mesh, surf, mesh.comps["cyto"])
+    sgeom.Memb("membrane", mesh, [patch])
+    mdl = smodel.Model()
+    smodel.Volsys("vsys", mdl)
+    sim = TetOpSplit(mdl, mesh, make_rng(9), EF_DV_CG_FP64)
+    sim.setEfieldTolerance(1e-12, 1e-4)
+    sim.setEfieldDT(1e-6)
+    sim.setMembPotential("membrane", -0.065)
+    sim.setMembCapac("membrane", 0.01)
+    sim.setMembRes("membrane", 1.0 / 0.3, -0.065)
+    ora = EFieldOracle(mesh.verts, mesh.tets, mesh.tris[surf])
+    ora.cm, ora.sigma, ora.g, ora.vext = 0.01, 1.0e3, 0.3e-3, -65.0
+    zmin = np.unique(mesh.tris[surf][np.all(mesh.verts[mesh.tris[surf]][:, :, 2] <= 1e-12, axis=1)])
+    for v in zmin:
+        sim.setVertIClamp(int(v), 1e-9 / len(zmin))
+        ora.iclamp[v] = 1e-9 / len(zmin) * 1e12
+    t = 0.0
+    for ends, steps in ((3.4e-6, [1e-3, 1e-3, 1e-3, 0.4e-3]), (6.4e-6, [1e-3, 1e-3, 1e-3]),
+                        (7.0e-6, [0.6e-3])):
+        sim.run(ends)
+        for dt in steps:
+            ora.advance(dt)
+    got = np.array([sim.getVertV(v) for v in range(mesh.nverts)]) * 1e3
+    assert np.max(np.abs(got - ora.V) / np.abs(ora.V)) < 1e-9
+    assert sim.getEfieldStats()[0] == 8
+
+
 @pytest.mark.parametrize("method", [EF_DV_CG_FP64, EF_DV_CG_MIXED])
 def test_rallpack1_membres(steps_lib, method):
     sim, v0s, vxs, ref0, refx = rallpack1_sim(method)

@@ -214,3 +214,65 @@ def test_batch_tet_counts_gather(steps_lib):
     assert np.allclose(conc, got / (6.02214179e23 * mesh.tet_vol[tets] * 1e3), rtol=1e-15)
     with pytest.raises(ArgErr):
         sim.getBatchTetSpecCountsNP(np.array([0, mesh.ntets]), "A", np.empty(2))
+
+
+@pytest.mark.parametrize("split", [False, True])
+def test_diffusion_boundary_matches_oracle(steps_lib, split):
+    """A diffusion boundary between two compartments (diffboundary.cpp): closed, opened in
+    both directions, then one direction with its own constant; every count equals the
+    oracle's after every run, and molecules are conserved."""
+    from steps_b200 import geom as sgeom
+    from steps_b200 import model as smodel
+    from steps_b200.solver import TetOpSplit
+    from oracle.pyoracle import Oracle
+    from tests.helpers import make_rng
+
+    n = 6
+    mesh = sgeom.kuhn_box(n, n, n, W.H)
+    x = mesh.tet_bary[:, 0]
+    left = np.nonzero(x < 0.5 * n * W.H)[0]
+    right = np.nonzero(x >= 0.5 * n * W.H)[0]
+    sgeom.TmComp("left", mesh, left).addVolsys("vl")
+    sgeom.TmComp("right", mesh, right).addVolsys("vr")
+    tt = mesh.tri_tets
+    side = np.zeros(mesh.ntets, dtype=int)
+    side[right] = 1
+    both = (tt[:, 0] >= 0) & (tt[:, 1] >= 0)
+    btris = np.nonzero(both & (side[np.maximum(tt[:, 0], 0)] != side[np.maximum(tt[:, 1], 0)]))[0]
+    sgeom.DiffBoundary("db", mesh, btris)
+    mdl = smodel.Model()
+    A, B = smodel.Spec("A", mdl), smodel.Spec("B", mdl)
+    vl, vr = smodel.Volsys("vl", mdl), smodel.Volsys("vr", mdl)
+    smodel.Reac("conv", vr, lhs=[A], rhs=[B], kcst=20.0)
+    smodel.Diff("dAl", vl, A, 2e-12)
+    smodel.Diff("dAr", vr, A, 1e-12)
+    smodel.Diff("dBr", vr, B, 1e-12)
+    sim = TetOpSplit(mdl, mesh, make_rng(13))
+    sim.setSplit(split)
+    ora = Oracle(sim.tables, seed=13)
+    sim.setCompSpecCount("left", "A", 20000)
+    sync_counts(sim, ora)
+    per = sim.getUpdPeriod()
+    t = 0.0
+    for phase in range(3):
+        if phase == 1:
+            sim.setDiffBoundarySpecDiffusionActive("db", "A", True)
+            ora.set_bnd_active(0, 0, True)
+            assert sim.getDiffBoundarySpecDiffusionActive("db", "A")
+        if phase == 2:
+            sim.setDiffBoundarySpecDiffusionActive("db", "A", False)
+            sim.setDiffBoundarySpecDcst("db", "A", 5e-13, direction_comp="left")
+            ora.set_bnd_active(0, 0, False)
+            ora.set_bnd_dcst(0, 0, 5e-13, direction_comp=0)
+        assert sim.getUpdPeriod() == ora.period()
+        for k in range(4):
+            t += 7.0 * sim.getUpdPeriod()
+            sim.run(t)
+            ora.run(t)
+            assert_same(sim, ora, f"phase {phase} t={t}")
+        if phase == 0:
+            assert sim.getCompSpecCount("right", "A") == 0
+        if phase == 1:
+            assert sim.getCompSpecCount("right", "A") > 0
+    total = sim.getCompSpecCount("left", "A") + sim.getCompSpecCount("right", "A") + sim.getCompSpecCount("right", "B")
+    assert total == 20000
