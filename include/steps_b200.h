@@ -157,6 +157,15 @@ int sg_set_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double n);    /* 
 int sg_get_patch_count(sg_solver* h, int32_t patch, int32_t sspec, int32_t real, double* n);
 int sg_set_patch_count(sg_solver* h, int32_t patch, int32_t sspec, int32_t real, double n);
 int sg_get_tri_ohmic_i(sg_solver* h, int32_t tri, double* amps);  /* getTriOhmicI: last EField step */
+/* GHKcurr (ghkcurr.cpp:168-280, math/ghk.cpp:71-90): channel state sspec of patch passes
+ * volume species ion of the given valence, permeability perm (m^3/s per channel), vshift
+ * (V), fixed outer concentration voconc (M; this solver's surface units hold no outer
+ * tets).  realflux = 1 moves the ions; the carried charge is the triangle's GHK current. */
+int sg_add_ghk(sg_solver* h, int32_t patch, int32_t sspec, int32_t ion, int32_t valence, double perm,
+               double vshift, double voconc, int32_t realflux, int32_t* out_idx);
+int sg_set_temp(sg_solver* h, double kelvin);                     /* API::setTemp (default 293.15) */
+int sg_get_temp(sg_solver* h, double* kelvin);                    /* API::getTemp */
+int sg_get_tri_ghk_i(sg_solver* h, int32_t tri, double* amps);    /* getTriGHKI: last EField step */
 /* Surface diffusion (SDiff, sdiff.cpp:62-83, 498-560; TOS:585-630 triangle neighbours):
  * for membrane triangle m and edge e, nbr[3m+e] is the membrane triangle across that edge
  * (-1 = none), nbr_edge its edge index, len the edge length (m) and dist the distance of

@@ -94,6 +94,10 @@ PROTOTYPES = {
     "sg_set_surface": [_P, _i32, _i32, _pi32, _pi32, _pf64, _i32],
     "sg_add_sreac": [_P, _i32, _pu32, _pu32, _pi32, _pi32, _f64, _pi32],
     "sg_add_vdep_sreac": [_P, _i32, _pu32, _pu32, _pi32, _pi32, _f64, _f64, _i32, _pf64, _pi32],
+    "sg_add_ghk": [_P, _i32, _i32, _i32, _i32, _f64, _f64, _f64, _i32, _pi32],
+    "sg_set_temp": [_P, _f64],
+    "sg_get_temp": [_P, _pf64],
+    "sg_get_tri_ghk_i": [_P, _i32, _pf64],
     "sg_set_tri_neighbours": [_P, _pi32, _pi32, _pf64, _pf64],
     "sg_add_sdiff": [_P, _i32, _i32, _f64, _pi32],
     "sg_add_ohmic": [_P, _i32, _i32, _f64, _f64, _pi32],

@@ -223,6 +223,43 @@ SG_HD double sg_log(double x) {
     return fma(de, SG_LN2_HEAD, fma(de, SG_LN2_TAIL, lm));
 }
 
+// e^x written from the mathematics: x = k ln2 + r with k = round(x / ln2) and
+// |r| <= ln2 / 2 (ln2 split into the head and tail above, so k ln2_head is exact), e^r by
+// its Taylor series to r^14 (truncation below 3e-19 relative), then 2^k by the exponent
+// bits.  Overflow gives +inf, underflow below 2^-1022 gives 0 (no subnormal results).
+SG_HD double sg_exp(double x) {
+    if (!(x < 709.78)) return x != x ? x : sg_bits_f64(0x7FF0000000000000ull);
+    if (x < -708.39) return 0.0;
+    const double k = floor(x * 1.4426950408889634 + 0.5);
+    double r = fma(-k, SG_LN2_HEAD, x);
+    r = fma(-k, SG_LN2_TAIL, r);
+    double p = 1.0 / 87178291200.0;             // 1/14!
+    p = fma(p, r, 1.0 / 6227020800.0);          // 1/13!
+    p = fma(p, r, 1.0 / 479001600.0);
+    p = fma(p, r, 1.0 / 39916800.0);
+    p = fma(p, r, 1.0 / 3628800.0);
+    p = fma(p, r, 1.0 / 362880.0);
+    p = fma(p, r, 1.0 / 40320.0);
+    p = fma(p, r, 1.0 / 5040.0);
+    p = fma(p, r, 1.0 / 720.0);
+    p = fma(p, r, 1.0 / 120.0);
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    int ki = (int)k;
+    if (ki > 1023) {  // e^r > 1 for x near the top of the range: scale in two steps
+        p = p * 2.0;
+        ki -= 1;
+    }
+    if (ki < -1022) {
+        p = p * 0.5;
+        ki += 1;
+    }
+    return p * sg_bits_f64((uint64_t)(ki + 1023) << 52);
+}
+
 // q^n by binary powering (multiplications only).
 SG_HD double sg_pow_u(double q, uint32_t n) {
     double r = 1.0;

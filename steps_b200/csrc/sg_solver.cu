@@ -37,9 +37,12 @@ __global__ void gather_counts_kernel(int n, const uint32_t* row, const int32_t* 
         out[i] = (double)row[idx[i]];
 }
 
+// Membrane current of each triangle over the EField step just taken (tri.cpp:664-719):
+// ohmic currents from the channel-state time integrals, plus the GHK charge the step's GHK
+// events carried out (echarge e / dt).  Resets both accumulators.
 __global__ void ohmic_current_kernel(int M, int nss, int noc, const sg_ohmic* oc, const int32_t* tri_patch,
                                      double* spec_int, const double* triV, double inv_dt, double* tri_I,
-                                     double* tri_I_last) {
+                                     double* tri_I_last, long long* echarge, double* tri_Ighk) {
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
         const int p = tri_patch[m];
         double I = 0.0;
@@ -49,8 +52,14 @@ __global__ void ohmic_current_kernel(int M, int nss, int noc, const sg_ohmic* oc
             I += (nbar * oc[k].g) * (triV[m] - oc[k].erev * 1.0e3);  // S * mV
         }
         I *= 1.0e9;  // S mV -> pA
-        tri_I[m] = I;
         tri_I_last[m] = I;
+        if (echarge) {
+            const double ig = (double)echarge[m] * 1.602176487e-19 * inv_dt;  // A
+            tri_Ighk[m] = ig;
+            I += ig * 1.0e12;
+            echarge[m] = 0;
+        }
+        tri_I[m] = I;
         for (int s = 0; s < nss; ++s) spec_int[(size_t)s * M + m] = 0.0;
     }
 }
@@ -161,6 +170,12 @@ struct Solver {
     std::vector<int32_t> sdiff_slot;                // [SS] compact index or -1
     std::vector<float> sgeo;                        // [M*4] c0, c1, 1, G (1/m^2)
     int nsdiff = 0;
+    // GHK currents.
+    std::vector<sg_ghk> ghks;
+    double temp = 293.15;                           // K (API::setTemp)
+    DevBuf<sg_ghk> d_ghks;
+    DevBuf<long long> d_tri_echarge;
+    DevBuf<double> d_tri_Ighk;
     DevBuf<uint32_t> d_tri_out;
     DevBuf<double> d_tri_occ, d_sdcst;
     DevBuf<int32_t> d_sdslot, d_sdspec, d_snbr, d_tri_inner;
@@ -246,10 +261,25 @@ struct Solver {
         for (auto& r : sreacs) patch_sb[r.patch + 1] += 1;
         for (int p = 0; p < npatch; ++p) patch_sb[p + 1] += patch_sb[p];
         max_sreac_per_patch = 1;
-        for (int p = 0; p < npatch; ++p) max_sreac_per_patch = std::max(max_sreac_per_patch, patch_sb[p + 1] - patch_sb[p]);
+        for (int p = 0; p < npatch; ++p) {
+            int ng = 0;
+            for (const auto& g : ghks)
+                if (g.patch == p) ++ng;
+            max_sreac_per_patch = std::max(max_sreac_per_patch, patch_sb[p + 1] - patch_sb[p] + ng);
+        }
         surf_touches_volume = false;
         for (auto& r : sreacs)
             if (r.niupd > 0) surf_touches_volume = true;
+        for (auto& g : ghks)
+            if (g.realflux) surf_touches_volume = true;
+        if (!ghks.empty()) {
+            d_ghks.alloc(ghks.size());
+            h2d(d_ghks.p, ghks.data(), ghks.size());
+            d_tri_echarge.alloc(ntris);
+            d_tri_Ighk.alloc(ntris);
+            SG_CUDA(cudaMemsetAsync(d_tri_echarge.p, 0, ntris * 8, stream));
+            SG_CUDA(cudaMemsetAsync(d_tri_Ighk.p, 0, ntris * 8, stream));
+        }
         // SSA units: each triangle joins the unit of its inner tet.
         std::vector<int32_t> tt((size_t)ntets * 4, -1);
         for (int m = 0; m < ntris; ++m) {
@@ -316,6 +346,12 @@ struct Solver {
         s.vtabs = d_vtabs.p;
         s.vtab_vals = d_vvals.p;
         s.spec_int = d_spec_int.p;
+        if (!ghks.empty()) {
+            s.ghks = d_ghks.p;
+            s.nghk = (int)ghks.size();
+            s.tri_echarge = d_tri_echarge.p;
+        }
+        s.temp = temp;
         if (nsdiff > 0) {
             s.tri_outflow = d_tri_out.p;
             s.tri_occ = d_tri_occ.p;
@@ -992,11 +1028,11 @@ struct Solver {
             check_status();
             double real_dt = time() - t0;
             // Membrane currents of the step from the channel-state time integrals.
-            if (has_surf() && !ohmics.empty()) {
+            if (has_surf() && (!ohmics.empty() || !ghks.empty())) {
                 int g = std::max(1, std::min((ntris + 255) / 256, nsm * 4));
                 ohmic_current_kernel<<<g, 256, 0, stream>>>(ntris, nsspec, (int)ohmics.size(), d_ohmics.p,
                                                             d_tri_patch.p, d_spec_int.p, ef.tri_V, 1.0 / real_dt,
-                                                            ef.tri_I, d_tri_Iohm.p);
+                                                            ef.tri_I, d_tri_Iohm.p, d_tri_echarge.p, d_tri_Ighk.p);
                 SG_CUDA(cudaGetLastError());
                 launches += 1;
             } else {
@@ -1519,6 +1555,14 @@ struct Solver {
         distribute_w(n, tris, tri_area, v, &st);
         h2d(d_tri_counts.p + (size_t)s * ntris, v.data(), (size_t)ntris);
         sync();
+    }
+    double get_tri_ghk_i(int m) {
+        check_tri(m, 0);
+        if (ghks.empty()) return 0.0;
+        double x = 0.0;
+        d2h(&x, d_tri_Ighk.p + m, 1);
+        sync();
+        return x;
     }
     double get_tri_ohmic_i(int m) {
         check_tri(m, 0);
@@ -2170,6 +2214,54 @@ int sg_set_surface(sg_solver* h, int32_t nsspec, int32_t ntris, const int32_t* t
             if (p < 0 || p >= npatch) throw sg::ArgErr("triangle patch index out of range");
         for (double a : s->tri_area)
             if (!(a > 0.0)) throw sg::ArgErr("triangle area must be positive");
+    });
+}
+
+int sg_add_ghk(sg_solver* h, int32_t patch, int32_t sspec, int32_t ion, int32_t valence, double perm,
+               double vshift, double voconc, int32_t realflux, int32_t* out_idx) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (s->nsspec <= 0) throw sg::ProgErr("call sg_set_surface first");
+        if (patch < 0 || patch >= s->npatch) throw sg::ArgErr("patch index out of range");
+        if (sspec < 0 || sspec >= s->nsspec) throw sg::ArgErr("surface species index out of range");
+        s->check_spec(ion);
+        if (valence == 0) throw sg::ArgErr("GHK current of an ion without valence");
+        if (!(perm > 0.0)) throw sg::ArgErr("GHK permeability must be positive (setP or setPInfo)");
+        if (!(voconc >= 0.0))
+            throw sg::NotImplErr("GHK current without a virtual outer concentration (no outer tets here)");
+        sg_ghk g{};
+        g.patch = patch;
+        g.sspec = sspec;
+        g.ion = ion;
+        g.valence = valence;
+        g.perm = perm;
+        g.vshift = vshift;
+        g.voconc = voconc;
+        g.realflux = realflux ? 1 : 0;
+        s->ghks.push_back(g);
+        if (out_idx) *out_idx = (int32_t)s->ghks.size() - 1;
+    });
+}
+
+int sg_set_temp(sg_solver* h, double kelvin) {
+    return guarded([&] {
+        if (!(kelvin > 0.0)) throw sg::ArgErr("temperature must be positive");
+        S(h)->temp = kelvin;
+    });
+}
+
+int sg_get_temp(sg_solver* h, double* kelvin) {
+    return guarded([&] {
+        need(kelvin, "kelvin");
+        *kelvin = S(h)->temp;
+    });
+}
+
+int sg_get_tri_ghk_i(sg_solver* h, int32_t tri, double* amps) {
+    return guarded([&] {
+        need(amps, "amps");
+        *amps = S(h)->get_tri_ghk_i(tri);
     });
 }
 

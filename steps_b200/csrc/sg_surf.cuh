@@ -57,6 +57,40 @@ __device__ inline double vdep_k(const sg_surf_args& sa, int tab, double v_mV, ui
     return (1.0 - r) * sa.vtab_vals[vt.off + lo] + r * sa.vtab_vals[vt.off + hi];
 }
 
+#define SG_FARADAY 96485.3399       // src/steps/math/constants.hpp:49
+#define SG_GAS_CONSTANT 8.314472    // constants.hpp:53
+#define SG_E_CHARGE 1.602176487e-19 // constants.hpp:57
+
+// Single-channel GHK current (A) of src/steps/math/ghk.cpp:71-90 at potential v (V), with
+// inner/outer concentrations in mol/m^3: P z F nu (ci - co e^-nu) / (1 - e^-nu),
+// nu = z v F / (R T); the limit P z F (ci - co) at nu = 0.  |nu| beyond the double range
+// is an error, as in the reference.
+__device__ inline double ghk_current(double P, double v, int z, double temp, double ci, double co,
+                                     uint32_t* status) {
+    const double nu = (double)z * v * SG_FARADAY / (SG_GAS_CONSTANT * temp);
+    if (!(nu < 700.0 && nu > -700.0)) {
+        atomicOr(status, SG_ERR_TABLE);
+        return 0.0;
+    }
+    if (fabs(nu) > 2.220446049250313e-16) {
+        const double e = sg_exp(-nu);
+        return P * (double)z * SG_FARADAY * nu * (ci - co * e) / (1.0 - e);
+    }
+    return P * (double)z * SG_FARADAY * (ci - co);
+}
+
+// Signed rate (ions/s) of one GHK current on a triangle with n channels in the state, inner
+// ion count c_ion in a tet of 1/(1e3 V N_A) = ivs, triangle potential vm (mV): positive is an
+// efflux (ghkcurr.cpp:168-212).
+__device__ inline double ghk_rate(const sg_ghk& g, double vm, uint32_t c_ion, uint32_t n, double ivs, double temp,
+                                  uint32_t* status) {
+    if (n == 0) return 0.0;
+    const double ci = (double)c_ion * ivs * 1.0e3;  // M -> mol/m^3
+    const double co = g.voconc * 1.0e3;
+    const double I = ghk_current(g.perm, vm * 1.0e-3 + g.vshift, g.valence, temp, ci, co, status);
+    return I / (SG_E_CHARGE * (double)g.valence) * (double)n;
+}
+
 // Scaled constant of a surface reaction on triangle m whose inner tet has 1/(1e3 V N_A) = ivs.
 __device__ inline double sreac_ccst(const sg_sreac& r, double k, double ivs, double area) {
     if (r.surf_surf) {

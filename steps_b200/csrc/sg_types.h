@@ -66,6 +66,20 @@ typedef struct sg_ohmic {
     double erev;                       // V
 } sg_ohmic;
 
+// GHK current (ghkcurr.cpp:168-280): channel state sspec of a patch passes ion (valence z)
+// with permeability perm (m^3/s per channel) against a fixed outer concentration voconc (M).
+typedef struct sg_ghk {
+    int32_t patch;
+    int32_t sspec;
+    int32_t ion;
+    int32_t valence;
+    double perm;
+    double vshift;                     // V
+    double voconc;                     // M
+    int32_t realflux;                  // ions move (else charge only)
+    int32_t pad_;
+} sg_ghk;
+
 // Surface part of the window kernel (null tables when the model has no membrane).
 typedef struct sg_surf_args {
     uint32_t* tri_counts;              // [SS][M] surface species per membrane triangle
@@ -89,10 +103,14 @@ typedef struct sg_surf_args {
     const float* sgeo;                 // [M][4]: conditional selectors c0, c1, 1, G = sum l/(A d)
     const int32_t* tri_inner;          // [M] inner tet (its realization owns the triangle)
     int32_t nsdiff;
+    const sg_ghk* ghks;                // [nghk]
+    long long* tri_echarge;            // [M] elementary charges carried out by GHK events this EField step
+    double temp;                       // K
+    int32_t nghk;
     int32_t nsspec;
     int32_t ntris;
     int32_t nsreac;
-    int32_t max_sreac_per_patch;
+    int32_t max_sreac_per_patch;       // surface events per triangle: reactions + GHK currents of its patch
 } sg_surf_args;
 
 // Per realization bookkeeping, advanced on the device by the last block of each

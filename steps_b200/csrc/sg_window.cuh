@@ -190,15 +190,17 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
     uint32_t* sc = L.cnt + tid;
     double* sd = L.tdel + tid;
     const int mm[4] = {tris.x, tris.y, tris.z, tris.w};
-    int pb[4], pe[4];
+    int pb[4], pe[4], pj[4];
     double area[4], vm[4];
     for (int j = 0; j < 4; ++j) {
         pb[j] = pe[j] = 0;
+        pj[j] = -1;
         area[j] = 0.0;
         vm[j] = 0.0;
         const int m = mm[j];
         if (m < 0) continue;
         const int p = sa.tri_patch[m];
+        pj[j] = p;
         pb[j] = sa.patch_sreac_begin[p];
         pe[j] = sa.patch_sreac_begin[p + 1];
         area[j] = sa.tri_area[m];
@@ -247,6 +249,18 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
                 SL.prop[(j * RSP + (q - pb[j])) * BLOCK + tid] = pq;
                 a0 = a0 + pq;
             }
+            // GHK currents of the triangle's patch, after its reactions (ghkcurr.cpp:168).
+            int kk = pe[j] - pb[j];
+            for (int g = 0; g < sa.nghk && pj[j] >= 0; ++g) {
+                const sg_ghk& gh = sa.ghks[g];
+                if (gh.patch != pj[j]) continue;
+                const double rt = ghk_rate(gh, vm[j], sc[gh.ion * BLOCK], SL.cnt[(j * SS + gh.sspec) * BLOCK + tid],
+                                           ivs, sa.temp, a.status);
+                const double pq = fabs(rt);
+                SL.prop[(j * RSP + kk) * BLOCK + tid] = pq;
+                a0 = a0 + pq;
+                ++kk;
+            }
         }
         if (!(a0 > 0.0)) break;
         double dt = -sg_log(sg_u01_oc(sg_next_u32(st))) / a0;
@@ -281,10 +295,50 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
                     }
                 }
             }
+            // GHK events are coded as sq = -10 - g.
+            int kk = pe[j] - pb[j];
+            for (int g = 0; g < sa.nghk && pj[j] >= 0 && sj == -2; ++g) {
+                if (sa.ghks[g].patch != pj[j]) continue;
+                double pq = SL.prop[(j * RSP + kk) * BLOCK + tid];
+                ++kk;
+                if (pq > 0.0) {
+                    lj = j;
+                    lq = -10 - g;
+                    cum = cum + pq;
+                    if (target < cum) {
+                        sj = j;
+                        sq = -10 - g;
+                    }
+                }
+            }
         }
         if (sj == -2) {
             sj = lj;
             sq = lq;
+        }
+        if (sq <= -10) {
+            // GHK event on triangle slot sj (ghkcurr.cpp:230-280): one ion out (efflux) or in,
+            // z elementary charges out or in for the triangle's current.
+            const sg_ghk& gh = sa.ghks[-10 - sq];
+            const int m = mm[sj];
+            const double rt = ghk_rate(gh, vm[sj], sc[gh.ion * BLOCK], SL.cnt[(sj * SS + gh.sspec) * BLOCK + tid],
+                                       ivs, sa.temp, a.status);
+            const bool eff = rt >= 0.0;
+            if (gh.realflux && !((clampm >> gh.ion) & 1u)) {
+                const int s = gh.ion;
+                const uint32_t old = sc[s * BLOCK];
+                long long nc = (long long)old + (eff ? -1 : 1);
+                if (nc < 0 || nc > 0xFFFFFFFFll) {
+                    atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
+                    nc = nc < 0 ? 0 : 0xFFFFFFFFll;
+                }
+                sd[s * BLOCK] = sd[s * BLOCK] + (double)(nc - (long long)old) * tt;
+                sc[s * BLOCK] = (uint32_t)nc;
+            }
+            atomicAdd((unsigned long long*)&sa.tri_echarge[m],
+                      (unsigned long long)(long long)(eff ? gh.valence : -gh.valence));
+            atomicAdd(a.surf_ext, 1ull);
+            continue;
         }
         if (sq < 0) break;
         if (sj == -1) {

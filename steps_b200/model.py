@@ -9,6 +9,8 @@ Python API_1 (``steps.model``).
 """
 from __future__ import annotations
 
+import math
+
 
 class Model:
     def __init__(self):
@@ -35,6 +37,12 @@ class Spec:
 
     def getID(self):
         return self.id
+
+    def setValence(self, v):
+        self.valence = int(v)
+
+    def getValence(self):
+        return self.valence
 
 
 class Chan:
@@ -70,6 +78,7 @@ class Surfsys:
         self.sreacs = {}
         self.vdepsreacs = {}
         self.ohmiccurrs = {}
+        self.ghkcurrs = {}
         self.diffs = {}
         model.surfsys[id] = self
 
@@ -134,6 +143,55 @@ class VDepSReac(SReac):
         self.kfunc = k
         self.vrange = tuple(float(x) for x in vrange)
         surfsys.vdepsreacs[id] = self
+
+
+FARADAY = 96485.3399       # src/steps/math/constants.hpp:49
+GAS_CONSTANT = 8.314472    # constants.hpp:53
+E_CHARGE = 1.602176487e-19 # constants.hpp:57
+
+
+def ghk_permeability(g, v, z, temp, iconc, oconc):
+    """Single-channel permeability (m^3/s) giving conductance g (S) at potential v (V),
+    temperature temp (K), inner/outer concentrations (M): the slope of the GHK current
+    equation (the quantity src/steps/math/ghk.cpp:36-69 computes)."""
+    b, c = iconc * 1000.0, oconc * 1000.0
+    d = -z * FARADAY / (GAS_CONSTANT * temp)
+    den = c * math.exp(2.0 * d * v) + ((b - c) * d * v - c - b) * math.exp(d * v) + b
+    num = math.exp(2.0 * d * v) - 2.0 * math.exp(d * v) + 1.0
+    a = g * (num / den) if (abs(num) > 2.220446049250313e-16 or abs(den) > 2.220446049250313e-16) else 2.0 * g / (c + b)
+    return (a * GAS_CONSTANT * temp) / (z * z * FARADAY * FARADAY)
+
+
+class GHKcurr:
+    """GHK current through channel state chanstate of ion (src/steps/model/ghkcurr.hpp):
+    per channel I = P z F nu (c_in - c_out e^-nu) / (1 - e^-nu), nu = z (V + vshift) F / (R T).
+    computeflux moves the ions (one per z e of charge); virtual_oconc (M) fixes the outer
+    concentration (required here: surface units hold no outer tets)."""
+
+    def __init__(self, id, surfsys, chanstate, ion, computeflux=True, virtual_oconc=-1.0, vshift=0.0):
+        self.id = id
+        self.surfsys = surfsys
+        self.chanstate = chanstate.id if isinstance(chanstate, Spec) else str(chanstate)
+        self.ion = ion.id if isinstance(ion, Spec) else str(ion)
+        self.valence = ion.valence if isinstance(ion, Spec) else 0
+        self.computeflux = bool(computeflux)
+        self.voconc = float(virtual_oconc)
+        self.vshift = float(vshift)
+        self.perm = None
+        surfsys.ghkcurrs[id] = self
+
+    def setP(self, p):
+        if not (p > 0.0):
+            raise ValueError("permeability must be positive")
+        self.perm = float(p)
+
+    def getP(self):
+        return self.perm
+
+    def setPInfo(self, g, V, T, oconc, iconc):
+        if self.valence == 0:
+            raise ValueError("the ion has no valence")
+        self.perm = ghk_permeability(g, V, self.valence, T, iconc, oconc)
 
 
 class OhmicCurr:

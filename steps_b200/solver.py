@@ -135,6 +135,8 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
                     sid(s)
             for oc in ss.ohmiccurrs.values():
                 sid(oc.chanstate)
+            for gh in ss.ghkcurrs.values():
+                sid(gh.chanstate)
     S, SS = len(spec_index), max(len(sspecs), 1)
 
     def rows(r):
@@ -154,7 +156,7 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
             iupd[spec_index[s]] += 1
         return slhs, ilhs, supd, iupd
 
-    sreacs, ohmics, sdiffs = [], [], []
+    sreacs, ohmics, sdiffs, ghks = [], [], [], []
     for pi, p in enumerate(patches):
         for ssn in p.surfsys:
             ss = model.surfsys[ssn]
@@ -169,6 +171,11 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
                 sreacs.append((pi, rid, rows(r), 0.0, (vmin, dv, tab)))
             for oid, oc in ss.ohmiccurrs.items():
                 ohmics.append((pi, oid, sid(oc.chanstate), oc.g, oc.erev))
+            for gid, gh in ss.ghkcurrs.items():
+                if gh.perm is None:
+                    raise ArgErr(f"GHK current '{gid}' has no permeability (setP or setPInfo)")
+                ghks.append((pi, gid, sid(gh.chanstate), spec_index[gh.ion], gh.valence, gh.perm, gh.vshift,
+                             gh.voconc, gh.computeflux))
     # Edge neighbours of every membrane triangle (sdiff.cpp:62-83, TOS:585-630): across edge j
     # = (v_j, v_j+1) the other membrane triangle on that edge, its edge index, the edge length
     # and the distance between the two barycentres.
@@ -195,7 +202,7 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
     nb = np.where(tri_nbr >= 0, tri_nbr, 0)
     tri_dist = np.where(tri_nbr >= 0, np.linalg.norm(bary[nb] - np.repeat(bary, 3, axis=0), axis=1), 0.0)
     return {
-        "sdiffs": sdiffs, "tri_nbr": tri_nbr, "tri_nbr_edge": tri_nbr_edge,
+        "sdiffs": sdiffs, "ghks": ghks, "tri_nbr": tri_nbr, "tri_nbr_edge": tri_nbr_edge,
         "tri_len": np.ascontiguousarray(tri_len, dtype=np.float64),
         "tri_dist": np.ascontiguousarray(tri_dist, dtype=np.float64),
         "patch_names": [p.id for p in patches], "tris": tris, "tri_index": tri_index,
@@ -282,6 +289,12 @@ class TetOpSplit:
             for (pi, oid, ss, g, erev) in sf["ohmics"]:
                 out = C.c_int32()
                 check(L.sg_add_ohmic(h, pi, ss, g, erev, C.byref(out)))
+            self.ghk_index = {}
+            for (pi, gid, ss, ion, z, perm, vshift, voconc, flux) in sf["ghks"]:
+                out = C.c_int32()
+                check(L.sg_add_ghk(h, pi, ss, ion, int(z), float(perm), float(vshift), float(voconc),
+                                   1 if flux else 0, C.byref(out)))
+                self.ghk_index[(sf["patch_names"][pi], gid)] = out.value
             if sf["sdiffs"]:
                 check(L.sg_set_tri_neighbours(h, ptr(sf["tri_nbr"], C.c_int32), ptr(sf["tri_nbr_edge"], C.c_int32),
                                               ptr(sf["tri_len"], C.c_double), ptr(sf["tri_dist"], C.c_double)))
@@ -560,6 +573,20 @@ class TetOpSplit:
         """Distribute n molecules over the patch's triangles by area (of one realization, or
         of all with realization=-1)."""
         check(self._L.sg_set_patch_count(self._h, self._patch(p), self._sspec(s), int(realization), float(n)))
+
+    def getTriGHKI(self, tidx, ghk=None):
+        """GHK current (A, outward positive) of the triangle over the last EField step."""
+        x = C.c_double()
+        check(self._L.sg_get_tri_ghk_i(self._h, self._tri(tidx), C.byref(x)))
+        return x.value
+
+    def setTemp(self, kelvin):
+        check(self._L.sg_set_temp(self._h, float(kelvin)))
+
+    def getTemp(self):
+        x = C.c_double()
+        check(self._L.sg_get_temp(self._h, C.byref(x)))
+        return x.value
 
     def getTriOhmicI(self, tidx, oc=None):
         x = C.c_double()
