@@ -218,12 +218,13 @@ int sg_set_efield_persistent(sg_solver* h, int32_t on);
  * (blocks stride over the tets), -1 = one tet per thread. */
 int sg_set_launch(sg_solver* h, int32_t block, int32_t grid);
 int sg_get_launch(sg_solver* h, int32_t* block, int32_t* grid);
-/* Autotune the launch shape at the next run() with more than 19 windows: after one
- * untimed window, two windows each are timed under block {64,128,256} x grid
- * {occupancy-sized (0), one tet per thread (-1)} with the full shared-memory carveout, then
- * the best of those with carveouts 75% and 50% and as a split window; the fastest is kept
- * (the sample path does not depend on the shape).  The nine timings (ms, in that order)
- * are read back with sg_get_autotune_ms, the kept carveout with sg_get_carveout. */
+/* Autotune the launch shape at the next run() with more than 21 windows: after one
+ * untimed window, ten candidates are timed on one window each in list order and on one
+ * more in reverse order (drift of the per-window work cancels): block {64,128,256} x grid
+ * {occupancy-sized (0), one tet per thread (-1)}; block 256, grid -1 at shared-memory
+ * carveouts 75% and 50%; split windows at block 128 and 256, grid -1.  The fastest is kept
+ * (the sample path does not depend on the shape).  The ten sums (ms, in that order) are
+ * read back with sg_get_autotune_ms, the kept carveout with sg_get_carveout. */
 int sg_set_autotune(sg_solver* h, int32_t on);
 int sg_get_carveout(sg_solver* h, int32_t* percent);
 /* Window as two kernels: reactions (gather, SSA) with one thread per tet, then the

@@ -268,7 +268,7 @@ void EFieldSystem::setup(int nv, const double* verts_um, int ntet, const int32_t
     dalloc(q32, nv);
     dalloc(x32, nv);
     dalloc(s32, nv);
-    dalloc(red, 4096);
+    dalloc(red, 8192);
     dalloc(scal, 32);
     dalloc(red_count, 4);
     dalloc(d_bar, 4);
@@ -544,6 +544,8 @@ __global__ void precond_kernel(Segs sg, Coarse cs, const double* diag, const T* 
 // than kSpinLimit polls sets bar[2] and every block leaves at its next barrier.
 // ---------------------------------------------------------------------------
 constexpr unsigned int kSpinLimit = 1u << 22;  // x ~100 ns polls: about half a second
+// The persistent solve is launched with at most 2048 blocks (3 x 2048 reduction partials
+// fit the 8192-value buffer); a 32-register bound keeps 8 blocks of 256 per SM resident.
 
 __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, unsigned int& gen) {
     __syncthreads();
@@ -622,7 +624,7 @@ struct PcgArgs {
 // set).  The same arithmetic as the multi-kernel loop: z = r / d + y, p' = z + beta p,
 // q = A p', x += alpha p', r -= alpha q.
 template <typename T>
-__global__ void __launch_bounds__(kBlock) pcg_persistent_kernel(PcgArgs<T> P) {
+__global__ void __launch_bounds__(kBlock, 8) pcg_persistent_kernel(PcgArgs<T> P) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     const int gt = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
@@ -1108,7 +1110,7 @@ void EFieldSystem::pcg_persistent(cudaStream_t stream, int n, const T* a, T* xv,
     int per_sm = 0;
     SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_persistent_kernel<T>, kBlock, 0));
     const int want = std::max((n + kBlock - 1) / kBlock, (nseg + 7) / 8);
-    const int G = std::max(1, std::min(std::min(want, std::max(per_sm, 1) * nsm), 1024));
+    const int G = std::max(1, std::min(std::min(want, std::max(per_sm, 1) * nsm), 2048));
     PcgArgs<T> P;
     P.n = n;
     P.width = width;

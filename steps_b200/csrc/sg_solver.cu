@@ -1076,13 +1076,14 @@ struct Solver {
 
     // ---- launch-shape autotuning ----
     // The sample path does not depend on the launch shape (every tet draws from its own
-    // counter stream), so tuning runs real windows: after one untimed window, the next
-    // windows of a run are timed under each candidate {block 64, 128, 256} x {occupancy-
-    // sized grid, one tet per thread} with the largest shared-memory carveout, then the best
-    // of those with carveouts of 75% and 50% (fewer resident blocks, more L1 for the
-    // kernel's local memory), and the fastest is kept.
+    // counter streams), so tuning runs real windows.  After one untimed window, each of a
+    // fixed list of candidates is timed on one window in list order and on one more in
+    // reverse order (a palindromic schedule, so that the drift of the per-window work as
+    // the run evolves cancels to first order): block {64, 128, 256} x grid {occupancy-
+    // sized, one tet per thread}; block 256, one tet per thread at shared-memory carveouts
+    // 75% and 50%; split windows at block 128 and 256.  The fastest is kept.
     static constexpr int kTuneWindows = 2;
-    static constexpr int kTuneCands = 9;
+    static constexpr int kTuneCands = 10;
     bool tune_pending = false;
     std::vector<float> tune_ms;
     int carveout = 100;  // preferred shared-memory carveout of the window kernels, percent
@@ -1100,52 +1101,46 @@ struct Solver {
     }
 
     uint64_t autotune(const sg_window_args& a) {
-        const int blocks[3] = {64, 128, 256};
-        int best_block = block, best_grid = grid, best_carve = 100;
-        float best = 0.0f;
-        tune_ms.clear();
+        struct Cand {
+            int block, grid, carve;
+            bool split;
+        };
+        const Cand cands[kTuneCands] = {{64, 0, 100, false},   {64, -1, 100, false},  {128, 0, 100, false},
+                                        {128, -1, 100, false}, {256, 0, 100, false},  {256, -1, 100, false},
+                                        {256, -1, 75, false},  {256, -1, 50, false},  {128, -1, 100, true},
+                                        {256, -1, 100, true}};
+        tune_ms.assign(kTuneCands, 0.0f);
         cudaEvent_t e0, e1;
         SG_CUDA(cudaEventCreate(&e0));
         SG_CUDA(cudaEventCreate(&e1));
-        bool best_split = false;
         ensure_split_buffers();
         const sg_window_args as = window_args();  // with the split buffers
-        auto timed = [&](int b, int gm, int cv, bool sp) {
-            block = b;
-            grid = gm;
-            split = sp;
-            set_carveout(cv);
+        auto timed = [&](const Cand& c) {
+            block = c.block;
+            grid = c.grid;
+            split = c.split;
+            set_carveout(c.carve);
             const int g = window_grid();
             SG_CUDA(cudaEventRecord(e0, stream));
-            for (int i = 0; i < kTuneWindows; ++i) launch_window(as, g);
+            launch_window(as, g);
             SG_CUDA(cudaEventRecord(e1, stream));
             SG_CUDA(cudaEventSynchronize(e1));
             float ms = 0.0f;
             SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            tune_ms.push_back(ms);
-            if (tune_ms.size() == 1 || ms < best) {
-                best = ms;
-                best_block = b;
-                best_grid = gm;
-                best_carve = cv;
-                best_split = sp;
-            }
+            return ms;
         };
-        set_carveout(100);
-        split = false;
-        launch_window(as, window_grid());  // untimed: first-launch costs
-        for (int bi = 0; bi < 3; ++bi)
-            for (int mode = 0; mode < 2; ++mode) timed(blocks[bi], mode ? -1 : 0, 100, false);
-        const int bb = best_block, bg = best_grid;
-        timed(bb, bg, 75, false);
-        timed(bb, bg, 50, false);
-        timed(bb, bg, 100, true);
+        timed(cands[5]);  // untimed: first-launch costs
+        for (int i = 0; i < kTuneCands; ++i) tune_ms[i] += timed(cands[i]);
+        for (int i = kTuneCands - 1; i >= 0; --i) tune_ms[i] += timed(cands[i]);
+        int best = 0;
+        for (int i = 1; i < kTuneCands; ++i)
+            if (tune_ms[i] < tune_ms[best]) best = i;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        block = best_block;
-        grid = best_grid;
-        split = best_split;
-        set_carveout(best_carve);
+        block = cands[best].block;
+        grid = cands[best].grid;
+        split = cands[best].split;
+        set_carveout(cands[best].carve);
         tune_pending = false;
         return (uint64_t)kTuneWindows * kTuneCands + 1;
     }

@@ -695,15 +695,15 @@ class TetOpSplit:
         return b.value, g.value
 
     def setAutotune(self, on=True):
-        """Time 18 windows of the next run (after one untimed window) under nine launch
-        shapes and keep the fastest (results do not depend on the shape)."""
+        """Time 20 windows of the next run (after one untimed window) under ten launch
+        shapes, two windows each in a palindromic order, and keep the fastest (results do
+        not depend on the shape)."""
         check(self._L.sg_set_autotune(self._h, 1 if on else 0))
 
     def getAutotuneTimes(self):
-        """ms of the two timed windows under each candidate shape, in the order block
-        64, 128, 256 x grid {occupancy-sized, one tet per thread} at the full shared-memory
-        carveout, then the best of those at carveouts 75% and 50% and split; empty before
-        tuning."""
+        """ms of the two timed windows of each candidate: block 64, 128, 256 x grid
+        {occupancy-sized, one tet per thread}; block 256 one tet per thread at carveouts 75%
+        and 50%; split at block 128 and 256; empty before tuning."""
         buf = (C.c_float * 16)()
         n = C.c_int32()
         check(self._L.sg_get_autotune_ms(self._h, buf, 16, C.byref(n)))
