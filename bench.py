@@ -143,6 +143,20 @@ def cpu_baseline(mdl, mesh, rows, windows=4):
                       f"{dt:.2f} s on {threads} host threads"}
 
 
+def replica_totals(dist, device, total_ms, updates, e2e_s, e2e_upd):
+    """Whole-job figures of N independent replicas: the slowest rank's device time and
+    end-to-end time (max over ranks) against the updates of all ranks (sum)."""
+    if dist is None:
+        return total_ms, float(updates), e2e_upd / e2e_s
+    import torch
+
+    t = torch.tensor([total_ms, e2e_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    u = torch.tensor([float(updates), float(e2e_upd)], dtype=torch.float64, device=device)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t[0].item()), float(u[0].item()), float(u[1].item()) / float(t[1].item())
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -253,17 +267,6 @@ def run_ours(args):
     sim.setProfiling(False)
     updates = mesh.ntets * NSPEC * windows
 
-    t_max = total_ms
-    upd_all = updates
-    if dist is not None:
-        tt = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-        uu = torch.tensor([updates], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(uu, op=dist.ReduceOp.SUM)
-        upd_all = float(uu.item())
-    value = upd_all / (t_max * 1e-3)
-
     # End-to-end through the C ABI with pinned host buffers.
     host = [torch.empty(mesh.ntets, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
             for _ in range(NSPEC)]
@@ -282,11 +285,8 @@ def run_ours(args):
             sim.getSpecCounts(s, host[i])
         e2e_s += time.perf_counter() - t0
         e2e_upd += mesh.ntets * NSPEC * (sim.getNIteration() - it_a)
-    e2e_val = e2e_upd / e2e_s
-    if dist is not None:
-        ee = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(ee, op=dist.ReduceOp.MAX)
-        e2e_val = e2e_upd * world / float(ee.item())
+    t_max, upd_all, e2e_val = replica_totals(dist, f"cuda:{local}", total_ms, updates, e2e_s, e2e_upd)
+    value = upd_all / (t_max * 1e-3)
 
     peak, peak_kind = peaks()
     bytes_per_window = mesh.ntets * (BYTES_PER_TET_SPEC * NSPEC + BYTES_PER_TET)
