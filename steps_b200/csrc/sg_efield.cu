@@ -171,9 +171,26 @@ void EFieldSystem::release() {
 
 EFieldSystem::~EFieldSystem() { release(); }
 
+static std::vector<int32_t> aggregate_order(int nv, const double* X, int ntet, const int32_t* tets);
+
 void EFieldSystem::setup(int nv, const double* verts_um, int ntet, const int32_t* tets, int nt,
                          const int32_t* tris, cudaStream_t stream, int nsm_) {
     if (nv <= 0) throw ArgErr("EField needs vertices");
+    for (size_t k = 0; k < (size_t)nt * 3; ++k)
+        if (tris[k] < 0 || tris[k] >= nv) throw ArgErr("triangle vertex index out of range");
+    std::vector<int32_t> perm = aggregate_order(nv, verts_um, ntet, tets);
+    std::vector<double> X((size_t)nv * 3);
+    for (int v = 0; v < nv; ++v)
+        for (int c = 0; c < 3; ++c) X[(size_t)perm[v] * 3 + c] = verts_um[(size_t)v * 3 + c];
+    std::vector<int32_t> tv((size_t)ntet * 4), rv((size_t)nt * 3);
+    for (size_t k = 0; k < tv.size(); ++k) tv[k] = perm[tets[k]];
+    for (size_t k = 0; k < rv.size(); ++k) rv[k] = perm[tris[k]];
+    setup_ordered(nv, X.data(), ntet, tv.data(), nt, rv.data(), stream, nsm_);
+    vperm = std::move(perm);
+}
+
+void EFieldSystem::setup_ordered(int nv, const double* verts_um, int ntet, const int32_t* tets, int nt,
+                                 const int32_t* tris, cudaStream_t stream, int nsm_) {
     nsm = nsm_;
     nverts = nv;
     ntris = nt;
@@ -845,11 +862,10 @@ static void spd_inverse(int n, std::vector<double>& E) {
         }
 }
 
-// Aggregates of one connected component: its bounding box cut into bins of about `target`
-// vertices (bins per axis in proportion to the box's extent); clamped vertices belong to
-// none.  Aggregate ids start at `base`; returns how many this component has.
-static int make_aggregates(const std::vector<int32_t>& verts, const std::vector<double>& X,
-                           const std::vector<uint8_t>& clamped, int target, int base, std::vector<int32_t>& agg) {
+// Coarse bins of one connected component: its bounding box cut into bins of about
+// `target` vertices (bins per axis in proportion to the box's extent); lin[q] is the
+// linear bin index of verts[q].
+static void component_bins(const std::vector<int32_t>& verts, const double* X, int target, std::vector<long>& lin) {
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (int i : verts)
         for (int c = 0; c < 3; ++c) {
@@ -865,15 +881,27 @@ static int make_aggregates(const std::vector<int32_t>& verts, const std::vector<
     double s = std::cbrt(vol / k);
     long nb[3];
     for (int c = 0; c < 3; ++c) nb[c] = std::max(1L, (long)std::llround(ext[c] / s));
-    std::vector<long> lin(verts.size()), keys;
+    lin.resize(verts.size());
     for (size_t q = 0; q < verts.size(); ++q) {
         const int i = verts[q];
         long id[3];
         for (int c = 0; c < 3; ++c)
             id[c] = std::min(nb[c] - 1, (long)((X[(size_t)i * 3 + c] - lo[c]) / ext[c] * nb[c]));
         lin[q] = id[0] + nb[0] * (id[1] + nb[1] * id[2]);
-        if (!clamped[i]) keys.push_back(lin[q]);
     }
+}
+
+// Vertices per aggregate a component of n vertices is cut into (about 1000 aggregates).
+static int aggregate_target(size_t n) { return std::max(16, (int)(n / 1000)); }
+
+// Aggregates of one connected component: its occupied coarse bins, clamped vertices in
+// none.  Aggregate ids start at `base`; returns how many this component has.
+static int make_aggregates(const std::vector<int32_t>& verts, const std::vector<double>& X,
+                           const std::vector<uint8_t>& clamped, int target, int base, std::vector<int32_t>& agg) {
+    std::vector<long> lin, keys;
+    component_bins(verts, X.data(), target, lin);
+    for (size_t q = 0; q < verts.size(); ++q)
+        if (!clamped[verts[q]]) keys.push_back(lin[q]);
     std::sort(keys.begin(), keys.end());
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
     for (size_t q = 0; q < verts.size(); ++q) {
@@ -882,6 +910,55 @@ static int make_aggregates(const std::vector<int32_t>& verts, const std::vector<
                             : base + (int32_t)(std::lower_bound(keys.begin(), keys.end(), lin[q]) - keys.begin());
     }
     return (int)keys.size();
+}
+
+// Device vertex order: by connected component (in order of their smallest mesh index),
+// then by coarse bin, then by mesh index.  Every aggregate is then one run of consecutive
+// device indices (clamped vertices leave holes), so the warp-per-aggregate phases of the
+// solve read and write consecutive addresses.  Returns mesh index -> device index.
+static std::vector<int32_t> aggregate_order(int nv, const double* X, int ntet, const int32_t* tets) {
+    std::vector<int32_t> up(nv);
+    for (int i = 0; i < nv; ++i) up[i] = i;
+    auto root = [&](int v) {
+        while (up[v] != v) {
+            up[v] = up[up[v]];
+            v = up[v];
+        }
+        return v;
+    };
+    for (int t = 0; t < ntet; ++t) {
+        const int32_t* tv = tets + (size_t)t * 4;
+        for (int k = 0; k < 4; ++k)
+            if (tv[k] < 0 || tv[k] >= nv) throw ArgErr("tet vertex index out of range");
+        const int r0 = root(tv[0]);
+        for (int k = 1; k < 4; ++k) {
+            const int rk = root(tv[k]);
+            if (rk != r0) up[std::max(rk, r0)] = std::min(rk, r0);
+        }
+    }
+    // Roots are the smallest vertex of their component; label components in that order.
+    std::vector<int32_t> label(nv, -1);
+    std::vector<std::vector<int32_t>> comps;
+    for (int i = 0; i < nv; ++i) {
+        const int r = root(i);
+        if (label[r] < 0) {
+            label[r] = (int32_t)comps.size();
+            comps.emplace_back();
+        }
+        comps[label[r]].push_back(i);
+    }
+    std::vector<int32_t> perm(nv);
+    int32_t next = 0;
+    std::vector<long> lin;
+    std::vector<std::pair<long, int32_t>> key;
+    for (const auto& cv : comps) {
+        component_bins(cv, X, aggregate_target(cv.size()), lin);
+        key.resize(cv.size());
+        for (size_t q = 0; q < cv.size(); ++q) key[q] = {lin[q], cv[q]};
+        std::sort(key.begin(), key.end());
+        for (const auto& kv : key) perm[kv.second] = next++;
+    }
+    return perm;
 }
 
 void EFieldSystem::set_potential(double v_mV, cudaStream_t stream) {
@@ -950,7 +1027,7 @@ void EFieldSystem::build_matrix(double dt_ms, cudaStream_t stream) {
     std::vector<int32_t> agg(n, -1);
     std::vector<int32_t> cbase(ncomp_v + 1, 0);
     for (int c = 0; c < ncomp_v; ++c) {
-        const int target = std::max(16, (int)comp_verts[c].size() / 1000);
+        const int target = aggregate_target(comp_verts[c].size());
         cbase[c + 1] = cbase[c] + make_aggregates(comp_verts[c], verts_um, vclamped, target, cbase[c], agg);
     }
     const int na = cbase[ncomp_v];

@@ -117,10 +117,19 @@ struct EFieldSystem {
     EFieldStats stats;
     int nsm = 148;
 
+    // Mesh vertex index -> index in the device arrays (vertices are stored grouped by
+    // connected component and coarse aggregate); every per-vertex array of this struct,
+    // host or device, is in device order.
+    std::vector<int32_t> vperm;
+    int vid(int mesh_vertex) const { return vperm.empty() ? mesh_vertex : vperm[mesh_vertex]; }
+
     ~EFieldSystem();
-    // verts in um, tets [ntet][4] (all tets that conduct), membrane tris [ntris][3] with areas.
+    // verts in um, tets [ntet][4] (all tets that conduct), membrane tris [ntris][3] with areas,
+    // all indexed by mesh vertex; renumbers the vertices (vperm) and calls setup_ordered.
     void setup(int nverts, const double* verts_um, int ntet, const int32_t* tets, int ntris,
                const int32_t* tris, cudaStream_t stream, int nsm);
+    void setup_ordered(int nverts, const double* verts_um, int ntet, const int32_t* tets, int ntris,
+                       const int32_t* tris, cudaStream_t stream, int nsm);
     void set_potential(double v_mV, cudaStream_t stream);
     void build_matrix(double dt_ms, cudaStream_t stream);
     // One EField step of dt_ms with tri_I already set on the device.

@@ -1054,7 +1054,7 @@ struct Solver {
         require_ef();
         check_vert(v);
         double x = 0.0;
-        d2h(&x, ef.V + v, 1);
+        d2h(&x, ef.V + ef.vid(v), 1);
         sync();
         return x * 1.0e-3;  // mV -> V
     }
@@ -1062,7 +1062,7 @@ struct Solver {
         require_ef();
         check_vert(v);
         double x = volts * 1.0e3;
-        h2d(ef.V + v, &x, 1);
+        h2d(ef.V + ef.vid(v), &x, 1);
         sync();
     }
     double get_tri_v(int t) {
@@ -2533,7 +2533,7 @@ int sg_set_vert_v_clamped(sg_solver* h, int32_t v, int32_t clamped) {
         Solver* s = S(h);
         s->require_ef();
         s->check_vert(v);
-        s->ef.vclamped[v] = clamped ? 1 : 0;
+        s->ef.vclamped[s->ef.vid(v)] = clamped ? 1 : 0;
         s->ef.dirty = true;
     });
 }
@@ -2543,7 +2543,7 @@ int sg_set_vert_iclamp(sg_solver* h, int32_t v, double amps) {
         Solver* s = S(h);
         s->require_ef();
         s->check_vert(v);
-        s->ef.vert_iclamp[v] = amps * 1.0e12;  // A -> pA, positive = into the cell (efield.cpp:214-225)
+        s->ef.vert_iclamp[s->ef.vid(v)] = amps * 1.0e12;  // A -> pA, positive = into the cell (efield.cpp:214-225)
         s->ef.dirty = true;
     });
 }
