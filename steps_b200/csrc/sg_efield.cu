@@ -512,6 +512,25 @@ struct Coarse {
 // sets z = r / diag + y_a on the aggregate's vertices; vertices in no aggregate get
 // z = r / diag.  Partial r.z; last block: beta = r.z / previous r.z (0 at the start of a
 // solve, where p = z is also written as the first direction).
+// Row `row` of a component's coarse inverse times the component's restricted residual
+// `cb` (len entries), summed over the warp: four independent accumulators per lane so
+// that eight loads are in flight, combined and shuffled in a fixed order.
+template <typename T>
+__device__ __forceinline__ T coarse_row_dot(const T* row, const T* cb, int len, int lane) {
+    T y0 = (T)0, y1 = (T)0, y2 = (T)0, y3 = (T)0;
+    int j = lane;
+    for (; j + 96 < len; j += 128) {
+        y0 += __ldg(&row[j]) * __ldcg(&cb[j]);
+        y1 += __ldg(&row[j + 32]) * __ldcg(&cb[j + 32]);
+        y2 += __ldg(&row[j + 64]) * __ldcg(&cb[j + 64]);
+        y3 += __ldg(&row[j + 96]) * __ldcg(&cb[j + 96]);
+    }
+    for (; j < len; j += 32) y0 += __ldg(&row[j]) * __ldcg(&cb[j]);
+    T y = (y0 + y1) + (y2 + y3);
+    for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
+    return __shfl_sync(0xffffffffu, y, 0);
+}
+
 template <typename T>
 __global__ void precond_kernel(Segs sg, Coarse cs, const double* diag, const T* rv, T* zv, T* pv, const T* einv,
                                const T* cvec, double* partials, unsigned int* counter, double* scal, int start) {
@@ -522,13 +541,7 @@ __global__ void precond_kernel(Segs sg, Coarse cs, const double* diag, const T* 
         const int ag = sg.agg[k];
         T y = (T)0;
         if (ag >= 0) {
-            const T* row = einv + cs.row[ag];
-            const T* cb = cvec + cs.base[ag];
-            const int len = cs.len[ag];
-#pragma unroll 4
-            for (int j = lane; j < len; j += 32) y += row[j] * cb[j];
-            for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
-            y = __shfl_sync(0xffffffffu, y, 0);
+            y = coarse_row_dot(einv + cs.row[ag], cvec + cs.base[ag], cs.len[ag], lane);
         }
         for (int m = sg.ptr[k] + lane; m < sg.ptr[k + 1]; m += 32) {
             const int i = sg.idx[m];
@@ -564,18 +577,33 @@ constexpr unsigned int kSpinLimit = 1u << 22;  // x ~100 ns polls: about half a 
 // The persistent solve is launched with at most 2048 blocks (3 x 2048 reduction partials
 // fit the 8192-value buffer); a 32-register bound keeps 8 blocks of 256 per SM resident.
 
+// GPU-scope acquire/release accesses of the barrier words.  __syncthreads orders the
+// block's writes before thread 0's release (releases are cumulative), and the block reads
+// other blocks' writes only after thread 0's acquire and the closing __syncthreads.
+__device__ __forceinline__ unsigned int atom_add_acq_rel_gpu(unsigned int* p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned int* p, unsigned int v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, unsigned int& gen) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
         const unsigned int g = gen;
-        if (atomicAdd(&bar[0], 1u) == nblocks - 1u) {
+        if (atom_add_acq_rel_gpu(&bar[0], 1u) == nblocks - 1u) {
             bar[0] = 0u;  // nobody arrives at the next barrier before the release below
-            __threadfence();
-            atomicExch(&bar[1], g + 1u);
+            st_release_gpu(&bar[1], g + 1u);
         } else {
             unsigned int spins = 0;
-            while (*(volatile unsigned int*)&bar[1] == g) {
+            while (ld_acquire_gpu(&bar[1]) == g) {
                 if (++spins > kSpinLimit) {
                     atomicOr(&bar[2], 1u);
                     break;
@@ -583,7 +611,6 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
                 __nanosleep(64);
             }
         }
-        __threadfence();
     }
     __syncthreads();
     gen += 1u;
@@ -663,13 +690,8 @@ __global__ void __launch_bounds__(kBlock, 8) pcg_persistent_kernel(PcgArgs<T> P)
             const int ag = __ldg(&P.sg.agg[k]);
             T y = (T)0;
             if (ag >= 0) {
-                const T* row = P.einv + __ldg(&P.cs.row[ag]);
-                const T* cb = P.c + __ldg(&P.cs.base[ag]);
-                const int len = __ldg(&P.cs.len[ag]);
-#pragma unroll 4
-                for (int j = lane; j < len; j += 32) y += __ldg(&row[j]) * __ldcg(&cb[j]);
-                for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
-                y = __shfl_sync(0xffffffffu, y, 0);
+                y = coarse_row_dot(P.einv + __ldg(&P.cs.row[ag]), P.c + __ldg(&P.cs.base[ag]),
+                                   __ldg(&P.cs.len[ag]), lane);
             }
             const int m1 = __ldg(&P.sg.ptr[k + 1]);
             for (int m = __ldg(&P.sg.ptr[k]) + lane; m < m1; m += 32) {
