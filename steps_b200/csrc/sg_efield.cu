@@ -664,11 +664,19 @@ struct PcgArgs {
     unsigned int* bar;  // count, generation, error
 };
 
+constexpr int kSegPass = 4;   // segments per block per preconditioner pass
+constexpr int kEllFast = 16;  // ELL widths up to this take the fully unrolled SpMV row
+constexpr int kMinbSmall = 3; // blocks per SM of the latency-bound (one-pass) solve
+
 // Two-level PCG from a started state (r and its restriction c set, scal[S_RR], scal[S_TOL2]
-// set).  The same arithmetic as the multi-kernel loop: z = r / d + y, p' = z + beta p,
-// q = A p', x += alpha p', r -= alpha q.
-template <typename T>
-__global__ void __launch_bounds__(kBlock, 8) pcg_persistent_kernel(PcgArgs<T> P) {
+// set).  The same algorithm as the multi-kernel loop (z = r / d + y, p' = z + beta p,
+// q = A p', x += alpha p', r -= alpha q); sums run in a different order.
+// MINB: resident blocks per SM the kernel is compiled for.  kMinbSmall (85 registers) for
+// systems that fit in one pass of the grid, where every phase is latency-bound: the SpMV row is
+// fully unrolled and the preconditioner is block-cooperative.  8 for larger systems
+// (bandwidth-bound SpMV, many segments per block): a warp per segment.
+template <typename T, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T> P) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     const int gt = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
@@ -683,24 +691,88 @@ __global__ void __launch_bounds__(kBlock, 8) pcg_persistent_kernel(PcgArgs<T> P)
     int iter = 0;
     bool ok = true;
 
-    // Phase C at the start: z = M^-1 r, p = z, r.z.
+    // Phase C: z = M^-1 r (p = z at the start), r.z.  Block-cooperative: a pass takes the
+    // segments k = k0 + i G (i < kSegPass) of this block; the whole block forms their
+    // coarse values y = (E^-1 c)[aggregate] together (thread t sums the row entries t,
+    // t + kBlock, ... in order, then a fixed shuffle tree and the warps in order, so y does
+    // not depend on the grid) with every segment's loads in flight at once, then applies
+    // z = r / d + y to the segments' vertices.
+    __shared__ T sy[kSegPass][kBlock / 32];
+    const int wid = threadIdx.x >> 5;
     auto precond = [&](bool start) -> double {
         double acc = 0.0;
-        for (int k = gw; k < P.sg.n; k += nw) {
-            const int ag = __ldg(&P.sg.agg[k]);
-            T y = (T)0;
-            if (ag >= 0) {
-                y = coarse_row_dot(P.einv + __ldg(&P.cs.row[ag]), P.c + __ldg(&P.cs.base[ag]),
-                                   __ldg(&P.cs.len[ag]), lane);
+        const int nseg = P.sg.n;
+        if (MINB > kMinbSmall || nseg > (int)G * kSegPass) {
+            // A warp per segment (coarse row dot by the warp).
+            for (int k = gw; k < nseg; k += nw) {
+                const int ag = __ldg(&P.sg.agg[k]);
+                T y = (T)0;
+                if (ag >= 0)
+                    y = coarse_row_dot(P.einv + __ldg(&P.cs.row[ag]), P.c + __ldg(&P.cs.base[ag]),
+                                       __ldg(&P.cs.len[ag]), lane);
+                const int m1 = __ldg(&P.sg.ptr[k + 1]);
+                for (int m = __ldg(&P.sg.ptr[k]) + lane; m < m1; m += 32) {
+                    const int iv = __ldg(&P.sg.idx[m]);
+                    const T ri = __ldcg(&P.r[iv]);
+                    const T zi = ri / (T)__ldg(&P.diag[iv]) + y;
+                    P.z[iv] = zi;
+                    if (start) P.p[iv] = zi;
+                    acc += (double)ri * (double)zi;
+                }
             }
-            const int m1 = __ldg(&P.sg.ptr[k + 1]);
-            for (int m = __ldg(&P.sg.ptr[k]) + lane; m < m1; m += 32) {
-                const int i = __ldg(&P.sg.idx[m]);
-                const T ri = __ldcg(&P.r[i]);
-                const T zi = ri / (T)__ldg(&P.diag[i]) + y;
-                P.z[i] = zi;
-                if (start) P.p[i] = zi;
-                acc += (double)ri * (double)zi;
+            return acc;
+        }
+        for (int k0 = blockIdx.x; k0 < nseg; k0 += (int)G * kSegPass) {
+            const T* rw[kSegPass];
+            const T* cb[kSegPass];
+            int len[kSegPass];
+            int lmax = 0;
+#pragma unroll
+            for (int i = 0; i < kSegPass; ++i) {
+                const int k = k0 + i * (int)G;
+                const int ag = (k < nseg) ? __ldg(&P.sg.agg[k]) : -1;
+                len[i] = (ag >= 0) ? __ldg(&P.cs.len[ag]) : 0;
+                rw[i] = (ag >= 0) ? P.einv + __ldg(&P.cs.row[ag]) : P.einv;
+                cb[i] = (ag >= 0) ? P.c + __ldg(&P.cs.base[ag]) : P.c;
+                lmax = max(lmax, len[i]);
+            }
+            T part[kSegPass];
+#pragma unroll
+            for (int i = 0; i < kSegPass; ++i) part[i] = (T)0;
+#pragma unroll 2
+            for (int j = threadIdx.x; j < lmax; j += kBlock) {
+#pragma unroll
+                for (int i = 0; i < kSegPass; ++i)
+                    if (j < len[i]) part[i] += __ldg(&rw[i][j]) * __ldcg(&cb[i][j]);
+            }
+#pragma unroll
+            for (int i = 0; i < kSegPass; ++i) {
+                T v = part[i];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) sy[i][wid] = v;
+            }
+            __syncthreads();
+            T y[kSegPass];
+#pragma unroll
+            for (int i = 0; i < kSegPass; ++i) {
+                T v = (T)0;
+                for (int w = 0; w < kBlock / 32; ++w) v += sy[i][w];
+                y[i] = v;
+            }
+            __syncthreads();  // sy is rewritten by the next pass
+#pragma unroll
+            for (int i = 0; i < kSegPass; ++i) {
+                const int k = k0 + i * (int)G;
+                if (k >= nseg) break;
+                const int m1 = __ldg(&P.sg.ptr[k + 1]);
+                for (int m = __ldg(&P.sg.ptr[k]) + threadIdx.x; m < m1; m += kBlock) {
+                    const int iv = __ldg(&P.sg.idx[m]);
+                    const T ri = __ldcg(&P.r[iv]);
+                    const T zi = ri / (T)__ldg(&P.diag[iv]) + y[i];
+                    P.z[iv] = zi;
+                    if (start) P.p[iv] = zi;
+                    acc += (double)ri * (double)zi;
+                }
             }
         }
         return acc;
@@ -718,10 +790,22 @@ __global__ void __launch_bounds__(kBlock, 8) pcg_persistent_kernel(PcgArgs<T> P)
             for (int i = gt; i < P.n; i += nt) {
                 const T pi = __ldcg(&P.z[i]) + bt * __ldcg(&pin[i]);
                 T s = (T)__ldg(&P.diag[i]) * pi;
+                if (MINB <= kMinbSmall && P.width <= kEllFast) {
+                    // All column indices first, then every gather: two dependent rounds.
+                    int jv[kEllFast];
+#pragma unroll
+                    for (int w = 0; w < kEllFast; ++w) jv[w] = (w < P.width) ? __ldg(&P.col[(size_t)w * P.n + i]) : -1;
+#pragma unroll
+                    for (int w = 0; w < kEllFast; ++w) {
+                        const int j = jv[w];
+                        if (j >= 0) s += __ldg(&P.a[(size_t)w * P.n + i]) * (__ldcg(&P.z[j]) + bt * __ldcg(&pin[j]));
+                    }
+                } else {
 #pragma unroll 4
-                for (int w = 0; w < P.width; ++w) {
-                    const int j = __ldg(&P.col[(size_t)w * P.n + i]);
-                    if (j >= 0) s += __ldg(&P.a[(size_t)w * P.n + i]) * (__ldcg(&P.z[j]) + bt * __ldcg(&pin[j]));
+                    for (int w = 0; w < P.width; ++w) {
+                        const int j = __ldg(&P.col[(size_t)w * P.n + i]);
+                        if (j >= 0) s += __ldg(&P.a[(size_t)w * P.n + i]) * (__ldcg(&P.z[j]) + bt * __ldcg(&pin[j]));
+                    }
                 }
                 pout[i] = pi;
                 P.q[i] = s;
@@ -1206,8 +1290,12 @@ void EFieldSystem::pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv
 template <typename T>
 void EFieldSystem::pcg_persistent(cudaStream_t stream, int n, const T* a, T* xv, T* rv, T* zv, T* pv, T* pv2,
                                   T* qv, const T* einv, T* cvec, double* h) {
+    // Systems whose rows fit one pass of a kMinbSmall-blocks-per-SM grid take the
+    // latency-bound form.
+    const void* kern = (n <= kMinbSmall * nsm * kBlock) ? (const void*)pcg_persistent_kernel<T, kMinbSmall>
+                                                        : (const void*)pcg_persistent_kernel<T, 8>;
     int per_sm = 0;
-    SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_persistent_kernel<T>, kBlock, 0));
+    SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0));
     const int want = std::max((n + kBlock - 1) / kBlock, (nseg + 7) / 8);
     const int G = std::max(1, std::min(std::min(want, std::max(per_sm, 1) * nsm), 2048));
     PcgArgs<T> P;
@@ -1232,7 +1320,7 @@ void EFieldSystem::pcg_persistent(cudaStream_t stream, int n, const T* a, T* xv,
     P.bar = d_bar;
     SG_CUDA(cudaMemsetAsync(d_bar, 0, 4 * sizeof(unsigned int), stream));
     void* args[] = {&P};
-    SG_CUDA(cudaLaunchCooperativeKernel((const void*)pcg_persistent_kernel<T>, dim3(G), dim3(kBlock), args, 0, stream));
+    SG_CUDA(cudaLaunchCooperativeKernel(kern, dim3(G), dim3(kBlock), args, 0, stream));
     unsigned int err = 0;
     SG_CUDA(cudaMemcpyAsync(h, scal, 10 * sizeof(double), cudaMemcpyDeviceToHost, stream));
     SG_CUDA(cudaMemcpyAsync(&err, d_bar + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
