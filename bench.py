@@ -468,8 +468,9 @@ def run_efield(args):
         sim = TetOpSplit(mdl, mesh, r, method)
         sim.setEfieldTolerance(args.ef_tol, args.ef_inner_tol)
         sim.setEfieldPersistent(bool(args.ef_persistent))
+        sim.setEfieldCheck(True, 1e-12)  # untimed FP64 solve of every step's system to 1e-12
         if method == EF_DV_CG_MIXED:
-            sim.setEfieldCheck(True, 1e-12)  # untimed FP64 solve of every step's system
+            sim.setEfieldReliableUpdates(bool(args.ef_reliable), args.ef_ru_delta)
         sim.setEfieldDT(1e-6)
         sim.setMembPotential("membrane", -0.065)
         sim.setMembCapac("membrane", 0.01)
@@ -482,7 +483,7 @@ def run_efield(args):
         sim.run(t_end)
         wall = time.perf_counter() - w0
         steps, iters, solve_ms, rr = sim.getEfieldStats()
-        chk = sim.getEfieldCheck() if method == EF_DV_CG_MIXED else None
+        chk = sim.getEfieldCheck()
         finals[name] = np.array([sim.getVertV(v) for v in range(0, mesh.nverts, 97)])
         out[name] = {"steps": steps, "cg_iterations_per_step": iters / max(steps, 1),
                      "solve_ms_per_step": solve_ms / max(steps, 1), "wall_s": wall,
@@ -496,10 +497,13 @@ def run_efield(args):
         "metric": "EField solve ms per step", "config": {"mesh": f"{nx}x{ny}x{nz} Kuhn cubes",
                                                          "tets": mesh.ntets, "verts": mesh.nverts,
                                                          "steps": args.ef_steps, "tol": args.ef_tol,
-                                                         "persistent_solve": bool(args.ef_persistent)},
+                                                         "persistent_solve": bool(args.ef_persistent),
+                                                         "mixed_reliable_updates": bool(args.ef_reliable),
+                                                         "reliable_update_delta": args.ef_ru_delta},
         "fp64": out["fp64"], "mixed": out["mixed"],
         "mixed_speedup_solve": out["fp64"]["solve_ms_per_step"] / out["mixed"]["solve_ms_per_step"],
         "max_rel_v_err_per_step": out["mixed"]["check_vs_fp64_solve"]["max_rel_v_err"],
+        "fp64_cg_max_rel_v_err_per_step": out["fp64"]["check_vs_fp64_solve"]["max_rel_v_err"],
         "max_rel_v_diff_end_of_run": err,
     }), flush=True)
     return 0
@@ -618,6 +622,9 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=64)
     ap.add_argument("--ef-dims", type=int, nargs=3, default=[20, 20, 200])
     ap.add_argument("--ef-steps", type=int, default=5000)
+    ap.add_argument("--ef-reliable", type=int, default=1,
+                    help="mixed method: 1 = one FP32 CG with reliable updates, 0 = restarted FP32 inner solves")
+    ap.add_argument("--ef-ru-delta", type=float, default=0.1)
     ap.add_argument("--ef-tol", type=float, default=1e-10)
     ap.add_argument("--ef-persistent", type=int, default=1, help="1: each EField solve in one cooperative launch")
     args = ap.parse_args()

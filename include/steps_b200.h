@@ -205,14 +205,20 @@ int sg_get_efield_stats(sg_solver* h, uint64_t* steps, uint64_t* iterations, dou
 
 /* ---- device options (no reference counterpart) ------------------------------ */
 
-/* Mixed-precision EField accuracy check: after each mixed step also solve the same system
- * in FP64 from zero to rel_tol (not counted in the solve time) and record the largest
- * per-vertex |V_mixed - V_fp64| / |V_fp64|; read it with sg_get_efield_check. */
+/* EField accuracy check: after each step (either method) also solve the same system in
+ * FP64 from zero to rel_tol (not counted in the solve time) and record the largest
+ * per-vertex |V - V_fp64| / |V_fp64|; read it with sg_get_efield_check. */
 int sg_set_efield_check(sg_solver* h, int32_t on, double rel_tol);
 int sg_get_efield_check(sg_solver* h, uint64_t* steps, double* max_rel, double* last_rel);
 /* EField solve form: 1 = every CG iteration inside one cooperative launch (grid barriers
  * between the phases), 0 = three kernel launches per iteration. */
 int sg_set_efield_persistent(sg_solver* h, int32_t on);
+/* Mixed method with the persistent solve: one FP32 CG with reliable updates (on, default;
+ * the FP64 residual b - A x replaces the FP32 one whenever the FP32 residual norm has
+ * fallen by the factor delta, default 0.1, since the last replacement) or restarted FP32
+ * inner solves inside an FP64 refinement loop (off).  Replaces the PETSc solve's precision
+ * choice (dVsolver_petsc.cpp:163-260); no reference counterpart for the factor. */
+int sg_set_efield_reliable_updates(sg_solver* h, int32_t on, double delta);
 
 /* Window-kernel launch shape: block in {64,128,256}; grid > 0 blocks, 0 = occupancy-sized
  * (blocks stride over the tets), -1 = one tet per thread. */

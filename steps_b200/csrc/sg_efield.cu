@@ -6,6 +6,7 @@
 #include <cstring>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "sg_efield.h"
@@ -310,7 +311,8 @@ namespace {
 
 constexpr int kBlock = 256;
 // Device scalar slots.
-enum { S_RZ = 0, S_PQ, S_ALPHA, S_BETA, S_RR, S_BB, S_DONE, S_ITER, S_TOL2, S_RZ0, S_CHK };
+enum { S_RZ = 0, S_PQ, S_ALPHA, S_BETA, S_RR, S_BB, S_DONE, S_ITER, S_TOL2, S_RZ0, S_CHK, S_NRU };
+constexpr int kScalOut = 12;  // device scalars copied back after a solve (S_RZ .. S_NRU)
 
 __global__ void fill_kernel(double* v, int n, double x) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = x;
@@ -662,6 +664,17 @@ struct PcgArgs {
     double* partials;  // [3][gridDim]
     double* scal;
     unsigned int* bar;  // count, generation, error
+    // Reliable updates (FP32 solve of the FP64 system, T = float only): x is the FP32
+    // correction accumulated since the last update; when the FP32 residual norm has fallen
+    // by delta2 from its largest value since the last update (or below tol2_64), x64 += x,
+    // x = 0 and r is replaced by the FP64 residual b - A64 x64 (rounded to FP32); the solve
+    // ends when that FP64 residual meets tol2_64.  The search direction is kept.
+    int ru;
+    double delta2, tol2_64;
+    const double* a64;
+    const double* b64;
+    double* x64;
+    double* r64;
 };
 
 constexpr int kSegPass = 4;   // segments per block per preconditioner pass
@@ -685,10 +698,10 @@ __global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T>
     double* part0 = P.partials;
     double* part1 = P.partials + G;
     double* part2 = P.partials + 2 * G;
-    const double tol2 = __ldcg(&P.scal[S_TOL2]);
     double rr = __ldcg(&P.scal[S_RR]);
-    double rz = 0.0, beta = 0.0;
-    int iter = 0;
+    const double tol2 = P.ru ? P.tol2_64 : __ldcg(&P.scal[S_TOL2]);
+    double rz = 0.0, beta = 0.0, rmax2 = rr;
+    int iter = 0, nru = 0;
     bool ok = true;
 
     // Phase C: z = M^-1 r (p = z at the start), r.z.  Block-cooperative: a pass takes the
@@ -834,7 +847,49 @@ __global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T>
             }
             if (!(ok = grid_sum(acc, part2, P.bar, gen, &rr))) break;
             ++iter;
-            if (rr <= tol2 || iter >= P.max_iter) break;
+            if constexpr (std::is_same<T, float>::value) {
+                if (P.ru) {
+                    rmax2 = fmax(rmax2, rr);
+                    if (rr <= P.delta2 * rmax2 || rr <= P.tol2_64 || iter >= P.max_iter) {
+                        // Reliable update: fold the correction into x64, FP64 residual.
+                        for (int i = gt; i < P.n; i += nt) {
+                            P.x64[i] += (double)__ldcg(&P.x[i]);
+                            P.x[i] = 0.0f;
+                        }
+                        if (!(ok = grid_barrier(P.bar, G, gen))) break;
+                        double acc64 = 0.0;
+                        for (int k = gw; k < P.sg.n; k += nw) {
+                            float cs = 0.0f;
+                            const int m1 = __ldg(&P.sg.ptr[k + 1]);
+                            for (int m = __ldg(&P.sg.ptr[k]) + lane; m < m1; m += 32) {
+                                const int i = __ldg(&P.sg.idx[m]);
+                                double sx = __ldg(&P.diag[i]) * __ldcg(&P.x64[i]);
+                                for (int w = 0; w < P.width; ++w) {
+                                    const int j = __ldg(&P.col[(size_t)w * P.n + i]);
+                                    if (j >= 0) sx += __ldg(&P.a64[(size_t)w * P.n + i]) * __ldcg(&P.x64[j]);
+                                }
+                                const double ri = __ldg(&P.b64[i]) - sx;
+                                P.r64[i] = ri;
+                                const float r32 = (float)ri;
+                                P.r[i] = r32;
+                                cs += r32;
+                                acc64 += ri * ri;
+                            }
+                            for (int o = 16; o > 0; o >>= 1) cs += __shfl_down_sync(0xffffffffu, cs, o);
+                            const int ag = __ldg(&P.sg.agg[k]);
+                            if (lane == 0 && ag >= 0) P.c[ag] = cs;
+                        }
+                        if (!(ok = grid_sum(acc64, part2, P.bar, gen, &rr))) break;
+                        ++nru;
+                        rmax2 = rr;
+                        if (rr <= P.tol2_64 || iter >= P.max_iter) break;
+                    }
+                } else if (rr <= tol2 || iter >= P.max_iter) {
+                    break;
+                }
+            } else {
+                if (rr <= tol2 || iter >= P.max_iter) break;
+            }
             // Phase C: z = M^-1 r, r.z, beta.
             double rzn = 0.0;
             if (!(ok = grid_sum(precond(false), part0, P.bar, gen, &rzn))) break;
@@ -850,6 +905,7 @@ __global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T>
         P.scal[S_ITER] = (double)iter;
         P.scal[S_RZ] = rz;
         P.scal[S_DONE] = 1.0;
+        P.scal[S_NRU] = (double)nru;
     }
 }
 
@@ -1280,7 +1336,7 @@ void EFieldSystem::pcg_loop(cudaStream_t stream, int n, int g, const T* a, T* xv
             std::swap(pin, pout);
         }
         SG_CUDA(cudaGetLastError());
-        SG_CUDA(cudaMemcpyAsync(h, scal, 10 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        SG_CUDA(cudaMemcpyAsync(h, scal, kScalOut * sizeof(double), cudaMemcpyDeviceToHost, stream));
         SG_CUDA(cudaStreamSynchronize(stream));
         if (h[S_DONE] != 0.0) break;
     }
@@ -1318,11 +1374,27 @@ void EFieldSystem::pcg_persistent(cudaStream_t stream, int n, const T* a, T* xv,
     P.partials = red;
     P.scal = scal;
     P.bar = d_bar;
+    P.ru = 0;
+    P.delta2 = 0.0;
+    P.tol2_64 = 0.0;
+    P.a64 = nullptr;
+    P.b64 = nullptr;
+    P.x64 = nullptr;
+    P.r64 = nullptr;
+    if (std::is_same<T, float>::value && ru_tol2 > 0.0) {
+        P.ru = 1;
+        P.delta2 = ru_delta * ru_delta;
+        P.tol2_64 = ru_tol2;
+        P.a64 = ell_a64;
+        P.b64 = b;
+        P.x64 = x;
+        P.r64 = r;
+    }
     SG_CUDA(cudaMemsetAsync(d_bar, 0, 4 * sizeof(unsigned int), stream));
     void* args[] = {&P};
     SG_CUDA(cudaLaunchCooperativeKernel(kern, dim3(G), dim3(kBlock), args, 0, stream));
     unsigned int err = 0;
-    SG_CUDA(cudaMemcpyAsync(h, scal, 10 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SG_CUDA(cudaMemcpyAsync(h, scal, kScalOut * sizeof(double), cudaMemcpyDeviceToHost, stream));
     SG_CUDA(cudaMemcpyAsync(&err, d_bar + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
     SG_CUDA(cudaStreamSynchronize(stream));
     if (err) throw DeviceErr("EField solve: a grid barrier wait timed out");
@@ -1376,7 +1448,7 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
     rhs_kernel<<<g, kBlock, 0, stream>>>(n, width, V, ell_col, ell_cc, cap_gext, v_leak, d_vert_iclamp, d_vt_ptr,
                                          d_vt_idx, tri_I, d_tri_iclamp, d_vclamped, b);
     SG_CUDA(cudaGetLastError());
-    double h[10];
+    double h[kScalOut];
     double check_ms = 0.0;
     if (method == EF_CG_FP64) {
         // Warm start from the previous step's dV (x keeps it): r = b - A x, restricted.
@@ -1397,6 +1469,16 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
         const double bb = h[S_BB];
         double rr = h[S_RR];
         int outer = 0;
+        if (persistent && reliable && bb > 0.0 && rr > tol * tol * bb) {
+            // One FP32 solve with reliable updates to the FP64 tolerance (x32 = 0, s32 = r32).
+            init_kernel<float><<<gs, kBlock, 0, stream>>>(sg, r32, x32, s32, d_c32, red, red_count, scal, inner_tol);
+            ru_tol2 = tol * tol * bb;
+            pcg<float>(stream, n, g, ell_a32, x32, s32, z32, p32, p2_32, q32, d_einv32, d_c32, h);
+            ru_tol2 = 0.0;
+            stats.iterations += (uint64_t)h[S_ITER];
+            stats.refinements += (uint64_t)h[S_NRU];
+            rr = h[S_RR];
+        }
         while (bb > 0.0 && rr > tol * tol * bb && outer < 50) {
             // Inner FP32 solve of A d = r32: s32 is its residual, q32 = A p32.
             init_kernel<float><<<gs, kBlock, 0, stream>>>(sg, r32, x32, s32, d_c32, red, red_count, scal, inner_tol);
@@ -1413,29 +1495,29 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
         }
         stats.last_rel_residual = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
         if (bb > 0.0 && rr > tol * tol * bb) throw DeviceErr("EField refinement did not converge");
-        if (check) {
-            // FP64 solve of the same system from zero, then the per-vertex comparison.
-            if (!xchk) dalloc(xchk, n);
-            if (!evc0) {
-                SG_CUDA(cudaEventCreate(&evc0));
-                SG_CUDA(cudaEventCreate(&evc1));
-            }
-            SG_CUDA(cudaEventRecord(evc0, stream));
-            init_kernel<double><<<gs, kBlock, 0, stream>>>(sg, b, xchk, r, d_c64, red, red_count, scal, check_tol);
-            pcg<double>(stream, n, g, ell_a64, xchk, r, z, p, p2, q, d_einv64, d_c64, h);
-            SG_CUDA(cudaMemsetAsync(scal + S_CHK, 0, sizeof(double), stream));
-            check_kernel<<<g, kBlock, 0, stream>>>(n, V, x, xchk, d_vclamped, scal);
-            double e = 0.0;
-            SG_CUDA(cudaMemcpyAsync(&e, scal + S_CHK, sizeof(double), cudaMemcpyDeviceToHost, stream));
-            SG_CUDA(cudaEventRecord(evc1, stream));
-            SG_CUDA(cudaEventSynchronize(evc1));
-            float cms = 0.0f;
-            SG_CUDA(cudaEventElapsedTime(&cms, evc0, evc1));
-            check_ms = cms;
-            stats.check_steps += 1;
-            stats.check_last_rel = e;
-            stats.check_max_rel = std::max(stats.check_max_rel, e);
+    }
+    if (check) {
+        // FP64 solve of the same system from zero, then the per-vertex comparison.
+        if (!xchk) dalloc(xchk, n);
+        if (!evc0) {
+            SG_CUDA(cudaEventCreate(&evc0));
+            SG_CUDA(cudaEventCreate(&evc1));
         }
+        SG_CUDA(cudaEventRecord(evc0, stream));
+        init_kernel<double><<<gs, kBlock, 0, stream>>>(sg, b, xchk, r, d_c64, red, red_count, scal, check_tol);
+        pcg<double>(stream, n, g, ell_a64, xchk, r, z, p, p2, q, d_einv64, d_c64, h);
+        SG_CUDA(cudaMemsetAsync(scal + S_CHK, 0, sizeof(double), stream));
+        check_kernel<<<g, kBlock, 0, stream>>>(n, V, x, xchk, d_vclamped, scal);
+        double e = 0.0;
+        SG_CUDA(cudaMemcpyAsync(&e, scal + S_CHK, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        SG_CUDA(cudaEventRecord(evc1, stream));
+        SG_CUDA(cudaEventSynchronize(evc1));
+        float cms = 0.0f;
+        SG_CUDA(cudaEventElapsedTime(&cms, evc0, evc1));
+        check_ms = cms;
+        stats.check_steps += 1;
+        stats.check_last_rel = e;
+        stats.check_max_rel = std::max(stats.check_max_rel, e);
     }
     apply_kernel<<<g, kBlock, 0, stream>>>(n, V, x, d_vclamped);
     if (ntris) tri_v_kernel<<<grid_for(ntris, nsm), kBlock, 0, stream>>>(ntris, d_tri_verts, V, tri_V);

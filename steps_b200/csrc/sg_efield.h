@@ -28,7 +28,7 @@ struct EFieldStats {
     uint64_t refinements = 0;       // FP64 residual evaluations
     double last_rel_residual = 0.0;
     double solve_ms = 0.0;          // device time of the solves (CUDA events)
-    // Per-step check of the mixed solve against an FP64 solve of the same system.
+    // Per-step check of the solve against an FP64 solve of the same system to check_tol.
     uint64_t check_steps = 0;
     double check_max_rel = 0.0;     // max over steps and vertices of |V_mixed - V_fp64| / |V_fp64|
     double check_last_rel = 0.0;
@@ -100,7 +100,13 @@ struct EFieldSystem {
     float* d_c32 = nullptr;
     int32_t* acol_dev = nullptr;          // [width][nverts] matrix columns (clamped ones removed)
     double inner_tol = 1.0e-4;            // relative residual of each FP32 inner solve
-    bool check = false;                   // mixed method: also solve in FP64 and compare
+    // Mixed method, persistent solve: one FP32 solve with reliable updates (the FP64
+    // residual replaces the FP32 one whenever the latter has fallen by ru_delta) instead of
+    // restarted inner solves; ru_tol2 > 0 only while such a solve runs.
+    bool reliable = true;
+    double ru_delta = 0.1;
+    double ru_tol2 = 0.0;
+    bool check = false;                   // also solve each step in FP64 to check_tol and compare
     double check_tol = 1.0e-12;           // relative residual of the FP64 check solve
     double* xchk = nullptr;               // [nverts] dV of the FP64 check solve
     double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *p2 = nullptr, *q = nullptr;

@@ -2578,6 +2578,16 @@ int sg_set_efield_persistent(sg_solver* h, int32_t on) {
     });
 }
 
+int sg_set_efield_reliable_updates(sg_solver* h, int32_t on, double delta) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        if (on && !(delta > 0.0 && delta < 1.0)) throw sg::ArgErr("reliable-update factor must be in (0, 1)");
+        s->ef.reliable = on != 0;
+        if (on) s->ef.ru_delta = delta;
+    });
+}
+
 int sg_get_efield_check(sg_solver* h, uint64_t* steps, double* max_rel, double* last_rel) {
     return guarded([&] {
         Solver* s = S(h);

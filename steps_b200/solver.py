@@ -652,14 +652,20 @@ class TetOpSplit:
         return s.value, it.value, ms.value, rr.value
 
     def setEfieldCheck(self, on, rel_tol=1e-12):
-        """Mixed-precision EField: after every step also solve the same system in FP64 (not
-        timed) and record the largest per-vertex relative voltage difference."""
+        """EField (either method): after every step also solve the same system in FP64 to
+        rel_tol (not timed) and record the largest per-vertex relative voltage difference."""
         check(self._L.sg_set_efield_check(self._h, 1 if on else 0, float(rel_tol)))
 
     def setEfieldPersistent(self, on):
         """Run each EField solve as one cooperative launch (True) or as three kernel
         launches per CG iteration (False)."""
         check(self._L.sg_set_efield_persistent(self._h, 1 if on else 0))
+
+    def setEfieldReliableUpdates(self, on, delta=0.1):
+        """Mixed method, persistent solve: one FP32 CG whose residual is replaced by the
+        FP64 one whenever it has fallen by `delta` (True, default), or restarted FP32
+        inner solves inside an FP64 refinement loop (False)."""
+        check(self._L.sg_set_efield_reliable_updates(self._h, 1 if on else 0, float(delta)))
 
     def getEfieldCheck(self):
         """(checked steps, max over steps of max_v |V_mixed - V_fp64| / |V_fp64|, last step's)."""

@@ -156,11 +156,11 @@ def test_rallpack1_membres(steps_lib, method):
     assert rms0 < 1.0e-3 and rmsx < 1.0e-3, (rms0, rmsx, iters / steps)
 
 
-@pytest.mark.parametrize("persistent", [False, True])
-def test_mixed_step_check_against_fp64(steps_lib, persistent):
-    """The mixed method's per-step check: every step's V from the FP32-inner solve is within
-    1e-6 relative of an FP64 solve of the same system; an FP64-method solver refuses nothing
-    and records no check steps."""
+@pytest.mark.parametrize("persistent,reliable", [(False, False), (True, False), (True, True)])
+def test_mixed_step_check_against_fp64(steps_lib, persistent, reliable):
+    """The mixed method's per-step check: every step's V from the FP32 solve (restarted
+    inner solves, or one solve with reliable updates) is within 1e-6 relative of an FP64
+    solve of the same system."""
     mesh = sgeom.kuhn_box(6, 6, 30, 1e-7)
     sgeom.TmComp("cyto", mesh, np.arange(mesh.ntets))
     surf = mesh.getSurfTris()
@@ -170,6 +170,7 @@ def test_mixed_step_check_against_fp64(steps_lib, persistent):
     smodel.Volsys("vsys", mdl)
     sim = TetOpSplit(mdl, mesh, make_rng(4), EF_DV_CG_MIXED)
     sim.setEfieldPersistent(persistent)
+    sim.setEfieldReliableUpdates(reliable)
     sim.setEfieldTolerance(1e-10, 1e-4)
     sim.setEfieldCheck(True, 1e-12)
     sim.setEfieldDT(1e-6)
