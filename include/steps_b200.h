@@ -257,9 +257,10 @@ int sg_get_profile(sg_solver* h, double* window_ms, uint64_t* windows, uint64_t*
 
 /* ---- allocation-free entry point (no counterpart in the reference) ----------
  *
- * For callers that cannot call cudaMalloc: code running while a stream is being
- * captured into a CUDA graph, programs whose device memory comes only from their own
- * pool allocator, and loops that cannot afford an allocation's device synchronisation.
+ * For callers that cannot call cudaMalloc: host programs whose device memory comes only
+ * from their own pool allocator (a simulator embedding this step next to other GPU
+ * code that owns the device's memory), and long-running loops that must not pay an
+ * allocation's implicit device-wide synchronisation on every call.
  * It advances one realization in one compartment (every tet) from t0 to t_end with the
  * same window kernel as sg_run, and returns with counts complete.  The caller owns all
  * inputs and outputs; the library allocates nothing.  Its scratch (packed mesh tables,
@@ -275,12 +276,16 @@ int sg_get_profile(sg_solver* h, double* window_ms, uint64_t* windows, uint64_t*
  * dcst [nspec] (0 = species does not diffuse).  seed, window0 (windows already run in
  * earlier calls: continues the same Philox streams) and t0 give the same results as a
  * solver created with that seed and run over the same times.  stream is a cudaStream_t
- * (NULL = legacy default stream); the call synchronises it before returning.
+ * (NULL = legacy default stream).  The call synchronises that stream twice: once to
+ * read the largest face coefficient (which sets the update period and the number of
+ * windows) and once at the end to read the device status word.
  * windows_out / period_out (optional) receive the windows run and the update period.
  *
- * The first call on a device looks up the scratch array's device address; make that
- * first call before any stream capture.  Every call reuses the same array and clears
- * what must start at zero; calls that overlap on the GPU race on it. */
+ * The first call on a device looks up the scratch array's device address (once per
+ * device, cached for the process); make that first call before any stream capture
+ * starts, and do not call this entry point after cudaDeviceReset on that device.
+ * Every call reuses the same array and clears what must start at zero (counters,
+ * status, face outflow); calls that overlap on the GPU race on it. */
 #define SG_NOALLOC_MAX_TETS 65536
 #define SG_NOALLOC_MAX_TET_SPECIES 262144
 #define SG_NOALLOC_MAX_REACS 64

@@ -7,7 +7,8 @@ Outputs:
   oracle/_build/liboracle.so     the C restatement (opsplit_oracle.c), gcc, OpenMP
   oracle/_ref/ref_philox_kat     Philox known-answer generator compiled against the
                                  reference's vendored Random123 header, read where it lies
-                                 under /root/reference (only when that tree is present)
+                                 in the reference tree ($STEPS_REFERENCE, default
+                                 /root/reference; only when that tree is present)
 """
 from __future__ import annotations
 
@@ -18,7 +19,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-REFERENCE = "/root/reference"
+REFERENCE = os.environ.get("STEPS_REFERENCE", "/root/reference")
 LIB = os.path.join(BUILD, "liboracle.so")
 
 CFLAGS = ["-O2", "-ffp-contract=off", "-mfma", "-fopenmp", "-fPIC", "-std=c11", "-Wall"]

@@ -1478,6 +1478,15 @@ void EFieldSystem::advance(double dt_ms, cudaStream_t stream) {
             stats.iterations += (uint64_t)h[S_ITER];
             stats.refinements += (uint64_t)h[S_NRU];
             rr = h[S_RR];
+            if (bb > 0.0 && rr > tol * tol * bb) {
+                // Stopped above the tolerance: the refinement loop below starts from the
+                // FP32 residual, which the reliable-update solve does not keep current.
+                residual_kernel<<<gs, kBlock, 0, stream>>>(n, width, acol_dev, ell_a64, diag64, b, x, r, r32, sg,
+                                                           nullptr, red, red_count, scal);
+                SG_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, stream));
+                SG_CUDA(cudaStreamSynchronize(stream));
+                rr = h[S_RR];
+            }
         }
         while (bb > 0.0 && rr > tol * tol * bb && outer < 50) {
             // Inner FP32 solve of A d = r32: s32 is its residual, q32 = A p32.

@@ -1,9 +1,9 @@
 // Allocation-free entry point: operator-split windows on caller-owned device buffers.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA stream is being
-// captured into a graph (allocation is not a capturable operation), host programs
-// whose device memory comes only from their own pool allocator, and real-time loops
-// where an allocation's implicit device synchronisation is not acceptable.  For them
+// Some callers cannot call cudaMalloc: host programs whose device memory comes only
+// from their own pool allocator (the step embedded next to other GPU code that owns
+// the device's memory), and long-running loops where an allocation's implicit
+// device-wide synchronisation on every call is not acceptable.  For them
 // sg_run_noalloc() runs the same window kernel as the solver object, but keeps every
 // piece of scratch the kernel needs (packed mesh tables, the double-buffered face
 // outflow, counters, the realization record, the status word) in one file-scope
@@ -11,9 +11,11 @@
 //
 // The array has a fixed size (SG_NOALLOC_SCRATCH_BYTES, about 11 MiB) that every GPU
 // which loads this library holds until the process exits.  All calls share it and it
-// keeps the contents of the last call: each call clears the counters and the status
-// word it relies on, and calls whose work overlaps on the GPU (different streams, or
+// keeps the contents of the last call: each call clears the counters, the status word
+// and the face outflow it relies on, and calls whose work overlaps on the GPU (different streams, or
 // different host threads on one device) race on it and must be serialised by the caller.
+// A call synchronises the caller's stream twice (after the table build, to read the
+// largest face coefficient, and at the end, to read the status word).
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -72,13 +74,15 @@ __global__ void noalloc_tables_kernel(int ntets, const double* vol, const int32_
                                       uint32_t* status) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntets; t += gridDim.x * blockDim.x) {
         double v = vol[t];
+        // A non-positive or non-finite volume would give infinite rates.
+        if (!(v > 0.0) || !(v < 1.0e300)) atomicOr(status, SG_ERR_TABLE);
         ivs[t] = 1.0 / (1.0e3 * v * kAvogadro);
         double g[4] = {0.0, 0.0, 0.0, 0.0};
         for (int f = 0; f < 4; ++f) {
             int n = neighb[(size_t)t * 4 + f];
             nbrp[(size_t)t * 4 + f] = -1;
-            if (n < 0) continue;
-            if (n >= ntets) {
+            if (n == -1) continue;
+            if (n < -1 || n >= ntets) {
                 atomicOr(status, SG_ERR_TABLE);
                 continue;
             }
@@ -90,6 +94,12 @@ __global__ void noalloc_tables_kernel(int ntets, const double* vol, const int32_
                 continue;
             }
             double d = dist[(size_t)t * 4 + f];
+            // Both sides must agree on whether the face is open: a face open on one side
+            // only would send molecules into a slot the other side never reads.
+            if ((d > 0.0) != (dist[(size_t)n * 4 + rf] > 0.0)) {
+                atomicOr(status, SG_ERR_TABLE);
+                continue;
+            }
             if (d > 0.0) {
                 g[f] = area[(size_t)t * 4 + f] / (v * d);
                 nbrp[(size_t)t * 4 + f] = (n << 2) | rf;
@@ -118,7 +128,9 @@ __global__ void noalloc_tables_kernel(int ntets, const double* vol, const int32_
 std::mutex g_symbol_mutex;
 void* g_symbol_addr[128] = {nullptr};
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array on the current device, looked up once per device
+// and cached for the life of the process (a cudaDeviceReset would invalidate it; the
+// header says not to call this entry point after one).
 unsigned char* scratch_on(int device) {
     if (device < 0 || device >= 128) throw sg::ArgErr("device index out of range");
     std::lock_guard<std::mutex> lock(g_symbol_mutex);
@@ -219,9 +231,12 @@ void run_noalloc(int32_t ntets, int32_t nspec, int32_t nreac, uint32_t* counts, 
     uint32_t* d_status = reinterpret_cast<uint32_t*>(base + kOffStatus);
     unsigned int* d_gmax = reinterpret_cast<unsigned int*>(base + kOffStatus + 4);
 
-    // Everything that must start at zero: counters, launch state, status, G max.
+    // Everything that must start at zero: counters, launch state, status, G max, and the
+    // face-outflow double buffer of this problem's size (an earlier call's values must
+    // never be gathered as inflow).
     SG_CUDA(cudaMemsetAsync(d_ctr, 0, kCounterWords * 8, stream));
     SG_CUDA(cudaMemsetAsync(d_status, 0, 8, stream));
+    SG_CUDA(cudaMemsetAsync(d_out, 0, 2 * (size_t)nspec * (size_t)ntets * 16, stream));
     if (nreac) SG_CUDA(cudaMemcpyAsync(d_reacs, reacs.data(), reacs.size() * sizeof(sg_reac),
                                        cudaMemcpyHostToDevice, stream));
     if (nreac) SG_CUDA(cudaMemcpyAsync(d_kcst, kcst, (size_t)nreac * 8, cudaMemcpyHostToDevice, stream));
@@ -238,7 +253,9 @@ void run_noalloc(int32_t ntets, int32_t nspec, int32_t nreac, uint32_t* counts, 
     uint32_t head[2] = {0u, 0u};  // status, G max bits
     SG_CUDA(cudaMemcpyAsync(head, d_status, 8, cudaMemcpyDeviceToHost, stream));
     SG_CUDA(cudaStreamSynchronize(stream));
-    if (head[0]) throw sg::ArgErr("sg_run_noalloc: neighbour table is out of range or not symmetric");
+    if (head[0])
+        throw sg::ArgErr("sg_run_noalloc: invalid mesh tables (a volume that is not positive and finite, a "
+                         "neighbour index out of range or not symmetric, or a face open on one side only)");
     float gmax_f;
     std::memcpy(&gmax_f, &head[1], 4);
     double mx = 0.0;

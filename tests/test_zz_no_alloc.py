@@ -1,8 +1,8 @@
 """The allocation-free entry point sg_run_noalloc against the solver object.
 
-sg_run_noalloc exists for callers that cannot call cudaMalloc (work recorded while a
-stream is being captured into a CUDA graph, hosts that hand out device memory only from
-their own pool, loops that cannot take an allocation's device synchronisation).  This
+sg_run_noalloc exists for callers that cannot call cudaMalloc (hosts that hand out device
+memory only from their own pool allocator, loops that must not pay an allocation's
+device-wide synchronisation on every call).  This
 test is that kind of caller: it owns every device buffer (made here with torch), calls
 the entry point twice in a row through the C ABI, and checks that the counts match the
 ones the ordinary solver (sg_create / sg_setup / sg_run) produces for the same seed and
@@ -92,3 +92,36 @@ def test_noalloc_rejects_oversize(steps_lib):
                      C.byref(nwin), None)
     assert st == 1
     assert "ntets" in steps_lib.sg_last_error().decode()
+
+
+def test_noalloc_rejects_face_open_on_one_side(steps_lib):
+    """A face whose barycentre distance is positive on one side only would send molecules
+    into a slot the other side never gathers; the table build reports it as an argument
+    error before any window runs."""
+    import torch
+
+    run_noalloc = _bind(steps_lib)
+    mesh = W.cube_mesh(4)
+    mdl = W.ab_c_model()
+    F = flatten(mdl, mesh)
+    S, T = 3, mesh.ntets
+    R = len(F["reacs"])
+    lhs = np.ascontiguousarray(np.stack([r[2] for r in F["reacs"]]), dtype=np.uint32)
+    upd = np.ascontiguousarray(np.stack([r[3] for r in F["reacs"]]), dtype=np.int32)
+    kcst = np.ascontiguousarray([r[4] for r in F["reacs"]], dtype=np.float64)
+    dcst = np.array([1e-12, 1e-12, 5e-13])
+    dist = F["dist"].copy()
+    t0 = int(np.nonzero((F["neighb"] >= 0).all(axis=1))[0][0])
+    dist[t0, 0] = 0.0  # closed from tet t0's side only
+    dev = torch.device("cuda", 0)
+    counts = torch.zeros(S * T, dtype=torch.int32, device=dev)
+    vol = torch.from_numpy(F["vol"]).to(dev)
+    neighb = torch.from_numpy(F["neighb"]).to(dev)
+    area = torch.from_numpy(F["area"]).to(dev)
+    d_dist = torch.from_numpy(dist).to(dev)
+    torch.cuda.synchronize()
+    st = run_noalloc(T, S, R, counts.data_ptr(), vol.data_ptr(), neighb.data_ptr(), area.data_ptr(),
+                     d_dist.data_ptr(), lhs.ctypes.data, upd.ctypes.data, kcst.ctypes.data,
+                     dcst.ctypes.data, 1, 0.0, 1e-3, 0, None, None, None)
+    assert st == 1
+    assert "face open on one side" in steps_lib.sg_last_error().decode()
