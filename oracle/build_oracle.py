@@ -5,6 +5,8 @@ reference that compile from their own sources here.
 
 Outputs:
   oracle/_build/liboracle.so     the C restatement (opsplit_oracle.c), gcc, OpenMP
+  oracle/_ref/libsteps_ref.so    the reference TetOpSplitP and Tetexact compiled from their
+                                 own sources (build_ref_tetopsplit.py)
   oracle/_ref/ref_philox_kat     Philox known-answer generator compiled against the
                                  reference's vendored Random123 header, read where it lies
                                  in the reference tree ($STEPS_REFERENCE, default
@@ -40,10 +42,17 @@ def build_oracle(force=False):
 
 
 def build_ref(force=False):
-    """Reference-side pieces; skipped when the reference tree is absent (GPU box)."""
+    """Reference-side pieces; skipped when the reference tree is absent (GPU box): the
+    Philox known-answer generator and the reference solvers (build_ref_tetopsplit)."""
     third = os.path.join(REFERENCE, "src", "third_party")
     if not os.path.isdir(third):
         return None
+    try:
+        from . import build_ref_tetopsplit
+    except ImportError:  # run as a script
+        import build_ref_tetopsplit
+
+    build_ref_tetopsplit.build(force=force)
     os.makedirs(REF_OUT, exist_ok=True)
     exe = os.path.join(REF_OUT, "ref_philox_kat")
     src = os.path.join(HERE, "ref_philox_kat.c")

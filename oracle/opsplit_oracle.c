@@ -234,6 +234,92 @@ static uint32_t or_binom(or_stream* st, uint32_t n, double p) {
     return flip ? n - k : k;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Placement of a compartment count over its tets (util/distribute.hpp:102-193, */
+/* math/sample.hpp:59-200): volume-weighted floor allocation, then the remainder */
+/* by adjusted Pareto order sampling on the fractional parts.  Draws come from   */
+/* the stream the solver uses for its n-th setter call (key (seed, 0), unit =   */
+/* call index, purpose 1), so the result can be compared bit for bit.          */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    double key;
+    int idx;
+} or_keyed;
+
+static int or_keyed_cmp(const void* a, const void* b) {
+    const or_keyed* x = (const or_keyed*)a;
+    const or_keyed* y = (const or_keyed*)b;
+    if (x->key < y->key) return -1;
+    if (x->key > y->key) return 1;
+    return (x->idx > y->idx) - (x->idx < y->idx);
+}
+
+/* Returns 0, or -1 for a non-positive total weight, -2 if the floors exceed x. */
+int or_distribute(uint64_t seed, uint64_t call, int n, const double* w, double x, uint32_t* out) {
+    if (n <= 0) return 0;
+    if (x == 0.0) {
+        for (int i = 0; i < n; ++i) out[i] = 0;
+        return 0;
+    }
+    or_stream st;
+    or_stream_init(&st, seed, 0u, (uint32_t)(call & 0xFFFFFFFFu), call >> 32, 1u);
+    double total = 0.0;
+    for (int i = 0; i < n; ++i) total += w[i];
+    if (!(total > 0.0)) return -1;
+    if (u_co(or_u32(&st)) < x - floor(x))
+        x = 1.0 + floor(x);
+    else
+        x = floor(x);
+    double xot = x / total;
+    unsigned long long allocated = 0;
+    double* pi = (double*)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        double xi = xot * w[i];
+        double fl = floor(xi);
+        pi[i] = xi - fl;
+        out[i] = (uint32_t)fl;
+        allocated += (unsigned long long)fl;
+    }
+    if ((double)allocated > x) {
+        free(pi);
+        return -2;
+    }
+    size_t rem = (size_t)(x - (double)allocated);
+    if (rem > 0) {
+        double psum = 0.0;
+        for (int i = 0; i < n; ++i) psum += pi[i];
+        double rescale = (double)rem / psum;
+        double d = 0.0;
+        for (int i = 0; i < n; ++i) {
+            pi[i] *= rescale;
+            if (pi[i] > 1.0) pi[i] = 1.0;
+            d += pi[i] * (1.0 - pi[i]);
+        }
+        double ood2 = (d == 0.0) ? 1.0 : 1.0 / (d * d);
+        or_keyed* keys = (or_keyed*)malloc(sizeof(or_keyed) * (size_t)n);
+        size_t nk = 0;
+        for (int i = 0; i < n; ++i) {
+            double q = pi[i];
+            if (q == 0.0) continue;
+            /* Rosen's adjusted Pareto rank: q_c U / (1 - U), q_c = (1-q)/q exp(q(1-q)(q-1/2)/d^2)
+               with the exponential to second order. */
+            double la = q * (1.0 - q) * (q - 0.5) * ood2;
+            double aa = 1.0 + la + 0.5 * la * la;
+            double qc = (1.0 - q) / q * aa;
+            double u = u_co(or_u32(&st));
+            keys[nk].key = qc * u / (1.0 - u);
+            keys[nk].idx = i;
+            ++nk;
+        }
+        if (nk < rem) rem = nk;
+        qsort(keys, nk, sizeof(or_keyed), or_keyed_cmp);
+        for (size_t j = 0; j < rem; ++j) out[keys[j].idx] += 1;
+        free(keys);
+    }
+    free(pi);
+    return 0;
+}
+
 /* Draw count binomials from one stream (sampler tests): out[i] = Binom(n, p). */
 void or_binom_many(uint64_t seed, uint32_t unit, uint32_t n, double p, uint32_t count, uint32_t* out) {
     or_stream st;

@@ -52,12 +52,28 @@ def load():
         lib.or_binom_many.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, pu]
         lib.or_set_boundaries.argtypes = [P, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         lib.or_set_btab.argtypes = [P, C.POINTER(C.c_double)]
+        lib.or_distribute.argtypes = [C.c_uint64, C.c_uint64, C.c_int, pf, C.c_double, pu]
+        lib.or_distribute.restype = C.c_int
         _lib = lib
     return _lib
 
 
 def _p(a, t):
     return a.ctypes.data_as(C.POINTER(t))
+
+
+def distribute(seed, call, weights, x):
+    """Counts of a compartment placement of x molecules over tets of the given weights
+    (util/distribute.hpp:102-193), drawn from the solver's stream of its setter call
+    number ``call``."""
+    L = load()
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    out = np.zeros(w.size, dtype=np.uint32)
+    st = L.or_distribute(C.c_uint64(seed), C.c_uint64(call), w.size, _p(w, C.c_double), float(x),
+                         _p(out, C.c_uint32))
+    if st != 0:
+        raise ValueError(f"distribute failed ({st})")
+    return out
 
 
 class Oracle:

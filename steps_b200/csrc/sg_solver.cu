@@ -1336,7 +1336,7 @@ struct Solver {
         }
         double total = 0.0;
         for (int t : tets) total += vol[t];
-        if (!(total > 0.0)) throw ArgErr("non-positive total weight for distribution");
+        if (!(total > 0.0)) throw ArgErr("cannot place molecules: the elements to fill have no volume (or area)");
         if (sg_u01_co(sg_next_u32(st)) < x - std::floor(x))
             x = 1.0 + std::floor(x);
         else
@@ -1351,7 +1351,7 @@ struct Solver {
             v[tets[i]] = (uint32_t)fl;
             allocated += (unsigned long long)fl;
         }
-        if ((double)allocated > x) throw ProgErr("internal error in count rounding");
+        if ((double)allocated > x) throw ProgErr("placement: the rounded-down shares add up to more than the count placed");
         size_t rem = (size_t)(x - (double)allocated);
         if (rem == 0) return;
         // Adjusted Pareto order sampling: rank Q_i = q_i U_i / (1 - U_i), keep the rem smallest.

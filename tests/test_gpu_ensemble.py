@@ -1,0 +1,95 @@
+"""Statistical parity of the GPU solver with the reference solvers themselves.
+
+The reference ensembles (tests/golden/ref_ensemble_*.npz) come from the reference
+TetOpSplitP (src/steps/mpi/tetopsplit/tetopsplit.cpp) and Tetexact
+(src/steps/tetexact/tetexact.cpp) compiled from the reference's own sources and run
+with seeds 1..200 (tests/golden/make_ref_ensembles.py).  Here the same configurations
+run as 200 batched realizations on the GPU (independent Philox keys per realization),
+and the two ensembles must agree in mean and variance within 3 sigma at every record
+and pass a two-sample KS test (p above 0.01, Bonferroni-corrected over the records).
+
+  * plain small configuration (10^3 Kuhn cubes, A + B <-> C, A = B = 10,000 placed by
+    setCompSpecCount): compartment counts of A and C every 1 ms to 100 ms;
+  * diffusion spread (10 A per tet in the first layer of cubes): counts of A per 0.1 um
+    slab along x every 2 ms to 40 ms.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from steps_b200 import geom as sgeom
+from steps_b200 import workloads as W
+from steps_b200.solver import TetOpSplit
+from tests.ensemble_stats import compare
+from tests.helpers import make_rng
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _batched(n, seed):
+    base = sgeom.kuhn_box(10, 10, 10, 1e-7)
+    mesh = sgeom.replicate(base, n)
+    comp = sgeom.TmComp("comp", mesh, np.arange(mesh.ntets))
+    comp.addVolsys("vsys")
+    sim = TetOpSplit(W.ab_c_model(), mesh, make_rng(seed), realizations=mesh.offsets)
+    return base, mesh, sim
+
+
+def _per_real(sim, mesh, s, n):
+    c = sim.getSpecCounts(s).astype(np.int64)
+    return np.add.reduceat(c, mesh.offsets[:-1])
+
+
+def gpu_c0(n, times, seed=1):
+    _, mesh, sim = _batched(n, seed)
+    sim.setCompSpecCount("comp", "A", 10000)
+    sim.setCompSpecCount("comp", "B", 10000)
+    out = np.zeros((n, len(times), 3), dtype=np.int64)
+    for i, t in enumerate(times):
+        if t > 0:
+            sim.run(t)
+        for j, s in enumerate(("A", "B", "C")):
+            out[:, i, j] = _per_real(sim, mesh, s, n)
+    return out
+
+
+def gpu_spread(n, times, seed=1):
+    base, mesh, sim = _batched(n, seed)
+    bary = base.verts[base.tets].mean(axis=1)
+    slab = np.clip((bary[:, 0] / 1e-7).astype(np.int64), 0, 9)
+    a0 = np.where(slab == 0, 10, 0).astype(np.uint32)
+    sim.setSpecCounts("A", np.tile(a0, n))
+    T = base.ntets
+    out = np.zeros((n, len(times), 10), dtype=np.int64)
+    for i, t in enumerate(times):
+        if t > 0:
+            sim.run(t)
+        c = sim.getSpecCounts("A").astype(np.int64).reshape(n, T)
+        for k in range(10):
+            out[:, i, k] = c[:, slab == k].sum(axis=1)
+    return out
+
+
+def test_c0_ensemble_matches_reference_tetopsplit_and_tetexact(steps_lib):
+    fx = np.load(os.path.join(GOLD, "ref_ensemble_c0.npz"))
+    times = fx["times"]
+    g = gpu_c0(fx["tos"].shape[0], times)
+    # A and B are equal in every member (they only react with each other); A + C is fixed.
+    assert np.array_equal(g[:, :, 0], g[:, :, 1])
+    assert np.all(g[:, :, 0] + g[:, :, 2] == 10000)
+    for arm in ("tos", "tetexact"):
+        rep = compare(g, fx[arm], cols=[0, 2])
+        assert rep["ok"], (arm, rep)
+
+
+def test_diffusion_spread_matches_reference_tetopsplit_and_tetexact(steps_lib):
+    fx = np.load(os.path.join(GOLD, "ref_ensemble_spread.npz"))
+    times = fx["times"]
+    g = gpu_spread(fx["tos"].shape[0], times)
+    assert np.all(g.sum(axis=2) == 6000)
+    for arm in ("tos", "tetexact"):
+        rep = compare(g, fx[arm])
+        assert rep["ok"], (arm, rep)

@@ -276,3 +276,41 @@ def test_diffusion_boundary_matches_oracle(steps_lib, split):
             assert sim.getCompSpecCount("right", "A") > 0
     total = sim.getCompSpecCount("left", "A") + sim.getCompSpecCount("right", "A") + sim.getCompSpecCount("right", "B")
     assert total == 20000
+
+
+def test_placement_matches_oracle_restatement(steps_lib):
+    """setCompSpecCount places molecules by the reference's rule (util/distribute.hpp:102-193:
+    volume-weighted floors, then adjusted Pareto order sampling of the remainder); the
+    solver's placement equals the oracle's restatement bit for bit, the n-th setter call
+    drawing from setup stream n.  The sphere mesh of the reference's validation has tets
+    of unequal volume; the batched case places each realization with its own call."""
+    import os
+
+    from oracle.pyoracle import distribute
+    from steps_b200 import geom as sgeom
+    from steps_b200.solver import TetOpSplit
+    from tests.helpers import make_rng
+
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sphere_rad1_37tets.npz"))
+    mesh = sgeom.Tetmesh(d["verts"], d["tets"])
+    sgeom.TmComp("comp", mesh, np.arange(mesh.ntets)).addVolsys("vsys")
+    seed = 77
+    sim = TetOpSplit(W.ab_c_model(), mesh, make_rng(seed))
+    vol = sim.tables["vol"]
+    sim.setCompSpecCount("comp", "A", 1000.5)
+    assert np.array_equal(sim.getSpecCounts("A"), distribute(seed, 0, vol, 1000.5))
+    sim.setCompSpecCount("comp", "B", 37.25)
+    assert np.array_equal(sim.getSpecCounts("B"), distribute(seed, 1, vol, 37.25))
+    sim.setCompSpecCount("comp", "A", 0.0)
+    assert not sim.getSpecCounts("A").any()
+
+    base = W.cube_mesh(3)
+    rep = sgeom.replicate(base, 3)
+    sgeom.TmComp("comp", rep, np.arange(rep.ntets)).addVolsys("vsys")
+    bs = TetOpSplit(W.ab_c_model(), rep, make_rng(seed), realizations=rep.offsets)
+    bs.setCompSpecCount("comp", "C", 55.5)
+    got = bs.getSpecCounts("C")
+    T = base.ntets
+    for r in range(3):
+        want = distribute(seed, r, bs.tables["vol"][r * T:(r + 1) * T], 55.5)
+        assert np.array_equal(got[r * T:(r + 1) * T], want), r
