@@ -113,6 +113,7 @@ struct Solver {
 
     // ---- device state ----
     DevBuf<uint32_t> d_counts, d_outflow, d_clamp, d_status;
+    DevBuf<unsigned int> d_work;  // [2][4] work counters of the split-window kernels
     DevBuf<int32_t> d_nbr, d_comp, d_crb, d_dslot, d_dspec;
     DevBuf<double> d_tdel;                      // [D][T] split mode only
     // Diffusion boundaries.
@@ -500,6 +501,7 @@ struct Solver {
         d_diff_total.alloc(1);
         d_launch.alloc(4);
         d_status.alloc(1);
+        d_work.alloc(8);
         h2d(d_nbr.p, nbrp.data(), nbrp.size());
         h2d(d_geo.p, geo.data(), geo.size());
         h2d(d_ivs.p, ivs.data(), ivs.size());
@@ -738,6 +740,7 @@ struct Solver {
         SG_CUDA(cudaMemsetAsync(d_ext_total.p, 0, d_ext_total.n * 8, stream));
         SG_CUDA(cudaMemsetAsync(d_diff_total.p, 0, 8, stream));
         SG_CUDA(cudaMemsetAsync(d_launch.p, 0, 32, stream));
+        SG_CUDA(cudaMemsetAsync(d_work.p, 0, 32, stream));
         SG_CUDA(cudaMemsetAsync(d_status.p, 0, 4, stream));
         const int R = (int)reacs.size();
         for (int r = 0; r < nreal; ++r)
@@ -797,6 +800,7 @@ struct Solver {
         a.surf_ext = has_surf() ? d_surf_ext.p : nullptr;
         a.tdel = d_tdel.p;
         a.diff_spec = d_dspec.p;
+        a.work = d_work.p;
         if (nbnd > 0) {
             a.bface = d_bface.p;
             a.bnbr = d_bnbr.p;
@@ -878,6 +882,40 @@ struct Solver {
         if (!d_tdel.p && ndiff > 0) d_tdel.alloc((size_t)ndiff * ntets);
     }
 
+    // Grids of the dynamically scheduled split kernels: every block resident at once (warps
+    // take their tets from a work counter), capped by the blocks the tets can fill.
+    int occ_cache_key[3] = {-1, -1, -1};
+    int occ_cache_val[3] = {0, 0, 0};
+    int resident_blocks(int which, int blk, size_t smem) {
+        const int key = blk * 1000003 + (int)smem;
+        if (occ_cache_key[which] == key) return occ_cache_val[which];
+        int per_sm = 0;
+        if (which == 0) {
+            switch (blk) {
+                case 64: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<64, false, true>, 64, smem)); break;
+                case 128: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<128, false, true>, 128, smem)); break;
+                case 256: SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<256, false, true>, 256, smem)); break;
+                default: throw ArgErr("block size must be 64, 128 or 256");
+            }
+        } else if (which == 1) {
+            SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<128, true, true>, 128, smem));
+        } else {
+            SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leave_kernel<256>, 256, 0));
+        }
+        occ_cache_key[which] = key;
+        occ_cache_val[which] = std::max(per_sm, 1) * nsm;
+        return occ_cache_val[which];
+    }
+    int split_ssa_grid(size_t smem, int ntodo) {
+        const long need = ((long)ntodo + block - 1) / block;
+        return (int)std::max(1L, std::min(need, (long)resident_blocks(0, block, smem)));
+    }
+    int surf_ssa_capacity(size_t smem) { return resident_blocks(1, 128, smem); }
+    int leave_grid() {
+        const long need = ((long)ntets + 255) / 256;
+        return (int)std::max(1L, std::min(need, (long)resident_blocks(2, 256, 0)));
+    }
+
     void launch_window(const sg_window_args& a, int g) {
         size_t sm = window_smem();
         int chk = check_flag();
@@ -886,7 +924,7 @@ struct Solver {
             // occupancy, the SURF SSA over the membrane tet list, then the diffusion leave.
             if (ndiff > 0 && !a.tdel) throw ProgErr("split window without its buffers");
             const size_t smv = smem_bytes(block, nspec, (int)reacs.size());
-            const int gv = (int)std::max(1L, ((long)ntets + block - 1) / block);
+            const int gv = split_ssa_grid(smv, ntets);
             switch (block) {
                 case 64: window_kernel<64, false, true><<<gv, 64, smv, stream>>>(a, chk); break;
                 case 128: window_kernel<128, false, true><<<gv, 128, smv, stream>>>(a, chk); break;
@@ -898,7 +936,8 @@ struct Solver {
                 sg_window_args am = a;
                 am.tet_list = d_memb_tets.p;
                 am.nlist = nmemb_tets;
-                window_kernel<128, true, true><<<(nmemb_tets + 127) / 128, 128, sm, stream>>>(am, chk);
+                const int gm = (int)std::min<long>(((long)nmemb_tets + 127) / 128, (long)surf_ssa_capacity(sm));
+                window_kernel<128, true, true><<<gm, 128, sm, stream>>>(am, chk);
                 SG_CUDA(cudaGetLastError());
             }
             if (nsdiff > 0) {
@@ -907,23 +946,20 @@ struct Solver {
                 sdiffuse_kernel<256><<<gsd, 256, 0, stream>>>(a);
                 SG_CUDA(cudaGetLastError());
             }
-            const long long pairs = (long long)ndiff * ntets;
-            const int gd = (int)std::max(1LL, std::min((pairs + 255) / 256, (long long)nsm * 64));
-            diffuse_kernel<256><<<gd, 256, 0, stream>>>(a, chk);
+            leave_kernel<256><<<leave_grid(), 256, 0, stream>>>(a, chk);
         } else if (has_surf()) {
             window_kernel<128, true><<<g, 128, sm, stream>>>(a, chk);
         } else if (use_split()) {
             if (ndiff > 0 && !a.tdel) throw ProgErr("split window without its buffers");
+            const int gs = split_ssa_grid(sm, ntets);
             switch (block) {
-                case 64: window_kernel<64, false, true><<<g, 64, sm, stream>>>(a, chk); break;
-                case 128: window_kernel<128, false, true><<<g, 128, sm, stream>>>(a, chk); break;
-                case 256: window_kernel<256, false, true><<<g, 256, sm, stream>>>(a, chk); break;
+                case 64: window_kernel<64, false, true><<<gs, 64, sm, stream>>>(a, chk); break;
+                case 128: window_kernel<128, false, true><<<gs, 128, sm, stream>>>(a, chk); break;
+                case 256: window_kernel<256, false, true><<<gs, 256, sm, stream>>>(a, chk); break;
                 default: throw ArgErr("block size must be 64, 128 or 256");
             }
             SG_CUDA(cudaGetLastError());
-            const long long pairs = (long long)ndiff * ntets;
-            const int gd = (int)std::max(1LL, std::min((pairs + 255) / 256, (long long)nsm * 64));
-            diffuse_kernel<256><<<gd, 256, 0, stream>>>(a, chk);
+            leave_kernel<256><<<leave_grid(), 256, 0, stream>>>(a, chk);
         } else {
             switch (block) {
                 case 64: window_kernel<64><<<g, 64, sm, stream>>>(a, chk); break;
@@ -1730,6 +1766,8 @@ struct Solver {
             get_dev(f, d_ext_total.p, d_ext_total.n, "extents");
             get_dev(f, d_diff_total.p, d_diff_total.n, "diffusion extent");
             get_dev(f, d_launch.p, d_launch.n, "launch state");
+            // The counters of the next window's parity are zero between windows.
+            SG_CUDA(cudaMemsetAsync(d_work.p, 0, 32, stream));
             if (nbnd > 0) {
                 get(f, bact.data(), bact.size(), "diffusion boundaries");
                 get(f, bdcst.data(), bdcst.size(), "diffusion boundary constants");

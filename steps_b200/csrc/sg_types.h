@@ -160,6 +160,10 @@ typedef struct sg_window_args {
     const int32_t* diff_spec;          // [D]: species of each diffusing index
     const int32_t* tet_list;           // [nlist] tets of this launch, or null for all tets
     int32_t nlist;
+    // Work counters of the split-window kernels, [2][4] by launch parity: the next chunk
+    // of 32 tets for the volume SSA (0), the membrane SSA (1) and the diffusion leave (2).
+    // Each window's last block zeroes the next parity's counters.  Null: static schedule.
+    unsigned int* work;
     // Diffusion boundaries (diffboundary.cpp, diff.cpp:307-398), null without any: per tet
     // the boundary of each face (byte f, 0xFF = none), the neighbour behind boundary faces
     // ((n << 2) | its face, -1), the face coefficients A / (V d), the two compartments of

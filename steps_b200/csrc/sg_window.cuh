@@ -65,6 +65,25 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
     return v;
 }
 
+// Sum of a uint32 over the 32 lanes as 64 bits, in every lane: two warp reductions of the
+// 16-bit halves (neither can overflow 32 bits) instead of a 64-bit shuffle tree.
+__device__ __forceinline__ unsigned long long warp_total_u32(uint32_t c) {
+    const uint32_t lo = __reduce_add_sync(0xffffffffu, c & 0xFFFFu);
+    const uint32_t hi = __reduce_add_sync(0xffffffffu, c >> 16);
+    return (unsigned long long)lo + ((unsigned long long)hi << 16);
+}
+
+// First tet of the warp's next chunk of 32: from the launch's work counter (dynamic
+// schedule) or the warp's fixed stride (static).  Uniform across the warp.
+__device__ __forceinline__ int next_warp_base(unsigned int* ctr, int it, int BLOCK) {
+    if (ctr) {
+        unsigned int c = 0u;
+        if ((threadIdx.x & 31) == 0) c = atomicAdd(ctr, 1u);
+        return (int)__shfl_sync(0xffffffffu, c, 0) * 32;
+    }
+    return (int)((blockIdx.x + (unsigned)it * gridDim.x) * (unsigned)BLOCK + (threadIdx.x & ~31u));
+}
+
 // Shared-memory carve-up for a block of BLOCK threads.
 struct smem_layout {
     uint32_t* cnt;             // [S][BLOCK]
@@ -578,6 +597,7 @@ __device__ __forceinline__ void window_last_block(const sg_window_args& a, int c
         a.ext[q * R + rr] = 0ull;
     }
     for (int s = tid; s < S; s += BLOCK) a.totals[q * S + s] = 0ull;
+    if (a.work && tid < 4) a.work[q * 4 + tid] = 0u;
     for (int i = tid; i < a.nreal; i += BLOCK) {
         sg_real* rl = &a.reals[i];
         double rt = __ldcg(&rl->t), rend = __ldcg(&rl->t_end), per = __ldcg(&rl->period);
@@ -617,7 +637,7 @@ __device__ __forceinline__ bool window_block_done(const sg_window_args& a, int* 
 
 // Window kernel: gather (if pending) -> totals -> SSA -> diffusion leave -> store.
 // SPLIT: reactions only (gather, SSA, counts and change-time sums to global memory); the
-// diffusion leave and the end of the window run in diffuse_kernel.
+// diffusion leave and the end of the window run in leave_kernel.
 template <int BLOCK, bool SURF = false, bool SPLIT = false>
 __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     window_kernel(sg_window_args a, int check) {
@@ -642,12 +662,17 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     const unsigned long long parity = __ldcg(&a.launch_state[1]) & 1ull;
     const size_t plane = (size_t)a.ntets * 4;  // uint32 words per diffusing species
     unsigned long long moved = 0ull;
+    // Split kernels take chunks of 32 tets per warp from the launch's work counter, so a
+    // warp whose tets drew few events moves on instead of idling until its block ends.
+    unsigned int* wctr = (SPLIT && a.work) ? a.work + parity * 4 + (SURF ? 1 : 0) : nullptr;
 
     // A tet list (split windows of membrane models) restricts the launch to those tets.
     const int nit = a.tet_list ? a.nlist : a.ntets;
-    for (int base = blockIdx.x * BLOCK; base < nit; base += gridDim.x * BLOCK) {
-        bool active = base + tid < nit;
-        const int t = !active ? 0 : (a.tet_list ? __ldg(&a.tet_list[base + tid]) : base + tid);
+    for (int it = 0;; ++it) {
+        const int base = next_warp_base(wctr, it, BLOCK);
+        if (base >= nit) break;
+        bool active = base + lane < nit;
+        const int t = !active ? 0 : (a.tet_list ? __ldg(&a.tet_list[base + lane]) : base + lane);
         int r = 0, comp = 0, tlocal = 0;
         double T = 0.0;
         unsigned long long w = 0;
@@ -702,7 +727,7 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
                 L.tdel[s * BLOCK + tid] = 0.0;
             }
             L.cnt[s * BLOCK + tid] = c;
-            unsigned long long v = warp_sum_u64((unsigned long long)c);
+            const unsigned long long v = warp_total_u32(c);
             if (lane == 0 && v) atomicAdd(&L.tot[s], v);
         }
         if (!active) continue;
@@ -788,16 +813,24 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     for (int i = tid; i < R; i += BLOCK)
         if (L.ext[i]) atomicAdd(&a.ext[parity * R + i], (unsigned long long)L.ext[i]);
     if (tid == 0 && L.moved[0]) atomicAdd(a.diff_total, L.moved[0]);
-    if (SPLIT) return;  // diffuse_kernel ends the window
+    if (SPLIT) return;  // leave_kernel ends the window
     if (!window_block_done(a, L.flag)) return;
     window_last_block(a, check, parity, L.flag, BLOCK);
 }
 
-// Split window, second kernel: the diffusion leave with one thread per (diffusing
-// species, tet), species-major so that a warp reads 32 consecutive tets of one species;
-// then the end of the window (last block).  Identical results to the fused kernel.
+// Resident threads per SM the leave kernel is compiled for (caps registers per thread).
+#ifndef SG_LEAVE_THREADS_PER_SM
+#define SG_LEAVE_THREADS_PER_SM 1024
+#endif
+
+// Split window, second kernel: the diffusion leave.  One thread per tet loops over the
+// diffusing species, so the tet's tables (neighbours, face selectors and their odds, the
+// window length, realization, compartment, clamps) are read and derived once; warps take
+// chunks of 32 tets from the launch's work counter, so no warp waits on slower ones until
+// the work runs out.  Then the end of the window (last block).  Each (tet, species) draws
+// from its own stream, so the results equal the fused kernel's bit for bit.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 4) diffuse_kernel(sg_window_args a, int check) {
+__global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_kernel(sg_window_args a, int check) {
     __shared__ double s_rcp[SG_RCP_TABLE];
     __shared__ int flag[2];
     __shared__ unsigned long long s_moved;
@@ -806,49 +839,70 @@ __global__ void __launch_bounds__(BLOCK, 4) diffuse_kernel(sg_window_args a, int
     if (tid == 0) s_moved = 0ull;
     __syncthreads();
     const unsigned long long parity = __ldcg(&a.launch_state[1]) & 1ull;
+    unsigned int* wctr = a.work ? a.work + parity * 4 + 2 : nullptr;
     const size_t plane = (size_t)a.ntets * 4;
-    const long long total = (long long)a.ndiff * a.ntets;
+    const int S = a.nspec;
     unsigned long long moved = 0ull;
-    for (long long idx = (long long)blockIdx.x * BLOCK + tid; idx < total; idx += (long long)gridDim.x * BLOCK) {
-        const int ds = (int)(idx / a.ntets);
-        const int t = (int)(idx - (long long)ds * a.ntets);
+    for (int it = 0;; ++it) {
+        const int base = next_warp_base(wctr, it, BLOCK);
+        if (base >= a.ntets) break;
+        const int t = base + lane;
+        if (t >= a.ntets) continue;
         const int r = find_real(a.reals, a.nreal, t);
         const sg_real* rl = &a.reals[r];
         const double rt = rl->t, rend = rl->t_end, per = rl->period;
         if (!(rt < rend)) continue;
         const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
         if (comp < 0) continue;
-        const int s = __ldg(&a.diff_spec[ds]);
-        const double D = __ldg(&a.dcst[((size_t)r * a.ncomp + comp) * a.nspec + s]);
-        if (!(D > 0.0)) continue;
         const double T = (rt + per > rend) ? rend - rt : per;
         const unsigned long long w = rl->window;
+        const uint32_t tl = (uint32_t)(t - rl->tet_begin);
         const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
         const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
-        const size_t ci = (size_t)s * a.ntets + t;
-        const uint32_t pop = a.counts[ci];
-        uint4 k = make_uint4(0u, 0u, 0u, 0u);
+        const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
         const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
-        if (pop > 0u) {
-            float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
-            double t1 = T * (D * (double)g.w);
-            if (bt) t1 = T * bnd_split(a, t, comp, s, D, nb, &g);
-            sg_stream st;
-            uint32_t Kn = 0u;
-            k = leave_species(a.seed, (uint32_t)r, (uint32_t)(t - rl->tet_begin), w, (uint32_t)s, pop,
-                              a.tdel[(size_t)ds * a.ntets + t], 1.0 / T, t1, g, sg_binom_odds((double)g.x),
-                              sg_binom_odds((double)g.y), sg_binom_odds((double)g.z), s_rcp, &st, &Kn);
-            if (Kn > 0u) {
-                if (!((clampm >> s) & 1u)) a.counts[ci] = pop - Kn;
-                moved += Kn;
+        const double* Dc = a.dcst + ((size_t)r * a.ncomp + comp) * S;
+        uint32_t* out = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane;
+        // Odds of the three face selectors and 1/T, once per tet.
+        const double odd1 = sg_binom_odds((double)g.x);
+        const double odd2 = sg_binom_odds((double)g.y);
+        const double odd3 = sg_binom_odds((double)g.z);
+        const double invT = 1.0 / T;
+        for (int s = 0; s < S; ++s) {
+            const int ds = __ldg(&a.diff_slot[s]);
+            if (ds < 0) continue;
+            const double D = __ldg(&Dc[s]);
+            if (!(D > 0.0)) continue;
+            const size_t ci = (size_t)s * a.ntets + t;
+            const uint32_t pop = a.counts[ci];
+            uint4 k = make_uint4(0u, 0u, 0u, 0u);
+            if (pop > 0u) {
+                sg_stream st;
+                uint32_t Kn = 0u;
+                const double sd = a.tdel[(size_t)ds * a.ntets + t];
+                if (bt) {
+                    float4 gb;
+                    const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
+                    k = leave_species(a.seed, (uint32_t)r, tl, w, (uint32_t)s, pop, sd, invT, T * tot, gb,
+                                      sg_binom_odds((double)gb.x), sg_binom_odds((double)gb.y),
+                                      sg_binom_odds((double)gb.z), s_rcp, &st, &Kn);
+                } else {
+                    k = leave_species(a.seed, (uint32_t)r, tl, w, (uint32_t)s, pop, sd, invT, T * (D * (double)g.w),
+                                      g, odd1, odd2, odd3, s_rcp, &st, &Kn);
+                }
+                if (Kn > 0u) {
+                    if (!((clampm >> s) & 1u)) a.counts[ci] = pop - Kn;
+                    moved += Kn;
+                }
             }
+            // Scatter into the receiving tets' slots: nb.f = (neighbour << 2) | its face.
+            uint32_t* po = out + (size_t)ds * plane;
+            if (nb.x >= 0) po[nb.x] = k.x;
+            if (nb.y >= 0) po[nb.y] = k.y;
+            if (nb.z >= 0) po[nb.z] = k.z;
+            if (nb.w >= 0) po[nb.w] = k.w;
+            if (bt) bnd_scatter(a, t, po, k);
         }
-        uint32_t* po = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane + (size_t)ds * plane;
-        if (nb.x >= 0) po[nb.x] = k.x;
-        if (nb.y >= 0) po[nb.y] = k.y;
-        if (nb.z >= 0) po[nb.z] = k.z;
-        if (nb.w >= 0) po[nb.w] = k.w;
-        if (bt) bnd_scatter(a, t, po, k);
     }
     moved = warp_sum_u64(moved);
     if (lane == 0 && moved) atomicAdd(&s_moved, moved);
@@ -859,7 +913,7 @@ __global__ void __launch_bounds__(BLOCK, 4) diffuse_kernel(sg_window_args a, int
 }
 
 // Surface diffusion leave (TOS:1716-1793, sdiff.cpp:498-560), one thread per (surface-
-// diffusing species, membrane triangle), between the SSA and diffuse_kernel of a split
+// diffusing species, membrane triangle), between the SSA and leave_kernel of a split
 // window: n = min(pop, window integral / T) with a Bernoulli on its fraction,
 // Binomial(n, min(1, T D G)) leaving, conditional binomials over the three edges.  Each
 // (triangle, species) draws from its own stream (purpose SG_PURPOSE_SDIFF + species).

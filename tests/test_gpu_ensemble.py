@@ -6,12 +6,16 @@ TetOpSplitP (src/steps/mpi/tetopsplit/tetopsplit.cpp) and Tetexact
 with seeds 1..200 (tests/golden/make_ref_ensembles.py).  Here the same configurations
 run as 200 batched realizations on the GPU (independent Philox keys per realization),
 and the two ensembles must agree in mean and variance within 3 sigma at every record
-and pass a two-sample KS test (p above 0.01, Bonferroni-corrected over the records).
+and pass a two-sample KS test (p above 0.01), each criterion family-wise over the
+records and columns (tests/ensemble_stats.py).
 
   * plain small configuration (10^3 Kuhn cubes, A + B <-> C, A = B = 10,000 placed by
     setCompSpecCount): compartment counts of A and C every 1 ms to 100 ms;
   * diffusion spread (10 A per tet in the first layer of cubes): counts of A per 0.1 um
-    slab along x every 2 ms to 40 ms.
+    slab along x every 2 ms to 40 ms, against TetOpSplitP.  Tetexact is not an arm here:
+    at these short times the operator split itself (every molecule of an interior tet
+    leaves in each window, t1 = 1) spreads molecules differently from the exact SSA, and
+    the reference TetOpSplitP ensemble differs from the Tetexact one by up to 16 sigma.
 """
 import os
 
@@ -85,11 +89,12 @@ def test_c0_ensemble_matches_reference_tetopsplit_and_tetexact(steps_lib):
         assert rep["ok"], (arm, rep)
 
 
-def test_diffusion_spread_matches_reference_tetopsplit_and_tetexact(steps_lib):
+def test_diffusion_spread_matches_reference_tetopsplit(steps_lib):
     fx = np.load(os.path.join(GOLD, "ref_ensemble_spread.npz"))
     times = fx["times"]
     g = gpu_spread(fx["tos"].shape[0], times)
     assert np.all(g.sum(axis=2) == 6000)
-    for arm in ("tos", "tetexact"):
-        rep = compare(g, fx[arm])
-        assert rep["ok"], (arm, rep)
+    rep = compare(g, fx["tos"])
+    assert rep["ok"], rep
+    # The split's own deviation from the exact SSA at short times is the reference's too.
+    assert not compare(fx["tos"], fx["tetexact"])["ok"]
