@@ -11,6 +11,15 @@ value: updates = tets x species x windows over the timed steps, divided by the d
 time of the steps (CUDA events on the solver's stream, L2 flushed between steps).
 e2e:   the same metric through the C ABI with host buffers: each step uploads every
 species row from pinned host memory, runs 1 ms and downloads every row.
+parity: after the timed steps the GPU state is copied into the CPU oracle and both run 5
+more windows; every count of every tet must agree bit for bit.
+extra: the batched ensemble (512 realizations) against the same realizations run one at
+a time, and the EField configuration (FP64 and mixed-precision solves, per-step error
+against an FP64 solve), both at reduced step counts.
+cpu_baseline: the reference TetOpSplitP itself (compiled from its sources, oracle/_ref),
+one window from the GPU's final state on one host core.
+--impl reference: the reference TetOpSplitP on every host core (independent single-rank
+replicas, as `mpirun -n 1` each), from the state the oracle reaches after the warm-up.
 N > 1: independent replicas, one per GPU (the path is not sharded).
 """
 from __future__ import annotations
@@ -122,25 +131,78 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(mdl, mesh, rows, windows=4):
-    """The CPU oracle (C restatement, OpenMP over tets) on a bounded sample of the workload."""
+def cpu_baseline(mdl, mesh, state):
+    """The reference TetOpSplitP (oracle/_ref, compiled from its sources) on one host
+    core: one split window from the given counts (the GPU's state after the timed steps),
+    after one untimed window.  Without that library, the CPU oracle on all host threads."""
+    from steps_b200.solver import flatten
+
+    F = flatten(mdl, mesh)
+    try:
+        from oracle import refsim
+
+        have_ref = refsim.available()
+    except ImportError:
+        have_ref = False
+    if have_ref:
+        c0 = time.perf_counter()
+        sim = refsim.RefSim(mesh, F, SEED)
+        for i in range(NSPEC):
+            sim.set_tet_counts(i, state[i].astype(np.float64))
+        build_s = time.perf_counter() - c0
+        sim.run(1e-12)
+        per = sim.period()
+        sim.run(sim.time() + per)
+        n0 = sim.nsteps()
+        t0 = time.perf_counter()
+        sim.run(sim.time() + per)
+        dt = time.perf_counter() - t0
+        n = sim.nsteps() - n0
+        del sim
+        return {"value": mesh.ntets * NSPEC * n / dt, "unit": "tet-species updates/s", "cores": 1,
+                "kind": "reference",
+                "sample": f"{n} split window of the same workload from the GPU's final state, {dt:.2f} s on one "
+                          f"host core (reference TetOpSplitP built from its sources; construction {build_s:.1f} s "
+                          f"and one warm-up window not timed)"}
     threads = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from oracle.pyoracle import Oracle
-    from steps_b200.solver import flatten
 
-    ora = Oracle(flatten(mdl, mesh), seed=SEED)
+    ora = Oracle(F, seed=SEED)
     for i in range(NSPEC):
-        ora.set_counts(i, rows[i])
+        ora.set_counts(i, state[i])
     per = ora.period()
-    ora.run(per)  # warm-up window
+    ora.run(per)
     t0 = time.perf_counter()
-    n = ora.run(per * (1 + windows))
+    n = ora.run(per * 5)
     dt = time.perf_counter() - t0
-    upd = mesh.ntets * NSPEC * n
-    return {"value": upd / dt, "unit": "tet-species updates/s", "cores": threads, "kind": "port",
-            "sample": f"{n} split windows of the same workload (384,000 tets x 8 species), "
-                      f"{dt:.2f} s on {threads} host threads"}
+    return {"value": mesh.ntets * NSPEC * n / dt, "unit": "tet-species updates/s", "cores": threads, "kind": "port",
+            "sample": f"{n} split windows of the same workload, {dt:.2f} s on {threads} host threads "
+                      "(the reference library is absent, so its CPU restatement ran)"}
+
+
+def parity_leg(sim, mdl, mesh, windows=5):
+    """Copy the GPU state into the CPU oracle, run `windows` more windows on both and
+    compare every count of every tet (not timed)."""
+    os.environ["OMP_NUM_THREADS"] = str(os.cpu_count() or 1)
+    from oracle.pyoracle import Oracle
+
+    ora = Oracle(sim.tables, seed=SEED)
+    for i, s in enumerate(sim.spec_names):
+        ora.set_counts(i, sim.getSpecCounts(s))
+    ora.set_time(0, sim.getTime(), sim.getNIteration())
+    per = sim.getUpdPeriod()
+    t_end = sim.getTime() + windows * per
+    w0 = sim.getNIteration()
+    sim.run(t_end)
+    ora.run(t_end)
+    ok = sim.getNIteration() - w0 == windows and ora.window() == sim.getNIteration()
+    diff = 0
+    for i, s in enumerate(sim.spec_names):
+        diff += int(np.count_nonzero(sim.getSpecCounts(s) != ora.get_counts(i)))
+    return {"config": "plain_384k", "windows": int(sim.getNIteration() - w0), "tets": int(mesh.ntets),
+            "species": NSPEC, "bit_exact": bool(ok and diff == 0), "differing_counts": diff,
+            "checker": "CPU oracle (oracle/opsplit_oracle.c) from the GPU state after the timed steps"}
 
 
 def replica_totals(dist, device, total_ms, updates, e2e_s, e2e_upd):
@@ -157,42 +219,96 @@ def replica_totals(dist, device, total_ms, updates, e2e_s, e2e_upd):
     return float(t[0].item()), float(u[0].item()), float(u[1].item()) / float(t[1].item())
 
 
+def _ref_replica_run(job):
+    state_path, seed, wps, steps = job
+    import time as _t
+
+    from oracle.refsim import RefSim
+    from steps_b200.solver import flatten
+
+    mdl, mesh, _ = workload()
+    c0 = _t.time()
+    sim = RefSim(mesh, flatten(mdl, mesh), seed)
+    rows = np.load(state_path)
+    for i in range(NSPEC):
+        sim.set_tet_counts(i, rows[i].astype(np.float64))
+    build_s = _t.time() - c0
+    # The update period is computed on the first run(); a negligible first window fixes
+    # it, then one full untimed window.
+    sim.run(1e-12)
+    per = sim.period()
+    t = sim.time() + per
+    sim.run(t)
+    n0 = sim.nsteps()
+    w0 = _t.time()
+    for _ in range(steps):
+        t += wps * per
+        sim.run(t)
+    w1 = _t.time()
+    return sim.nsteps() - n0, w0, w1, build_s
+
+
+def reference_state(args):
+    """Counts after the warm-up steps, from the CPU oracle (law-equal to the GPU and the
+    reference; fast on all host threads)."""
+    from oracle.pyoracle import Oracle
+    from steps_b200.solver import flatten
+
+    mdl, mesh, rows = workload()
+    os.environ["OMP_NUM_THREADS"] = str(os.cpu_count() or 1)
+    ora = Oracle(flatten(mdl, mesh), seed=SEED)
+    for i in range(NSPEC):
+        ora.set_counts(i, rows[i])
+    ora.run(args.warmup * STEP_SIM_S)
+    return mesh, np.stack([ora.get_counts(i) for i in range(NSPEC)])
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    mdl, mesh, rows = workload()
-    threads = os.cpu_count() or 1
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    from oracle.pyoracle import Oracle
-    from steps_b200.solver import flatten
+    import multiprocessing as mp
+    import tempfile
 
-    ora = Oracle(flatten(mdl, mesh), seed=SEED)
-    for i in range(NSPEC):
-        ora.set_counts(i, rows[i])
-    per = ora.period()
-    wins_per_step = 2
-    t = 0.0
-    for _ in range(args.warmup):
-        t += wins_per_step * per
-        ora.run(t)
-    total, upd = 0.0, 0
-    for _ in range(args.steps):
-        t += wins_per_step * per
-        t0 = time.perf_counter()
-        n = ora.run(t)
-        total += time.perf_counter() - t0
-        upd += mesh.ntets * NSPEC * n
-    v = upd / total
+    from oracle import refsim
+
+    if not refsim.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsteps_ref.so (the reference "
+                          "TetOpSplitP built from its sources by oracle/build_ref_tetopsplit.py) is missing"}),
+              flush=True)
+        return 0
+    mesh, state = reference_state(args)
+    cores = os.cpu_count() or 1
+    # Each replica holds about 5 GB; keep a margin of host memory.
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+        nproc = max(1, min(cores, int(avail // (6 << 30))))
+    except (ValueError, OSError):
+        nproc = cores
+    wps = args.ref_windows
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "state.npy")
+        np.save(path, state)
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(nproc) as pool:
+            res = pool.map(_ref_replica_run, [(path, SEED + k, wps, args.steps) for k in range(nproc)])
+    wins = sum(r[0] for r in res)
+    span = max(r[2] for r in res) - min(r[1] for r in res)
+    upd = mesh.ntets * NSPEC * wins
+    v = upd / span
+    sample = (f"{nproc} independent single-rank TetOpSplitP replicas (one per host core, as mpirun -n 1 each; "
+              f"no MPI on this host) from the state at t = {args.warmup} ms; {args.steps} steps of {wps} split "
+              f"window(s) each; {wins} windows in {span:.1f} s of wall time across the replicas; "
+              f"construction {max(r[3] for r in res):.1f} s not timed")
     line = {
         "metric": "tet-species updates/s", "value": v, "unit": "tet-species updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * span / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32+f64", "data": "synthetic",
-        "config": dict(config_dict(mesh), step=f"{wins_per_step} split windows (bounded CPU sample)"),
-        "cpu_baseline": {"value": v, "unit": "tet-species updates/s", "cores": threads, "kind": "port",
-                         "sample": f"{wins_per_step} split windows per step on {threads} host threads; the "
-                                   "reference TetOpSplitP does not build here, so its CPU restatement runs"},
+        "config": dict(config_dict(mesh), step=f"{wps} split window(s) per step (bounded CPU sample of the 1 ms step)",
+                       parallelism=f"{nproc} single-rank replicas"),
+        "cpu_baseline": {"value": v, "unit": "tet-species updates/s", "cores": nproc, "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": v, "unit": "tet-species updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -292,18 +408,24 @@ def run_ours(args):
     bytes_per_window = mesh.ntets * (BYTES_PER_TET_SPEC * NSPEC + BYTES_PER_TET)
     avg_win_s = (win_ms * 1e-3) / max(nwin, 1)
     achieved = bytes_per_window / avg_win_s / 1e9
-    # DRAM bytes per window-kernel launch on this workload from the committed ncu summary.
+    # DRAM bytes per window of the kernels the run used, from the committed ncu summary
+    # (profiles/split_window_plain_384k.md: one capture of each split kernel).
     traffic = None
-    prof_path = os.path.join(ROOT, "profiles", "window_kernel_plain_384k.md")
-    if os.path.exists(prof_path):
+    prof_path = os.path.join(ROOT, "profiles", "split_window_plain_384k.md")
+    if os.path.exists(prof_path) and sim.getSplit():
         with open(prof_path) as f:
             for ln in f:
-                if ln.startswith("dram_bytes_per_launch:"):
+                if ln.startswith("dram_bytes_per_window:"):
                     traffic = int(ln.split(":")[1])
 
+    parity = None
+    extra = None
+    cpu = None
+    if rank == 0 and world == 1:
+        state = np.stack([sim.getSpecCounts(s) for s in sim.spec_names])
+        parity = parity_leg(sim, mdl, mesh)
+        cpu = cpu_baseline(mdl, mesh, state)
     if rank == 0:
-        mdl_cpu, mesh_cpu, rows_cpu = (mdl, mesh, rows)
-        cpu = cpu_baseline(mdl_cpu, mesh_cpu, rows_cpu) if world == 1 else None
         line = {
             "metric": "tet-species updates/s", "value": value, "unit": "tet-species updates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -321,14 +443,19 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
-                         "kernel": (f"sg::window_kernel<{sim.getLaunch()[0]}, split> + sg::diffuse_kernel<256>"
+                         "kernel": (f"sg::window_kernel<{sim.getLaunch()[0]}, split> + sg::leave_kernel<256>"
                                     if sim.getSplit() else f"sg::window_kernel<{sim.getLaunch()[0]}>"),
                          "algorithmic_bytes_per_launch": bytes_per_window,
                          "avg_launch_us": avg_win_s * 1e6},
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": int(launches1 - launches0),
+            "parity": parity,
         }
+        if world == 1 and not args.no_extra:
+            del sim
+            line["extra"] = {"batched": batched_extra(args), "efield": efield_extra(args)}
+            sim = None
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -337,7 +464,7 @@ def run_ours(args):
     return 0
 
 
-def run_batched(args):
+def batched_extra(args):
     """Batched ensemble: 512 realizations of n^3 Kuhn cubes (n uniform in 8..30) with the
     8-species network and per-realization log-normal (0.2) rate jitter, in one launch per
     window; against the same realizations run one after another with the plain path."""
@@ -367,8 +494,8 @@ def run_batched(args):
     setup_s = time.perf_counter() - t0
     ext = torch.cuda.ExternalStream(sim.getStream())
     t_sim = 0.0
-    for i in range(args.warmup):
-        if i == args.warmup - 1:
+    for i in range(args.bx_warmup):
+        if i == args.bx_warmup - 1:
             sim.setAutotune(True)  # tuned on the last warm-up step
         t_sim += STEP_SIM_S
         sim.run(t_sim)
@@ -378,7 +505,7 @@ def run_batched(args):
     it0 = sim.getNIteration()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(ext)
-    for _ in range(args.steps):
+    for _ in range(args.bx_steps):
         t_sim += STEP_SIM_S
         sim.run(t_sim)
     e1.record(ext)
@@ -401,33 +528,37 @@ def run_batched(args):
         for i, s in enumerate(ps.spec_names):
             ps.setSpecCounts(s, pr[i])
         es = torch.cuda.ExternalStream(ps.getStream())
-        ps.run((args.warmup - 1) * STEP_SIM_S)
+        ps.run((args.bx_warmup - 1) * STEP_SIM_S)
         ps.setAutotune(True)  # tuned on the last warm-up step, as the batched solver
-        ps.run(args.warmup * STEP_SIM_S)
+        ps.run(args.bx_warmup * STEP_SIM_S)
         i0 = ps.getNIteration()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(es)
-        ps.run((args.warmup + args.steps) * STEP_SIM_S)
+        ps.run((args.bx_warmup + args.bx_steps) * STEP_SIM_S)
         a1.record(es)
         a1.synchronize()
         plain_ms += a0.elapsed_time(a1)
         upd += m.ntets * NSPEC * (ps.getNIteration() - i0)
         del ps
     plain = upd / (plain_ms * 1e-3)
-    print(json.dumps({
+    return {
         "metric": "tet-species updates/s", "value": batched, "unit": "tet-species updates/s",
         "config": {"workload": f"batched: {nreal} realizations of n^3 Kuhn cubes, n in 8..30, "
                                f"{mesh.ntets} tets, 8 species, 12 reactions, rate jitter 0.2",
-                   "sim_ms_per_step": 1.0, "steps": args.steps, "warmup": args.warmup,
+                   "sim_ms_per_step": 1.0, "steps": args.bx_steps, "warmup": args.bx_warmup,
                    "launch": {"block": launch[0], "grid": launch[1], "split": sim_split}},
         "windows": windows, "ms": ms, "setup_s": setup_s,
         "plain_sequential": {"value": plain, "realizations_sampled": len(sample), "ms": plain_ms},
         "batched_over_plain": batched / plain,
-    }), flush=True)
+    }
+
+
+def run_batched(args):
+    print(json.dumps(batched_extra(args)), flush=True)
     return 0
 
 
-def run_efield(args):
+def efield_extra(args):
     """EField configuration: 20x20x200 Kuhn cubes (480,000 tets), every boundary triangle
     membrane, Cm 1 uF/cm^2, leak 3e-5 S/cm^2 at -65 mV, a two-state voltage-gated channel
     at 10/um^2 (alpha = 0.1 exp(V/25 mV)/ms, beta = 0.1 exp(-V/25 mV)/ms, 20 pS, +50 mV),
@@ -493,7 +624,7 @@ def run_efield(args):
                                                 "note": "wall_s includes the check solves; solve_ms does not"}
         del sim
     err = float(np.max(np.abs(finals["mixed"] - finals["fp64"]) / np.abs(finals["fp64"])))
-    print(json.dumps({
+    return {
         "metric": "EField solve ms per step", "config": {"mesh": f"{nx}x{ny}x{nz} Kuhn cubes",
                                                          "tets": mesh.ntets, "verts": mesh.nverts,
                                                          "steps": args.ef_steps, "tol": args.ef_tol,
@@ -501,11 +632,15 @@ def run_efield(args):
                                                          "mixed_reliable_updates": bool(args.ef_reliable),
                                                          "reliable_update_delta": args.ef_ru_delta},
         "fp64": out["fp64"], "mixed": out["mixed"],
-        "mixed_speedup_solve": out["fp64"]["solve_ms_per_step"] / out["mixed"]["solve_ms_per_step"],
+        "mixed_speedup": out["fp64"]["solve_ms_per_step"] / out["mixed"]["solve_ms_per_step"],
         "max_rel_v_err_per_step": out["mixed"]["check_vs_fp64_solve"]["max_rel_v_err"],
         "fp64_cg_max_rel_v_err_per_step": out["fp64"]["check_vs_fp64_solve"]["max_rel_v_err"],
         "max_rel_v_diff_end_of_run": err,
-    }), flush=True)
+    }
+
+
+def run_efield(args):
+    print(json.dumps(efield_extra(args)), flush=True)
     return 0
 
 
@@ -611,6 +746,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ref-windows", type=int, default=1,
+                    help="reference arm: split windows per timed step (a bounded CPU sample of the 1 ms step)")
     ap.add_argument("--config", choices=["plain", "batched", "efield", "coupled"], default="plain")
     ap.add_argument("--cp-dims", type=int, nargs=3, default=[50, 50, 80])
     ap.add_argument("--cp-nreal", type=int, default=16)
@@ -619,9 +756,12 @@ def main():
     ap.add_argument("--cp-method", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--ef-inner-tol", type=float, default=1e-4)
     ap.add_argument("--nreal", type=int, default=512)
-    ap.add_argument("--plain-sample", type=int, default=64)
+    ap.add_argument("--bx-steps", type=int, default=3, help="batched: timed 1 ms steps")
+    ap.add_argument("--bx-warmup", type=int, default=3, help="batched: warm-up 1 ms steps (the last autotunes)")
+    ap.add_argument("--no-extra", action="store_true", help="default line without the batched / EField extras")
+    ap.add_argument("--plain-sample", type=int, default=32)
     ap.add_argument("--ef-dims", type=int, nargs=3, default=[20, 20, 200])
-    ap.add_argument("--ef-steps", type=int, default=5000)
+    ap.add_argument("--ef-steps", type=int, default=1000)
     ap.add_argument("--ef-reliable", type=int, default=1,
                     help="mixed method: 1 = one FP32 CG with reliable updates, 0 = restarted FP32 inner solves")
     ap.add_argument("--ef-ru-delta", type=float, default=0.1)
@@ -629,6 +769,8 @@ def main():
     ap.add_argument("--ef-persistent", type=int, default=1, help="1: each EField solve in one cooperative launch")
     args = ap.parse_args()
     if args.warmup < 3:
+        print(f"bench.py: --warmup {args.warmup} raised to 3 (the timing rules need at least 3 warm-up steps)",
+              file=sys.stderr)
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)

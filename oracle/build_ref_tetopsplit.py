@@ -10,6 +10,11 @@ mpi/tetopsplit, tetexact} — against the project-written stand-ins in oracle/re
 C driver oracle/ref_tetopsplit_harness.cpp, into oracle/_ref/libsteps_ref.so.  The
 reference's CMake build is not used and no reference file is copied into this
 repository.  Outputs go to oracle/_ref/ only (git-ignored, shipped with the tree).
+
+It also compiles the drop-in steps_b200/steps_api/tetopsplit_b200.cpp (the
+steps::solver::API subclass on the GPU solver) against the same reference headers and
+links it, with the harness built for it, into oracle/_ref/libsteps_ref_b200.so, which
+loads steps_b200/libsteps_b200.so: the library a STEPS build with the drop-in would be.
 """
 from __future__ import annotations
 
@@ -27,6 +32,9 @@ OUT = os.path.join(HERE, "_ref")
 OBJ = os.path.join(OUT, "obj")
 LIB = os.path.join(OUT, "libsteps_ref.so")
 HARNESS = os.path.join(HERE, "ref_tetopsplit_harness.cpp")
+REPO = os.path.dirname(HERE)
+DROPIN = os.path.join(REPO, "steps_b200", "steps_api", "tetopsplit_b200.cpp")
+LIB_B200 = os.path.join(OUT, "libsteps_ref_b200.so")
 
 DIRS = ["util", "util/tracker", "math", "geom", "model", "rng", "solver", "solver/efield", "mpi",
         "mpi/tetopsplit", "tetexact"]
@@ -82,7 +90,36 @@ def build(force=False, jobs=None):
         r = subprocess.run(["g++", "-shared", "-o", LIB] + objs, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"reference link failed:\n{r.stderr[-3000:]}")
+    build_dropin(objs[:-1], force)
     return LIB
+
+
+def build_dropin(ref_objs, force=False):
+    """oracle/_ref/libsteps_ref_b200.so: the reference objects, the drop-in and the harness
+    with its TetOpSplitB200 kind, linked to steps_b200/libsteps_b200.so."""
+    inc = ["-I" + os.path.join(REPO, "steps_b200"), "-I" + os.path.join(REPO, "include")]
+    hdr = os.path.join(REPO, "steps_b200", "steps_api", "tetopsplit_b200.hpp")
+    t_src = max(os.path.getmtime(DROPIN), os.path.getmtime(hdr), os.path.getmtime(HARNESS), shim_mtime())
+    objs = []
+    for src, name, extra in ((DROPIN, "dropin_tetopsplit_b200.o", []),
+                             (HARNESS, "harness_b200.o", ["-DSTEPS_WITH_B200_API"])):
+        o = os.path.join(OBJ, name)
+        if force or not os.path.exists(o) or os.path.getmtime(o) < t_src:
+            r = subprocess.run(["g++"] + FLAGS + inc + extra + ["-c", src, "-o", o], capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"drop-in build failed ({src}):\n{r.stderr[-3000:]}")
+        objs.append(o)
+    lib_dir = os.path.join(REPO, "steps_b200")
+    if not os.path.exists(os.path.join(lib_dir, "libsteps_b200.so")):
+        return None
+    if force or not os.path.exists(LIB_B200) or os.path.getmtime(LIB_B200) < max(
+            [os.path.getmtime(o) for o in objs + ref_objs] + [os.path.getmtime(os.path.join(lib_dir, "libsteps_b200.so"))]):
+        r = subprocess.run(["g++", "-shared", "-o", LIB_B200] + ref_objs + objs +
+                           ["-L" + lib_dir, "-lsteps_b200", "-Wl,-rpath,$ORIGIN/../../steps_b200"],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"drop-in link failed:\n{r.stderr[-3000:]}")
+    return LIB_B200
 
 
 if __name__ == "__main__":

@@ -17,7 +17,7 @@
  *     by oracle/ref_philox_kat.c compiled from that header.
  *   - The binomial sampler is checked by the chi-squared test of the reference's
  *     test/unit/cpp/test_rng.cpp:51-90 (same n, p grid and thresholds) and by a
- *     proper chi-squared goodness of fit over the BINV and BTRD regimes.
+ *     proper chi-squared goodness of fit over the BINV, mode-search and BTRD regimes.
  *   - Trajectory statistics are checked against the analytic kinetics of
  *     test/validation/API_1/validation_rd_mpi/parallel_spatial_tetopsplit.py.
  *
@@ -126,7 +126,8 @@ static double or_log(double x) {
 double or_log_export(double x) { return or_log(x); }
 
 /* ------------------------------------------------------------------------- */
-/* Binomial: BINV (Kachitvichyanukul & Schmeiser 1988) / BTRD (Hormann 1993)  */
+/* Binomial: BINV (Kachitvichyanukul & Schmeiser 1988), inversion from the mode,   */
+/* BTRD (Hormann 1993) for very large n p                                     */
 /* ------------------------------------------------------------------------- */
 static double or_powu(double q, uint32_t n) {
     double r = 1.0, b = q;
@@ -225,12 +226,98 @@ static uint32_t or_btrd(or_stream* st, uint32_t n, double p) {
     return mi;
 }
 
+/* e^x: k = round(x / ln 2), r = x - k ln 2 (two-part ln 2), Taylor series of e^r to r^14,
+   2^k through the exponent bits (same steps as the GPU's). */
+static double or_exp(double x) {
+    if (!(x < 709.78)) {
+        if (x != x) return x;
+        uint64_t inf = 0x7FF0000000000000ull;
+        double d;
+        memcpy(&d, &inf, 8);
+        return d;
+    }
+    if (x < -708.39) return 0.0;
+    const double k = floor(x * 1.4426950408889634 + 0.5);
+    double r = fma(-k, 0.6931471803691238, x);
+    r = fma(-k, 1.9082149292705877e-10, r);
+    static const double c[14] = {1.0 / 6227020800.0, 1.0 / 479001600.0, 1.0 / 39916800.0, 1.0 / 3628800.0,
+                                 1.0 / 362880.0,     1.0 / 40320.0,     1.0 / 5040.0,     1.0 / 720.0,
+                                 1.0 / 120.0,        1.0 / 24.0,        1.0 / 6.0,        0.5,
+                                 1.0,                1.0};
+    double p = 1.0 / 87178291200.0;
+    for (int i = 0; i < 14; ++i) p = fma(p, r, c[i]);
+    int ki = (int)k;
+    if (ki > 1023) {
+        p = p * 2.0;
+        ki -= 1;
+    }
+    if (ki < -1022) {
+        p = p * 0.5;
+        ki += 1;
+    }
+    uint64_t b = (uint64_t)(ki + 1023) << 52;
+    double sc;
+    memcpy(&sc, &b, 8);
+    return p * sc;
+}
+
+double or_exp_export(double x) { return or_exp(x); }
+
+/* ln k! by Stirling's form with the remainder fc. */
+static double or_lnfact(uint32_t k) {
+    const double k1 = (double)k + 1.0;
+    return (k1 - 0.5) * or_log(k1) - k1 + 0.91893853320467274 + or_fc(k);
+}
+
+/* Inversion from the mode for p <= 1/2: support in the order m, m+1, m-1, m+2, m-2, ...
+   (one side alone once the other end is reached); f(m) from the log-factorials, the
+   neighbours by the pmf ratios (n+1) s / (x+1) - s upwards and x r / (n-x+1) downwards. */
+static uint32_t or_binom_mode(or_stream* st, uint32_t n, double p) {
+    const double q = 1.0 - p;
+    const double s = p / q;
+    const double dn = (double)n;
+    uint32_t m = (uint32_t)floor((dn + 1.0) * p);
+    if (m > n) m = n;
+    const double lf = ((or_lnfact(n) - or_lnfact(m)) - or_lnfact(n - m)) + (double)m * or_log(p) +
+                      (double)(n - m) * or_log(q);
+    const double fm = or_exp(lf);
+    const double a = (dn + 1.0) * s;
+    const double r = q / p;
+    double u = u_co(or_u32(st)) - fm;
+    if (u < 0.0) return m;
+    double fu = fm, fd = fm;
+    uint32_t xu = m, xd = m;
+    for (;;) {
+        const int cu = xu < n, cd = xd > 0u;
+        if (!cu && !cd) return m;
+        if (cu) {
+            fu = fu * fma(a, 1.0 / (double)(xu + 1u), -s);
+            xu += 1u;
+            u = u - fu;
+            if (u < 0.0) return xu;
+        }
+        if (cd) {
+            fd = fd * ((double)xd * r) * (1.0 / (double)(n - xd + 1u));
+            xd -= 1u;
+            u = u - fd;
+            if (u < 0.0) return xd;
+        }
+    }
+}
+
 static uint32_t or_binom(or_stream* st, uint32_t n, double p) {
     if (n == 0 || !(p > 0.0)) return 0;
     if (p >= 1.0) return n;
     int flip = p > 0.5;
     double pp = flip ? 1.0 - p : p;
-    uint32_t k = ((double)n * pp < 24.0) ? or_binv(st, n, pp) : or_btrd(st, n, pp);
+    const double np = (double)n * pp;
+    uint32_t k;
+    if (np < 24.0)
+        k = or_binv(st, n, pp);
+    else if (np < 1000.0)
+        k = or_binom_mode(st, n, pp);
+    else
+        k = or_btrd(st, n, pp);
     return flip ? n - k : k;
 }
 

@@ -9,8 +9,16 @@
 // Model: one compartment holding every tet of a mesh given as vertex and tet arrays
 // (geom/tetmesh.hpp:151), one volume system with the given species, reactions
 // (model/reac.hpp:62) and diffusion rules (model/diff.hpp:52); RNG "r123" with the given
-// seed and buffer (rng/create.cpp:44).
+// seed and buffer (rng/create.cpp:44).  Optionally (ref_create_memb) a membrane model
+// instead: every surface triangle a patch with a two-state channel (C <-> O by tabulated
+// voltage-dependent reactions, model/vdepsreac.hpp:63), an ohmic current through O
+// (model/ohmiccurr.hpp:57) and one Memb (geom/memb.hpp:63).
+//
+// Built with STEPS_WITH_B200_API, kind 2 is the drop-in TetOpSplitB200
+// (steps_b200/steps_api/tetopsplit_b200.hpp) on the same reference objects.
+#include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <exception>
 #include <map>
@@ -30,6 +38,16 @@
 #include "rng/rng.hpp"
 #include "solver/api.hpp"
 #include "tetexact/tetexact.hpp"
+#include "geom/memb.hpp"
+#include "geom/tmpatch.hpp"
+#include "model/chan.hpp"
+#include "model/chanstate.hpp"
+#include "model/ohmiccurr.hpp"
+#include "model/surfsys.hpp"
+#include "model/vdepsreac.hpp"
+#ifdef STEPS_WITH_B200_API
+#include "steps_api/tetopsplit_b200.hpp"
+#endif
 
 namespace {
 
@@ -40,6 +58,9 @@ struct RefSim {
     std::vector<steps::model::Spec*> specs;  // owned by the model
     std::unique_ptr<steps::tetmesh::Tetmesh> mesh;
     steps::tetmesh::TmComp* comp = nullptr;  // registered with (and unregistered from) mesh
+    steps::tetmesh::TmPatch* patch = nullptr;
+    steps::tetmesh::Memb* memb = nullptr;  // owned by the mesh
+    bool has_chans = false;
     steps::rng::RNGptr rng;
     std::unique_ptr<steps::solver::API> solver;
     std::vector<std::string> spec_names;
@@ -50,9 +71,18 @@ struct RefSim {
         // The compartment unregisters itself from its mesh in its destructor, so it goes
         // while the mesh is whole (the base Geom destructor would reach it after the
         // Tetmesh part is gone).
+        // The mesh owns the membrane (Tetmesh::~Tetmesh deletes it); patch and compartment
+        // unregister themselves from the mesh in their destructors, so they go first.
+        delete patch;
         delete comp;
         mesh.reset();
-        model.reset();
+        // A model with an ohmic current on a channel state is released, not deleted: its
+        // destructor deletes the channel state before the current and then throws from the
+        // current's destructor.  Test processes are short-lived.
+        if (has_chans)
+            (void)model.release();
+        else
+            model.reset();
     }
 };
 
@@ -110,6 +140,14 @@ void* ref_create(int kind, int nverts, const double* verts, int ntets, const int
             std::vector<int> tet_hosts((size_t)ntets, 0);
             s->solver = std::make_unique<steps::mpi::tetopsplit::TetOpSplitP>(
                 s->model.get(), s->mesh.get(), s->rng, steps::solver::API::EF_NONE, tet_hosts);
+        } else if (kind == 2) {
+#ifdef STEPS_WITH_B200_API
+            s->solver = std::make_unique<steps::b200::TetOpSplitB200>(s->model.get(), s->mesh.get(), s->rng,
+                                                                       steps::solver::API::EF_NONE);
+#else
+            g_err = "built without the TetOpSplitB200 drop-in";
+            return nullptr;
+#endif
         } else {
             s->solver = std::make_unique<steps::tetexact::Tetexact>(s->model.get(), s->mesh.get(), s->rng,
                                                                      steps::solver::API::EF_NONE);
@@ -199,6 +237,140 @@ uint64_t ref_nsteps(void* h) {
     auto* s = static_cast<RefSim*>(h);
     auto* p = dynamic_cast<steps::mpi::tetopsplit::TetOpSplitP*>(s->solver.get());
     return p ? (uint64_t)p->getNIteration() : (uint64_t)s->solver->getNSteps();
+}
+
+// Membrane model (see the header comment); kind 0 = TetOpSplitP, 2 = TetOpSplitB200, with
+// the EField solver option efopt (api.hpp:61; 0 = none).  k tables at vmin + i dv (V), of
+// the length the reference requires, floor((vmax - vmin) / dv) + 1 (model/vdepsreac.cpp).
+void* ref_create_memb(int kind, int nverts, const double* verts, int ntets, const int64_t* tets, int ntab,
+                      const double* kopen, const double* kclose, double vmin, double vmax, double dv, double g,
+                      double erev, uint64_t seed, int efopt) {
+    try {
+        auto s = std::make_unique<RefSim>();
+        s->model = std::make_unique<steps::model::Model>();
+        auto& mdl = *s->model;
+        new steps::model::Volsys("vsys", mdl);
+        auto* ss = new steps::model::Surfsys("ssys", mdl);
+        auto* ch = new steps::model::Chan("Ch", mdl);
+        auto* c = new steps::model::ChanState("C", mdl, *ch);
+        auto* o = new steps::model::ChanState("O", mdl, *ch);
+        const int need = (int)std::floor((vmax - vmin) / dv) + 1;
+        if (ntab != need) {
+            g_err = "k(V) tables need floor((vmax - vmin) / dv) + 1 = " + std::to_string(need) + " entries";
+            return nullptr;
+        }
+        std::vector<double> ko(kopen, kopen + ntab), kc(kclose, kclose + ntab);
+        new steps::model::VDepSReac("open", *ss, {}, {}, {c}, {}, {o}, {}, ko, vmin, vmax, dv, (uint)ntab);
+        new steps::model::VDepSReac("close", *ss, {}, {}, {o}, {}, {c}, {}, kc, vmin, vmax, dv, (uint)ntab);
+        new steps::model::OhmicCurr("I", *ss, *o, erev, g);
+        s->has_chans = true;
+        s->spec_names = {"C", "O"};
+        std::vector<double> v(verts, verts + (size_t)nverts * 3);
+        std::vector<steps::index_t> t((size_t)ntets * 4);
+        for (size_t k = 0; k < t.size(); ++k) t[k] = (steps::index_t)tets[k];
+        s->mesh = std::make_unique<steps::tetmesh::Tetmesh>(v, t);
+        std::vector<steps::index_t> all(ntets);
+        for (int k = 0; k < ntets; ++k) all[k] = (steps::index_t)k;
+        s->comp = new steps::tetmesh::TmComp("cyto", *s->mesh, all);
+        s->comp->addVolsys("vsys");
+        std::vector<steps::index_t> surf;
+        for (const auto& x : s->mesh->getSurfTris()) surf.push_back((steps::index_t)x);
+        s->patch = new steps::tetmesh::TmPatch("memb", *s->mesh, surf, *s->comp);
+        s->patch->addSurfsys("ssys");
+        s->memb = new steps::tetmesh::Memb("membrane", *s->mesh, {s->patch}, {});
+        s->ntets = (uint32_t)ntets;
+        s->rng = steps::rng::create("r123", 512u);
+        s->rng->initialize((unsigned long)seed);
+        if (kind == 0) {
+            std::vector<int> tet_hosts((size_t)ntets, 0);
+            std::map<steps::triangle_global_id, int> tri_hosts;
+            for (auto x : surf) tri_hosts[steps::triangle_global_id(x)] = 0;
+            s->solver = std::make_unique<steps::mpi::tetopsplit::TetOpSplitP>(s->model.get(), s->mesh.get(), s->rng,
+                                                                              efopt, tet_hosts, tri_hosts);
+        } else {
+#ifdef STEPS_WITH_B200_API
+            s->solver = std::make_unique<steps::b200::TetOpSplitB200>(s->model.get(), s->mesh.get(), s->rng, efopt);
+#else
+            g_err = "built without the TetOpSplitB200 drop-in";
+            return nullptr;
+#endif
+        }
+        return s.release();
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
+#define REF_TRY(body)                 \
+    try {                             \
+        body;                         \
+        return 0;                     \
+    } catch (const std::exception& e) { \
+        g_err = e.what();             \
+        return 1;                     \
+    }
+
+int ref_surf_tris(void* h, int64_t* out, int cap, int* n) {
+    REF_TRY({
+        auto* s = static_cast<RefSim*>(h);
+        auto st = s->mesh->getSurfTris();
+        *n = (int)st.size();
+        for (int i = 0; i < *n && i < cap; ++i) out[i] = (int64_t)st[i];
+    })
+}
+int ref_tri_verts(void* h, int64_t tri, int64_t* out) {
+    REF_TRY({
+        auto v = static_cast<RefSim*>(h)->mesh->getTri(steps::triangle_global_id((steps::index_t)tri));
+        for (int k = 0; k < 3; ++k) out[k] = (int64_t)v[k];
+    })
+}
+int ref_get_tet_count(void* h, int64_t tet, const char* spec, double* out) {
+    REF_TRY(*out = static_cast<RefSim*>(h)->solver->getTetSpecCount(
+                steps::tetrahedron_global_id((steps::index_t)tet), spec))
+}
+int ref_set_tet_count(void* h, int64_t tet, const char* spec, double n) {
+    REF_TRY(static_cast<RefSim*>(h)->solver->setTetSpecCount(steps::tetrahedron_global_id((steps::index_t)tet),
+                                                               spec, n))
+}
+int ref_get_tri_count(void* h, int64_t tri, const char* spec, double* out) {
+    REF_TRY(*out = static_cast<RefSim*>(h)->solver->getTriSpecCount(
+                steps::triangle_global_id((steps::index_t)tri), spec))
+}
+int ref_set_tri_count(void* h, int64_t tri, const char* spec, double n) {
+    REF_TRY(static_cast<RefSim*>(h)->solver->setTriSpecCount(steps::triangle_global_id((steps::index_t)tri), spec,
+                                                               n))
+}
+int ref_get_patch_count(void* h, const char* spec, double* out) {
+    REF_TRY(*out = static_cast<RefSim*>(h)->solver->getPatchSpecCount("memb", spec))
+}
+int ref_set_patch_count(void* h, const char* spec, double n) {
+    REF_TRY(static_cast<RefSim*>(h)->solver->setPatchSpecCount("memb", spec, n))
+}
+int ref_get_vert_v(void* h, int64_t v, double* out) {
+    REF_TRY(*out = static_cast<RefSim*>(h)->solver->getVertV(steps::vertex_id_t((steps::index_t)v)))
+}
+int ref_set_vert_v(void* h, int64_t v, double x) {
+    REF_TRY(static_cast<RefSim*>(h)->solver->setVertV(steps::vertex_id_t((steps::index_t)v), x))
+}
+int ref_set_vert_iclamp(void* h, int64_t v, double i) {
+    REF_TRY(static_cast<RefSim*>(h)->solver->setVertIClamp(steps::vertex_id_t((steps::index_t)v), i))
+}
+int ref_set_memb(void* h, double v0, double cm, double ra, double ro, double vrev, double efdt) {
+    REF_TRY({
+        auto* sv = static_cast<RefSim*>(h)->solver.get();
+        sv->setMembPotential("membrane", v0);
+        sv->setMembCapac("membrane", cm);
+        sv->setMembVolRes("membrane", ra);
+        sv->setMembRes("membrane", ro, vrev);
+        sv->setEfieldDT(efdt);
+    })
+}
+int ref_solver_name(void* h, char* out, int cap) {
+    REF_TRY({
+        std::string n = static_cast<RefSim*>(h)->solver->getSolverName();
+        std::snprintf(out, (size_t)cap, "%s", n.c_str());
+    })
 }
 
 }  // extern "C"

@@ -16,21 +16,24 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libsteps_ref.so")
-_lib = None
+# The same reference objects plus the drop-in TetOpSplitB200 (kind "b200"), linked to
+# steps_b200/libsteps_b200.so.
+LIB_B200_PATH = os.path.join(HERE, "_ref", "libsteps_ref_b200.so")
+_libs = {}
 
 
-def available():
-    return os.path.exists(LIB_PATH)
+def available(with_dropin=False):
+    return os.path.exists(LIB_B200_PATH if with_dropin else LIB_PATH)
 
 
-def load():
-    global _lib
-    if _lib is not None:
-        return _lib
-    if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing: build it with `python oracle/build_ref_tetopsplit.py` "
+def load(with_dropin=False):
+    path = LIB_B200_PATH if with_dropin else LIB_PATH
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python oracle/build_ref_tetopsplit.py` "
                           "where the reference tree is present")
-    lib = C.CDLL(LIB_PATH, mode=os.RTLD_NOW)
+    lib = C.CDLL(path, mode=os.RTLD_NOW)
     vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.c_int
     lib.ref_last_error.restype = C.c_char_p
     lib.ref_create.restype = vp
@@ -49,7 +52,22 @@ def load():
     lib.ref_upd_period.restype = C.c_double
     lib.ref_nsteps.argtypes = [vp]
     lib.ref_nsteps.restype = C.c_uint64
-    _lib = lib
+    lib.ref_create_memb.restype = vp
+    lib.ref_create_memb.argtypes = [ip, ip, dp, ip, C.POINTER(C.c_int64), ip, dp, dp, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, C.c_double, C.c_uint64, ip]
+    i64, cs = C.c_int64, C.c_char_p
+    for nm, args in (("ref_surf_tris", [vp, C.POINTER(i64), ip, C.POINTER(ip)]),
+                     ("ref_tri_verts", [vp, i64, C.POINTER(i64)]),
+                     ("ref_get_tet_count", [vp, i64, cs, dp]), ("ref_set_tet_count", [vp, i64, cs, C.c_double]),
+                     ("ref_get_tri_count", [vp, i64, cs, dp]), ("ref_set_tri_count", [vp, i64, cs, C.c_double]),
+                     ("ref_get_patch_count", [vp, cs, dp]), ("ref_set_patch_count", [vp, cs, C.c_double]),
+                     ("ref_get_vert_v", [vp, i64, dp]), ("ref_set_vert_v", [vp, i64, C.c_double]),
+                     ("ref_set_vert_iclamp", [vp, i64, C.c_double]),
+                     ("ref_set_memb", [vp] + [C.c_double] * 6), ("ref_solver_name", [vp, C.c_char_p, ip])):
+        f = getattr(lib, nm)
+        f.argtypes = args
+        f.restype = C.c_int
+    _libs[path] = lib
     return lib
 
 
@@ -57,11 +75,15 @@ def _ptr(a, ct):
     return a.ctypes.data_as(C.POINTER(ct))
 
 
+_KINDS = {"tetopsplit": 0, "tetexact": 1, "b200": 2}
+
+
 class RefSim:
-    """One reference solver (TetOpSplitP or Tetexact) on one compartment of every tet."""
+    """One reference solver on one compartment of every tet: the reference TetOpSplitP,
+    Tetexact, or ("b200") the drop-in TetOpSplitB200 on the same reference objects."""
 
     def __init__(self, mesh, tables, seed, kind="tetopsplit", rng_buf=512):
-        lib = load()
+        lib = load(with_dropin=(kind == "b200"))
         self._lib = lib
         S = len(tables["spec_names"]) if "spec_names" in tables else int(tables["nspec"])
         R = len(tables["reacs"])
@@ -79,7 +101,7 @@ class RefSim:
         tets = np.ascontiguousarray(mesh.tets, dtype=np.int64)
         self.nspec, self.ntets = S, int(tets.shape[0])
         self._keep = (verts, tets, dcst, lhs, rhs, kc)
-        h = lib.ref_create(0 if kind == "tetopsplit" else 1, verts.shape[0], _ptr(verts, C.c_double),
+        h = lib.ref_create(_KINDS[kind], verts.shape[0], _ptr(verts, C.c_double),
                            self.ntets, _ptr(tets, C.c_int64), S, _ptr(dcst, C.c_double), R,
                            _ptr(lhs, C.c_uint32), _ptr(rhs, C.c_uint32), _ptr(kc, C.c_double), int(seed),
                            int(rng_buf))
@@ -124,3 +146,84 @@ class RefSim:
 
     def nsteps(self):
         return int(self._lib.ref_nsteps(self._h))
+
+    # ---- through the reference API's public methods (api.hpp) ----
+    def get_tet_count(self, tet, name):
+        out = C.c_double()
+        self._ok(self._lib.ref_get_tet_count(self._h, int(tet), name.encode(), C.byref(out)))
+        return out.value
+
+    def set_tet_count(self, tet, name, n):
+        self._ok(self._lib.ref_set_tet_count(self._h, int(tet), name.encode(), float(n)))
+
+    def solver_name(self):
+        buf = C.create_string_buffer(128)
+        self._ok(self._lib.ref_solver_name(self._h, buf, 128))
+        return buf.value.decode()
+
+
+class RefMemb(RefSim):
+    """The membrane model of ref_create_memb: every surface triangle a patch with channel
+    states C and O (k(V) tables kopen / kclose at vmin + i dv), an ohmic current through O
+    (g per channel, erev) and one membrane; kind "tetopsplit" or "b200"; efopt the
+    reference's EField option (0 = none, 1 = EF_DEFAULT)."""
+
+    def __init__(self, mesh, seed, kopen, kclose, vmin, vmax, dv, g, erev, kind="tetopsplit", efopt=1):
+        lib = load(with_dropin=(kind == "b200"))
+        self._lib = lib
+        verts = np.ascontiguousarray(mesh.verts, dtype=np.float64)
+        tets = np.ascontiguousarray(mesh.tets, dtype=np.int64)
+        ko = np.ascontiguousarray(kopen, dtype=np.float64)
+        kc = np.ascontiguousarray(kclose, dtype=np.float64)
+        self._keep = (verts, tets, ko, kc)
+        self.ntets = int(tets.shape[0])
+        self.nspec = 0
+        h = lib.ref_create_memb(_KINDS[kind], verts.shape[0], _ptr(verts, C.c_double), self.ntets,
+                                _ptr(tets, C.c_int64), ko.size, _ptr(ko, C.c_double), _ptr(kc, C.c_double),
+                                vmin, vmax, dv, g, erev, int(seed), int(efopt))
+        if not h:
+            raise RuntimeError("reference membrane model construction failed: " + lib.ref_last_error().decode())
+        self._h = h
+
+    def surf_tris(self):
+        n = C.c_int()
+        self._ok(self._lib.ref_surf_tris(self._h, None, 0, C.byref(n)))
+        out = np.zeros(n.value, dtype=np.int64)
+        self._ok(self._lib.ref_surf_tris(self._h, _ptr(out, C.c_int64), n.value, C.byref(n)))
+        return out
+
+    def tri_verts(self, tri):
+        out = np.zeros(3, dtype=np.int64)
+        self._ok(self._lib.ref_tri_verts(self._h, int(tri), _ptr(out, C.c_int64)))
+        return out
+
+    def get_tri_count(self, tri, name):
+        out = C.c_double()
+        self._ok(self._lib.ref_get_tri_count(self._h, int(tri), name.encode(), C.byref(out)))
+        return out.value
+
+    def set_tri_count(self, tri, name, n):
+        self._ok(self._lib.ref_set_tri_count(self._h, int(tri), name.encode(), float(n)))
+
+    def get_patch_count(self, name):
+        out = C.c_double()
+        self._ok(self._lib.ref_get_patch_count(self._h, name.encode(), C.byref(out)))
+        return out.value
+
+    def set_patch_count(self, name, n):
+        self._ok(self._lib.ref_set_patch_count(self._h, name.encode(), float(n)))
+
+    def get_vert_v(self, v):
+        out = C.c_double()
+        self._ok(self._lib.ref_get_vert_v(self._h, int(v), C.byref(out)))
+        return out.value
+
+    def set_vert_v(self, v, x):
+        self._ok(self._lib.ref_set_vert_v(self._h, int(v), float(x)))
+
+    def set_vert_iclamp(self, v, amps):
+        self._ok(self._lib.ref_set_vert_iclamp(self._h, int(v), float(amps)))
+
+    def set_memb(self, v0, cm, ra, ro, vrev, efdt):
+        """setMembPotential, setMembCapac, setMembVolRes, setMembRes, setEfieldDT."""
+        self._ok(self._lib.ref_set_memb(self._h, v0, cm, ra, ro, vrev, efdt))

@@ -15,7 +15,8 @@
 //   * src/steps/rng/rng.cpp:512-514     getExp (Ahrens-Dieter in float) -> -log(U)/a0
 //                                        with the project log below.
 //   * src/steps/rng/rng.cpp:516-527     getBinom (small_binomial / libstdc++) ->
-//                                        BINV inversion and BTRD rejection.
+//                                        BINV inversion, inversion from the mode,
+//                                        BTRD rejection for very large n p.
 #pragma once
 #include <stdint.h>
 #include <math.h>
@@ -277,13 +278,21 @@ SG_HD double sg_pow_u(double q, uint32_t n) {
 //   n * min(p, 1-p) < SG_BINV_CUT : BINV sequential-search inversion
 //       (Kachitvichyanukul & Schmeiser, "Binomial random variate generation",
 //        CACM 31(2), 1988), one uniform per sample.
+//   n * min(p, 1-p) < SG_MODE_CUT : inversion by a search that starts at the mode and
+//       alternates up and down (sequential-search inversion over the support taken in
+//       order of distance from the mode; Devroye, "Non-Uniform Random Variate
+//       Generation", 1986, sections III.2 and X.4), one uniform per sample, about
+//       1 + 1.6 sqrt(n p q) pmf steps instead of n p.
 //   otherwise                     : BTRD transformed rejection with decomposition
 //       (Hormann, "The generation of binomial random variates", J. Statist.
 //        Comput. Simul. 46, 1993).
 // ---------------------------------------------------------------------------
 #define SG_BINV_CUT 24.0
+#define SG_MODE_CUT 1000.0
 #define SG_BTRD_MAX_ITERS 256
 #define SG_RCP_TABLE 128   // 1/x for x < SG_RCP_TABLE, precomputed (same value as 1.0/x)
+#define SG_MODE_TABLE 1024 // 1/x and ln x! for x < SG_MODE_TABLE (mode search), same values
+#define SG_HALF_LN_2PI 0.91893853320467274
 
 // 1/x, read from a table of correctly rounded reciprocals when one is given.
 SG_HD double sg_rcp(const double* tab, uint32_t x) {
@@ -344,7 +353,60 @@ SG_HD double sg_stirling_fc(uint32_t k) {
     return (1.0 / 12.0 - (1.0 / 360.0 - 1.0 / 1260.0 / k1sq) / k1sq) / k1;
 }
 
-// BTRD for p <= 1/2 and n p >= SG_BINV_CUT.  Candidates outside [0, n] are
+// ln k! = (k + 1/2) ln(k + 1) - (k + 1) + ln(2 pi)/2 + fc(k): the Stirling form with the
+// remainder above (exact to rounding for every k).
+SG_HD double sg_lnfact(uint32_t k) {
+    const double k1 = (double)k + 1.0;
+    return (k1 - 0.5) * sg_log(k1) - k1 + SG_HALF_LN_2PI + sg_stirling_fc(k);
+}
+
+// Table lookups with the same values as the direct forms (tables may be null).
+SG_HD double sg_lnfact_t(uint32_t k, const double* lnf) {
+    return (lnf && k < (uint32_t)SG_MODE_TABLE) ? lnf[k] : sg_lnfact(k);
+}
+SG_HD double sg_rcp_l(const double* rcpl, uint32_t x) {
+    return (rcpl && x < (uint32_t)SG_MODE_TABLE) ? rcpl[x] : 1.0 / (double)x;
+}
+
+// Inversion from the mode for p <= 1/2, s = p / q: the support is searched in the order
+// m, m+1, m-1, m+2, m-2, ... (one side alone once the other end is reached), subtracting
+// each pmf value from one uniform until it goes negative.  f(m) from the log-factorials;
+// the neighbours by the pmf ratios f(x+1)/f(x) = (n+1) s / (x+1) - s and
+// f(x-1)/f(x) = x r / (n - x + 1), r = q / p.
+SG_HD uint32_t sg_binom_mode(sg_stream* st, uint32_t n, double p, double s, const double* rcpl,
+                             const double* lnf) {
+    const double q = 1.0 - p;
+    const double dn = (double)n;
+    uint32_t m = (uint32_t)floor((dn + 1.0) * p);
+    if (m > n) m = n;
+    const double lf = ((sg_lnfact_t(n, lnf) - sg_lnfact_t(m, lnf)) - sg_lnfact_t(n - m, lnf)) +
+                      (double)m * sg_log(p) + (double)(n - m) * sg_log(q);
+    const double fm = sg_exp(lf);
+    const double a = (dn + 1.0) * s;
+    const double r = q / p;
+    double u = sg_u01_co(sg_next_u32(st)) - fm;
+    if (u < 0.0) return m;
+    double fu = fm, fd = fm;
+    uint32_t xu = m, xd = m;
+    for (;;) {
+        const bool cu = xu < n, cd = xd > 0u;
+        if (!cu && !cd) return m;  // only when rounding left mass uncovered
+        if (cu) {
+            fu = fu * fma(a, sg_rcp_l(rcpl, xu + 1u), -s);
+            xu += 1u;
+            u = u - fu;
+            if (u < 0.0) return xu;
+        }
+        if (cd) {
+            fd = fd * ((double)xd * r) * sg_rcp_l(rcpl, n - xd + 1u);
+            xd -= 1u;
+            u = u - fd;
+            if (u < 0.0) return xd;
+        }
+    }
+}
+
+// BTRD for p <= 1/2 and n p >= SG_MODE_CUT.  Candidates outside [0, n] are
 // rejected.  The iteration cap is never reached in practice (acceptance rate
 // is above 0.8 per round); if it were, the mode is returned.
 SG_HD uint32_t sg_btrd(sg_stream* st, uint32_t n, double p) {
@@ -421,13 +483,22 @@ SG_HD double sg_binom_odds(double p) {
     return pp / (1.0 - pp);
 }
 
-// Binomial(n, p) with odds = sg_binom_odds(p) supplied by the caller.
-SG_HD uint32_t sg_binom_o(sg_stream* st, uint32_t n, double p, double odds, const double* rcp) {
+// Binomial(n, p) with odds = sg_binom_odds(p) supplied by the caller; rcp (SG_RCP_TABLE
+// entries), rcpl and lnf (SG_MODE_TABLE entries) are optional tables of 1/x and ln x!.
+SG_HD uint32_t sg_binom_o(sg_stream* st, uint32_t n, double p, double odds, const double* rcp,
+                          const double* rcpl = nullptr, const double* lnf = nullptr) {
     if (n == 0 || !(p > 0.0)) return 0;
     if (p >= 1.0) return n;
     bool flip = p > 0.5;
     double pp = flip ? 1.0 - p : p;
-    uint32_t k = ((double)n * pp < SG_BINV_CUT) ? sg_binv(st, n, pp, rcp, odds) : sg_btrd(st, n, pp);
+    const double np = (double)n * pp;
+    uint32_t k;
+    if (np < SG_BINV_CUT)
+        k = sg_binv(st, n, pp, rcp, odds);
+    else if (np < SG_MODE_CUT)
+        k = sg_binom_mode(st, n, pp, odds, rcpl, lnf);
+    else
+        k = sg_btrd(st, n, pp);
     return flip ? n - k : k;
 }
 

@@ -422,7 +422,8 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
 }
 
 __device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, double t1, float4 g, double odd1,
-                                             double odd2, double odd3, const double* rcp, uint32_t* out_kn);
+                                             double odd2, double odd3, const double* rcp, const double* rcpl,
+                                             const double* lnf, uint32_t* out_kn);
 
 // Inflow of species s through the diffusion-boundary faces of tet t (slots v.f of the tet's
 // own inflow): counted when the tet behind face f diffuses s, because that tet then wrote
@@ -509,7 +510,8 @@ __device__ __forceinline__ void bnd_scatter(const sg_window_args& a, int t, uint
 __device__ __forceinline__ uint4 leave_species(uint64_t seed, uint32_t real, uint32_t unit, unsigned long long w,
                                                uint32_t s, uint32_t pop, double sd, double invT, double t1,
                                                float4 g, double odd1, double odd2, double odd3, const double* rcp,
-                                               sg_stream* st, uint32_t* out_kn) {
+                                               const double* rcpl, const double* lnf, sg_stream* st,
+                                               uint32_t* out_kn) {
     sg_stream_init(st, seed, real, unit, w, SG_PURPOSE_DIFF + s);
     if (t1 >= 1.0) t1 = 1.0;
     uint32_t mean_n = pop;
@@ -523,13 +525,14 @@ __device__ __forceinline__ uint4 leave_species(uint64_t seed, uint32_t real, uin
             if (sg_u01_co(sg_next_u32(st)) < frc) mean_n += 1u;
         }
     }
-    return leave_split(st, mean_n, t1, g, odd1, odd2, odd3, rcp, out_kn);
+    return leave_split(st, mean_n, t1, g, odd1, odd2, odd3, rcp, rcpl, lnf, out_kn);
 }
 
 // Binomial(mean_n, t1) molecules leave, split over the directions by conditional
 // binomials on the selectors g.x, g.y, g.z; the last direction takes the rest.
 __device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, double t1, float4 g, double odd1,
-                                             double odd2, double odd3, const double* rcp, uint32_t* out_kn) {
+                                             double odd2, double odd3, const double* rcp, const double* rcpl,
+                                             const double* lnf, uint32_t* out_kn) {
     // Stage 0: molecules leaving; stages 1-3: the split.  One sampler call site.
     uint4 k = make_uint4(0u, 0u, 0u, 0u);
     uint32_t n = mean_n, Kn = 0u;
@@ -537,7 +540,7 @@ __device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, dou
     double ost = (t1 > 0.0 && t1 < 1.0) ? sg_binom_odds(t1) : 0.0;
 #pragma unroll 1
     for (int stage = 0; stage < 4; ++stage) {
-        uint32_t v = sg_binom_o(st, n, pst, ost, rcp);
+        uint32_t v = sg_binom_o(st, n, pst, ost, rcp, rcpl, lnf);
         if (stage == 0) {
             Kn = v;
             n = v;
@@ -781,10 +784,11 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
                     const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
                     k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
                                       invT, T * tot, gb, sg_binom_odds((double)gb.x), sg_binom_odds((double)gb.y),
-                                      sg_binom_odds((double)gb.z), s_rcp, &st, &Kn);
+                                      sg_binom_odds((double)gb.z), s_rcp, nullptr, nullptr, &st, &Kn);
                 } else {
                     k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
-                                      invT, T * (D * (double)g.w), g, odd1, odd2, odd3, s_rcp, &st, &Kn);
+                                      invT, T * (D * (double)g.w), g, odd1, odd2, odd3, s_rcp, nullptr, nullptr, &st,
+                                      &Kn);
                 }
                 if (Kn > 0u) {
                     if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
@@ -832,10 +836,16 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_kernel(sg_window_args a, int check) {
     __shared__ double s_rcp[SG_RCP_TABLE];
+    __shared__ double s_rcpl[SG_MODE_TABLE];  // 1/x and ln x! of the mode search
+    __shared__ double s_lnf[SG_MODE_TABLE];
     __shared__ int flag[2];
     __shared__ unsigned long long s_moved;
     const int tid = threadIdx.x, lane = tid & 31;
     for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
+    for (int i = tid; i < SG_MODE_TABLE; i += BLOCK) {
+        s_rcpl[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
+        s_lnf[i] = sg_lnfact((uint32_t)i);
+    }
     if (tid == 0) s_moved = 0ull;
     __syncthreads();
     const unsigned long long parity = __ldcg(&a.launch_state[1]) & 1ull;
@@ -885,10 +895,10 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
                     const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
                     k = leave_species(a.seed, (uint32_t)r, tl, w, (uint32_t)s, pop, sd, invT, T * tot, gb,
                                       sg_binom_odds((double)gb.x), sg_binom_odds((double)gb.y),
-                                      sg_binom_odds((double)gb.z), s_rcp, &st, &Kn);
+                                      sg_binom_odds((double)gb.z), s_rcp, s_rcpl, s_lnf, &st, &Kn);
                 } else {
                     k = leave_species(a.seed, (uint32_t)r, tl, w, (uint32_t)s, pop, sd, invT, T * (D * (double)g.w),
-                                      g, odd1, odd2, odd3, s_rcp, &st, &Kn);
+                                      g, odd1, odd2, odd3, s_rcp, s_rcpl, s_lnf, &st, &Kn);
                 }
                 if (Kn > 0u) {
                     if (!((clampm >> s) & 1u)) a.counts[ci] = pop - Kn;
@@ -960,7 +970,7 @@ __global__ void __launch_bounds__(BLOCK) sdiffuse_kernel(sg_window_args a) {
             }
             uint32_t Kn = 0u;
             k = leave_split(&st, mean_n, t1, g, sg_binom_odds((double)g.x), sg_binom_odds((double)g.y), 0.0, s_rcp,
-                            &Kn);
+                            nullptr, nullptr, &Kn);
             if (Kn > 0u) {
                 sa.tri_counts[ci] = pop - Kn;
                 moved += Kn;

@@ -5,7 +5,7 @@
 - The project log against math.log.
 - The binomial sampler with the chi-squared check of the reference's
   test/unit/cpp/test_rng.cpp:51-90 (same (n, p) grid, sample sizes and levels), and a
-  goodness-of-fit test with the proper degrees of freedom over both sampler regimes.
+  goodness-of-fit test with the proper degrees of freedom over every sampler regime.
 """
 import json
 import math
@@ -69,9 +69,11 @@ def test_binomial_reference_grid_rejects_wrong(t_test, p_test):
 
 @pytest.mark.parametrize("n,p", [(10, 0.3), (40, 0.2), (1000, 0.3), (200, 0.93), (5000, 0.5),
                                  (1 << 20, 3e-6), (60, 0.999), (4000000000, 2e-9), (25, 0.4),
-                                 (47, 0.5), (120, 0.19)])
+                                 (47, 0.5), (120, 0.19), (49, 0.5), (95, 0.5), (95, 0.75), (60, 0.45),
+                                 (400, 0.5), (2100, 0.47), (2150, 0.47), (48, 0.999)])
 def test_binomial_goodness_of_fit(n, p):
-    """BINV below the cut, BTRD above it, against the exact binomial pmf."""
+    """BINV below n min(p, 1-p) = 24, the search from the mode up to 1000, BTRD above,
+    against the exact binomial pmf."""
     m = 200000
     x = pyoracle.binom_many(777, n % 1000, n, p, m).astype(np.int64)
     mean, var = n * p, n * p * (1 - p)
