@@ -644,6 +644,35 @@ def run_efield(args):
     return 0
 
 
+def run_windows(args):
+    """Profiling mode: the plain 384k workload with a fixed launch (block 256, one tet per
+    thread, split or fused by --split), run to the warm-up time (--warmup ms), then
+    --windows more windows; prints the mean window time.  The ncu summaries under
+    profiles/ capture the kernels of these last windows."""
+    import torch
+
+    from steps_b200 import rng as srng
+    from steps_b200.solver import TetOpSplit
+
+    mdl, mesh, rows = workload()
+    r = srng.create("r123", 512)
+    r.initialize(SEED)
+    sim = TetOpSplit(mdl, mesh, r, device=0)
+    for i, s in enumerate(sim.spec_names):
+        sim.setSpecCounts(s, rows[i])
+    sim.setLaunch(256, -1)
+    sim.setSplit(bool(args.split))
+    sim.run(args.warmup * STEP_SIM_S)
+    torch.cuda.synchronize()
+    per = sim.getUpdPeriod()
+    sim.setProfiling(True)
+    sim.run(sim.getTime() + args.windows * per * 0.999999)
+    wms, nw, _ = sim.getProfile()
+    print(json.dumps({"mode": "windows", "split": bool(args.split), "warmup_ms": args.warmup, "windows": nw,
+                      "ms_per_window": wms / max(nw, 1)}), flush=True)
+    return 0
+
+
 def run_coupled(args):
     """Full coupled batched configuration: 16 realizations of a 5x5x8 um box (50x50x80 Kuhn
     cubes, 1.2 M tets each) in one launch per window.  Volume: Ca + CB <-> CaCB (kf 1e8 /M/s,
@@ -748,7 +777,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--ref-windows", type=int, default=1,
                     help="reference arm: split windows per timed step (a bounded CPU sample of the 1 ms step)")
-    ap.add_argument("--config", choices=["plain", "batched", "efield", "coupled"], default="plain")
+    ap.add_argument("--config", choices=["plain", "batched", "efield", "coupled", "windows"], default="plain")
+    ap.add_argument("--windows", type=int, default=4, help="--config windows: windows after the warm-up")
+    ap.add_argument("--split", type=int, default=1, help="--config windows: 1 split window kernels, 0 fused")
     ap.add_argument("--cp-dims", type=int, nargs=3, default=[50, 50, 80])
     ap.add_argument("--cp-nreal", type=int, default=16)
     ap.add_argument("--cp-ms", type=float, default=0.5, help="timed simulated ms (the configuration runs 20)")
@@ -780,6 +811,8 @@ def main():
         return run_efield(args)
     if args.config == "coupled":
         return run_coupled(args)
+    if args.config == "windows":
+        return run_windows(args)
     return run_ours(args)
 
 
