@@ -464,7 +464,61 @@ typedef struct {
     double* btab;
     float* bcoef;
     int32_t* bnbr;
+    /* Membrane (sreac.cpp, vdepsreac.cpp, ghkcurr.cpp, sdiff.cpp): triangles m = 0..M-1
+     * with inner tet, patch and area; surface counts [SS][M]; the triangles of each tet's
+     * SSA unit (slot order = ascending m); surface reactions grouped by patch; k(V) tables;
+     * GHK currents; surface diffusion tables.  Triangle potentials (mV) default to 0. */
+    int nsspec, ntris, npatch;
+    const int32_t* tri_inner;
+    const int32_t* tri_patch;
+    const double* tri_area;
+    int32_t* tet_tris;         /* [T][4] */
+    uint32_t* tri_counts;      /* [SS][M] */
+    double* tri_v;             /* [M] mV */
+    double* spec_int;          /* [SS][M] count time integrals */
+    int64_t* echarge;          /* [M] elementary charges carried by GHK events */
+    uint64_t surf_ext;
+    struct or_sreac* sreacs;
+    int nsreac;
+    int* patch_sb;             /* [npatch + 1] */
+    double* vt_vmin;
+    double* vt_dv;
+    int* vt_off;
+    int* vt_n;
+    int nvt;
+    double* vt_vals;
+    int nvt_vals;
+    struct or_ghk* ghks;
+    int nghk;
+    double temp;
+    double* sdcst;             /* [npatch][SS] */
+    const int32_t* tri_nbr;    /* [M][3] */
+    const int32_t* tri_nbr_edge;
+    const double* tri_len;
+    const double* tri_dist;
+    int32_t* sdiff_slot;       /* [SS] */
+    int nsdiff;
+    int32_t* sdspec;           /* [SD] */
+    float* sgeo;               /* [M][4] */
+    int32_t* snbr;             /* [M][4] (q << 2) | edge */
+    double* tri_occ;           /* [SD][M] */
+    uint32_t* tri_out;         /* [SD][M][4] */
 } or_solver;
+
+typedef struct or_sreac {
+    int patch, order, surf_surf, vdep;
+    int nslhs, nilhs, nsupd, niupd;
+    int slhs_spec[4], slhs_ord[4], ilhs_spec[4], ilhs_ord[4];
+    int supd_spec[8], supd_delta[8], iupd_spec[8], iupd_delta[8];
+    double k;
+} or_sreac;
+
+typedef struct or_ghk {
+    int patch, sspec, ion, valence, realflux;
+    double perm, vshift, voconc;
+} or_ghk;
+
+static void or_setup_surface(or_solver* s);
 
 or_solver* or_create(uint64_t seed, int ntets, int nspec, int ncomp, const double* vol,
                      const int32_t* neighb, const double* area, const double* dist,
@@ -509,6 +563,26 @@ void or_destroy(or_solver* s) {
     free(s->btab);
     free(s->bcoef);
     free(s->bnbr);
+    free(s->tet_tris);
+    free(s->tri_counts);
+    free(s->tri_v);
+    free(s->spec_int);
+    free(s->echarge);
+    free(s->sreacs);
+    free(s->patch_sb);
+    free(s->vt_vmin);
+    free(s->vt_dv);
+    free(s->vt_off);
+    free(s->vt_n);
+    free(s->vt_vals);
+    free(s->ghks);
+    free(s->sdcst);
+    free(s->sdiff_slot);
+    free(s->sdspec);
+    free(s->sgeo);
+    free(s->snbr);
+    free(s->tri_occ);
+    free(s->tri_out);
     free(s);
 }
 
@@ -615,6 +689,16 @@ static void or_periods(or_solver* s) {
                 if (sd > mx) mx = sd;
             }
         }
+        /* Surface diffusion rules count too (TOS:5373-5411 takes the max over both). */
+        for (int m = 0; s->nsdiff > 0 && m < s->ntris; ++m) {
+            const int t = s->tri_inner[m];
+            if (t < s->real_begin[r] || t >= s->real_begin[r + 1]) continue;
+            const double G = (double)s->sgeo[(size_t)m * 4 + 3];
+            for (int sp = 0; sp < s->nsspec; ++sp) {
+                const double sd = s->sdcst[(size_t)s->tri_patch[m] * s->nsspec + sp] * G;
+                if (sd > mx) mx = sd;
+            }
+        }
         s->period[r] = (mx > 0.0) ? 1.0 / mx : INFINITY;
     }
 }
@@ -690,8 +774,182 @@ int or_setup(or_solver* s) {
             }
         }
     }
+    if (s->ntris > 0) or_setup_surface(s);
     or_periods(s);
     return 0;
+}
+
+/* ---- membrane builders (before or_setup; arrays kept by reference) ---- */
+void or_set_surface(or_solver* s, int nsspec, int ntris, const int32_t* tri_inner, const int32_t* tri_patch,
+                    const double* tri_area, int npatch) {
+    s->nsspec = nsspec;
+    s->ntris = ntris;
+    s->npatch = npatch;
+    s->tri_inner = tri_inner;
+    s->tri_patch = tri_patch;
+    s->tri_area = tri_area;
+    s->tri_counts = (uint32_t*)calloc((size_t)nsspec * ntris, 4);
+    s->tri_v = (double*)calloc((size_t)ntris, sizeof(double));
+    s->spec_int = (double*)calloc((size_t)nsspec * ntris, sizeof(double));
+    s->echarge = (int64_t*)calloc((size_t)ntris, sizeof(int64_t));
+    s->sdcst = (double*)calloc((size_t)npatch * nsspec, sizeof(double));
+    s->temp = 293.15;
+}
+
+/* One surface reaction: dense rows over the surface (slhs, supd) and volume (ilhs, iupd)
+ * species, compacted in increasing species order as the GPU solver's tables; a k(V) table
+ * (vmin, dv, n values) when vals is given, else the constant k.  Returns its index. */
+int or_add_sreac(or_solver* s, int patch, const uint32_t* slhs, const uint32_t* ilhs, const int32_t* supd,
+                 const int32_t* iupd, double k, double vmin, double dv, int ntab, const double* vals) {
+    s->sreacs = (or_sreac*)realloc(s->sreacs, sizeof(or_sreac) * (size_t)(s->nsreac + 1));
+    or_sreac* r = &s->sreacs[s->nsreac];
+    memset(r, 0, sizeof(*r));
+    r->patch = patch;
+    r->vdep = -1;
+    r->k = k;
+    for (int i = 0; i < s->nsspec; ++i)
+        if (slhs[i]) {
+            r->slhs_spec[r->nslhs] = i;
+            r->slhs_ord[r->nslhs++] = (int)slhs[i];
+            r->order += (int)slhs[i];
+        }
+    for (int i = 0; i < s->nspec; ++i)
+        if (ilhs[i]) {
+            r->ilhs_spec[r->nilhs] = i;
+            r->ilhs_ord[r->nilhs++] = (int)ilhs[i];
+            r->order += (int)ilhs[i];
+        }
+    r->surf_surf = r->nilhs == 0;
+    for (int i = 0; i < s->nsspec; ++i)
+        if (supd[i]) {
+            r->supd_spec[r->nsupd] = i;
+            r->supd_delta[r->nsupd++] = supd[i];
+        }
+    for (int i = 0; i < s->nspec; ++i)
+        if (iupd[i]) {
+            r->iupd_spec[r->niupd] = i;
+            r->iupd_delta[r->niupd++] = iupd[i];
+        }
+    if (vals) {
+        int v = s->nvt++;
+        s->vt_vmin = (double*)realloc(s->vt_vmin, sizeof(double) * s->nvt);
+        s->vt_dv = (double*)realloc(s->vt_dv, sizeof(double) * s->nvt);
+        s->vt_off = (int*)realloc(s->vt_off, sizeof(int) * s->nvt);
+        s->vt_n = (int*)realloc(s->vt_n, sizeof(int) * s->nvt);
+        s->vt_vmin[v] = vmin;
+        s->vt_dv[v] = dv;
+        s->vt_off[v] = s->nvt_vals;
+        s->vt_n[v] = ntab;
+        s->vt_vals = (double*)realloc(s->vt_vals, sizeof(double) * (size_t)(s->nvt_vals + ntab));
+        memcpy(s->vt_vals + s->nvt_vals, vals, sizeof(double) * (size_t)ntab);
+        s->nvt_vals += ntab;
+        r->vdep = v;
+        r->k = 0.0;
+    }
+    return s->nsreac++;
+}
+
+void or_add_ghk(or_solver* s, int patch, int sspec, int ion, int valence, double perm, double vshift,
+                double voconc, int realflux) {
+    s->ghks = (or_ghk*)realloc(s->ghks, sizeof(or_ghk) * (size_t)(s->nghk + 1));
+    or_ghk* g = &s->ghks[s->nghk++];
+    g->patch = patch;
+    g->sspec = sspec;
+    g->ion = ion;
+    g->valence = valence;
+    g->perm = perm;
+    g->vshift = vshift;
+    g->voconc = voconc;
+    g->realflux = realflux;
+}
+
+void or_set_temp(or_solver* s, double kelvin) { s->temp = kelvin; }
+
+void or_set_tri_neighbours(or_solver* s, const int32_t* nbr, const int32_t* nbr_edge, const double* len,
+                           const double* dist) {
+    s->tri_nbr = nbr;
+    s->tri_nbr_edge = nbr_edge;
+    s->tri_len = len;
+    s->tri_dist = dist;
+}
+
+void or_add_sdiff(or_solver* s, int patch, int sspec, double dcst) { s->sdcst[(size_t)patch * s->nsspec + sspec] = dcst; }
+
+/* Surface reactions grouped by patch (stable), the SSA units' triangle slots, and the
+ * surface diffusion tables (sdiff.cpp:62-83): edge coefficients l / (A d) towards same-patch
+ * neighbours, G = their sum, conditional selectors c0 = g0 / G, c1 = g1 / (g1 + g2). */
+static void or_setup_surface(or_solver* s) {
+    const int R = s->nsreac, P = s->npatch, M = s->ntris, SS = s->nsspec;
+    or_sreac* sorted = (or_sreac*)malloc(sizeof(or_sreac) * (size_t)(R > 0 ? R : 1));
+    int n = 0;
+    for (int p = 0; p < P; ++p)
+        for (int i = 0; i < R; ++i)
+            if (s->sreacs[i].patch == p) sorted[n++] = s->sreacs[i];
+    free(s->sreacs);
+    s->sreacs = sorted;
+    s->patch_sb = (int*)calloc((size_t)P + 1, sizeof(int));
+    for (int i = 0; i < R; ++i) s->patch_sb[s->sreacs[i].patch + 1] += 1;
+    for (int p = 0; p < P; ++p) s->patch_sb[p + 1] += s->patch_sb[p];
+    s->tet_tris = (int32_t*)malloc(sizeof(int32_t) * (size_t)s->ntets * 4);
+    for (size_t i = 0; i < (size_t)s->ntets * 4; ++i) s->tet_tris[i] = -1;
+    for (int m = 0; m < M; ++m) {
+        const int t = s->tri_inner[m];
+        int slot = 0;
+        while (slot < 4 && s->tet_tris[(size_t)t * 4 + slot] >= 0) ++slot;
+        s->tet_tris[(size_t)t * 4 + slot] = m;
+    }
+    s->sdiff_slot = (int32_t*)malloc(sizeof(int32_t) * (size_t)(SS > 0 ? SS : 1));
+    s->nsdiff = 0;
+    int any = 0;
+    for (size_t i = 0; i < (size_t)P * SS; ++i)
+        if (s->sdcst[i] > 0.0) any = 1;
+    for (int sp = 0; sp < SS; ++sp) s->sdiff_slot[sp] = -1;
+    if (!any) return;
+    s->sdspec = (int32_t*)malloc(sizeof(int32_t) * (size_t)SS);
+    for (int sp = 0; sp < SS; ++sp) {
+        int has = 0;
+        for (int p = 0; p < P; ++p)
+            if (s->sdcst[(size_t)p * SS + sp] > 0.0) has = 1;
+        if (has) {
+            s->sdiff_slot[sp] = s->nsdiff;
+            s->sdspec[s->nsdiff++] = sp;
+        }
+    }
+    s->sgeo = (float*)calloc((size_t)M * 4, sizeof(float));
+    s->snbr = (int32_t*)malloc(sizeof(int32_t) * (size_t)M * 4);
+    for (int m = 0; m < M; ++m) {
+        double g[3] = {0.0, 0.0, 0.0};
+        for (int e = 0; e < 4; ++e) s->snbr[(size_t)m * 4 + e] = -1;
+        for (int e = 0; e < 3; ++e) {
+            const int q = s->tri_nbr[(size_t)m * 3 + e];
+            if (q < 0 || s->tri_patch[q] != s->tri_patch[m]) continue;
+            const double d = s->tri_dist[(size_t)m * 3 + e];
+            if (!(d > 0.0)) continue;
+            g[e] = s->tri_len[(size_t)m * 3 + e] / (s->tri_area[m] * d);
+            s->snbr[(size_t)m * 4 + e] = (q << 2) | s->tri_nbr_edge[(size_t)m * 3 + e];
+        }
+        const double G = g[0] + g[1] + g[2];
+        const double r12 = g[1] + g[2];
+        s->sgeo[(size_t)m * 4 + 0] = G > 0.0 ? (float)(g[0] / G) : 0.0f;
+        s->sgeo[(size_t)m * 4 + 1] = r12 > 0.0 ? (float)(g[1] / r12) : 0.0f;
+        s->sgeo[(size_t)m * 4 + 2] = 1.0f;
+        s->sgeo[(size_t)m * 4 + 3] = (float)G;
+    }
+    s->tri_occ = (double*)calloc((size_t)s->nsdiff * M, sizeof(double));
+    s->tri_out = (uint32_t*)calloc((size_t)s->nsdiff * M * 4, 4);
+}
+
+void or_set_tri_counts(or_solver* s, int sspec, const uint32_t* row) {
+    memcpy(s->tri_counts + (size_t)sspec * s->ntris, row, (size_t)s->ntris * 4);
+}
+void or_get_tri_counts(or_solver* s, int sspec, uint32_t* row) {
+    memcpy(row, s->tri_counts + (size_t)sspec * s->ntris, (size_t)s->ntris * 4);
+}
+void or_set_tri_v(or_solver* s, const double* v_mV) { memcpy(s->tri_v, v_mV, sizeof(double) * (size_t)s->ntris); }
+uint64_t or_get_surf_ext(or_solver* s) { return s->surf_ext; }
+void or_get_echarge(or_solver* s, int64_t* out) { memcpy(out, s->echarge, sizeof(int64_t) * (size_t)s->ntris); }
+void or_get_spec_int(or_solver* s, double* out) {
+    memcpy(out, s->spec_int, sizeof(double) * (size_t)s->nsspec * s->ntris);
 }
 
 /* setDiffBoundarySpecDiffusionActive / setDiffBoundarySpecDcst outcome: the rate table. */
@@ -752,6 +1010,325 @@ static double or_prop(const or_solver* s, const or_reac* r, const uint32_t* cnt,
     return h * ccst;
 }
 
+/* ---- membrane SSA units ---- */
+#define OR_FARADAY 96485.3399       /* math/constants.hpp:49 */
+#define OR_GAS_CONSTANT 8.314472    /* constants.hpp:53 */
+#define OR_E_CHARGE 1.602176487e-19 /* constants.hpp:57 */
+#define OR_AVOGADRO 6.02214179e23   /* constants.hpp:45 */
+
+/* k(V) by linear interpolation in the table (vdepsreacdef.cpp:194-218). */
+static double or_vdep_k(const or_solver* s, int v, double v_mV) {
+    double vv = v_mV * 1.0e-3;
+    double v2 = (vv - s->vt_vmin[v]) / s->vt_dv[v];
+    if (!(v2 >= 0.0) || v2 > (double)(s->vt_n[v] - 1)) v2 = v2 < 0.0 ? 0.0 : (double)(s->vt_n[v] - 1);
+    double lv = floor(v2);
+    int lo = (int)lv, hi = (int)ceil(v2);
+    double r = v2 - lv;
+    const double* K = s->vt_vals + s->vt_off[v];
+    return (1.0 - r) * K[lo] + r * K[hi];
+}
+
+/* Single-channel GHK current (math/ghk.cpp:71-90), concentrations in mol/m^3. */
+static double or_ghk_current(double P, double v, int z, double temp, double ci, double co) {
+    const double nu = (double)z * v * OR_FARADAY / (OR_GAS_CONSTANT * temp);
+    if (!(nu < 700.0 && nu > -700.0)) return 0.0;
+    if (fabs(nu) > 2.220446049250313e-16) {
+        const double e = or_exp(-nu);
+        return P * (double)z * OR_FARADAY * nu * (ci - co * e) / (1.0 - e);
+    }
+    return P * (double)z * OR_FARADAY * (ci - co);
+}
+
+/* Signed ion rate (/s) of a GHK current on a triangle with n channels (ghkcurr.cpp:168-212). */
+static double or_ghk_rate(const or_ghk* g, double vm, uint32_t c_ion, uint32_t n, double ivs, double temp) {
+    if (n == 0) return 0.0;
+    const double ci = (double)c_ion * ivs * 1.0e3;
+    const double co = g->voconc * 1.0e3;
+    const double I = or_ghk_current(g->perm, vm * 1.0e-3 + g->vshift, g->valence, temp, ci, co);
+    return I / (OR_E_CHARGE * (double)g->valence) * (double)n;
+}
+
+/* Scaled constant of a surface reaction (sreac.cpp:40-68: by area when no volume reactant). */
+static double or_sreac_ccst(const or_sreac* r, double k, double ivs, double area) {
+    if (r->surf_surf) {
+        double ascale = area * OR_AVOGADRO;
+        if (r->order == 0) return k * ascale;
+        double c = k;
+        for (int i = 1; i < r->order; ++i) c = c / ascale;
+        return c;
+    }
+    if (r->order == 0) return k / ivs;
+    double c = k;
+    for (int i = 1; i < r->order; ++i) c = c * ivs;
+    return c;
+}
+
+static double or_falling(uint32_t c, uint32_t o) {
+    double h = 1.0;
+    if (o >= 4) h = h * (double)(c - 3);
+    if (o >= 3) h = h * (double)(c - 2);
+    if (o >= 2) h = h * (double)(c - 1);
+    return h * (double)c;
+}
+
+static double or_sreac_h(const or_sreac* r, const uint32_t* sc, const uint32_t* vc) {
+    double h = 1.0;
+    for (int i = 0; i < r->nslhs; ++i) {
+        uint32_t c = sc[r->slhs_spec[i]], o = (uint32_t)r->slhs_ord[i];
+        if (o > c) return 0.0;
+        h = h * or_falling(c, o);
+    }
+    for (int i = 0; i < r->nilhs; ++i) {
+        uint32_t c = vc[r->ilhs_spec[i]], o = (uint32_t)r->ilhs_ord[i];
+        if (o > c) return 0.0;
+        h = h * or_falling(c, o);
+    }
+    return h;
+}
+
+static uint32_t or_bump(uint32_t old, int64_t d) {
+    int64_t nc = (int64_t)old + d;
+    if (nc < 0) nc = 0;
+    if (nc > 0xFFFFFFFFll) nc = 0xFFFFFFFFll;
+    return (uint32_t)nc;
+}
+
+/* SSA of the unit tet t + its membrane triangles over [0, T) (sreac.cpp:305-520): volume
+ * reactions, then each triangle's surface reactions and GHK currents, all propensities
+ * re-evaluated after every event; surface counts integrate their occupancy (tri.cpp:486-561).
+ * Draws continue the unit's stream st.  Surface-diffusion inflow of the last window was
+ * already added to the triangle counts. */
+static void or_ssa_surf(or_solver* s, int t, double T, uint32_t* cnt, double* tdel, or_stream* st, uint32_t clampm,
+                        double ivs, const double* K, int rb, int re) {
+    const int SS = s->nsspec, M = s->ntris;
+    int mm[4], pb[4], pe[4], pj[4];
+    double area[4], vm[4];
+    uint32_t sc[4][OR_MAXS];
+    double occ[4][OR_MAXS], last[4][OR_MAXS];
+    double prop[OR_MAXR], sprop[4][OR_MAXR];
+    for (int j = 0; j < 4; ++j) {
+        mm[j] = s->tet_tris[(size_t)t * 4 + j];
+        pb[j] = pe[j] = 0;
+        pj[j] = -1;
+        area[j] = vm[j] = 0.0;
+        if (mm[j] < 0) continue;
+        const int m = mm[j], p = s->tri_patch[m];
+        pj[j] = p;
+        pb[j] = s->patch_sb[p];
+        pe[j] = s->patch_sb[p + 1];
+        area[j] = s->tri_area[m];
+        vm[j] = s->tri_v[m];
+        for (int k = 0; k < SS; ++k) {
+            sc[j][k] = s->tri_counts[(size_t)k * M + m];
+            occ[j][k] = 0.0;
+            last[j][k] = 0.0;
+        }
+    }
+    double tt = 0.0;
+    for (;;) {
+        double a0 = 0.0;
+        for (int q = rb; q >= 0 && q < re; ++q) {
+            const double pq = or_prop(s, &s->reac[q], cnt, K[q], ivs);
+            prop[q] = pq;
+            a0 = a0 + pq;
+        }
+        for (int j = 0; j < 4; ++j) {
+            for (int q = pb[j]; q < pe[j]; ++q) {
+                const or_sreac* r = &s->sreacs[q];
+                const double k = (r->vdep >= 0) ? or_vdep_k(s, r->vdep, vm[j]) : r->k;
+                const double h = or_sreac_h(r, sc[j], cnt);
+                const double pq = h * or_sreac_ccst(r, k, ivs, area[j]);
+                sprop[j][q - pb[j]] = pq;
+                a0 = a0 + pq;
+            }
+            int kk = pe[j] - pb[j];
+            for (int g = 0; g < s->nghk && pj[j] >= 0; ++g) {
+                const or_ghk* gh = &s->ghks[g];
+                if (gh->patch != pj[j]) continue;
+                const double rt = or_ghk_rate(gh, vm[j], cnt[gh->ion], sc[j][gh->sspec], ivs, s->temp);
+                const double pq = fabs(rt);
+                sprop[j][kk] = pq;
+                a0 = a0 + pq;
+                ++kk;
+            }
+        }
+        if (!(a0 > 0.0)) break;
+        double dt = -or_log(u_oc(or_u32(st))) / a0;
+        if (tt + dt > T) break;
+        tt = tt + dt;
+        double target = u_co(or_u32(st)) * a0;
+        double cum = 0.0;
+        int sj = -2, sq = -1, lj = -2, lq = -1;
+        for (int q = rb; q >= 0 && q < re && sj == -2; ++q) {
+            double pq = prop[q];
+            if (pq > 0.0) {
+                lj = -1;
+                lq = q;
+                cum = cum + pq;
+                if (target < cum) {
+                    sj = -1;
+                    sq = q;
+                }
+            }
+        }
+        for (int j = 0; j < 4 && sj == -2; ++j) {
+            for (int q = pb[j]; q < pe[j]; ++q) {
+                double pq = sprop[j][q - pb[j]];
+                if (pq > 0.0) {
+                    lj = j;
+                    lq = q;
+                    cum = cum + pq;
+                    if (target < cum) {
+                        sj = j;
+                        sq = q;
+                        break;
+                    }
+                }
+            }
+            int kk = pe[j] - pb[j];
+            for (int g = 0; g < s->nghk && pj[j] >= 0 && sj == -2; ++g) {
+                if (s->ghks[g].patch != pj[j]) continue;
+                double pq = sprop[j][kk];
+                ++kk;
+                if (pq > 0.0) {
+                    lj = j;
+                    lq = -10 - g;
+                    cum = cum + pq;
+                    if (target < cum) {
+                        sj = j;
+                        sq = -10 - g;
+                    }
+                }
+            }
+        }
+        if (sj == -2) {
+            sj = lj;
+            sq = lq;
+        }
+        if (sq <= -10) {
+            /* GHK event (ghkcurr.cpp:230-280): one ion out (efflux) or in, z charges. */
+            const or_ghk* gh = &s->ghks[-10 - sq];
+            const int m = mm[sj];
+            const double rt = or_ghk_rate(gh, vm[sj], cnt[gh->ion], sc[sj][gh->sspec], ivs, s->temp);
+            const int eff = rt >= 0.0;
+            if (gh->realflux && !((clampm >> gh->ion) & 1u)) {
+                const int k = gh->ion;
+                const uint32_t old = cnt[k];
+                const uint32_t nc = or_bump(old, eff ? -1 : 1);
+                tdel[k] = tdel[k] + (double)((int64_t)nc - (int64_t)old) * tt;
+                cnt[k] = nc;
+            }
+#pragma omp atomic
+            s->echarge[m] += eff ? gh->valence : -gh->valence;
+#pragma omp atomic
+            s->surf_ext += 1;
+            continue;
+        }
+        if (sq < 0) break;
+        if (sj == -1) {
+            const or_reac* rc = &s->reac[sq];
+            for (int i = 0; i < s->nspec; ++i) {
+                int32_t d = rc->upd[i];
+                if (d == 0 || ((clampm >> i) & 1u)) continue;
+                const uint32_t old = cnt[i];
+                const uint32_t nc = or_bump(old, d);
+                tdel[i] = tdel[i] + (double)((int64_t)nc - (int64_t)old) * tt;
+                cnt[i] = nc;
+            }
+#pragma omp atomic
+            s->ext[sq] += 1;
+        } else {
+            const or_sreac* r = &s->sreacs[sq];
+            for (int i = 0; i < r->nsupd; ++i) {
+                const int k = r->supd_spec[i];
+                const uint32_t old = sc[sj][k];
+                occ[sj][k] = occ[sj][k] + (double)old * (tt - last[sj][k]);
+                last[sj][k] = tt;
+                sc[sj][k] = or_bump(old, r->supd_delta[i]);
+            }
+            for (int i = 0; i < r->niupd; ++i) {
+                const int k = r->iupd_spec[i];
+                if ((clampm >> k) & 1u) continue;
+                const uint32_t old = cnt[k];
+                const uint32_t nc = or_bump(old, r->iupd_delta[i]);
+                tdel[k] = tdel[k] + (double)((int64_t)nc - (int64_t)old) * tt;
+                cnt[k] = nc;
+            }
+#pragma omp atomic
+            s->surf_ext += 1;
+        }
+    }
+    for (int j = 0; j < 4; ++j) {
+        const int m = mm[j];
+        if (m < 0) continue;
+        for (int k = 0; k < SS; ++k) {
+            const uint32_t c = sc[j][k];
+            s->tri_counts[(size_t)k * M + m] = c;
+            const double o = occ[j][k] + (double)c * (T - last[j][k]);
+            s->spec_int[(size_t)k * M + m] += o;
+            if (s->nsdiff > 0) {
+                const int sd = s->sdiff_slot[k];
+                if (sd >= 0) s->tri_occ[(size_t)sd * M + m] = o;
+            }
+        }
+    }
+}
+
+/* Surface diffusion leave of triangle m (TOS:1716-1793, sdiff.cpp:498-560): n = min(pop,
+ * window integral / T) with a Bernoulli on its fraction, Binomial(n, min(1, T D G)) leaving,
+ * split over the three edges by the conditional selectors (purpose 80 + species stream). */
+static void or_tri_leave(or_solver* s, int r, int m, double T, uint64_t w) {
+    const int M = s->ntris, SS = s->nsspec;
+    for (int sd = 0; sd < s->nsdiff; ++sd) {
+        const int sp = s->sdspec[sd];
+        uint32_t* o = s->tri_out + ((size_t)sd * M + m) * 4;
+        o[0] = o[1] = o[2] = o[3] = 0;
+        const double D = s->sdcst[(size_t)s->tri_patch[m] * SS + sp];
+        if (!(D > 0.0)) continue;
+        const size_t ci = (size_t)sp * M + m;
+        const uint32_t pop = s->tri_counts[ci];
+        if (pop == 0) continue;
+        const float* g = s->sgeo + (size_t)m * 4;
+        double t1 = T * (D * (double)g[3]);
+        if (t1 >= 1.0) t1 = 1.0;
+        double nd = s->tri_occ[(size_t)sd * M + m] / T;
+        if (nd > (double)pop) nd = (double)pop;
+        const double nint = floor(nd), frc = nd - nint;
+        uint32_t mean_n = (uint32_t)nint;
+        or_stream st;
+        or_stream_init(&st, s->seed, (uint32_t)r, (uint32_t)m, w, 80u + (uint32_t)sp);
+        if (frc > 0.0 && u_co(or_u32(&st)) < frc) mean_n += 1u;
+        const uint32_t Kn = or_binom(&st, mean_n, t1);
+        uint32_t rem = Kn;
+        o[0] = or_binom(&st, rem, (double)g[0]);
+        rem -= o[0];
+        o[1] = or_binom(&st, rem, (double)g[1]);
+        rem -= o[1];
+        o[2] = rem;
+        if (Kn > 0) {
+            s->tri_counts[ci] = pop - Kn;
+#pragma omp atomic
+            s->diff_moved += Kn;
+        }
+    }
+}
+
+/* Surface arrivals: each edge slot holds what the neighbour across it sent. */
+static void or_tri_enter(or_solver* s, int m) {
+    const int M = s->ntris, SS = s->nsspec;
+    for (int sd = 0; sd < s->nsdiff; ++sd) {
+        const int sp = s->sdspec[sd];
+        if (!(s->sdcst[(size_t)s->tri_patch[m] * SS + sp] > 0.0)) continue;
+        uint64_t sum = s->tri_counts[(size_t)sp * M + m];
+        for (int e = 0; e < 3; ++e) {
+            const int nb = s->snbr[(size_t)m * 4 + e];
+            if (nb < 0) continue;
+            sum += s->tri_out[((size_t)sd * M + (nb >> 2)) * 4 + (nb & 3)];
+        }
+        s->tri_counts[(size_t)sp * M + m] = (uint32_t)(sum > 0xFFFFFFFFull ? 0xFFFFFFFFull : sum);
+    }
+}
+
 /* SSA phase (TOS:1565-1588) then diffusion phase (TOS:1633-1712) of tet t. */
 static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
     const int S = s->nspec;
@@ -778,7 +1355,10 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
             re = q + 1;
         }
     }
-    if (rb >= 0) {
+    const int has_tris = s->ntris > 0 && (s->tet_tris[(size_t)t * 4] >= 0);
+    if (has_tris) {
+        or_ssa_surf(s, t, T, cnt, tdel, &st, clampm, ivs, K, rb, re);
+    } else if (rb >= 0) {
         double tt = 0.0;
         for (;;) {
             double a0 = 0.0;
@@ -903,8 +1483,14 @@ uint64_t or_run(or_solver* s, double endtime) {
             for (int tet = tb; tet < te; ++tet)
                 if (s->tcomp[tet] >= 0) or_tet_window(s, r, tet, T, w);
 #pragma omp parallel for schedule(static)
+            for (int m = 0; m < s->ntris * (s->nsdiff > 0); ++m)
+                if (s->tri_inner[m] >= tb && s->tri_inner[m] < te) or_tri_leave(s, r, m, T, w);
+#pragma omp parallel for schedule(static)
             for (int tet = tb; tet < te; ++tet)
                 if (s->tcomp[tet] >= 0) or_tet_enter(s, r, tet);
+#pragma omp parallel for schedule(static)
+            for (int m = 0; m < s->ntris * (s->nsdiff > 0); ++m)
+                if (s->tri_inner[m] >= tb && s->tri_inner[m] < te) or_tri_enter(s, m);
             s->t[r] = (t + per > endtime) ? endtime : t + per;
             s->window[r] = w + 1;
             total += 1;

@@ -54,6 +54,22 @@ def load():
         lib.or_set_btab.argtypes = [P, C.POINTER(C.c_double)]
         lib.or_distribute.argtypes = [C.c_uint64, C.c_uint64, C.c_int, pf, C.c_double, pu]
         lib.or_distribute.restype = C.c_int
+        lib.or_set_surface.argtypes = [P, C.c_int, C.c_int, pi, pi, pf, C.c_int]
+        lib.or_add_sreac.argtypes = [P, C.c_int, pu, pu, pi, pi, C.c_double, C.c_double, C.c_double, C.c_int, pf]
+        lib.or_add_sreac.restype = C.c_int
+        lib.or_add_ghk.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                   C.c_int]
+        lib.or_set_temp.argtypes = [P, C.c_double]
+        lib.or_set_tri_neighbours.argtypes = [P, pi, pi, pf, pf]
+        lib.or_add_sdiff.argtypes = [P, C.c_int, C.c_int, C.c_double]
+        lib.or_set_tri_counts.argtypes = [P, C.c_int, pu]
+        lib.or_get_tri_counts.argtypes = [P, C.c_int, pu]
+        lib.or_set_tri_v.argtypes = [P, pf]
+        lib.or_get_surf_ext.argtypes = [P]
+        lib.or_get_surf_ext.restype = C.c_uint64
+        lib.or_get_echarge.argtypes = [P, C.POINTER(C.c_int64)]
+        lib.or_exp_export.argtypes = [C.c_double]
+        lib.or_exp_export.restype = C.c_double
         _lib = lib
     return _lib
 
@@ -102,6 +118,36 @@ class Oracle:
             self.L.or_add_reac(self.h, ci, _p(lhs, C.c_uint32), _p(upd, C.c_int32), k)
         for (ci, _did, s, d) in F["diffs"]:
             self.L.or_add_diff(self.h, ci, s, d)
+        sf = F.get("surf")
+        self.ntris = 0
+        if sf is not None:
+            # Membrane triangles, surface reactions (k(V) tables), GHK currents and surface
+            # diffusion, from the same tables the GPU solver receives.
+            tri_inner = np.ascontiguousarray(sf["tri_inner"], dtype=np.int32)
+            tri_patch = np.ascontiguousarray(sf["tri_patch"], dtype=np.int32)
+            self.ntris, self.nsspec = len(sf["tris"]), sf["nsspec"]
+            self._keep += [tri_inner, tri_patch, sf["tri_area"], sf["tri_nbr"], sf["tri_nbr_edge"], sf["tri_len"],
+                           sf["tri_dist"]]
+            self.L.or_set_surface(self.h, sf["nsspec"], self.ntris, _p(tri_inner, C.c_int32),
+                                  _p(tri_patch, C.c_int32), _p(sf["tri_area"], C.c_double),
+                                  len(sf["patch_names"]))
+            for (pi, _rid, (slhs, ilhs, supd, iupd), k, vdep) in sf["sreacs"]:
+                args = (self.h, pi, _p(slhs, C.c_uint32), _p(ilhs, C.c_uint32), _p(supd, C.c_int32),
+                        _p(iupd, C.c_int32))
+                if vdep is None:
+                    self.L.or_add_sreac(*args, k, 0.0, 0.0, 0, None)
+                else:
+                    vmin, dv, tab = vdep
+                    tab = np.ascontiguousarray(tab, dtype=np.float64)
+                    self.L.or_add_sreac(*args, 0.0, vmin, dv, tab.size, _p(tab, C.c_double))
+            for (pi, _gid, ss, ion, z, perm, vshift, voconc, flux) in sf["ghks"]:
+                self.L.or_add_ghk(self.h, pi, ss, ion, int(z), float(perm), float(vshift), float(voconc),
+                                  1 if flux else 0)
+            if sf["sdiffs"]:
+                self.L.or_set_tri_neighbours(self.h, _p(sf["tri_nbr"], C.c_int32), _p(sf["tri_nbr_edge"], C.c_int32),
+                                             _p(sf["tri_len"], C.c_double), _p(sf["tri_dist"], C.c_double))
+                for (pi, _did, ss, d) in sf["sdiffs"]:
+                    self.L.or_add_sdiff(self.h, pi, ss, float(d))
         self.nbnd = len(F.get("diffbound_names", []))
         if self.nbnd:
             self._keep += [F["face_bnd"], F["bnd_comps"]]
@@ -143,6 +189,26 @@ class Oracle:
     def get_counts(self, s):
         a = np.empty(self.ntets, dtype=np.uint32)
         self.L.or_get_counts(self.h, s, _p(a, C.c_uint32))
+        return a
+
+    def set_tri_counts(self, ss, row):
+        a = np.ascontiguousarray(row, dtype=np.uint32)
+        self.L.or_set_tri_counts(self.h, ss, _p(a, C.c_uint32))
+
+    def get_tri_counts(self, ss):
+        a = np.empty(self.ntris, dtype=np.uint32)
+        self.L.or_get_tri_counts(self.h, ss, _p(a, C.c_uint32))
+        return a
+
+    def set_temp(self, kelvin):
+        self.L.or_set_temp(self.h, float(kelvin))
+
+    def surf_extent(self):
+        return self.L.or_get_surf_ext(self.h)
+
+    def echarge(self):
+        a = np.empty(self.ntris, dtype=np.int64)
+        self.L.or_get_echarge(self.h, a.ctypes.data_as(C.POINTER(C.c_int64)))
         return a
 
     def set_reac_k(self, reac, real, k):
