@@ -53,13 +53,47 @@ def couple(verts_um, tets):
     return acc
 
 
+def couple_fast(verts_um, tets):
+    """The coupling of couple() for every (tet, vertex) pair at once with batched numpy
+    linear algebra (the same flux integration), as a CSR matrix (um)."""
+    X = np.asarray(verts_um, dtype=np.float64)
+    T = np.asarray(tets, dtype=np.int64)
+    others = np.array([[b for b in range(4) if b != a] for a in range(4)])   # (4, 3)
+    ve = X[T]                                      # (T, 4, 3)
+    own = np.repeat(np.arange(4)[None, :], len(T), axis=0)                   # (T, 4)
+    nb = T[:, others]                              # (T, 4, 3) vertex ids of the other three
+    m = X[nb] - ve[:, :, None, :]                  # (T, 4, 3 rows, 3)
+    m = m.reshape(-1, 3, 3)
+    swap = np.linalg.det(m) < 0.0
+    m[swap] = m[swap][:, [0, 2, 1]]
+    vmi = np.linalg.inv(m)
+    f, g = 1.0 / 12.0, 2.0 / 12.0
+    ret = np.zeros((m.shape[0], 3))
+    for ivert in range(3):
+        ip, iq, ir = ivert, (ivert + 1) % 3, (ivert + 2) % 3
+        c1 = np.cross(m[:, ip], m[:, iq])
+        c2 = np.cross(m[:, iq], m[:, ir])
+        c3 = np.cross(m[:, ir], m[:, ip])
+        vec = f * c1 + g * c2 + f * c3
+        ret += 0.5 * np.einsum("ni,nij->nj", vec, vmi)
+    ret[swap] = ret[swap][:, [0, 2, 1]]
+    rows = np.repeat(T[np.arange(len(T))[:, None], own].reshape(-1), 3)
+    cols = nb.reshape(-1)
+    n = len(X)
+    return sp.coo_matrix((ret.reshape(-1), (rows, cols)), shape=(n, n)).tocsr()
+
+
 class EFieldOracle:
-    def __init__(self, verts_m, tets, memb_tri_verts):
+    def __init__(self, verts_m, tets, memb_tri_verts, fast=False):
         self.X = np.asarray(verts_m, dtype=np.float64) * 1.0e6
         self.n = len(self.X)
-        cc = couple(self.X, np.asarray(tets))
-        rows, cols, vals = zip(*[(i, j, w) for (i, j), w in cc.items()])
-        self.CC = sp.csr_matrix((vals, (rows, cols)), shape=(self.n, self.n))
+        if fast:
+            self.CC = couple_fast(self.X, tets)
+        else:
+            cc = couple(self.X, np.asarray(tets))
+            rows, cols, vals = zip(*[(i, j, w) for (i, j), w in cc.items()])
+            self.CC = sp.csr_matrix((vals, (rows, cols)), shape=(self.n, self.n))
+        self._lu = {}
         self.area = np.zeros(self.n)
         for t in np.asarray(memb_tri_verts):
             p = self.X[t]
@@ -79,7 +113,12 @@ class EFieldOracle:
         A = sp.diags(C / dt_ms + G + ksum) - K
         free = ~self.clamped
         dv = np.zeros(self.n)
-        Af = A[free][:, free].tocsc()
-        dv[free] = spla.spsolve(Af, b[free])
+        # One factorisation per step length, clamp pattern and membrane parameters.
+        key = (dt_ms, self.clamped.tobytes(), self.cm, self.g, self.sigma)
+        lu = self._lu.get(key)
+        if lu is None:
+            lu = spla.splu(A[free][:, free].tocsc())
+            self._lu = {key: lu}
+        dv[free] = lu.solve(b[free])
         self.V = self.V + dv
         return dv

@@ -29,14 +29,18 @@
 #include <string.h>
 
 /* ------------------------------------------------------------------------- */
-/* Philox4x32-10 (Salmon et al., SC'11)                                       */
+/* Philox4x32 (Salmon et al., SC'11), 8 rounds as the reference's R123         */
 /* ------------------------------------------------------------------------- */
 typedef struct {
     uint32_t v[4];
 } or_ctr;
 
-static or_ctr or_philox(or_ctr c, uint32_t k0, uint32_t k1) {
-    for (int r = 0; r < 10; ++r) {
+/* Rounds of the stream generator: 8, as the reference's R123 (src/steps/rng/r123.hpp:76
+   Philox4x32_R<8>). */
+#define OR_PHILOX_ROUNDS 8
+
+static or_ctr or_philox_r(or_ctr c, uint32_t k0, uint32_t k1, int rounds) {
+    for (int r = 0; r < rounds; ++r) {
         uint64_t p0 = (uint64_t)0xD2511F53u * c.v[0];
         uint64_t p1 = (uint64_t)0xCD9E8D57u * c.v[2];
         or_ctr n;
@@ -51,10 +55,12 @@ static or_ctr or_philox(or_ctr c, uint32_t k0, uint32_t k1) {
     return c;
 }
 
-/* Exported for the known-answer test. */
-void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+static or_ctr or_philox(or_ctr c, uint32_t k0, uint32_t k1) { return or_philox_r(c, k0, k1, OR_PHILOX_ROUNDS); }
+
+/* Exported for the known-answer test (any round count). */
+void or_philox4x32_r(int rounds, const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
     or_ctr c = {{ctr[0], ctr[1], ctr[2], ctr[3]}};
-    or_ctr r = or_philox(c, key[0], key[1]);
+    or_ctr r = or_philox_r(c, key[0], key[1], rounds);
     memcpy(out, r.v, 16);
 }
 

@@ -46,7 +46,7 @@ def load():
         lib.or_get_diff_extent.restype = C.c_uint64
         lib.or_run.argtypes = [P, C.c_double]
         lib.or_run.restype = C.c_uint64
-        lib.or_philox4x32_10.argtypes = [pu, pu, pu]
+        lib.or_philox4x32_r.argtypes = [C.c_int, pu, pu, pu]
         lib.or_log_export.argtypes = [C.c_double]
         lib.or_log_export.restype = C.c_double
         lib.or_binom_many.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, pu]
@@ -239,12 +239,13 @@ class Oracle:
         return self.L.or_run(self.h, endtime)
 
 
-def philox(ctr, key):
+def philox(ctr, key, rounds=8):
+    """One Philox4x32 block; the streams use 8 rounds (the reference's R123)."""
     L = load()
     c = np.ascontiguousarray(ctr, dtype=np.uint32)
     k = np.ascontiguousarray(key, dtype=np.uint32)
     o = np.empty(4, dtype=np.uint32)
-    L.or_philox4x32_10(_p(c, C.c_uint32), _p(k, C.c_uint32), _p(o, C.c_uint32))
+    L.or_philox4x32_r(int(rounds), _p(c, C.c_uint32), _p(k, C.c_uint32), _p(o, C.c_uint32))
     return [int(x) for x in o]
 
 

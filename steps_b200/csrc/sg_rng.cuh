@@ -8,7 +8,7 @@
 // counters produce bit-identical samples on CPU and GPU.
 //
 // Reference behaviour replaced:
-//   * src/steps/rng/r123.cpp:43-82      Philox4x32 buffered serial stream (key 0,
+//   * src/steps/rng/r123.cpp:43-82      Philox4x32-8 buffered serial stream (key 0,
 //                                        seed in the counter) -> one independent
 //                                        counter stream per (unit, window).
 //   * src/steps/rng/rng.hpp:87-105      getUnfII / getUnfIE / getUnfEE.
@@ -30,14 +30,15 @@
 #endif
 
 // ---------------------------------------------------------------------------
-// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
-// as 1, 2, 3", SC'11).  Multipliers and Weyl constants are the published ones.
+// Philox4x32 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11), 8 rounds as the reference's generator.  Multipliers and Weyl constants are the
+// published ones.
 // ---------------------------------------------------------------------------
 #define SG_PHILOX_M0 0xD2511F53u
 #define SG_PHILOX_M1 0xCD9E8D57u
 #define SG_PHILOX_W0 0x9E3779B9u
 #define SG_PHILOX_W1 0xBB67AE85u
-#define SG_PHILOX_ROUNDS 10
+#define SG_PHILOX_ROUNDS 8  // the reference's R123 generator (src/steps/rng/r123.hpp:76, Philox4x32_R<8>)
 
 struct sg_u32x4 {
     uint32_t x, y, z, w;

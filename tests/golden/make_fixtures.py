@@ -6,7 +6,7 @@
                           tets of test/validation/API_1/validation_rd_mpi/meshes/
                           sphere_rad1_37tets.inp, the mesh of the reference's analytic
                           TetOpSplit kinetics validation (parallel_spatial_tetopsplit.py).
-  philox_kat.json         Philox4x32-10 known answers from the reference's vendored Random123
+  philox_kat.json         Philox4x32 known answers (8 and 10 rounds) from the reference's vendored Random123
                           (oracle/ref_philox_kat.c, built by oracle/build_oracle.py).
 """
 from __future__ import annotations

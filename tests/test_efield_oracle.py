@@ -58,3 +58,18 @@ def test_oracle_charges_membrane():
     dq = (ora.cm * ora.area * (ora.V - (-65.0))).sum()
     assert abs(dq - 1.0 * 20e-3) < 1e-9
     assert ora.V.mean() > v0 and total_c > 0
+
+
+def test_vectorised_coupling_equals_the_loop():
+    """couple_fast (batched over every tet and vertex) gives the coupling of couple()."""
+    from oracle.efield_oracle import couple, couple_fast
+    from steps_b200 import geom as sgeom
+
+    mesh = sgeom.kuhn_box(3, 2, 4, 1e-7)
+    X = mesh.verts * 1e6
+    cc = couple(X, mesh.tets)
+    fast = couple_fast(X, mesh.tets).tocoo()
+    got = {(int(i), int(j)): float(v) for i, j, v in zip(fast.row, fast.col, fast.data)}
+    assert set(got) == set(cc)
+    for k, v in cc.items():
+        assert abs(got[k] - v) <= 1e-12 * max(1.0, abs(v)), k

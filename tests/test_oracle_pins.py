@@ -1,7 +1,8 @@
 """Pins of the CPU oracle: known answers and distribution tests (CPU only).
 
-- Philox4x32-10 against tests/golden/philox_kat.json, produced by the reference's own
-  vendored Random123 header (src/third_party/Random123/philox.h) via oracle/ref_philox_kat.c.
+- Philox4x32 with 8 rounds (the streams, as the reference's R123) and 10 rounds against
+  tests/golden/philox_kat.json, produced by the reference's own vendored Random123 header
+  (src/third_party/Random123/philox.h) via oracle/ref_philox_kat.c.
 - The project log against math.log.
 - The binomial sampler with the chi-squared check of the reference's
   test/unit/cpp/test_rng.cpp:51-90 (same (n, p) grid, sample sizes and levels), and a
@@ -23,14 +24,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 def test_philox_known_answers():
     with open(os.path.join(HERE, "golden", "philox_kat.json")) as f:
         kat = json.load(f)
-    assert len(kat) >= 8
+    assert len(kat) >= 16
+    assert {c["rounds"] for c in kat} == {8, 10}
     for c in kat:
-        assert pyoracle.philox(c["ctr"], c["key"]) == c["out"]
+        assert pyoracle.philox(c["ctr"], c["key"], c["rounds"]) == c["out"]
 
 
 def test_philox_published_zero_vector():
     # Random123 known-answer for philox4x32_10 with zero counter and key.
-    assert pyoracle.philox([0, 0, 0, 0], [0, 0]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert pyoracle.philox([0, 0, 0, 0], [0, 0], rounds=10) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
 
 
 def test_log_matches_libm():
