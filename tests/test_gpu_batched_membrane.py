@@ -122,8 +122,11 @@ def test_split_window_equals_fused_with_membrane(steps_lib, batched):
         sim.setMembRes("membrane", 1.0 / 0.3, -0.065)
         sim.setCompSpecConc("cyto", "CB", 50e-6)
         # 50 channels of 20 pS: the explicit channel current stays stable at dt = 2 us
-        # (membrane time constant C / g ~ 13 us on this 1.28 um^2 box).
-        sim.setPatchSpecCount("memb", "C", 50)
+        # (membrane time constant C / g ~ 13 us on this 1.28 um^2 box).  Five start open,
+        # so Ca is emitted on every sample path (at -65 mV a closed channel opens about
+        # once per 4.5 ms, so from all-closed no channel may open in 100 us).
+        sim.setPatchSpecCount("memb", "C", 45)
+        sim.setPatchSpecCount("memb", "O", 5)
         sim.setVertIClamp(0, 5e-12)
         return mesh, patch, sim
 

@@ -74,8 +74,11 @@ def test_batched_512_realizations_two_windows(steps_lib):
     assert_same(sim, ora, "512 realizations after 2 windows")
 
 
-@pytest.mark.parametrize("method,rtol", [(EF_DV_CG_FP64, 1e-8), (EF_DV_CG_MIXED, 1e-6)])
-def test_efield_88k_vertices_twenty_steps(steps_lib, method, rtol):
+@pytest.mark.parametrize("method,tol,rtol", [(EF_DV_CG_FP64, 1e-12, 1e-8), (EF_DV_CG_MIXED, 1e-11, 1e-6)])
+def test_efield_88k_vertices_twenty_steps(steps_lib, method, tol, rtol):
+    """The mixed method stops on the true FP64 residual b - A x, which cannot fall much
+    below 1.3e-12 of |b| on this system (the rounding of that product), so it is held to
+    1e-11; FP64 CG stops on its recurrence residual and is run to 1e-12."""
     from oracle.efield_oracle import EFieldOracle
 
     mesh = sgeom.kuhn_box(20, 20, 200, 1e-7)
@@ -86,7 +89,7 @@ def test_efield_88k_vertices_twenty_steps(steps_lib, method, rtol):
     mdl = smodel.Model()
     smodel.Volsys("vsys", mdl)
     sim = TetOpSplit(mdl, mesh, make_rng(2), method)
-    sim.setEfieldTolerance(1e-12, 1e-4)
+    sim.setEfieldTolerance(tol, 1e-4)
     sim.setEfieldDT(1e-6)
     sim.setMembPotential("membrane", -0.065)
     sim.setMembCapac("membrane", 0.01)
