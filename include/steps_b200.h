@@ -289,7 +289,7 @@ int sg_get_profile(sg_solver* h, double* window_ms, uint64_t* windows, uint64_t*
 #define SG_NOALLOC_MAX_TETS 65536
 #define SG_NOALLOC_MAX_TET_SPECIES 262144
 #define SG_NOALLOC_MAX_REACS 64
-#define SG_NOALLOC_SCRATCH_BYTES 11021824
+#define SG_NOALLOC_SCRATCH_BYTES 11022080
 int sg_run_noalloc(int32_t ntets, int32_t nspec, int32_t nreac, uint32_t* counts, const double* vol,
                    const int32_t* neighb, const double* area, const double* dist, const uint32_t* lhs,
                    const int32_t* upd, const double* kcst, const double* dcst, uint64_t seed, double t0,

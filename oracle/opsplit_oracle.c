@@ -311,6 +311,37 @@ static uint32_t or_binom_mode(or_stream* st, uint32_t n, double p) {
     }
 }
 
+/* Up to OR_PM_MAX molecules the leave draws each molecule's fate with one uniform v: it
+   leaves when v < t1 and then takes face f when v < t1 cum_f, cum_f the cumulative face
+   probabilities of the conditional selectors c (a selector of 1 takes all that remain).
+   v < x is decided as u32 v < ceil(x 2^32).  Returns the leavers, per face in k. */
+#define OR_PM_MAX 16u
+static uint64_t or_thr(double x) { return x > 0.0 ? (uint64_t)ceil(x * 4294967296.0) : 0ull; }
+static uint32_t or_leave_molecules(or_stream* st, uint32_t n, double t1, const double c[3], uint32_t k[4]) {
+    const double c0 = c[0], c1 = c[1], c2 = c[2];
+    const double r0 = 1.0 - c0;
+    const double cum0 = c0;
+    const double cum1 = cum0 + c1 * r0;
+    const double cum2 = cum1 + c2 * (r0 * (1.0 - c1));
+    uint64_t thr[4];
+    thr[3] = or_thr(t1);
+    thr[2] = c2 >= 1.0 ? thr[3] : or_thr(t1 * cum2);
+    thr[1] = c1 >= 1.0 ? thr[3] : or_thr(t1 * cum1);
+    thr[0] = c0 >= 1.0 ? thr[3] : or_thr(t1 * cum0);
+    if (c1 >= 1.0) thr[2] = thr[3];
+    if (c0 >= 1.0) thr[1] = thr[2] = thr[3];
+    for (int f = 2; f >= 0; --f)
+        if (thr[f] > thr[f + 1]) thr[f] = thr[f + 1];
+    uint32_t below[4] = {0, 0, 0, 0};
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint64_t v = or_u32(st);
+        for (int f = 0; f < 4; ++f) below[f] += v < thr[f];
+    }
+    k[0] = below[0];
+    for (int f = 1; f < 4; ++f) k[f] = below[f] - below[f - 1];
+    return below[3];
+}
+
 static uint32_t or_binom(or_stream* st, uint32_t n, double p) {
     if (n == 0 || !(p > 0.0)) return 0;
     if (p >= 1.0) return n;
@@ -414,6 +445,15 @@ int or_distribute(uint64_t seed, uint64_t call, int n, const double* w, double x
 }
 
 /* Draw count binomials from one stream (sampler tests): out[i] = Binom(n, p). */
+/* count per-molecule leaves of n molecules from one stream: out[4 i + f] leave through face f. */
+void or_leave_many(uint64_t seed, uint32_t unit, uint32_t n, double t1, double c0, double c1, double c2,
+                   uint32_t count, uint32_t* out) {
+    or_stream st;
+    or_stream_init(&st, seed, 0u, unit, 0u, 16u);
+    const double c[3] = {c0, c1, c2};
+    for (uint32_t i = 0; i < count; ++i) or_leave_molecules(&st, n, t1, c, out + 4 * (size_t)i);
+}
+
 void or_binom_many(uint64_t seed, uint32_t unit, uint32_t n, double p, uint32_t count, uint32_t* out) {
     or_stream st;
     or_stream_init(&st, seed, 0, unit, 0, 0);
@@ -1304,13 +1344,25 @@ static void or_tri_leave(or_solver* s, int r, int m, double T, uint64_t w) {
         or_stream st;
         or_stream_init(&st, s->seed, (uint32_t)r, (uint32_t)m, w, 80u + (uint32_t)sp);
         if (frc > 0.0 && u_co(or_u32(&st)) < frc) mean_n += 1u;
-        const uint32_t Kn = or_binom(&st, mean_n, t1);
-        uint32_t rem = Kn;
-        o[0] = or_binom(&st, rem, (double)g[0]);
-        rem -= o[0];
-        o[1] = or_binom(&st, rem, (double)g[1]);
-        rem -= o[1];
-        o[2] = rem;
+        uint32_t Kn = 0;
+        if (mean_n <= OR_PM_MAX) {
+            if (mean_n > 0 && t1 > 0.0) {
+                const double c3[3] = {(double)g[0], (double)g[1], 1.0};
+                uint32_t k4[4];
+                Kn = or_leave_molecules(&st, mean_n, t1, c3, k4);
+                o[0] = k4[0];
+                o[1] = k4[1];
+                o[2] = k4[2];
+            }
+        } else {
+            Kn = or_binom(&st, mean_n, t1);
+            uint32_t rem = Kn;
+            o[0] = or_binom(&st, rem, (double)g[0]);
+            rem -= o[0];
+            o[1] = or_binom(&st, rem, (double)g[1]);
+            rem -= o[1];
+            o[2] = rem;
+        }
         if (Kn > 0) {
             s->tri_counts[ci] = pop - Kn;
 #pragma omp atomic
@@ -1418,6 +1470,7 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
         double t1 = T * (D * G);
         float gs[3] = {g[0], g[1], g[2]};
         if (or_has_bnd(s, t)) t1 = T * or_bnd_split(s, t, i, D, gs);
+        const double cs[3] = {(double)gs[0], (double)gs[1], (double)gs[2]};
         if (t1 >= 1.0) t1 = 1.0;
         uint32_t mean_n = pop;
         if (tdel[i] != 0.0) {
@@ -1428,14 +1481,22 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
             mean_n = (uint32_t)nint;
             if (frc > 0.0 && u_co(or_u32(&st)) < frc) mean_n += 1;
         }
-        uint32_t Kn = or_binom(&st, mean_n, t1);
-        if (Kn == 0) continue;
-        uint32_t rem = Kn;
-        for (int f = 0; f < 3; ++f) {
-            o[f] = or_binom(&st, rem, (double)gs[f]);
-            rem -= o[f];
+        uint32_t Kn, kk[4] = {0, 0, 0, 0};
+        if (mean_n <= OR_PM_MAX) {
+            if (mean_n == 0 || !(t1 > 0.0)) continue;
+            Kn = or_leave_molecules(&st, mean_n, t1, cs, kk);
+            if (Kn == 0) continue;
+        } else {
+            Kn = or_binom(&st, mean_n, t1);
+            if (Kn == 0) continue;
+            uint32_t rem = Kn;
+            for (int f = 0; f < 3; ++f) {
+                kk[f] = or_binom(&st, rem, cs[f]);
+                rem -= kk[f];
+            }
+            kk[3] = rem;
         }
-        o[3] = rem;
+        for (int f = 0; f < 4; ++f) o[f] = kk[f];
         if (!((clampm >> i) & 1u)) cnt[i] = pop - Kn;
         moved += Kn;
     }

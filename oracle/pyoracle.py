@@ -50,6 +50,8 @@ def load():
         lib.or_log_export.argtypes = [C.c_double]
         lib.or_log_export.restype = C.c_double
         lib.or_binom_many.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, pu]
+        lib.or_leave_many.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_uint32, pu]
         lib.or_set_boundaries.argtypes = [P, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         lib.or_set_btab.argtypes = [P, C.POINTER(C.c_double)]
         lib.or_distribute.argtypes = [C.c_uint64, C.c_uint64, C.c_int, pf, C.c_double, pu]
@@ -251,6 +253,15 @@ def philox(ctr, key, rounds=8):
 
 def log(x):
     return load().or_log_export(float(x))
+
+
+def leave_many(seed, unit, n, t1, c, count):
+    """count per-molecule leaves of n molecules (leave probability t1, conditional face
+    selectors c): [count][4] molecules per face."""
+    out = np.empty(count * 4, dtype=np.uint32)
+    load().or_leave_many(seed, unit, n, float(t1), float(c[0]), float(c[1]), float(c[2]), count,
+                         _p(out, C.c_uint32))
+    return out.reshape(count, 4)
 
 
 def binom_many(seed, unit, n, p, count):

@@ -178,6 +178,7 @@ std::vector<sg_reac> compact_reacs(int nspec, int nreac, const uint32_t* lhs, co
             r.nupd += 1;
             r.upd_mask |= 1u << i;
         }
+        r.fast = sg_reac_fast_code(&r);
         out[q] = r;
     }
     return out;

@@ -116,6 +116,7 @@ struct Solver {
     DevBuf<unsigned int> d_work;  // [2][4] work counters of the split-window kernels
     DevBuf<int32_t> d_nbr, d_comp, d_crb, d_dslot, d_dspec;
     DevBuf<double> d_tdel;                      // [D][T] split mode only
+    DevBuf<uint32_t> d_tmask;                   // [T] split mode only: species with a nonzero tdel
     // Diffusion boundaries.
     int nbnd = 0;
     std::vector<int32_t> face_bnd, bnd_comps;   // [T*4] boundary of each face or -1; [nbnd*2]
@@ -799,6 +800,7 @@ struct Solver {
         a.surf = surf_args();
         a.surf_ext = has_surf() ? d_surf_ext.p : nullptr;
         a.tdel = d_tdel.p;
+        a.tmask = d_tmask.p;
         a.diff_spec = d_dspec.p;
         a.work = d_work.p;
         if (nbnd > 0) {
@@ -880,6 +882,7 @@ struct Solver {
     bool use_split() const { return split || nsdiff > 0; }
     void ensure_split_buffers() {
         if (!d_tdel.p && ndiff > 0) d_tdel.alloc((size_t)ndiff * ntets);
+        if (!d_tmask.p && ndiff > 0) d_tmask.alloc((size_t)ntets);
     }
 
     // Grids of the dynamically scheduled split kernels: every block resident at once (warps
@@ -922,7 +925,7 @@ struct Solver {
         if (has_surf() && use_split()) {
             // Membrane models: the volume-only SSA for every other tet at the volume kernel's
             // occupancy, the SURF SSA over the membrane tet list, then the diffusion leave.
-            if (ndiff > 0 && !a.tdel) throw ProgErr("split window without its buffers");
+            if (ndiff > 0 && (!a.tdel || !a.tmask)) throw ProgErr("split window without its buffers");
             const size_t smv = smem_bytes(block, nspec, (int)reacs.size());
             const int gv = split_ssa_grid(smv, ntets);
             switch (block) {
@@ -950,7 +953,7 @@ struct Solver {
         } else if (has_surf()) {
             window_kernel<128, true><<<g, 128, sm, stream>>>(a, chk);
         } else if (use_split()) {
-            if (ndiff > 0 && !a.tdel) throw ProgErr("split window without its buffers");
+            if (ndiff > 0 && (!a.tdel || !a.tmask)) throw ProgErr("split window without its buffers");
             const int gs = split_ssa_grid(sm, ntets);
             switch (block) {
                 case 64: window_kernel<64, false, true><<<gs, 64, sm, stream>>>(a, chk); break;
@@ -1984,6 +1987,7 @@ int sg_add_reac(sg_solver* h, int32_t comp, const uint32_t* lhs, const int32_t* 
             r.nupd += 1;
             r.upd_mask |= 1u << i;
         }
+        r.fast = sg_reac_fast_code(&r);
         s->reacs.push_back(r);
         s->reac_kdef.push_back(kcst);
         if (out_idx) *out_idx = (int32_t)s->reacs.size() - 1;

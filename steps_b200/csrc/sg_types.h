@@ -32,7 +32,39 @@ typedef struct sg_reac {
     int32_t upd_delta[SG_MAX_UPD];     // signed change
     uint32_t lhs_mask;                 // bit per reactant species (propensity dependencies)
     uint32_t upd_mask;                 // bit per changed species
+    uint32_t fast;                     // propensity form: kind | first species << 8 | second << 16
 } sg_reac;
+
+// Propensity forms with a closed count product (order <= 2); everything else takes the
+// general product.  The product of the counts is formed exactly in 64-bit integers and
+// rounded once to double, which is the value the reference's double product gives
+// (src/steps/mpi/tetopsplit/reac.cpp:184-232: the factors are exact, one rounding).
+#define SG_RK_ZERO 0u                  // no reactant: h = 1
+#define SG_RK_ONE 1u                   // A: h = c_A
+#define SG_RK_PAIR 2u                  // A + B, A != B: h = c_A c_B
+#define SG_RK_DIMER 3u                 // 2 A: h = c_A (c_A - 1)
+#define SG_RK_GENERIC 4u               // order 3 or 4: the general product
+
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+static inline uint32_t sg_reac_fast_code(const sg_reac* r) {
+    uint32_t kind = SG_RK_GENERIC, a = 0u, b = 0u;
+    if (r->nlhs == 0) {
+        kind = SG_RK_ZERO;
+    } else if (r->nlhs == 1 && r->lhs_ord[0] == 1) {
+        kind = SG_RK_ONE;
+        a = (uint32_t)r->lhs_spec[0];
+    } else if (r->nlhs == 1 && r->lhs_ord[0] == 2) {
+        kind = SG_RK_DIMER;
+        a = (uint32_t)r->lhs_spec[0];
+    } else if (r->nlhs == 2 && r->lhs_ord[0] == 1 && r->lhs_ord[1] == 1) {
+        kind = SG_RK_PAIR;
+        a = (uint32_t)r->lhs_spec[0];
+        b = (uint32_t)r->lhs_spec[1];
+    }
+    return kind | (a << 8) | (b << 16);
+}
 
 // One surface reaction of a patch (Patchdef sreac_lhs_S/I, sreac_upd_S/I,
 // src/steps/solver/patchdef.hpp), optionally with a voltage-dependent constant
@@ -157,12 +189,15 @@ typedef struct sg_window_args {
     sg_surf_args surf;                 // membrane triangles (SURF kernels only)
     unsigned long long* surf_ext;      // [1] surface reaction events since reset
     double* tdel;                      // [D][T] change-time sums handed to the diffusion kernel (split mode)
+    uint32_t* tmask;                   // [T] split mode: bit s set when tdel of species s is nonzero
+                                       // (tdel is written only for those species)
     const int32_t* diff_spec;          // [D]: species of each diffusing index
     const int32_t* tet_list;           // [nlist] tets of this launch, or null for all tets
     int32_t nlist;
     // Work counters of the split-window kernels, [2][4] by launch parity: the next chunk
-    // of 32 tets for the volume SSA (0), the membrane SSA (1) and the diffusion leave (2).
-    // Each window's last block zeroes the next parity's counters.  Null: static schedule.
+    // of 32 tets for the volume SSA (0), the membrane SSA (1) and the diffusion leave (2)
+    // (3 unused).  Each window's last block zeroes the next parity's counters.  Null:
+    // static schedule.
     unsigned int* work;
     // Diffusion boundaries (diffboundary.cpp, diff.cpp:307-398), null without any: per tet
     // the boundary of each face (byte f, 0xFF = none), the neighbour behind boundary faces

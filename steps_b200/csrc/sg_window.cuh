@@ -48,6 +48,30 @@ __device__ __forceinline__ double reac_prop(const sg_reac* rc, const uint32_t* s
     return h * ccst;
 }
 
+// h_mu * ccst through the reaction's closed form (sg_reac::fast); equal bit for bit to
+// reac_prop for every count: the exact integer product rounded once is the value of the
+// reference's double product of exact factors, and a zero factor gives +0 in both.
+__device__ __forceinline__ double reac_prop_fast(const sg_reac* rc, const uint32_t* sc, int stride, double ccst) {
+    const uint32_t code = rc->fast;
+    const uint32_t kind = code & 0xFFu;
+    if (kind == SG_RK_GENERIC) return reac_prop(rc, sc, stride, ccst);
+    unsigned long long h = 1ull;
+    if (kind != SG_RK_ZERO) {
+        const uint32_t ca = sc[((code >> 8) & 0xFFu) * stride];
+        uint32_t cb = 1u;
+        if (kind == SG_RK_PAIR) cb = sc[(code >> 16) * stride];
+        else if (kind == SG_RK_DIMER) cb = ca - 1u;  // ca = 0 wraps, and 0 * cb = 0
+        h = (unsigned long long)ca * cb;
+    }
+    return (double)h * ccst;
+}
+
+// Margin of the first waiting-time test: with x = a0 T, (1 - u) > x (1 + 2^-40) implies
+// -log(u) / a0 > T as the full computation rounds it (-log u >= 1 - u; the project log is
+// within a few ulp and the division and the products round by 2^-53 each), so the log and
+// the division can be skipped without changing any outcome.
+#define SG_SQUEEZE 1.0000000000009095  // 1 + 2^-40
+
 __device__ __forceinline__ int find_real(const sg_real* reals, int nreal, int t) {
     if (nreal == 1) return 0;
     int lo = 0, hi = nreal - 1;
@@ -153,12 +177,15 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
         double a0 = 0.0;
         for (int q = rb; q < re; ++q) {
             const sg_reac* rc = &L.reac[q];
-            if (rc->lhs_mask & changed) sp[q * BLOCK] = reac_prop(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
-            else if (changed == 0xFFFFFFFFu) sp[q * BLOCK] = reac_prop(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
+            if ((rc->lhs_mask & changed) || changed == 0xFFFFFFFFu)
+                sp[q * BLOCK] = reac_prop_fast(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
             a0 = a0 + sp[q * BLOCK];
         }
         if (!(a0 > 0.0)) break;
-        double dt = -sg_log(sg_u01_oc(sg_next_u32(st))) / a0;
+        const double u = sg_u01_oc(sg_next_u32(st));
+        // First draw of the window: most units see no event, decided without the log.
+        if (tt == 0.0 && 1.0 - u > (a0 * T) * SG_SQUEEZE) break;
+        double dt = -sg_log(u) / a0;
         if (tt + dt > T) break;
         tt = tt + dt;
         double target = sg_u01_co(sg_next_u32(st)) * a0;
@@ -194,6 +221,57 @@ __device__ __forceinline__ void tet_ssa(const sg_window_args& a, const smem_layo
         }
         atomicAdd(&L.ext[sel], 1u);
     }
+}
+
+// First pass of a split window's SSA: the tet's total propensity and its first draw.
+// False when that draw shows, by the squeeze of tet_ssa, that no event falls in the window
+// (the tet's SSA is then complete); true when the tet has to run tet_ssa, which sums the
+// same propensities in the same order and redraws the same first uniform.
+__device__ __forceinline__ bool tet_may_fire(const smem_layout& L, int tid, int BLOCK, int rb, int re,
+                                             const double* K, double ivs, double T, sg_stream* st) {
+    const uint32_t* sc = L.cnt + tid;
+    double a0 = 0.0;
+    for (int q = rb; q < re; ++q) {
+        const sg_reac* rc = &L.reac[q];
+        a0 = a0 + reac_prop_fast(rc, sc, BLOCK, reac_ccst(rc, __ldg(&K[q]), ivs));
+    }
+    if (!(a0 > 0.0)) return false;
+    const double u = sg_u01_oc(sg_next_u32(st));
+    return !(1.0 - u > (a0 * T) * SG_SQUEEZE);
+}
+
+// Whole SSA of tet t from its gathered counts (stored in counts by the first pass), with
+// its stream restarted, so the draws are the ones the first pass took; then its counts,
+// the nonzero change-time sums of its diffusing species and tmask.
+__device__ __forceinline__ void tet_ssa_queued(const sg_window_args& a, const smem_layout& L, int tid, int BLOCK,
+                                               int t) {
+    const int S = a.nspec;
+    const int r = find_real(a.reals, a.nreal, t);
+    const sg_real* rl = &a.reals[r];
+    const double rt = rl->t, rend = rl->t_end, per = rl->period;
+    const double T = (rt + per > rend) ? rend - rt : per;
+    const unsigned long long w = rl->window;
+    const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
+    const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
+    for (int s = 0; s < S; ++s) {
+        L.cnt[s * BLOCK + tid] = a.counts[(size_t)s * a.ntets + t];
+        L.tdel[s * BLOCK + tid] = 0.0;
+    }
+    sg_stream st;
+    sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)(t - rl->tet_begin), w, SG_PURPOSE_WINDOW);
+    tet_ssa(a, L, tid, BLOCK, __ldg(&a.comp_reac_begin[comp]), __ldg(&a.comp_reac_begin[comp + 1]),
+            a.kcst + (size_t)r * a.nreac, __ldg(&a.ivs[t]), clampm, T, &st);
+    uint32_t tm = 0u;
+    for (int s = 0; s < S; ++s) {
+        const int ds = __ldg(&a.diff_slot[s]);
+        const double sdv = L.tdel[s * BLOCK + tid];
+        if (ds >= 0 && sdv != 0.0) {
+            a.tdel[(size_t)ds * a.ntets + t] = sdv;
+            tm |= 1u << s;
+        }
+        a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
+    }
+    if (a.tmask) a.tmask[t] = tm;
 }
 
 // SSA of a unit made of a tet and up to four membrane triangles (inner tet = this tet):
@@ -421,9 +499,9 @@ static __device__ __noinline__ void tet_ssa_surf(const sg_window_args& a, const 
     }
 }
 
-__device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, double t1, float4 g, double odd1,
-                                             double odd2, double odd3, const double* rcp, const double* rcpl,
-                                             const double* lnf, uint32_t* out_kn);
+__device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, double t1, double c0, double c1,
+                                             double c2, double odd1, double odd2, double odd3, const double* rcp,
+                                             const double* rcpl, const double* lnf, uint32_t* out_kn);
 
 // Inflow of species s through the diffusion-boundary faces of tet t (slots v.f of the tet's
 // own inflow): counted when the tet behind face f diffuses s, because that tet then wrote
@@ -509,9 +587,9 @@ __device__ __forceinline__ void bnd_scatter(const sg_window_args& a, int t, uint
 // depend on the SSA's draws, on the other species or on which kernel runs it.
 __device__ __forceinline__ uint4 leave_species(uint64_t seed, uint32_t real, uint32_t unit, unsigned long long w,
                                                uint32_t s, uint32_t pop, double sd, double invT, double t1,
-                                               float4 g, double odd1, double odd2, double odd3, const double* rcp,
-                                               const double* rcpl, const double* lnf, sg_stream* st,
-                                               uint32_t* out_kn) {
+                                               const double* c, double odd1, double odd2, double odd3,
+                                               const double* rcp, const double* rcpl, const double* lnf,
+                                               sg_stream* st, uint32_t* out_kn) {
     sg_stream_init(st, seed, real, unit, w, SG_PURPOSE_DIFF + s);
     if (t1 >= 1.0) t1 = 1.0;
     uint32_t mean_n = pop;
@@ -525,14 +603,66 @@ __device__ __forceinline__ uint4 leave_species(uint64_t seed, uint32_t real, uin
             if (sg_u01_co(sg_next_u32(st)) < frc) mean_n += 1u;
         }
     }
-    return leave_split(st, mean_n, t1, g, odd1, odd2, odd3, rcp, rcpl, lnf, out_kn);
+    return leave_split(st, mean_n, t1, c[0], c[1], c[2], odd1, odd2, odd3, rcp, rcpl, lnf, out_kn);
+}
+
+// Below this many molecules the leave draws each molecule's fate (stay, or which face)
+// instead of four binomials: the reference's own per-molecule direction draws for small
+// counts (diff.cpp:473-512), with the leaving draw folded into the same uniform.
+#define SG_PM_MAX 16u
+
+// Threshold of a probability x in [0, 1] for a 32-bit draw v: v < sg_thr(x) exactly when
+// v 2^-32 < x (the scaling by 2^32 is exact).
+__host__ __device__ __forceinline__ uint64_t sg_thr(double x) {
+    return x > 0.0 ? (uint64_t)ceil(x * 4294967296.0) : 0ull;
+}
+
+// Per-molecule leave of n <= SG_PM_MAX molecules with 0 < t1 <= 1: one uniform v per
+// molecule; it leaves when v < t1 and then takes face f when v < t1 cum_f, cum_f the
+// cumulative face probabilities of the conditional selectors (a selector of 1 sends all
+// that remain to its face).  The joint law is the multinomial of Binomial(n, t1) and the
+// conditional face binomials.
+__device__ __forceinline__ uint4 leave_molecules(sg_stream* st, uint32_t n, double t1, double c0, double c1,
+                                                 double c2, uint32_t* out_kn) {
+    const double r0 = 1.0 - c0;
+    const double cum0 = c0;
+    const double cum1 = cum0 + c1 * r0;
+    const double cum2 = cum1 + c2 * (r0 * (1.0 - c1));
+    const uint64_t T3 = sg_thr(t1);
+    uint64_t T2 = (c2 >= 1.0) ? T3 : sg_thr(t1 * cum2);
+    uint64_t T1 = (c1 >= 1.0) ? T3 : sg_thr(t1 * cum1);
+    uint64_t T0 = (c0 >= 1.0) ? T3 : sg_thr(t1 * cum0);
+    if (c1 >= 1.0) T2 = T3;
+    if (c0 >= 1.0) T1 = T2 = T3;
+    T2 = T2 < T3 ? T2 : T3;
+    T1 = T1 < T2 ? T1 : T2;
+    T0 = T0 < T1 ? T0 : T1;
+    uint32_t a0 = 0u, a1 = 0u, a2 = 0u, a3 = 0u;
+#pragma unroll 1
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint64_t v = sg_next_u32(st);
+        a0 += v < T0 ? 1u : 0u;
+        a1 += v < T1 ? 1u : 0u;
+        a2 += v < T2 ? 1u : 0u;
+        a3 += v < T3 ? 1u : 0u;
+    }
+    *out_kn = a3;
+    return make_uint4(a0, a1 - a0, a2 - a1, a3 - a2);
 }
 
 // Binomial(mean_n, t1) molecules leave, split over the directions by conditional
-// binomials on the selectors g.x, g.y, g.z; the last direction takes the rest.
-__device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, double t1, float4 g, double odd1,
-                                             double odd2, double odd3, const double* rcp, const double* rcpl,
-                                             const double* lnf, uint32_t* out_kn) {
+// binomials on the selectors g.x, g.y, g.z; the last direction takes the rest.  Up to
+// SG_PM_MAX molecules, molecule by molecule (leave_molecules).
+__device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, double t1, double c0, double c1,
+                                             double c2, double odd1, double odd2, double odd3, const double* rcp,
+                                             const double* rcpl, const double* lnf, uint32_t* out_kn) {
+    if (mean_n <= SG_PM_MAX) {
+        if (mean_n == 0u || !(t1 > 0.0)) {
+            *out_kn = 0u;
+            return make_uint4(0u, 0u, 0u, 0u);
+        }
+        return leave_molecules(st, mean_n, t1 < 1.0 ? t1 : 1.0, c0, c1, c2, out_kn);
+    }
     // Stage 0: molecules leaving; stages 1-3: the split.  One sampler call site.
     uint4 k = make_uint4(0u, 0u, 0u, 0u);
     uint32_t n = mean_n, Kn = 0u;
@@ -544,17 +674,17 @@ __device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, dou
         if (stage == 0) {
             Kn = v;
             n = v;
-            pst = (double)g.x;
+            pst = c0;
             ost = odd1;
         } else if (stage == 1) {
             k.x = v;
             n -= v;
-            pst = (double)g.y;
+            pst = c1;
             ost = odd2;
         } else if (stage == 2) {
             k.y = v;
             n -= v;
-            pst = (double)g.z;
+            pst = c2;
             ost = odd3;
         } else {
             k.z = v;
@@ -646,6 +776,9 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     window_kernel(sg_window_args a, int check) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double s_rcp[SG_RCP_TABLE];
+    // Volume pass of a split window: per warp, up to 63 tets whose first draw may fall in
+    // the window wait here and run their SSA 32 at a time (all lanes busy with events).
+    __shared__ int s_q[(SPLIT && !SURF) ? 2 * BLOCK : 1];
     const int S = a.nspec;
     const int R = a.nreac;
     const int tid = threadIdx.x;
@@ -669,11 +802,20 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     // warp whose tets drew few events moves on instead of idling until its block ends.
     unsigned int* wctr = (SPLIT && a.work) ? a.work + parity * 4 + (SURF ? 1 : 0) : nullptr;
 
+    int* wq = s_q + (SPLIT && !SURF ? (tid & ~31) * 2 : 0);  // this warp's queue
+    int qn = 0;                                                 // its length (warp-uniform)
+
     // A tet list (split windows of membrane models) restricts the launch to those tets.
     const int nit = a.tet_list ? a.nlist : a.ntets;
     for (int it = 0;; ++it) {
         const int base = next_warp_base(wctr, it, BLOCK);
-        if (base >= nit) break;
+        if (base >= nit) {
+            if (SPLIT && !SURF) {
+                __syncwarp();
+                if (lane < qn) tet_ssa_queued(a, L, tid, BLOCK, wq[lane]);
+            }
+            break;
+        }
         bool active = base + lane < nit;
         const int t = !active ? 0 : (a.tet_list ? __ldg(&a.tet_list[base + lane]) : base + lane);
         int r = 0, comp = 0, tlocal = 0;
@@ -733,6 +875,31 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             const unsigned long long v = warp_total_u32(c);
             if (lane == 0 && v) atomicAdd(&L.tot[s], v);
         }
+        if (SPLIT && !SURF) {
+            // First draw only; tets that may see an event join the warp's queue.
+            bool fire = false;
+            if (active) {
+                const int rb = __ldg(&a.comp_reac_begin[comp]);
+                const int re = __ldg(&a.comp_reac_begin[comp + 1]);
+                if (re > rb) {
+                    sg_stream st;
+                    sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)tlocal, w, SG_PURPOSE_WINDOW);
+                    fire = tet_may_fire(L, tid, BLOCK, rb, re, a.kcst + (size_t)r * R, __ldg(&a.ivs[t]), T, &st);
+                }
+                for (int s = 0; s < S; ++s) a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
+                if (!fire && a.tmask) a.tmask[t] = 0u;  // no change-time sums
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, fire);
+            if (fire) wq[qn + __popc(bal & ((1u << lane) - 1u))] = t;
+            qn += __popc(bal);
+            if (qn >= 32) {
+                __syncwarp();
+                tet_ssa_queued(a, L, tid, BLOCK, wq[qn - 32 + lane]);
+                qn -= 32;
+                __syncwarp();
+            }
+            continue;
+        }
         if (!active) continue;
 
         sg_stream st;
@@ -754,19 +921,29 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
         }
 
         if (SPLIT) {
+            // Counts, and the change-time sums of the diffusing species that changed (their
+            // bits in tmask; the leave reads the others as zero).
+            uint32_t tm = 0u;
             for (int s = 0; s < S; ++s) {
                 const int ds = __ldg(&a.diff_slot[s]);
-                if (ds >= 0) a.tdel[(size_t)ds * a.ntets + t] = L.tdel[s * BLOCK + tid];
+                const double sdv = L.tdel[s * BLOCK + tid];
+                if (ds >= 0 && sdv != 0.0) {
+                    a.tdel[(size_t)ds * a.ntets + t] = sdv;
+                    tm |= 1u << s;
+                }
                 a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
             }
+            if (a.tmask) a.tmask[t] = tm;
             continue;
         }
         // Phase 3: diffusion leave, one (tet, species) at a time.
         const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
-        // Odds ratios of the three face selectors, once per tet instead of once per draw.
-        const double odd1 = sg_binom_odds((double)g.x);
-        const double odd2 = sg_binom_odds((double)g.y);
-        const double odd3 = sg_binom_odds((double)g.z);
+        const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
+        // The face selectors and their odds, once per tet.
+        const double cs[3] = {(double)g.x, (double)g.y, (double)g.z};
+        const double odd1 = sg_binom_odds(cs[0]);
+        const double odd2 = sg_binom_odds(cs[1]);
+        const double odd3 = sg_binom_odds(cs[2]);
         uint32_t* out = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane;
         const double invT = 1.0 / T;  // one division per tet for the occupancy means
         for (int s = 0; s < S; ++s) {
@@ -776,27 +953,28 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             if (!(D > 0.0)) continue;
             uint32_t pop = L.cnt[s * BLOCK + tid];
             uint4 k = make_uint4(0u, 0u, 0u, 0u);
-            const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
             if (pop > 0u) {
                 uint32_t Kn = 0u;
                 if (bt) {
+                    // Diffusion-boundary tet: face rates, and so selectors, per species.
                     float4 gb;
                     const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
+                    const double cb[3] = {(double)gb.x, (double)gb.y, (double)gb.z};
                     k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
-                                      invT, T * tot, gb, sg_binom_odds((double)gb.x), sg_binom_odds((double)gb.y),
-                                      sg_binom_odds((double)gb.z), s_rcp, nullptr, nullptr, &st, &Kn);
+                                      invT, T * tot, cb, sg_binom_odds(cb[0]), sg_binom_odds(cb[1]),
+                                      sg_binom_odds(cb[2]), s_rcp, nullptr, nullptr, &st, &Kn);
                 } else {
                     k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
-                                      invT, T * (D * (double)g.w), g, odd1, odd2, odd3, s_rcp, nullptr, nullptr, &st,
-                                      &Kn);
+                                      invT, T * (D * (double)g.w), cs, odd1, odd2, odd3, s_rcp, nullptr, nullptr,
+                                      &st, &Kn);
                 }
                 if (Kn > 0u) {
                     if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
                     moved += Kn;
                 }
             }
-            // Scatter into the receiving tets' slots: nb.f = (neighbour << 2) | its face,
-            // i.e. the word index inside this species' plane.  Each slot has one writer.
+            // Scatter into the receiving tets' slots: nb.f = (neighbour << 2) | its face, i.e.
+            // the word index inside this species' plane.  Each slot has one writer.
             uint32_t* po = out + (size_t)ds * plane;
             if (nb.x >= 0) po[nb.x] = k.x;
             if (nb.y >= 0) po[nb.y] = k.y;
@@ -873,11 +1051,13 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
         const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
         const double* Dc = a.dcst + ((size_t)r * a.ncomp + comp) * S;
         uint32_t* out = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane;
-        // Odds of the three face selectors and 1/T, once per tet.
-        const double odd1 = sg_binom_odds((double)g.x);
-        const double odd2 = sg_binom_odds((double)g.y);
-        const double odd3 = sg_binom_odds((double)g.z);
+        // The face selectors and their odds, once per tet.
+        const double cs[3] = {(double)g.x, (double)g.y, (double)g.z};
+        const double odd1 = sg_binom_odds(cs[0]);
+        const double odd2 = sg_binom_odds(cs[1]);
+        const double odd3 = sg_binom_odds(cs[2]);
         const double invT = 1.0 / T;
+        const uint32_t tm = a.tmask ? a.tmask[t] : 0u;
         for (int s = 0; s < S; ++s) {
             const int ds = __ldg(&a.diff_slot[s]);
             if (ds < 0) continue;
@@ -889,16 +1069,18 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
             if (pop > 0u) {
                 sg_stream st;
                 uint32_t Kn = 0u;
-                const double sd = a.tdel[(size_t)ds * a.ntets + t];
+                const double sd = ((tm >> s) & 1u) ? a.tdel[(size_t)ds * a.ntets + t] : 0.0;
                 if (bt) {
+                    // Diffusion-boundary tet: face rates, and so selectors, per species.
                     float4 gb;
                     const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
-                    k = leave_species(a.seed, (uint32_t)r, tl, w, (uint32_t)s, pop, sd, invT, T * tot, gb,
-                                      sg_binom_odds((double)gb.x), sg_binom_odds((double)gb.y),
-                                      sg_binom_odds((double)gb.z), s_rcp, s_rcpl, s_lnf, &st, &Kn);
+                    const double cb[3] = {(double)gb.x, (double)gb.y, (double)gb.z};
+                    k = leave_species(a.seed, (uint32_t)r, tl, w, (uint32_t)s, pop, sd, invT, T * tot, cb,
+                                      sg_binom_odds(cb[0]), sg_binom_odds(cb[1]), sg_binom_odds(cb[2]), s_rcp,
+                                      s_rcpl, s_lnf, &st, &Kn);
                 } else {
                     k = leave_species(a.seed, (uint32_t)r, tl, w, (uint32_t)s, pop, sd, invT, T * (D * (double)g.w),
-                                      g, odd1, odd2, odd3, s_rcp, s_rcpl, s_lnf, &st, &Kn);
+                                      cs, odd1, odd2, odd3, s_rcp, s_rcpl, s_lnf, &st, &Kn);
                 }
                 if (Kn > 0u) {
                     if (!((clampm >> s) & 1u)) a.counts[ci] = pop - Kn;
@@ -969,7 +1151,8 @@ __global__ void __launch_bounds__(BLOCK) sdiffuse_kernel(sg_window_args a) {
                 if (sg_u01_co(sg_next_u32(&st)) < frc) mean_n += 1u;
             }
             uint32_t Kn = 0u;
-            k = leave_split(&st, mean_n, t1, g, sg_binom_odds((double)g.x), sg_binom_odds((double)g.y), 0.0, s_rcp,
+            k = leave_split(&st, mean_n, t1, (double)g.x, (double)g.y, (double)g.z, sg_binom_odds((double)g.x),
+                            sg_binom_odds((double)g.y), 0.0, s_rcp,
                             nullptr, nullptr, &Kn);
             if (Kn > 0u) {
                 sa.tri_counts[ci] = pop - Kn;

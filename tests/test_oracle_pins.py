@@ -72,10 +72,11 @@ def test_binomial_reference_grid_rejects_wrong(t_test, p_test):
 @pytest.mark.parametrize("n,p", [(10, 0.3), (40, 0.2), (1000, 0.3), (200, 0.93), (5000, 0.5),
                                  (1 << 20, 3e-6), (60, 0.999), (4000000000, 2e-9), (25, 0.4),
                                  (47, 0.5), (120, 0.19), (49, 0.5), (95, 0.5), (95, 0.75), (60, 0.45),
-                                 (400, 0.5), (2100, 0.47), (2150, 0.47), (48, 0.999)])
+                                 (400, 0.5), (2100, 0.47), (2150, 0.47), (48, 0.999), (3, 0.13),
+                                 (1, 0.5), (2, 0.71), (95, 0.0083), (1 << 30, 5e-9)])
 def test_binomial_goodness_of_fit(n, p):
-    """BINV below n min(p, 1-p) = 24, the search from the mode up to 1000, BTRD above,
-    against the exact binomial pmf."""
+    """BINV below n min(p, 1-p) = 24 (down to a single trial and n p far below 1), the
+    search from the mode up to 1000, BTRD above, against the exact binomial pmf."""
     m = 200000
     x = pyoracle.binom_many(777, n % 1000, n, p, m).astype(np.int64)
     mean, var = n * p, n * p * (1 - p)
@@ -96,7 +97,7 @@ def test_binomial_goodness_of_fit(n, p):
     assert stats.chi2.sf(chi, dof) > 1e-4, (n, p, chi, dof)
 
 
-@pytest.mark.parametrize("n,p", [(12, 0.25), (37, 0.33), (25, 0.5)])
+@pytest.mark.parametrize("n,p", [(12, 0.25), (37, 0.33), (25, 0.5), (48, 0.145), (41, 0.415)])
 def test_binv_large_sample(n, p):
     """The BINV search at the face-split sizes of the benchmark, 4 M draws: chi-squared over
     every outcome with expectation >= 5."""
@@ -115,3 +116,47 @@ def test_binomial_edges():
     assert (pyoracle.binom_many(1, 0, 17, 1.0, 10) == 17).all()
     x = pyoracle.binom_many(1, 0, 3, 0.9999999, 1000)
     assert x.max() <= 3
+
+
+@pytest.mark.parametrize("n,t1,c", [(5, 0.6, (0.145, 0.415, 0.29)), (16, 1.0, (0.355, 0.225, 0.5)),
+                                    (3, 0.133, (0.145, 0.415, 0.71)), (7, 0.9, (0.0, 1.0, 0.0)),
+                                    (4, 0.5, (0.2, 0.25, 1.0))])
+def test_per_molecule_leave_law(n, t1, c):
+    """The per-molecule leave of small counts against the multinomial it replaces: stay with
+    1 - t1, face f with t1 s_f (s_f from the conditional selectors, a selector of 1 taking
+    all that remain), chi-squared over every joint outcome with expectation >= 5."""
+    from math import comb
+    m = 400000
+    k = pyoracle.leave_many(2024, n, n, t1, c, m).astype(np.int64)
+    s0 = c[0]
+    s1 = (1 - c[0]) * c[1]
+    s2 = (1 - c[0]) * (1 - c[1]) * c[2]
+    s3 = 1 - s0 - s1 - s2
+    probs = [t1 * s0, t1 * s1, t1 * s2, t1 * s3, 1 - t1]
+    assert (k.sum(axis=1) <= n).all()
+    for f, sf in enumerate((s0, s1, s2, s3)):
+        if sf == 0:
+            assert (k[:, f] == 0).all()
+    keys = k[:, 0] * (n + 1) ** 3 + k[:, 1] * (n + 1) ** 2 + k[:, 2] * (n + 1) + k[:, 3]
+    uniq, obs = np.unique(keys, return_counts=True)
+    expd = {}
+    for a in range(n + 1):
+        for b in range(n + 1 - a):
+            for d in range(n + 1 - a - b):
+                for e in range(n + 1 - a - b - d):
+                    rest = n - a - b - d - e
+                    pr = comb(n, a) * comb(n - a, b) * comb(n - a - b, d) * comb(n - a - b - d, e)
+                    pr *= probs[0] ** a * probs[1] ** b * probs[2] ** d * probs[3] ** e * probs[4] ** rest
+                    if pr > 0:
+                        expd[a * (n + 1) ** 3 + b * (n + 1) ** 2 + d * (n + 1) + e] = pr
+    assert set(uniq.tolist()) <= set(expd)
+    ob = dict(zip(uniq.tolist(), obs.tolist()))
+    big = [key for key, pr in expd.items() if pr * m >= 5]
+    chi = sum((ob.get(key, 0) - m * expd[key]) ** 2 / (m * expd[key]) for key in big)
+    rest_e = m * (1 - sum(expd[key] for key in big))
+    rest_o = m - sum(ob.get(key, 0) for key in big)
+    dof = len(big) - 1
+    if rest_e >= 5:
+        chi += (rest_o - rest_e) ** 2 / rest_e
+        dof += 1
+    assert stats.chi2.sf(chi, max(dof, 1)) > 1e-4, (chi, dof)
