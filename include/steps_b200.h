@@ -213,6 +213,13 @@ int sg_get_efield_check(sg_solver* h, uint64_t* steps, double* max_rel, double* 
 /* EField solve form: 1 = every CG iteration inside one cooperative launch (grid barriers
  * between the phases), 0 = three kernel launches per iteration. */
 int sg_set_efield_persistent(sg_solver* h, int32_t on);
+/* Polls of one grid-barrier wait (about 100 ns each) after which the persistent EField
+ * solve gives up: the launch ends and the step returns SG_EDEVICE ("a grid barrier wait
+ * timed out"), with the device left usable.  Default 2^22 (about half a second).  No
+ * counterpart in the reference (whose solve has no device-side waits); small values make
+ * the error path testable. */
+int sg_set_efield_barrier_limit(sg_solver* h, uint32_t polls);
+
 /* Mixed method with the persistent solve: one FP32 CG with reliable updates (on, default;
  * the FP64 residual b - A x replaces the FP32 one whenever the FP32 residual norm has
  * fallen by the factor delta, default 0.1, since the last replacement) or restarted FP32

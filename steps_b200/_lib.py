@@ -122,6 +122,7 @@ PROTOTYPES = {
     "sg_get_efield_stats": [_P, _pu64, _pu64, _pf64, _pf64],
     "sg_set_efield_check": [_P, _i32, _f64],
     "sg_set_efield_persistent": [_P, _i32],
+    "sg_set_efield_barrier_limit": [_P, _u32],
     "sg_set_efield_reliable_updates": [_P, _i32, _f64],
     "sg_get_efield_check": [_P, _pu64, _pf64, _pf64],
     "sg_get_stream": [_P, C.POINTER(_P)],

@@ -573,7 +573,8 @@ __global__ void precond_kernel(Segs sg, Coarse cs, const double* diag, const T* 
 // partials in the same order, so all blocks take identical decisions without a second
 // barrier.  Vectors written by other blocks inside the launch are read with __ldcg (L2),
 // never from a stale L1 line.  The barrier waits are bounded: a block that waits longer
-// than kSpinLimit polls sets bar[2] and every block leaves at its next barrier.
+// than the solve's poll limit (kSpinLimit unless set otherwise) sets bar[2] and every block
+// leaves at its next barrier.
 // ---------------------------------------------------------------------------
 constexpr unsigned int kSpinLimit = 1u << 22;  // x ~100 ns polls: about half a second
 // The persistent solve is launched with at most 2048 blocks (3 x 2048 reduction partials
@@ -596,7 +597,8 @@ __device__ __forceinline__ void st_release_gpu(unsigned int* p, unsigned int v) 
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, unsigned int& gen) {
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, unsigned int& gen,
+                                             unsigned int limit) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned int g = gen;
@@ -606,7 +608,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
         } else {
             unsigned int spins = 0;
             while (ld_acquire_gpu(&bar[1]) == g) {
-                if (++spins > kSpinLimit) {
+                if (++spins > limit) {
                     atomicOr(&bar[2], 1u);
                     break;
                 }
@@ -622,7 +624,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
 // Block partial of v -> partials[blockIdx]; barrier; the sum over all blocks in block
 // order (thread-strided, fixed shuffle tree, warps in order), the same in every block.
 __device__ __forceinline__ bool grid_sum(double v, double* partials, unsigned int* bar, unsigned int& gen,
-                                         double* out) {
+                                         unsigned int limit, double* out) {
     __shared__ double sh[kBlock / 32];
     __shared__ double tot;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -634,7 +636,7 @@ __device__ __forceinline__ bool grid_sum(double v, double* partials, unsigned in
         for (int w = 0; w < kBlock / 32; ++w) s += sh[w];
         partials[blockIdx.x] = s;
     }
-    if (!grid_barrier(bar, gridDim.x, gen)) return false;
+    if (!grid_barrier(bar, gridDim.x, gen, limit)) return false;
     double a = 0.0;
     for (int b = threadIdx.x; b < (int)gridDim.x; b += kBlock) a += __ldcg(&partials[b]);
     for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
@@ -664,6 +666,7 @@ struct PcgArgs {
     double* partials;  // [3][gridDim]
     double* scal;
     unsigned int* bar;  // count, generation, error
+    unsigned int spin_limit;  // polls of a barrier wait before the solve gives up
     // Reliable updates (FP32 solve of the FP64 system, T = float only): x is the FP32
     // correction accumulated since the last update; when the FP32 residual norm has fallen
     // by delta2 from its largest value since the last update (or below tol2_64), x64 += x,
@@ -793,7 +796,7 @@ __global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T>
 
     if (rr > tol2) {
         double v = precond(true);
-        ok = grid_sum(v, part0, P.bar, gen, &rz);
+        ok = grid_sum(v, part0, P.bar, gen, P.spin_limit, &rz);
         T* pin = P.p;
         T* pout = P.p2;
         while (ok) {
@@ -825,7 +828,7 @@ __global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T>
                 acc += (double)pi * (double)s;
             }
             double pq = 0.0;
-            if (!(ok = grid_sum(acc, part1, P.bar, gen, &pq))) break;
+            if (!(ok = grid_sum(acc, part1, P.bar, gen, P.spin_limit, &pq))) break;
             const T alpha = (T)((pq != 0.0) ? rz / pq : 0.0);
             // Phase B: x += alpha p', r -= alpha q, restriction c, r.r.
             acc = 0.0;
@@ -845,7 +848,7 @@ __global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T>
                 const int ag = __ldg(&P.sg.agg[k]);
                 if (lane == 0 && ag >= 0) P.c[ag] = cs;
             }
-            if (!(ok = grid_sum(acc, part2, P.bar, gen, &rr))) break;
+            if (!(ok = grid_sum(acc, part2, P.bar, gen, P.spin_limit, &rr))) break;
             ++iter;
             if constexpr (std::is_same<T, float>::value) {
                 if (P.ru) {
@@ -856,7 +859,7 @@ __global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T>
                             P.x64[i] += (double)__ldcg(&P.x[i]);
                             P.x[i] = 0.0f;
                         }
-                        if (!(ok = grid_barrier(P.bar, G, gen))) break;
+                        if (!(ok = grid_barrier(P.bar, G, gen, P.spin_limit))) break;
                         double acc64 = 0.0;
                         for (int k = gw; k < P.sg.n; k += nw) {
                             float cs = 0.0f;
@@ -879,7 +882,7 @@ __global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T>
                             const int ag = __ldg(&P.sg.agg[k]);
                             if (lane == 0 && ag >= 0) P.c[ag] = cs;
                         }
-                        if (!(ok = grid_sum(acc64, part2, P.bar, gen, &rr))) break;
+                        if (!(ok = grid_sum(acc64, part2, P.bar, gen, P.spin_limit, &rr))) break;
                         ++nru;
                         rmax2 = rr;
                         if (rr <= P.tol2_64 || iter >= P.max_iter) break;
@@ -892,7 +895,7 @@ __global__ void __launch_bounds__(kBlock, MINB) pcg_persistent_kernel(PcgArgs<T>
             }
             // Phase C: z = M^-1 r, r.z, beta.
             double rzn = 0.0;
-            if (!(ok = grid_sum(precond(false), part0, P.bar, gen, &rzn))) break;
+            if (!(ok = grid_sum(precond(false), part0, P.bar, gen, P.spin_limit, &rzn))) break;
             beta = (rz != 0.0) ? rzn / rz : 0.0;
             rz = rzn;
             T* tp = pin;
@@ -1374,6 +1377,7 @@ void EFieldSystem::pcg_persistent(cudaStream_t stream, int n, const T* a, T* xv,
     P.partials = red;
     P.scal = scal;
     P.bar = d_bar;
+    P.spin_limit = spin_limit;
     P.ru = 0;
     P.delta2 = 0.0;
     P.tol2_64 = 0.0;

@@ -117,6 +117,7 @@ struct EFieldSystem {
     unsigned int* red_count = nullptr;
     unsigned int* d_bar = nullptr;        // grid barrier of the persistent solve: count, generation, error
     bool persistent = true;               // whole solve in one cooperative launch (else a launch per phase)
+    unsigned int spin_limit = 1u << 22;   // polls of a grid-barrier wait before the persistent solve gives up
     double dt_built = -1.0;
     bool dirty = true;                    // clamps / membrane properties changed
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc0 = nullptr, evc1 = nullptr;

@@ -2620,6 +2620,14 @@ int sg_set_efield_persistent(sg_solver* h, int32_t on) {
     });
 }
 
+int sg_set_efield_barrier_limit(sg_solver* h, uint32_t polls) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_ef();
+        s->ef.spin_limit = polls;
+    });
+}
+
 int sg_set_efield_reliable_updates(sg_solver* h, int32_t on, double delta) {
     return guarded([&] {
         Solver* s = S(h);

@@ -661,6 +661,11 @@ class TetOpSplit:
         launches per CG iteration (False)."""
         check(self._L.sg_set_efield_persistent(self._h, 1 if on else 0))
 
+    def setEfieldBarrierLimit(self, polls):
+        """Polls (about 100 ns each) of a grid-barrier wait after which the persistent EField
+        solve gives up and the step raises DeviceError; default 2**22 (about 0.5 s)."""
+        check(self._L.sg_set_efield_barrier_limit(self._h, int(polls)))
+
     def setEfieldReliableUpdates(self, on, delta=0.1):
         """Mixed method, persistent solve: one FP32 CG whose residual is replaced by the
         FP64 one whenever it has fallen by `delta` (True, default), or restarted FP32

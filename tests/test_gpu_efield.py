@@ -187,3 +187,32 @@ def test_mixed_step_check_against_fp64(steps_lib, persistent, reliable):
     assert last <= mx
     v = np.array([sim.getVertV(i) for i in range(mesh.nverts)])
     assert np.ptp(v) > 1e-6  # the injection moved V
+
+
+def test_persistent_barrier_wait_runs_out(steps_lib):
+    """A grid-barrier wait of the persistent EField solve that runs out ends the launch with
+    an error status instead of waiting on: with a poll limit of 0 every block that is not
+    the last to arrive gives up at once, the step raises DeviceError, and with the default
+    limit restored the same solver steps on (the device is still usable)."""
+    from steps_b200._lib import DeviceError
+
+    mesh = sgeom.kuhn_box(8, 8, 40, 1e-7)  # 3321 vertices: several blocks in the solve
+    sgeom.TmComp("cyto", mesh, np.arange(mesh.ntets))
+    patch = sgeom.TmPatch("memb", mesh, mesh.getSurfTris(), mesh.comps["cyto"])
+    sgeom.Memb("membrane", mesh, [patch])
+    mdl = smodel.Model()
+    smodel.Volsys("vsys", mdl)
+    sim = TetOpSplit(mdl, mesh, make_rng(5), EF_DV_CG_FP64)
+    sim.setEfieldPersistent(True)
+    sim.setEfieldDT(1e-6)
+    sim.setMembPotential("membrane", -0.065)
+    sim.setMembCapac("membrane", 0.01)
+    sim.setMembRes("membrane", 1.0 / 0.3, -0.065)
+    sim.setVertIClamp(0, 1e-12)
+    sim.setEfieldBarrierLimit(0)
+    with pytest.raises(DeviceError, match="timed out"):
+        sim.run(3e-6)
+    sim.setEfieldBarrierLimit(1 << 22)
+    sim.run(sim.getTime() + 5e-6)
+    v = np.array([sim.getVertV(i) for i in range(0, mesh.nverts, 11)])
+    assert np.all(np.isfinite(v)) and np.all(np.abs(v + 0.065) < 0.01)

@@ -4,6 +4,8 @@ Every reference iteration becomes one realization of a batched solver (the 37-te
 mesh repeated niter times), with the reference's seed, iteration counts, sampling times
 and tolerances (validation_rd_mpi/parallel_spatial_tetopsplit.py).
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -30,3 +32,80 @@ def test_reference_kinetics(steps_lib, name):
             counts[s][i] = np.add.reduceat(row, mesh.offsets[:-1])
     fails = check(name, TPNTS, counts, vol)
     assert not fails, fails[:5]
+
+
+def test_reference_surface_second_order_2d(steps_lib):
+    """Second-order irreversible reaction on a surface with surface diffusion, the
+    reference's "so2d" case (parallel_spatial_tetopsplit.py:139-152, 225-237, 479-486):
+    A + B -> C on the sphere mesh's whole surface patch, kcst 10e10, D_A = D_B = 1e-12,
+    A = 100 and B = 50 per realization, 1000 realizations; ln(B/A) of the mean counts must
+    follow ln(B0/A0) - (A0 - B0) CCST t with CCST = kcst / (N_A area), within 2% at every
+    sampling time."""
+    import math
+
+    from steps_b200 import geom as sgeom
+    from steps_b200 import model as smodel
+    from tests.kinetics import AVOGADRO, sphere, tolerable
+
+    n = 1000
+    base = sphere()
+    rep = sgeom.replicate(base, n)
+    comp = sgeom.TmComp("comp1", rep, np.arange(rep.ntets))
+    comp.addVolsys("vsys")
+    patch = sgeom.TmPatch("patch1", rep, rep.getSurfTris(), comp)
+    patch.addSurfsys("ssys")
+    mdl = smodel.Model()
+    a, b, c = smodel.Spec("A", mdl), smodel.Spec("B", mdl), smodel.Spec("C", mdl)
+    smodel.Volsys("vsys", mdl)
+    ss = smodel.Surfsys("ssys", mdl)
+    smodel.Diff("dA", ss, a, 1.0e-12)
+    smodel.Diff("dB", ss, b, 1.0e-12)
+    smodel.SReac("SR1", ss, slhs=[a, b], srhs=[c], kcst=10.0e10)
+    sim = TetOpSplit(mdl, rep, make_rng(100), realizations=rep.offsets)
+    for r in range(n):
+        sim.setPatchSpecCount("patch1", "A", 100.0, realization=r)
+        sim.setPatchSpecCount("patch1", "B", 50.0, realization=r)
+    area = patch.getArea() / n
+    ccst = 10.0e10 / (AVOGADRO * area)
+    fails = []
+    for t in TPNTS:
+        sim.run(t)
+        ma = sim.getPatchSpecCount("patch1", "A") / n
+        mb = sim.getPatchSpecCount("patch1", "B") / n
+        assert sim.getPatchSpecCount("patch1", "C") / n == pytest.approx(100.0 - ma)
+        lhs = math.log(mb / ma)
+        line = math.log(50.0 / 100.0) - 50.0 * ccst * t
+        if not tolerable(lhs, line, 0.02):
+            fails.append((t, lhs, line))
+    assert not fails, fails
+
+
+def test_zero_order_production(steps_lib):
+    """Zero-order production A from nothing at kcst 1e-3 M/s in a 1 um^3 compartment for 1 s
+    (parallel_zero_order.py, which checks count > 0; its 1x1x1 mesh is not in this
+    repository, so a Kuhn cube of the same volume stands in): every realization produces
+    molecules, and over 400 realizations the counts have the Poisson law of mean
+    k 1e3 V N_A t = 602.2 (mean within 5 standard errors, variance within 25%, 3.5
+    standard errors of a sample variance of 400)."""
+    from steps_b200 import geom as sgeom
+    from steps_b200 import model as smodel
+    from steps_b200 import workloads as W
+    from tests.kinetics import AVOGADRO
+
+    n = 400
+    one = sgeom.kuhn_box(5, 5, 5, 2.0e-7)
+    mesh = W.ConcatMesh([one] * n)
+    comp = sgeom.TmComp("comp", mesh, np.arange(mesh.ntets))
+    comp.addVolsys("vsys")
+    mdl = smodel.Model()
+    A = smodel.Spec("A", mdl)
+    vs = smodel.Volsys("vsys", mdl)
+    smodel.Reac("R1", vs, lhs=[], rhs=[A], kcst=1e-3)
+    sim = TetOpSplit(mdl, mesh, make_rng(1000), realizations=mesh.offsets)
+    sim.run(1.0)
+    row = sim.getSpecCounts("A").astype(np.int64)
+    per = np.add.reduceat(row, mesh.offsets[:-1])
+    expect = 1e-3 * 1.0e3 * float(one.tet_vol.sum()) * AVOGADRO * 1.0
+    assert (per > 0).all()
+    assert abs(per.mean() - expect) < 5.0 * math.sqrt(expect / n)
+    assert abs(per.var(ddof=1) / expect - 1.0) < 0.25
