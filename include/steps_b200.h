@@ -148,6 +148,16 @@ int sg_add_sreac(sg_solver* h, int32_t patch, const uint32_t* slhs, const uint32
 int sg_add_vdep_sreac(sg_solver* h, int32_t patch, const uint32_t* slhs, const uint32_t* ilhs,
                       const int32_t* supd, const int32_t* iupd, double vmin, double dv, int32_t ntab,
                       const double* ktab, int32_t* out_idx);
+/* Outer tets of the membrane triangles (Tri::oTet, tri.hpp; -1 = none): the tet on the
+ * side of the patch's outer compartment.  Needed when a surface reaction or GHK current
+ * reaches the outer volume; the triangles of such patches then join one SSA unit with both
+ * of their tets (sreac.cpp:200-300). */
+int sg_set_tri_outer(sg_solver* h, const int32_t* tri_outer_tet);
+/* Outer-volume terms of surface reaction sreac (Patchdef sreac_lhs_O / sreac_upd_O,
+ * sreac.cpp:40-68, 305-520): olhs, dense over nspec, are reactants in the outer tet (then
+ * the reaction has no inner-volume reactants and its constant scales with the outer tet's
+ * volume, SReacdef::outside); oupd the changes of outer-tet species. */
+int sg_set_sreac_outer(sg_solver* h, int32_t sreac, const uint32_t* olhs, const int32_t* oupd);
 /* OhmicCurr (ohmiccurrdef): g (S per channel) through surface species sspec, erev (V). */
 int sg_add_ohmic(sg_solver* h, int32_t patch, int32_t sspec, double g, double erev, int32_t* out_idx);
 int sg_get_tri_count(sg_solver* h, int32_t tri, int32_t sspec, double* n);   /* TOS:4831 getTriSpecCount */
@@ -159,8 +169,10 @@ int sg_set_patch_count(sg_solver* h, int32_t patch, int32_t sspec, int32_t real,
 int sg_get_tri_ohmic_i(sg_solver* h, int32_t tri, double* amps);  /* getTriOhmicI: last EField step */
 /* GHKcurr (ghkcurr.cpp:168-280, math/ghk.cpp:71-90): channel state sspec of patch passes
  * volume species ion of the given valence, permeability perm (m^3/s per channel), vshift
- * (V), fixed outer concentration voconc (M; this solver's surface units hold no outer
- * tets).  realflux = 1 moves the ions; the carried charge is the triangle's GHK current. */
+ * (V), against a fixed outer concentration voconc (M), or, with voconc < 0, against the
+ * concentration in the triangle's outer tet (sg_set_tri_outer).  realflux = 1 moves the
+ * ions (between the two tets when the outer tet is used); the carried charge is the
+ * triangle's GHK current. */
 int sg_add_ghk(sg_solver* h, int32_t patch, int32_t sspec, int32_t ion, int32_t valence, double perm,
                double vshift, double voconc, int32_t realflux, int32_t* out_idx);
 int sg_set_temp(sg_solver* h, double kelvin);                     /* API::setTemp (default 293.15) */
@@ -231,21 +243,37 @@ int sg_set_efield_reliable_updates(sg_solver* h, int32_t on, double delta);
  * (blocks stride over the tets), -1 = one tet per thread. */
 int sg_set_launch(sg_solver* h, int32_t block, int32_t grid);
 int sg_get_launch(sg_solver* h, int32_t* block, int32_t* grid);
-/* Autotune the launch shape at the next run() with more than 21 windows: after one
- * untimed window, ten candidates are timed on one window each in list order and on one
+/* Autotune the launch shape at the next run() with more than 25 windows: after one
+ * untimed window, twelve candidates are timed on one window each in list order and on one
  * more in reverse order (drift of the per-window work cancels): block {64,128,256} x grid
- * {occupancy-sized (0), one tet per thread (-1)}; block 256, grid -1 at shared-memory
- * carveouts 75% and 50%; split windows at block 128 and 256, grid -1.  The fastest is kept
- * (the sample path does not depend on the shape).  The ten sums (ms, in that order) are
- * read back with sg_get_autotune_ms, the kept carveout with sg_get_carveout. */
+ * {occupancy-sized (0), one tet per thread (-1)}; block 256, grid -1 at a shared-memory
+ * carveout of 75%; split windows at block 128 and 256, grid -1; the persistent form
+ * (sg_set_persistent) at block 128 and 256 with one tet per lane and at block 256 with
+ * two (skipped unless every realization takes the same windows and the model has no
+ * membrane).  The fastest is kept (the sample path does not depend on the shape).  The
+ * twelve sums (ms, in that order) are read back with sg_get_autotune_ms, the kept
+ * carveout with sg_get_carveout. */
 int sg_set_autotune(sg_solver* h, int32_t on);
 int sg_get_carveout(sg_solver* h, int32_t* percent);
 /* Window as two kernels: reactions (gather, SSA) with one thread per tet, then the
- * diffusion leave with one thread per (diffusing species, tet); the same results as the
- * fused kernel.  Models with membrane triangles always run fused.  The autotuner also
- * tries it (after the carveouts: a ninth candidate). */
+ * diffusion leave with one thread per tet over its diffusing species; the same results as
+ * the fused kernel.  Models with membrane triangles run split by default and always when
+ * they have merged SSA units.  The autotuner also tries it. */
 int sg_set_split(sg_solver* h, int32_t on);
 int sg_get_split(sg_solver* h, int32_t* on);
+/* Persistent form of the batched window loop (TOS:1528-1839 for every realization): the
+ * windows of a run() call (up to 64 per launch) of every realization in one cooperative
+ * launch, warps taking chunks of 32 x tets_per_lane (1 or 2) tets of one realization in
+ * window order and waiting, bounded, until that realization has finished the previous
+ * window.  The same results as the window launches, bit for bit.  Used when the model has
+ * no membrane triangles and every realization takes the same windows; the per-window
+ * conservation check does not run inside it. */
+int sg_set_persistent(sg_solver* h, int32_t on, int32_t tets_per_lane);
+int sg_get_persistent(sg_solver* h, int32_t* on, int32_t* tets_per_lane);
+/* Polls (about 100 ns each) a persistent launch's wait on a realization makes before it
+ * gives up; run() then fails with "a persistent window launch gave up waiting" and the
+ * state of that call is undefined.  Default 2^22 (about half a second). */
+int sg_set_window_wait_limit(sg_solver* h, uint32_t polls);
 int sg_get_autotune_ms(sg_solver* h, float* ms, int32_t cap, int32_t* count);
 /* Replay window launches from a captured CUDA graph of 16 windows (on by default). */
 int sg_set_graphs(sg_solver* h, int32_t on);

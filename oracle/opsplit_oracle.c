@@ -549,6 +549,17 @@ typedef struct {
     int32_t* snbr;             /* [M][4] (q << 2) | edge */
     double* tri_occ;           /* [SD][M] */
     uint32_t* tri_out;         /* [SD][M][4] */
+    /* Merged SSA units (sreac.cpp:200-300: a triangle and both its tets in one SSA): outer
+     * tet of each triangle, unit of each tet (-1), the units' tets and triangles (ascending),
+     * and the change-time sums their SSA hands to the diffusion leave. */
+    const int32_t* tri_outer;  /* [M] or NULL */
+    int nunits;
+    int32_t* tet_unit;         /* [T] */
+    int32_t* u_tb;             /* [U + 1] */
+    int32_t* u_tets;
+    int32_t* u_mb;             /* [U + 1] */
+    int32_t* u_tris;
+    double* utdel;             /* [T][S] */
 } or_solver;
 
 typedef struct or_sreac {
@@ -556,6 +567,7 @@ typedef struct or_sreac {
     int nslhs, nilhs, nsupd, niupd;
     int slhs_spec[4], slhs_ord[4], ilhs_spec[4], ilhs_ord[4];
     int supd_spec[8], supd_delta[8], iupd_spec[8], iupd_delta[8];
+    int vside, noupd, oupd_spec[8], oupd_delta[8]; /* volume reactants in the outer tet; outer changes */
     double k;
 } or_sreac;
 
@@ -610,6 +622,12 @@ void or_destroy(or_solver* s) {
     free(s->bcoef);
     free(s->bnbr);
     free(s->tet_tris);
+    free(s->tet_unit);
+    free(s->u_tb);
+    free(s->u_tets);
+    free(s->u_mb);
+    free(s->u_tris);
+    free(s->utdel);
     free(s->tri_counts);
     free(s->tri_v);
     free(s->spec_int);
@@ -911,6 +929,107 @@ void or_add_ghk(or_solver* s, int patch, int sspec, int ion, int valence, double
 
 void or_set_temp(or_solver* s, double kelvin) { s->temp = kelvin; }
 
+/* Outer tet of every membrane triangle (-1 none); kept by reference. */
+void or_set_tri_outer(or_solver* s, const int32_t* tri_outer) { s->tri_outer = tri_outer; }
+
+/* Outer-volume terms of surface reaction idx (the index or_add_sreac returned): reactants
+ * olhs in the outer tet (SReacdef::outside; the constant then scales with the outer tet's
+ * volume) and changes oupd of outer-tet species, dense over the volume species. */
+void or_set_sreac_outer(or_solver* s, int idx, const uint32_t* olhs, const int32_t* oupd) {
+    or_sreac* r = &s->sreacs[idx];
+    int n = 0;
+    for (int i = 0; i < s->nspec; ++i)
+        if (olhs[i]) ++n;
+    if (n > 0) {
+        r->nilhs = 0;
+        for (int i = 0; i < s->nspec; ++i)
+            if (olhs[i]) {
+                r->ilhs_spec[r->nilhs] = i;
+                r->ilhs_ord[r->nilhs++] = (int)olhs[i];
+                r->order += (int)olhs[i];
+            }
+        r->vside = 1;
+        r->surf_surf = 0;
+    }
+    r->noupd = 0;
+    for (int i = 0; i < s->nspec; ++i)
+        if (oupd[i]) {
+            r->oupd_spec[r->noupd] = i;
+            r->oupd_delta[r->noupd++] = oupd[i];
+        }
+}
+
+static int or_patch_coupled(const or_solver* s, int p) {
+    for (int i = 0; i < s->nsreac; ++i)
+        if (s->sreacs[i].patch == p && (s->sreacs[i].vside || s->sreacs[i].noupd > 0)) return 1;
+    for (int g = 0; g < s->nghk; ++g)
+        if (s->ghks[g].patch == p && s->ghks[g].voconc < 0.0) return 1;
+    return 0;
+}
+
+static int or_find(int32_t* par, int x) {
+    while (par[x] != x) x = par[x] = par[par[x]];
+    return x;
+}
+
+/* Units: tets joined through the triangles of coupled patches (inner with outer tet);
+ * groups of two or more tets, numbered by their lowest tet, each with the triangles whose
+ * inner tet is in the group. */
+static void or_setup_units(or_solver* s) {
+    const int T = s->ntets, M = s->ntris;
+    s->nunits = 0;
+    if (!s->tri_outer) return;
+    int any = 0;
+    for (int p = 0; p < s->npatch; ++p) any |= or_patch_coupled(s, p);
+    if (!any) return;
+    int32_t* par = (int32_t*)malloc(sizeof(int32_t) * (size_t)T);
+    int32_t* sz = (int32_t*)calloc((size_t)T, sizeof(int32_t));
+    int32_t* uid = (int32_t*)malloc(sizeof(int32_t) * (size_t)T);
+    for (int t = 0; t < T; ++t) par[t] = t, uid[t] = -1;
+    for (int m = 0; m < M; ++m) {
+        if (!or_patch_coupled(s, s->tri_patch[m]) || s->tri_outer[m] < 0) continue;
+        int a = or_find(par, s->tri_inner[m]), b = or_find(par, s->tri_outer[m]);
+        if (a != b) par[a < b ? b : a] = a < b ? a : b;
+    }
+    for (int t = 0; t < T; ++t) sz[or_find(par, t)] += 1;
+    s->tet_unit = (int32_t*)malloc(sizeof(int32_t) * (size_t)T);
+    for (int t = 0; t < T; ++t) {
+        const int root = or_find(par, t);
+        s->tet_unit[t] = -1;
+        if (sz[root] < 2) continue;
+        if (uid[root] < 0) uid[root] = s->nunits++;
+        s->tet_unit[t] = uid[root];
+    }
+    const int U = s->nunits;
+    s->u_tb = (int32_t*)calloc((size_t)U + 1, sizeof(int32_t));
+    s->u_mb = (int32_t*)calloc((size_t)U + 1, sizeof(int32_t));
+    for (int t = 0; t < T; ++t)
+        if (s->tet_unit[t] >= 0) s->u_tb[s->tet_unit[t] + 1] += 1;
+    for (int m = 0; m < M; ++m)
+        if (s->tet_unit[s->tri_inner[m]] >= 0) s->u_mb[s->tet_unit[s->tri_inner[m]] + 1] += 1;
+    for (int u = 0; u < U; ++u) {
+        s->u_tb[u + 1] += s->u_tb[u];
+        s->u_mb[u + 1] += s->u_mb[u];
+    }
+    s->u_tets = (int32_t*)malloc(sizeof(int32_t) * (size_t)(s->u_tb[U] + 1));
+    s->u_tris = (int32_t*)malloc(sizeof(int32_t) * (size_t)(s->u_mb[U] + 1));
+    int32_t* fill = (int32_t*)calloc((size_t)U + 1, sizeof(int32_t));
+    for (int t = 0; t < T; ++t) {
+        const int u = s->tet_unit[t];
+        if (u >= 0) s->u_tets[s->u_tb[u] + fill[u]++] = t;
+    }
+    memset(fill, 0, sizeof(int32_t) * (size_t)(U + 1));
+    for (int m = 0; m < M; ++m) {
+        const int u = s->tet_unit[s->tri_inner[m]];
+        if (u >= 0) s->u_tris[s->u_mb[u] + fill[u]++] = m;
+    }
+    s->utdel = (double*)calloc((size_t)T * s->nspec, sizeof(double));
+    free(fill);
+    free(par);
+    free(sz);
+    free(uid);
+}
+
 void or_set_tri_neighbours(or_solver* s, const int32_t* nbr, const int32_t* nbr_edge, const double* len,
                            const double* dist) {
     s->tri_nbr = nbr;
@@ -944,6 +1063,7 @@ static void or_setup_surface(or_solver* s) {
         while (slot < 4 && s->tet_tris[(size_t)t * 4 + slot] >= 0) ++slot;
         s->tet_tris[(size_t)t * 4 + slot] = m;
     }
+    or_setup_units(s);
     s->sdiff_slot = (int32_t*)malloc(sizeof(int32_t) * (size_t)(SS > 0 ? SS : 1));
     s->nsdiff = 0;
     int any = 0;
@@ -1320,6 +1440,316 @@ static void or_ssa_surf(or_solver* s, int t, double T, uint32_t* cnt, double* td
     }
 }
 
+/* Signed GHK ion rate with the outer tet's concentration (ghkcurr.cpp:176-181, voconc < 0). */
+static double or_ghk_rate_outer(const or_ghk* g, double vm, uint32_t c_ion, uint32_t n, double ivs, uint32_t c_out,
+                                double ivs_out, double temp) {
+    if (n == 0) return 0.0;
+    const double ci = (double)c_ion * ivs * 1.0e3;
+    const double co = (double)c_out * ivs_out * 1.0e3;
+    const double I = or_ghk_current(g->perm, vm * 1.0e-3 + g->vshift, g->valence, temp, ci, co);
+    return I / (OR_E_CHARGE * (double)g->valence) * (double)n;
+}
+
+/* State of one merged unit during its window: local copies of the counts of its nt tets
+ * (cnt[k][S]) and nm triangles (sc[j][SS]), the tets' change-time sums, the triangles'
+ * occupancy integrals, element propensities and the sum tree. */
+typedef struct {
+    const or_solver* s;
+    int nt, nm, E, P, rmax, r;
+    const int32_t* tets;
+    const int32_t* tris;
+    int* loc;          /* [nt + nm]: local index of the inner tet of triangle j at [nt + j] */
+    int* loco;         /* [nm]: local index of the coupled outer tet, -1 */
+    uint32_t* cnt;
+    double* tdel;
+    uint32_t* sc;
+    double* occ;
+    double* last;
+    double* prop;
+    double* tree;
+} or_unit;
+
+static int or_comp_rb(const or_solver* s, int c, int* re) {
+    int rb = -1;
+    *re = -1;
+    for (int q = 0; q < s->nreac; ++q)
+        if (s->reac[q].comp == c) {
+            if (rb < 0) rb = q;
+            *re = q + 1;
+        }
+    return rb;
+}
+
+/* Propensities of element e in reaction order (a tet: its compartment's reactions; a
+ * triangle: its patch's surface reactions, then its GHK currents); returns their sum. */
+static double or_unit_elem(or_unit* U, int e, int* nq) {
+    const or_solver* s = U->s;
+    const int S = s->nspec, SS = s->nsspec;
+    double* pr = U->prop + (size_t)e * U->rmax;
+    double sum = 0.0;
+    int k = 0;
+    if (e < U->nt) {
+        const int t = U->tets[e];
+        int re;
+        const int rb = or_comp_rb(s, s->tcomp[t], &re);
+        const double* K = s->kcst + (size_t)U->r * s->nreac;
+        for (int q = rb; q >= 0 && q < re; ++q, ++k) {
+            pr[k] = or_prop(s, &s->reac[q], U->cnt + (size_t)e * S, K[q], s->ivs[t]);
+            sum = sum + pr[k];
+        }
+        *nq = k;
+        return sum;
+    }
+    const int j = e - U->nt, m = U->tris[j];
+    const int p = s->tri_patch[m];
+    const int ki = U->loc[U->nt + j], ko = U->loco[j];
+    const int ti = s->tri_inner[m];
+    const int to = s->tri_outer ? s->tri_outer[m] : -1;
+    const double ivs_i = s->ivs[ti], ivs_o = to >= 0 ? s->ivs[to] : 0.0;
+    const double vm = s->tri_v[m];
+    for (int q = s->patch_sb[p]; q < s->patch_sb[p + 1]; ++q, ++k) {
+        const or_sreac* r = &s->sreacs[q];
+        const double kk = (r->vdep >= 0) ? or_vdep_k(s, r->vdep, vm) : r->k;
+        double pq = 0.0;
+        const int kv = r->vside ? ko : ki;
+        if (kv >= 0) {
+            const double h = or_sreac_h(r, U->sc + (size_t)j * SS, U->cnt + (size_t)kv * S);
+            pq = h * or_sreac_ccst(r, kk, r->vside ? ivs_o : ivs_i, s->tri_area[m]);
+        }
+        pr[k] = pq;
+        sum = sum + pq;
+    }
+    for (int g = 0; g < s->nghk; ++g) {
+        const or_ghk* gh = &s->ghks[g];
+        if (gh->patch != p) continue;
+        const uint32_t n = U->sc[(size_t)j * SS + gh->sspec];
+        const uint32_t ci = U->cnt[(size_t)ki * S + gh->ion];
+        const double rt = (gh->voconc >= 0.0 || ko < 0)
+                              ? or_ghk_rate(gh, vm, ci, n, ivs_i, s->temp)
+                              : or_ghk_rate_outer(gh, vm, ci, n, ivs_i, U->cnt[(size_t)ko * S + gh->ion], ivs_o, s->temp);
+        pr[k] = fabs(rt);
+        sum = sum + pr[k];
+        ++k;
+    }
+    *nq = k;
+    return sum;
+}
+
+static int or_unit_nq(const or_unit* U, int e) {
+    const or_solver* s = U->s;
+    if (e < U->nt) {
+        int re;
+        const int rb = or_comp_rb(s, s->tcomp[U->tets[e]], &re);
+        return rb < 0 ? 0 : re - rb;
+    }
+    const int p = s->tri_patch[U->tris[e - U->nt]];
+    int n = s->patch_sb[p + 1] - s->patch_sb[p];
+    for (int g = 0; g < s->nghk; ++g) n += s->ghks[g].patch == p;
+    return n;
+}
+
+static void or_unit_refresh(or_unit* U, int f) {
+    int nq;
+    int i = U->P + f;
+    U->tree[i] = or_unit_elem(U, f, &nq);
+    for (i >>= 1; i >= 1; i >>= 1) U->tree[i] = U->tree[2 * i] + U->tree[2 * i + 1];
+}
+
+/* A tet's counts changed: the tet and every triangle of the unit whose rates read it
+ * (inner tet, or outer tet of a coupled triangle), triangles in ascending order. */
+static void or_unit_refresh_tet(or_unit* U, int k) {
+    if (k < 0) return;
+    or_unit_refresh(U, k);
+    for (int j = 0; j < U->nm; ++j)
+        if (U->loc[U->nt + j] == k || U->loco[j] == k) or_unit_refresh(U, U->nt + j);
+}
+
+static void or_unit_bump(or_unit* U, int k, int sp, int d, double tt) {
+    const or_solver* s = U->s;
+    const int t = U->tets[k];
+    if ((s->clamp[t] >> sp) & 1u) return;
+    uint32_t* c = U->cnt + (size_t)k * s->nspec + sp;
+    const uint32_t old = *c, nc = or_bump(old, d);
+    U->tdel[(size_t)k * s->nspec + sp] += (double)((int64_t)nc - (int64_t)old) * tt;
+    *c = nc;
+}
+
+/* SSA of merged unit u over [0, T) (window w of realization r): the direct method over all
+ * its elements' reactions, the element chosen by descending the sum tree (left while the
+ * target is below the left sum or the right sum is zero, else subtract the left sum and go
+ * right), the reaction by the cumulative sum inside the element; draws from the window
+ * stream of the unit's first tet. */
+static void or_unit_ssa(or_solver* s, int r, int u, double T, uint64_t w) {
+    const int S = s->nspec, SS = s->nsspec, M = s->ntris;
+    or_unit U;
+    memset(&U, 0, sizeof(U));
+    U.s = s;
+    U.r = r;
+    U.tets = s->u_tets + s->u_tb[u];
+    U.nt = s->u_tb[u + 1] - s->u_tb[u];
+    U.tris = s->u_tris + s->u_mb[u];
+    U.nm = s->u_mb[u + 1] - s->u_mb[u];
+    U.E = U.nt + U.nm;
+    U.P = 1;
+    while (U.P < U.E) U.P <<= 1;
+    U.rmax = 1;
+    for (int c = 0; c < s->ncomp; ++c) {
+        int re;
+        const int rb = or_comp_rb(s, c, &re);
+        if (rb >= 0 && re - rb > U.rmax) U.rmax = re - rb;
+    }
+    for (int p = 0; p < s->npatch; ++p) {
+        int n = s->patch_sb[p + 1] - s->patch_sb[p];
+        for (int g = 0; g < s->nghk; ++g) n += s->ghks[g].patch == p;
+        if (n > U.rmax) U.rmax = n;
+    }
+    U.loc = (int*)malloc(sizeof(int) * (size_t)U.E);
+    U.loco = (int*)malloc(sizeof(int) * (size_t)(U.nm + 1));
+    for (int k = 0; k < U.nt; ++k) U.loc[k] = k;
+    for (int j = 0; j < U.nm; ++j) {
+        const int m = U.tris[j];
+        U.loc[U.nt + j] = -1;
+        U.loco[j] = -1;
+        for (int k = 0; k < U.nt; ++k) {
+            if (U.tets[k] == s->tri_inner[m]) U.loc[U.nt + j] = k;
+            if (or_patch_coupled(s, s->tri_patch[m]) && s->tri_outer && U.tets[k] == s->tri_outer[m]) U.loco[j] = k;
+        }
+    }
+    U.cnt = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)U.nt * S);
+    U.tdel = (double*)calloc((size_t)U.nt * S, sizeof(double));
+    U.sc = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(U.nm * SS + 1));
+    U.occ = (double*)calloc((size_t)(U.nm * SS + 1), sizeof(double));
+    U.last = (double*)calloc((size_t)(U.nm * SS + 1), sizeof(double));
+    U.prop = (double*)calloc((size_t)U.E * U.rmax, sizeof(double));
+    U.tree = (double*)calloc((size_t)2 * U.P, sizeof(double));
+    for (int k = 0; k < U.nt; ++k)
+        for (int i = 0; i < S; ++i) U.cnt[(size_t)k * S + i] = s->counts[(size_t)i * s->ntets + U.tets[k]];
+    for (int j = 0; j < U.nm; ++j)
+        for (int i = 0; i < SS; ++i) U.sc[(size_t)j * SS + i] = s->tri_counts[(size_t)i * M + U.tris[j]];
+    for (int e = 0; e < U.E; ++e) {
+        int nq;
+        U.tree[U.P + e] = or_unit_elem(&U, e, &nq);
+    }
+    for (int i = U.P - 1; i >= 1; --i) U.tree[i] = U.tree[2 * i] + U.tree[2 * i + 1];
+    or_stream st;
+    or_stream_init(&st, s->seed, (uint32_t)r, (uint32_t)(U.tets[0] - s->real_begin[r]), w, 0u);
+    double tt = 0.0;
+    for (;;) {
+        const double a0 = U.tree[1];
+        if (!(a0 > 0.0)) break;
+        const double dt = -or_log(u_oc(or_u32(&st))) / a0;
+        if (tt + dt > T) break;
+        tt = tt + dt;
+        double target = u_co(or_u32(&st)) * a0;
+        int node = 1;
+        while (node < U.P) {
+            const double l = U.tree[2 * node], rr = U.tree[2 * node + 1];
+            if (target < l || !(rr > 0.0))
+                node = 2 * node;
+            else {
+                target = target - l;
+                node = 2 * node + 1;
+            }
+        }
+        const int e = node - U.P;
+        const int nq = or_unit_nq(&U, e);
+        const double* pq = U.prop + (size_t)e * U.rmax;
+        double cum = 0.0;
+        int sel = -1, lastnz = -1;
+        for (int q = 0; q < nq; ++q)
+            if (pq[q] > 0.0) {
+                lastnz = q;
+                cum = cum + pq[q];
+                if (target < cum) {
+                    sel = q;
+                    break;
+                }
+            }
+        if (sel < 0) sel = lastnz;
+        if (sel < 0) break;
+        if (e < U.nt) {
+            int re;
+            const int q = or_comp_rb(s, s->tcomp[U.tets[e]], &re) + sel;
+            for (int i = 0; i < S; ++i)
+                if (s->reac[q].upd[i]) or_unit_bump(&U, e, i, s->reac[q].upd[i], tt);
+#pragma omp atomic
+            s->ext[q] += 1;
+            or_unit_refresh_tet(&U, e);
+            continue;
+        }
+        const int j = e - U.nt, m = U.tris[j], p = s->tri_patch[m];
+        const int pb = s->patch_sb[p], npr = s->patch_sb[p + 1] - pb;
+        const int ki = U.loc[U.nt + j], ko = U.loco[j];
+        int chi = 0, cho = 0;
+        if (sel < npr) {
+            const or_sreac* rs = &s->sreacs[pb + sel];
+            for (int i = 0; i < rs->nsupd; ++i) {
+                const size_t o = (size_t)j * SS + rs->supd_spec[i];
+                const uint32_t old = U.sc[o];
+                U.occ[o] = U.occ[o] + (double)old * (tt - U.last[o]);
+                U.last[o] = tt;
+                U.sc[o] = or_bump(old, rs->supd_delta[i]);
+            }
+            for (int i = 0; i < rs->niupd; ++i) or_unit_bump(&U, ki, rs->iupd_spec[i], rs->iupd_delta[i], tt);
+            for (int i = 0; i < rs->noupd && ko >= 0; ++i) or_unit_bump(&U, ko, rs->oupd_spec[i], rs->oupd_delta[i], tt);
+            chi = rs->niupd > 0;
+            cho = rs->noupd > 0;
+        } else {
+            int g = 0, left = sel - npr;
+            for (; g < s->nghk; ++g)
+                if (s->ghks[g].patch == p && left-- == 0) break;
+            const or_ghk* gh = &s->ghks[g];
+            const int outer = gh->voconc < 0.0 && ko >= 0;
+            const uint32_t n = U.sc[(size_t)j * SS + gh->sspec];
+            const uint32_t ci = U.cnt[(size_t)ki * S + gh->ion];
+            const double sr = outer ? or_ghk_rate_outer(gh, s->tri_v[m], ci, n, s->ivs[s->tri_inner[m]],
+                                                        U.cnt[(size_t)ko * S + gh->ion], s->ivs[s->tri_outer[m]], s->temp)
+                                    : or_ghk_rate(gh, s->tri_v[m], ci, n, s->ivs[s->tri_inner[m]], s->temp);
+            const int eff = sr >= 0.0;
+            if (gh->realflux) {
+                or_unit_bump(&U, ki, gh->ion, eff ? -1 : 1, tt);
+                if (outer) or_unit_bump(&U, ko, gh->ion, eff ? 1 : -1, tt);
+                chi = 1;
+                cho = outer;
+            }
+#pragma omp atomic
+            s->echarge[m] += eff ? gh->valence : -gh->valence;
+        }
+#pragma omp atomic
+        s->surf_ext += 1;
+        or_unit_refresh(&U, e);
+        if (chi) or_unit_refresh_tet(&U, ki);
+        if (cho) or_unit_refresh_tet(&U, ko);
+    }
+    for (int j = 0; j < U.nm; ++j) {
+        const int m = U.tris[j];
+        for (int i = 0; i < SS; ++i) {
+            const uint32_t c = U.sc[(size_t)j * SS + i];
+            s->tri_counts[(size_t)i * M + m] = c;
+            const double o = U.occ[(size_t)j * SS + i] + (double)c * (T - U.last[(size_t)j * SS + i]);
+            s->spec_int[(size_t)i * M + m] += o;
+            if (s->nsdiff > 0) {
+                const int sd = s->sdiff_slot[i];
+                if (sd >= 0) s->tri_occ[(size_t)sd * M + m] = o;
+            }
+        }
+    }
+    for (int k = 0; k < U.nt; ++k)
+        for (int i = 0; i < S; ++i) {
+            s->counts[(size_t)i * s->ntets + U.tets[k]] = U.cnt[(size_t)k * S + i];
+            s->utdel[(size_t)U.tets[k] * S + i] = U.tdel[(size_t)k * S + i];
+        }
+    free(U.loc);
+    free(U.loco);
+    free(U.cnt);
+    free(U.tdel);
+    free(U.sc);
+    free(U.occ);
+    free(U.last);
+    free(U.prop);
+    free(U.tree);
+}
+
 /* Surface diffusion leave of triangle m (TOS:1716-1793, sdiff.cpp:498-560): n = min(pop,
  * window integral / T) with a Bernoulli on its fraction, Binomial(n, min(1, T D G)) leaving,
  * split over the three edges by the conditional selectors (purpose 80 + species stream). */
@@ -1396,9 +1826,12 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
      * the integral of a count over [0, T) is c_end T - sum_k (change_k) t_k, so tdel keeps
      * sum_k (change_k) t_k. */
     double tdel[OR_MAXS];
+    /* A tet of a merged unit: its SSA ran in or_unit_ssa, which left the counts and the
+     * change-time sums. */
+    const int merged = s->nunits > 0 && s->tet_unit[t] >= 0;
     for (int i = 0; i < S; ++i) {
         cnt[i] = s->counts[(size_t)i * s->ntets + t];
-        tdel[i] = 0.0;
+        tdel[i] = merged ? s->utdel[(size_t)t * S + i] : 0.0;
     }
     const uint32_t clampm = s->clamp[t];
     or_stream st;
@@ -1414,7 +1847,8 @@ static void or_tet_window(or_solver* s, int r, int t, double T, uint64_t w) {
         }
     }
     const int has_tris = s->ntris > 0 && (s->tet_tris[(size_t)t * 4] >= 0);
-    if (has_tris) {
+    if (merged) {
+    } else if (has_tris) {
         or_ssa_surf(s, t, T, cnt, tdel, &st, clampm, ivs, K, rb, re);
     } else if (rb >= 0) {
         double tt = 0.0;
@@ -1546,6 +1980,9 @@ uint64_t or_run(or_solver* s, double endtime) {
             double t = s->t[r], per = s->period[r];
             double T = (t + per > endtime) ? endtime - t : per;
             uint64_t w = s->window[r];
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int u = 0; u < s->nunits; ++u)
+                if (s->u_tets[s->u_tb[u]] >= tb && s->u_tets[s->u_tb[u]] < te) or_unit_ssa(s, r, u, T, w);
 #pragma omp parallel for schedule(dynamic, 256)
             for (int tet = tb; tet < te; ++tet)
                 if (s->tcomp[tet] >= 0) or_tet_window(s, r, tet, T, w);

@@ -62,6 +62,8 @@ def load():
         lib.or_add_ghk.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                    C.c_int]
         lib.or_set_temp.argtypes = [P, C.c_double]
+        lib.or_set_tri_outer.argtypes = [P, pi]
+        lib.or_set_sreac_outer.argtypes = [P, C.c_int, pu, pi]
         lib.or_set_tri_neighbours.argtypes = [P, pi, pi, pf, pf]
         lib.or_add_sdiff.argtypes = [P, C.c_int, C.c_int, C.c_double]
         lib.or_set_tri_counts.argtypes = [P, C.c_int, pu]
@@ -133,15 +135,24 @@ class Oracle:
             self.L.or_set_surface(self.h, sf["nsspec"], self.ntris, _p(tri_inner, C.c_int32),
                                   _p(tri_patch, C.c_int32), _p(sf["tri_area"], C.c_double),
                                   len(sf["patch_names"]))
-            for (pi, _rid, (slhs, ilhs, supd, iupd), k, vdep) in sf["sreacs"]:
+            if sf.get("tri_outer") is not None:
+                tri_outer = np.ascontiguousarray(sf["tri_outer"], dtype=np.int32)
+                self._keep.append(tri_outer)
+                self.L.or_set_tri_outer(self.h, _p(tri_outer, C.c_int32))
+            outer_rows = sf.get("sreac_outer") or [None] * len(sf["sreacs"])
+            for (pi, _rid, (slhs, ilhs, supd, iupd), k, vdep), orow in zip(sf["sreacs"], outer_rows):
                 args = (self.h, pi, _p(slhs, C.c_uint32), _p(ilhs, C.c_uint32), _p(supd, C.c_int32),
                         _p(iupd, C.c_int32))
                 if vdep is None:
-                    self.L.or_add_sreac(*args, k, 0.0, 0.0, 0, None)
+                    idx = self.L.or_add_sreac(*args, k, 0.0, 0.0, 0, None)
                 else:
                     vmin, dv, tab = vdep
                     tab = np.ascontiguousarray(tab, dtype=np.float64)
-                    self.L.or_add_sreac(*args, 0.0, vmin, dv, tab.size, _p(tab, C.c_double))
+                    idx = self.L.or_add_sreac(*args, 0.0, vmin, dv, tab.size, _p(tab, C.c_double))
+                if orow is not None:
+                    olhs = np.ascontiguousarray(orow[0], dtype=np.uint32)
+                    oupd = np.ascontiguousarray(orow[1], dtype=np.int32)
+                    self.L.or_set_sreac_outer(self.h, idx, _p(olhs, C.c_uint32), _p(oupd, C.c_int32))
             for (pi, _gid, ss, ion, z, perm, vshift, voconc, flux) in sf["ghks"]:
                 self.L.or_add_ghk(self.h, pi, ss, ion, int(z), float(perm), float(vshift), float(voconc),
                                   1 if flux else 0)

@@ -45,6 +45,7 @@
 #include "model/ohmiccurr.hpp"
 #include "model/surfsys.hpp"
 #include "model/vdepsreac.hpp"
+#include "model/sreac.hpp"
 #ifdef STEPS_WITH_B200_API
 #include "steps_api/tetopsplit_b200.hpp"
 #endif
@@ -58,6 +59,7 @@ struct RefSim {
     std::vector<steps::model::Spec*> specs;  // owned by the model
     std::unique_ptr<steps::tetmesh::Tetmesh> mesh;
     steps::tetmesh::TmComp* comp = nullptr;  // registered with (and unregistered from) mesh
+    steps::tetmesh::TmComp* comp2 = nullptr; // outer compartment of ref_create_outer
     steps::tetmesh::TmPatch* patch = nullptr;
     steps::tetmesh::Memb* memb = nullptr;  // owned by the mesh
     bool has_chans = false;
@@ -75,6 +77,7 @@ struct RefSim {
         // unregister themselves from the mesh in their destructors, so they go first.
         delete patch;
         delete comp;
+        delete comp2;
         mesh.reset();
         // A model with an ohmic current on a channel state is released, not deleted: its
         // destructor deletes the channel state before the current and then throws from the
@@ -302,6 +305,88 @@ void* ref_create_memb(int kind, int nverts, const double* verts, int ntets, cons
     }
 }
 
+// A membrane between two compartments (kind 0 TetOpSplitP, 1 Tetexact, 2 the drop-in):
+// tets with is_outer[t] = 0 form "cyto" (volume system vin: Ca and B diffuse, Ca + B <->
+// CaB), the others "ecs" (vout: Ca diffuses); the patch "memb" (inner cyto, outer ecs) is
+// every triangle between the two, with surface system ssys: pump P binds inner Ca (pin) and
+// releases it to the outer side (pout); channel Kc <-> Ko (open, close); open channels let
+// outer Ca in (back: outer-volume reactant, inner product).  Constants as given.
+void* ref_create_outer(int kind, int nverts, const double* verts, int ntets, const int64_t* tets,
+                       const int32_t* is_outer, const double* k, uint64_t seed) {
+    try {
+        auto s = std::make_unique<RefSim>();
+        s->model = std::make_unique<steps::model::Model>();
+        auto& mdl = *s->model;
+        auto* ca = new steps::model::Spec("Ca", mdl, 2);
+        auto* b = new steps::model::Spec("B", mdl);
+        auto* cab = new steps::model::Spec("CaB", mdl);
+        auto* p = new steps::model::Spec("P", mdl);
+        auto* pc = new steps::model::Spec("PCa", mdl);
+        auto* ch = new steps::model::Chan("CaCh", mdl);
+        auto* kc = new steps::model::ChanState("Kc", mdl, *ch);
+        auto* ko = new steps::model::ChanState("Ko", mdl, *ch);
+        auto* vin = new steps::model::Volsys("vin", mdl);
+        auto* vout = new steps::model::Volsys("vout", mdl);
+        new steps::model::Diff("dCa_i", *vin, *ca, k[0]);
+        new steps::model::Diff("dB_i", *vin, *b, k[1]);
+        new steps::model::Reac("bind", *vin, {ca, b}, {cab}, k[2]);
+        new steps::model::Reac("unbind", *vin, {cab}, {ca, b}, k[3]);
+        new steps::model::Diff("dCa_o", *vout, *ca, k[4]);
+        auto* ss = new steps::model::Surfsys("ssys", mdl);
+        // SReac(id, surfsys, olhs, ilhs, slhs, irhs, srhs, orhs, kcst) (model/sreac.hpp:67)
+        new steps::model::SReac("pin", *ss, {}, {ca}, {p}, {}, {pc}, {}, k[5]);
+        new steps::model::SReac("pout", *ss, {}, {}, {pc}, {}, {p}, {ca}, k[6]);
+        new steps::model::SReac("open", *ss, {}, {}, {kc}, {}, {ko}, {}, k[7]);
+        new steps::model::SReac("close", *ss, {}, {}, {ko}, {}, {kc}, {}, k[8]);
+        new steps::model::SReac("back", *ss, {ca}, {}, {ko}, {ca}, {ko}, {}, k[9]);
+        s->has_chans = true;
+        std::vector<double> v(verts, verts + (size_t)nverts * 3);
+        std::vector<steps::index_t> t((size_t)ntets * 4);
+        for (size_t q = 0; q < t.size(); ++q) t[q] = (steps::index_t)tets[q];
+        s->mesh = std::make_unique<steps::tetmesh::Tetmesh>(v, t);
+        std::vector<steps::index_t> in, out;
+        for (int q = 0; q < ntets; ++q) (is_outer[q] ? out : in).push_back((steps::index_t)q);
+        s->comp = new steps::tetmesh::TmComp("cyto", *s->mesh, in);
+        s->comp->addVolsys("vin");
+        s->comp2 = new steps::tetmesh::TmComp("ecs", *s->mesh, out);
+        s->comp2->addVolsys("vout");
+        std::vector<steps::index_t> iface;
+        const auto ntris = s->mesh->countTris();
+        for (steps::index_t m = 0; m < ntris; ++m) {
+            const auto& tt = s->mesh->_getTriTetNeighb(steps::triangle_global_id(m));
+            if (!tt[0].valid() || !tt[1].valid()) continue;
+            if ((is_outer[tt[0].get()] != 0) != (is_outer[tt[1].get()] != 0)) iface.push_back(m);
+        }
+        s->patch = new steps::tetmesh::TmPatch("memb", *s->mesh, iface, *s->comp, s->comp2);
+        s->patch->addSurfsys("ssys");
+        s->ntets = (uint32_t)ntets;
+        s->rng = steps::rng::create("r123", 512u);
+        s->rng->initialize((unsigned long)seed);
+        if (kind == 0) {
+            std::vector<int> tet_hosts((size_t)ntets, 0);
+            std::map<steps::triangle_global_id, int> tri_hosts;
+            for (auto x : iface) tri_hosts[steps::triangle_global_id(x)] = 0;
+            s->solver = std::make_unique<steps::mpi::tetopsplit::TetOpSplitP>(
+                s->model.get(), s->mesh.get(), s->rng, steps::solver::API::EF_NONE, tet_hosts, tri_hosts);
+        } else if (kind == 2) {
+#ifdef STEPS_WITH_B200_API
+            s->solver = std::make_unique<steps::b200::TetOpSplitB200>(s->model.get(), s->mesh.get(), s->rng,
+                                                                       steps::solver::API::EF_NONE);
+#else
+            g_err = "built without the TetOpSplitB200 drop-in";
+            return nullptr;
+#endif
+        } else {
+            s->solver = std::make_unique<steps::tetexact::Tetexact>(s->model.get(), s->mesh.get(), s->rng,
+                                                                     steps::solver::API::EF_NONE);
+        }
+        return s.release();
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
 #define REF_TRY(body)                 \
     try {                             \
         body;                         \
@@ -340,6 +425,12 @@ int ref_get_tri_count(void* h, int64_t tri, const char* spec, double* out) {
 int ref_set_tri_count(void* h, int64_t tri, const char* spec, double n) {
     REF_TRY(static_cast<RefSim*>(h)->solver->setTriSpecCount(steps::triangle_global_id((steps::index_t)tri), spec,
                                                                n))
+}
+int ref_get_comp_count_named(void* h, const char* comp, const char* spec, double* out) {
+    REF_TRY(*out = static_cast<RefSim*>(h)->solver->getCompSpecCount(comp, spec))
+}
+int ref_set_comp_count_named(void* h, const char* comp, const char* spec, double n) {
+    REF_TRY(static_cast<RefSim*>(h)->solver->setCompSpecCount(comp, spec, n))
 }
 int ref_get_patch_count(void* h, const char* spec, double* out) {
     REF_TRY(*out = static_cast<RefSim*>(h)->solver->getPatchSpecCount("memb", spec))

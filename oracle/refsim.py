@@ -63,10 +63,14 @@ def load(with_dropin=False):
                      ("ref_get_patch_count", [vp, cs, dp]), ("ref_set_patch_count", [vp, cs, C.c_double]),
                      ("ref_get_vert_v", [vp, i64, dp]), ("ref_set_vert_v", [vp, i64, C.c_double]),
                      ("ref_set_vert_iclamp", [vp, i64, C.c_double]),
-                     ("ref_set_memb", [vp] + [C.c_double] * 6), ("ref_solver_name", [vp, C.c_char_p, ip])):
+                     ("ref_set_memb", [vp] + [C.c_double] * 6), ("ref_solver_name", [vp, C.c_char_p, ip]),
+                     ("ref_get_comp_count_named", [vp, cs, cs, dp]),
+                     ("ref_set_comp_count_named", [vp, cs, cs, C.c_double])):
         f = getattr(lib, nm)
         f.argtypes = args
         f.restype = C.c_int
+    lib.ref_create_outer.restype = vp
+    lib.ref_create_outer.argtypes = [ip, ip, dp, ip, C.POINTER(C.c_int64), C.POINTER(C.c_int32), dp, C.c_uint64]
     _libs[path] = lib
     return lib
 
@@ -227,3 +231,36 @@ class RefMemb(RefSim):
     def set_memb(self, v0, cm, ra, ro, vrev, efdt):
         """setMembPotential, setMembCapac, setMembVolRes, setMembRes, setEfieldDT."""
         self._ok(self._lib.ref_set_memb(self._h, v0, cm, ra, ro, vrev, efdt))
+
+
+class RefOuter(RefMemb):
+    """The two-compartment membrane of ref_create_outer: tets with is_outer = 0 in "cyto",
+    the rest in "ecs", the triangles between them the patch "memb" with pump and channel
+    surface reactions that reach both volumes; k the ten constants (D_Ca inner, D_B,
+    bind, unbind, D_Ca outer, pin, pout, open, close, back); kind "tetopsplit", "tetexact"
+    or "b200"."""
+
+    def __init__(self, mesh, is_outer, k, seed, kind="tetopsplit"):
+        lib = load(with_dropin=(kind == "b200"))
+        self._lib = lib
+        verts = np.ascontiguousarray(mesh.verts, dtype=np.float64)
+        tets = np.ascontiguousarray(mesh.tets, dtype=np.int64)
+        flag = np.ascontiguousarray(is_outer, dtype=np.int32)
+        kk = np.ascontiguousarray(k, dtype=np.float64)
+        self._keep = (verts, tets, flag, kk)
+        self.ntets = int(tets.shape[0])
+        self.nspec = 0
+        h = lib.ref_create_outer(_KINDS[kind], verts.shape[0], _ptr(verts, C.c_double), self.ntets,
+                                 _ptr(tets, C.c_int64), _ptr(flag, C.c_int32), _ptr(kk, C.c_double), int(seed))
+        if not h:
+            raise RuntimeError("reference outer-membrane model construction failed: "
+                               + lib.ref_last_error().decode())
+        self._h = h
+
+    def get_comp(self, comp, spec):
+        out = C.c_double()
+        self._ok(self._lib.ref_get_comp_count_named(self._h, comp.encode(), spec.encode(), C.byref(out)))
+        return out.value
+
+    def set_comp(self, comp, spec, n):
+        self._ok(self._lib.ref_set_comp_count_named(self._h, comp.encode(), spec.encode(), float(n)))

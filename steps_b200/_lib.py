@@ -87,12 +87,17 @@ PROTOTYPES = {
     "sg_get_carveout": [_P, _pi32],
     "sg_set_split": [_P, _i32],
     "sg_get_split": [_P, _pi32],
+    "sg_set_persistent": [_P, _i32, _i32],
+    "sg_get_persistent": [_P, _pi32, _pi32],
+    "sg_set_window_wait_limit": [_P, C.c_uint32],
     "sg_get_autotune_ms": [_P, C.POINTER(C.c_float), _i32, _pi32],
     "sg_set_conservation_check": [_P, _i32],
     "sg_set_graphs": [_P, _i32],
     "sg_get_status": [_P, _pu32],
     "sg_set_surface": [_P, _i32, _i32, _pi32, _pi32, _pf64, _i32],
     "sg_add_sreac": [_P, _i32, _pu32, _pu32, _pi32, _pi32, _f64, _pi32],
+    "sg_set_tri_outer": [_P, _pi32],
+    "sg_set_sreac_outer": [_P, _i32, _pu32, _pi32],
     "sg_add_vdep_sreac": [_P, _i32, _pu32, _pu32, _pi32, _pi32, _f64, _f64, _i32, _pf64, _pi32],
     "sg_add_ghk": [_P, _i32, _i32, _i32, _i32, _f64, _f64, _f64, _i32, _pi32],
     "sg_set_temp": [_P, _f64],

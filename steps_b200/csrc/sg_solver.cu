@@ -131,6 +131,16 @@ struct Solver {
     DevBuf<float> d_bcoef;
     DevBuf<double> d_btab;
     bool split = false;                         // window as two kernels (reactions, diffusion)
+    // Persistent form: all windows of a run() chunk in one cooperative launch
+    // (persistent_window_kernel), tets per lane 1 or 2 (32 or 64 tets per work chunk).
+    bool persist = false;
+    int persist_tpl = 1;
+    unsigned int persist_spin_limit = 1u << 22;  // polls (~100 ns each) before a wait gives up
+    DevBuf<int32_t> d_pchunk;                   // [nreal + 1] first chunk of each realization
+    DevBuf<unsigned int> d_pstate;              // done [nreal], ready [nreal], abort [1]
+    DevBuf<unsigned long long> d_pnext;         // [1] next work item
+    int pchunk_tpl = 0;                         // tets per lane d_pchunk was built for
+    int pchunks = 0;
     DevBuf<float> d_geo;
     DevBuf<double> d_ivs, d_kcst, d_dcst;
     DevBuf<sg_reac> d_reacs;
@@ -184,6 +194,169 @@ struct Solver {
     DevBuf<float> d_sgeo;
     bool has_surf() const { return ntris > 0 && nsspec > 0; }
 
+    // Merged SSA units (triangles coupled to their outer tet, sreac.cpp:200-300).
+    std::vector<int32_t> tri_outer;                 // [M] outer tet, -1 none (empty: not given)
+    std::vector<int32_t> tet_unit_h;                // [T] unit of a merged tet, -1
+    int nunits = 0, unit_rmax = 0;
+    DevBuf<int32_t> d_tri_outer, d_u_tet_begin, d_u_tets, d_u_tri_begin, d_u_tris, d_u_elem_base, d_u_tree_base,
+        d_tet_unit, d_u_tet_adj, d_u_tri_side;
+    DevBuf<double> d_u_prop, d_u_tree, d_u_socc, d_u_slast;
+
+    // A patch couples its triangles' outer tets when a surface reaction counts or changes an
+    // outer-volume species or a GHK current reads the outer tet's concentration.
+    bool patch_coupled(int p) const {
+        for (const auto& r : sreacs)
+            if (r.patch == p && (r.vside != 0 || r.noupd > 0)) return true;
+        for (const auto& g : ghks)
+            if (g.patch == p && g.voconc < 0.0) return true;
+        return false;
+    }
+
+    // Units: connected groups of tets linked by coupled triangles (union of inner and outer
+    // tet), with every membrane triangle whose inner tet is in the group.  Elements in
+    // canonical order: the unit's tets ascending, then its triangles ascending.
+    void setup_units() {
+        nunits = 0;
+        tet_unit_h.assign(ntets, -1);
+        std::vector<char> coupled(npatch, 0);
+        bool any = false;
+        for (int p = 0; p < npatch; ++p) {
+            coupled[p] = patch_coupled(p) ? 1 : 0;
+            any = any || coupled[p];
+        }
+        if (!any) return;
+        if (tri_outer.size() != (size_t)ntris)
+            throw ArgErr("surface reactions or GHK currents that reach the outer volume need the triangles' outer tets");
+        std::vector<int32_t> par(ntets);
+        for (int t = 0; t < ntets; ++t) par[t] = t;
+        auto find = [&](int x) {
+            while (par[x] != x) {
+                par[x] = par[par[x]];
+                x = par[x];
+            }
+            return x;
+        };
+        for (int m = 0; m < ntris; ++m) {
+            if (!coupled[tri_patch[m]]) continue;
+            const int o = tri_outer[m], i = tri_inner[m];
+            if (o < 0) throw ArgErr("membrane triangle " + std::to_string(m) + " of a patch whose reactions reach the outer volume has no outer tet");
+            if (realization_of(o) != realization_of(i)) throw ArgErr("a membrane triangle links tets of two realizations");
+            const int a = find(i), b = find(o);
+            if (a != b) par[a < b ? b : a] = a < b ? a : b;
+        }
+        std::vector<int32_t> size(ntets, 0), uid(ntets, -1);
+        for (int t = 0; t < ntets; ++t) size[find(t)] += 1;
+        for (int t = 0; t < ntets; ++t) {
+            const int root = find(t);
+            if (size[root] < 2) continue;
+            if (uid[root] < 0) uid[root] = nunits++;
+            tet_unit_h[t] = uid[root];
+        }
+        if (nunits == 0) return;
+        std::vector<std::vector<int32_t>> ut(nunits), um(nunits);
+        for (int t = 0; t < ntets; ++t)
+            if (tet_unit_h[t] >= 0) ut[tet_unit_h[t]].push_back(t);
+        for (int m = 0; m < ntris; ++m) {
+            const int u = tet_unit_h[tri_inner[m]];
+            if (u >= 0) um[u].push_back(m);
+        }
+        std::vector<int32_t> tb(nunits + 1, 0), mb(nunits + 1, 0), eb(nunits + 1, 0), trb(nunits + 1, 0);
+        std::vector<int32_t> tets, tris;
+        std::vector<int32_t> local(ntets, -1);
+        for (int u = 0; u < nunits; ++u) {
+            for (size_t k = 0; k < ut[u].size(); ++k) local[ut[u][k]] = (int32_t)k;
+            tets.insert(tets.end(), ut[u].begin(), ut[u].end());
+            tris.insert(tris.end(), um[u].begin(), um[u].end());
+            const int E = (int)(ut[u].size() + um[u].size());
+            int P = 1;
+            while (P < E) P <<= 1;
+            tb[u + 1] = tb[u] + (int)ut[u].size();
+            mb[u + 1] = mb[u] + (int)um[u].size();
+            eb[u + 1] = eb[u] + E;
+            if ((long long)trb[u] + 2LL * P > 0x7FFFFFFFLL) throw ArgErr("merged SSA units too large");
+            trb[u + 1] = trb[u] + 2 * P;
+        }
+        const int E = eb[nunits];
+        std::vector<int32_t> adj((size_t)E * 4, -1), side((size_t)ntris * 2, -1);
+        auto add_adj = [&](int e, int f) {
+            for (int k = 0; k < 4; ++k) {
+                int32_t& x = adj[(size_t)e * 4 + k];
+                if (x == f) return;
+                if (x < 0) {
+                    x = f;
+                    return;
+                }
+            }
+            throw ArgErr("a tet borders more than four membrane triangles");
+        };
+        for (int u = 0; u < nunits; ++u) {
+            const int nt = (int)ut[u].size();
+            for (size_t j = 0; j < um[u].size(); ++j) {
+                const int m = um[u][j];
+                const int f = nt + (int)j;
+                const int ei = local[tri_inner[m]];
+                add_adj(eb[u] + ei, f);
+                side[(size_t)m * 2] = ei;
+                if (coupled[tri_patch[m]]) {
+                    const int eo = local[tri_outer[m]];
+                    add_adj(eb[u] + eo, f);
+                    side[(size_t)m * 2 + 1] = eo;
+                }
+            }
+        }
+        unit_rmax = max_sreac_per_patch;
+        for (int c = 0; c < ncomp; ++c) unit_rmax = std::max(unit_rmax, comp_reac_begin[c + 1] - comp_reac_begin[c]);
+        unit_rmax = std::max(unit_rmax, 1);
+        if (tri_outer.size() == (size_t)ntris) {
+            d_tri_outer.alloc(ntris);
+            h2d(d_tri_outer.p, tri_outer.data(), tri_outer.size());
+        }
+        d_u_tet_begin.alloc(tb.size());
+        d_u_tets.alloc(tets.size());
+        d_u_tri_begin.alloc(mb.size());
+        d_u_tris.alloc(std::max<size_t>(tris.size(), 1));
+        d_u_elem_base.alloc(eb.size());
+        d_u_tree_base.alloc(trb.size());
+        d_tet_unit.alloc(ntets);
+        d_u_tet_adj.alloc(adj.size());
+        d_u_tri_side.alloc(side.size());
+        d_u_prop.alloc((size_t)E * unit_rmax);
+        d_u_tree.alloc((size_t)trb[nunits]);
+        d_u_socc.alloc((size_t)nsspec * ntris);
+        d_u_slast.alloc((size_t)nsspec * ntris);
+        h2d(d_u_tet_begin.p, tb.data(), tb.size());
+        h2d(d_u_tets.p, tets.data(), tets.size());
+        h2d(d_u_tri_begin.p, mb.data(), mb.size());
+        if (!tris.empty()) h2d(d_u_tris.p, tris.data(), tris.size());
+        h2d(d_u_elem_base.p, eb.data(), eb.size());
+        h2d(d_u_tree_base.p, trb.data(), trb.size());
+        h2d(d_tet_unit.p, tet_unit_h.data(), tet_unit_h.size());
+        h2d(d_u_tet_adj.p, adj.data(), adj.size());
+        h2d(d_u_tri_side.p, side.data(), side.size());
+    }
+
+    sg_unit_args unit_args() const {
+        sg_unit_args u;
+        std::memset(&u, 0, sizeof(u));
+        if (nunits == 0) return u;
+        u.tet_begin = d_u_tet_begin.p;
+        u.tets = d_u_tets.p;
+        u.tri_begin = d_u_tri_begin.p;
+        u.tris = d_u_tris.p;
+        u.elem_base = d_u_elem_base.p;
+        u.tree_base = d_u_tree_base.p;
+        u.tet_unit = d_tet_unit.p;
+        u.tet_adj = d_u_tet_adj.p;
+        u.tri_side = d_u_tri_side.p;
+        u.prop = d_u_prop.p;
+        u.tree = d_u_tree.p;
+        u.socc = d_u_socc.p;
+        u.slast = d_u_slast.p;
+        u.nunits = nunits;
+        u.rmax = unit_rmax;
+        return u;
+    }
+
     // Surface diffusion tables (sdiff.cpp:62-83): per triangle the edge coefficients
     // g_e = l_e / (A d_e) towards same-patch neighbours, G = sum g_e, and the conditional
     // selectors c0 = g0 / G, c1 = g1 / (g1 + g2); the scaled constant is D G.
@@ -233,7 +406,7 @@ struct Solver {
         d_sdspec.alloc(nsdiff);
         d_snbr.alloc(snbr.size());
         d_sgeo.alloc(sgeo.size());
-        d_tri_inner.alloc(ntris);
+        if (!d_tri_inner.p) d_tri_inner.alloc(ntris);
         h2d(d_sdcst.p, sdcst.data(), sdcst.size());
         h2d(d_sdslot.p, sdiff_slot.data(), sdiff_slot.size());
         h2d(d_sdspec.p, sdspec.data(), sdspec.size());
@@ -271,7 +444,7 @@ struct Solver {
         }
         surf_touches_volume = false;
         for (auto& r : sreacs)
-            if (r.niupd > 0) surf_touches_volume = true;
+            if (r.niupd > 0 || r.noupd > 0) surf_touches_volume = true;
         for (auto& g : ghks)
             if (g.realflux) surf_touches_volume = true;
         if (!ghks.empty()) {
@@ -306,10 +479,16 @@ struct Solver {
         d_ohmics.alloc(std::max<size_t>(ohmics.size(), 1));
         d_surf_ext.alloc(1);
         h2d(d_tet_tris.p, tt.data(), tt.size());
-        // Tets with membrane triangles, ascending: the SURF launch of a split window.
+        if (!d_tri_inner.p) {
+            d_tri_inner.alloc(ntris);
+            h2d(d_tri_inner.p, tri_inner.data(), tri_inner.size());
+        }
+        setup_units();
+        // Tets with membrane triangles and no merged unit, ascending: the SURF launch of a
+        // split window.
         std::vector<int32_t> mt;
         for (int t = 0; t < ntets; ++t)
-            if (tt[(size_t)t * 4] >= 0) mt.push_back(t);
+            if (tt[(size_t)t * 4] >= 0 && tet_unit_h[t] < 0) mt.push_back(t);
         nmemb_tets = (int)mt.size();
         d_memb_tets.alloc(std::max<size_t>(mt.size(), 1));
         if (!mt.empty()) h2d(d_memb_tets.p, mt.data(), mt.size());
@@ -354,6 +533,8 @@ struct Solver {
             s.tri_echarge = d_tri_echarge.p;
         }
         s.temp = temp;
+        s.tri_inner = d_tri_inner.p;
+        s.tri_outer = d_tri_outer.p;
         if (nsdiff > 0) {
             s.tri_outflow = d_tri_out.p;
             s.tri_occ = d_tri_occ.p;
@@ -362,7 +543,6 @@ struct Solver {
             s.sdcst = d_sdcst.p;
             s.snbr = d_snbr.p;
             s.sgeo = d_sgeo.p;
-            s.tri_inner = d_tri_inner.p;
             s.nsdiff = nsdiff;
         }
         s.nsspec = nsspec;
@@ -798,6 +978,7 @@ struct Solver {
         a.launch_state = d_launch.p;
         a.status = d_status.p;
         a.surf = surf_args();
+        a.units = unit_args();
         a.surf_ext = has_surf() ? d_surf_ext.p : nullptr;
         a.tdel = d_tdel.p;
         a.tmask = d_tmask.p;
@@ -879,7 +1060,7 @@ struct Solver {
         return (int)std::max(1L, std::min(need, cap));
     }
 
-    bool use_split() const { return split || nsdiff > 0; }
+    bool use_split() const { return split || nsdiff > 0 || nunits > 0; }
     void ensure_split_buffers() {
         if (!d_tdel.p && ndiff > 0) d_tdel.alloc((size_t)ndiff * ntets);
         if (!d_tmask.p && ndiff > 0) d_tmask.alloc((size_t)ntets);
@@ -943,6 +1124,10 @@ struct Solver {
                 window_kernel<128, true, true><<<gm, 128, sm, stream>>>(am, chk);
                 SG_CUDA(cudaGetLastError());
             }
+            if (nunits > 0) {
+                unit_ssa_kernel<32><<<(nunits + 31) / 32, 32, 0, stream>>>(a);
+                SG_CUDA(cudaGetLastError());
+            }
             if (nsdiff > 0) {
                 const long long sp = (long long)nsdiff * ntris;
                 const int gsd = (int)std::max(1LL, std::min((sp + 255) / 256, (long long)nsm * 64));
@@ -972,6 +1157,68 @@ struct Solver {
             }
         }
         SG_CUDA(cudaGetLastError());
+    }
+
+    // ---- persistent form ----
+    // Models without membrane triangles whose realizations all take the same windows.
+    bool persist_ok(const std::vector<uint64_t>& k, uint64_t n) const {
+        if (has_surf() || nunits > 0) return false;
+        for (uint64_t x : k)
+            if (x != n) return false;
+        return true;
+    }
+    void ensure_persist_tables() {
+        if (pchunk_tpl == persist_tpl && d_pchunk.p) return;
+        const int tpw = 32 * persist_tpl;
+        std::vector<int32_t> cb(nreal + 1, 0);
+        for (int r = 0; r < nreal; ++r) cb[r + 1] = cb[r] + (real_begin[r + 1] - real_begin[r] + tpw - 1) / tpw;
+        d_pchunk.alloc(cb.size());
+        h2d(d_pchunk.p, cb.data(), cb.size());
+        if (!d_pstate.p) d_pstate.alloc((size_t)2 * nreal + 1);
+        if (!d_pnext.p) d_pnext.alloc(1);
+        pchunks = cb[nreal];
+        pchunk_tpl = persist_tpl;
+    }
+    template <int B, int TPL>
+    void persist_launch(sg_window_args a, sg_persist_args P, size_t sm) {
+        auto fn = persistent_window_kernel<B, TPL>;
+        if (sm > 48 * 1024) SG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int per_sm = 0;
+        SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, B, sm));
+        if (per_sm < 1) throw NotImplErr("the persistent window kernel does not fit an SM");
+        const long need = ((long)P.nchunks * 32 + B - 1) / B;
+        const int grid = (int)std::max(1L, std::min(need, (long)per_sm * nsm));
+        void* args[] = {&a, &P};
+        SG_CUDA(cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(B), args, sm, stream));
+    }
+    // nwin windows of every realization in one launch; the next ordinary window launch skips
+    // its conservation check (the persistent launch keeps no per-window totals).
+    void launch_persistent(const sg_window_args& a, int nwin) {
+        ensure_persist_tables();
+        SG_CUDA(cudaMemsetAsync(d_pstate.p, 0, d_pstate.n * sizeof(unsigned int), stream));
+        SG_CUDA(cudaMemsetAsync(d_pnext.p, 0, sizeof(unsigned long long), stream));
+        sg_persist_args P;
+        std::memset(&P, 0, sizeof(P));
+        P.chunk_begin = d_pchunk.p;
+        P.done = d_pstate.p;
+        P.ready = d_pstate.p + nreal;
+        P.abort = d_pstate.p + 2 * nreal;
+        P.next = d_pnext.p;
+        P.spin_limit = persist_spin_limit;
+        P.nchunks = pchunks;
+        P.nwin = nwin;
+        P.tpw = 32 * persist_tpl;
+        const int B = block >= 256 ? 256 : 128;
+        const size_t sm = smem_bytes(B, nspec, (int)reacs.size());
+        if (B == 256) {
+            if (persist_tpl == 2) persist_launch<256, 2>(a, P, sm);
+            else persist_launch<256, 1>(a, P, sm);
+        } else {
+            if (persist_tpl == 2) persist_launch<128, 2>(a, P, sm);
+            else persist_launch<128, 1>(a, P, sm);
+        }
+        SG_CUDA(cudaGetLastError());
+        SG_CUDA(cudaMemsetAsync(d_launch.p + 3, 0, sizeof(unsigned long long), stream));
     }
 
     // ---- CUDA graph of kGraphChunk window launches, rebuilt when the launch changes ----
@@ -1119,10 +1366,13 @@ struct Solver {
     // fixed list of candidates is timed on one window in list order and on one more in
     // reverse order (a palindromic schedule, so that the drift of the per-window work as
     // the run evolves cancels to first order): block {64, 128, 256} x grid {occupancy-
-    // sized, one tet per thread}; block 256, one tet per thread at shared-memory carveouts
-    // 75% and 50%; split windows at block 128 and 256.  The fastest is kept.
+    // sized, one tet per thread}; block 256, one tet per thread at a shared-memory carveout
+    // of 75%; split windows at block 128 and 256; the persistent form at block 128 and 256
+    // with 32 tets per work chunk and at block 256 with 64 (two tets per lane), when every
+    // realization takes the same windows.  The fastest is kept.
     static constexpr int kTuneWindows = 2;
-    static constexpr int kTuneCands = 10;
+    static constexpr int kTuneCands = 12;
+    static constexpr uint64_t kPersistMaxWindows = 64;  // windows per persistent launch
     bool tune_pending = false;
     std::vector<float> tune_ms;
     int carveout = 100;  // preferred shared-memory carveout of the window kernels, percent
@@ -1139,15 +1389,18 @@ struct Solver {
         SG_CUDA(cudaFuncSetAttribute(window_kernel<128, true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
     }
 
-    uint64_t autotune(const sg_window_args& a) {
+    uint64_t autotune(const sg_window_args& a, bool persist_allowed) {
         struct Cand {
             int block, grid, carve;
             bool split;
+            int ptpl;  // > 0: persistent form with this many tets per lane
         };
-        const Cand cands[kTuneCands] = {{64, 0, 100, false},   {64, -1, 100, false},  {128, 0, 100, false},
-                                        {128, -1, 100, false}, {256, 0, 100, false},  {256, -1, 100, false},
-                                        {256, -1, 75, false},  {256, -1, 50, false},  {128, -1, 100, true},
-                                        {256, -1, 100, true}};
+        const Cand cands[kTuneCands] = {{64, 0, 100, false, 0},   {64, -1, 100, false, 0},
+                                        {128, 0, 100, false, 0},  {128, -1, 100, false, 0},
+                                        {256, 0, 100, false, 0},  {256, -1, 100, false, 0},
+                                        {256, -1, 75, false, 0},  {128, -1, 100, true, 0},
+                                        {256, -1, 100, true, 0},  {128, 0, 100, false, 1},
+                                        {256, 0, 100, false, 1},  {256, 0, 100, false, 2}};
         tune_ms.assign(kTuneCands, 0.0f);
         cudaEvent_t e0, e1;
         SG_CUDA(cudaEventCreate(&e0));
@@ -1161,7 +1414,12 @@ struct Solver {
             set_carveout(c.carve);
             const int g = window_grid();
             SG_CUDA(cudaEventRecord(e0, stream));
-            launch_window(as, g);
+            if (c.ptpl > 0 && persist_allowed) {
+                persist_tpl = c.ptpl;
+                launch_persistent(as, 1);
+            } else {
+                launch_window(as, g);
+            }
             SG_CUDA(cudaEventRecord(e1, stream));
             SG_CUDA(cudaEventSynchronize(e1));
             float ms = 0.0f;
@@ -1173,12 +1431,14 @@ struct Solver {
         for (int i = kTuneCands - 1; i >= 0; --i) tune_ms[i] += timed(cands[i]);
         int best = 0;
         for (int i = 1; i < kTuneCands; ++i)
-            if (tune_ms[i] < tune_ms[best]) best = i;
+            if (tune_ms[i] < tune_ms[best] && (cands[i].ptpl == 0 || persist_allowed)) best = i;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         block = cands[best].block;
         grid = cands[best].grid;
         split = cands[best].split;
+        persist = cands[best].ptpl > 0;
+        if (persist) persist_tpl = cands[best].ptpl;
         set_carveout(cands[best].carve);
         tune_pending = false;
         return (uint64_t)kTuneWindows * kTuneCands + 1;
@@ -1197,8 +1457,9 @@ struct Solver {
         if (n == 0) return 0;
         sg_window_args a = window_args();
         uint64_t done = 0;
+        const bool pok = persist_ok(k, n);
         if (tune_pending && !has_surf() && n > (uint64_t)kTuneWindows * kTuneCands + 1) {
-            done = autotune(a);
+            done = autotune(a, pok);
             a = window_args();  // the tuner may have allocated the split buffers
         }
         if (use_split()) {
@@ -1207,14 +1468,24 @@ struct Solver {
         }
         int g = window_grid();
         if (profiling) SG_CUDA(cudaEventRecord(ev_begin, stream));
-        // Windows advance their own time on the device, so a captured chunk of window
-        // launches replays unchanged; the remainder is launched directly.
-        if (use_graphs && n - done >= (uint64_t)kGraphChunk) {
-            cudaGraphExec_t ge = window_graph(a, g);
-            for (; done + kGraphChunk <= n; done += kGraphChunk) SG_CUDA(cudaGraphLaunch(ge, stream));
+        if (persist && pok) {
+            // Persistent form: up to kPersistMaxWindows windows of every realization per launch.
+            while (done < n) {
+                const uint64_t nw = std::min(n - done, kPersistMaxWindows);
+                launch_persistent(a, (int)nw);
+                done += nw;
+                launches += 1;
+            }
+        } else {
+            // Windows advance their own time on the device, so a captured chunk of window
+            // launches replays unchanged; the remainder is launched directly.
+            if (use_graphs && n - done >= (uint64_t)kGraphChunk) {
+                cudaGraphExec_t ge = window_graph(a, g);
+                for (; done + kGraphChunk <= n; done += kGraphChunk) SG_CUDA(cudaGraphLaunch(ge, stream));
+            }
+            for (; done < n; ++done) launch_window(a, g);
+            launches += n;
         }
-        for (; done < n; ++done) launch_window(a, g);
-        launches += n;
         if (profiling) {
             SG_CUDA(cudaEventRecord(ev_end, stream));
             SG_CUDA(cudaEventSynchronize(ev_end));
@@ -1246,6 +1517,7 @@ struct Solver {
             if (st & SG_ERR_NEGATIVE) m += " negative count;";
             if (st & SG_ERR_TABLE) m += " table index out of range;";
             if (st & SG_ERR_CG) m += " EField CG did not converge;";
+            if (st & SG_ERR_WAIT) m += " a persistent window launch gave up waiting on a realization;";
             throw DeviceErr(m);
         }
     }
@@ -2194,6 +2466,28 @@ int sg_set_split(sg_solver* h, int32_t on) {
     return guarded([&] { S(h)->split = on != 0; });
 }
 
+int sg_set_persistent(sg_solver* h, int32_t on, int32_t tets_per_lane) {
+    return guarded([&] {
+        if (tets_per_lane != 1 && tets_per_lane != 2) throw sg::ArgErr("tets per lane must be 1 or 2");
+        Solver* s = S(h);
+        s->persist = on != 0;
+        s->persist_tpl = tets_per_lane;
+    });
+}
+
+int sg_get_persistent(sg_solver* h, int32_t* on, int32_t* tets_per_lane) {
+    return guarded([&] {
+        need(on, "on");
+        need(tets_per_lane, "tets_per_lane");
+        *on = S(h)->persist ? 1 : 0;
+        *tets_per_lane = S(h)->persist_tpl;
+    });
+}
+
+int sg_set_window_wait_limit(sg_solver* h, uint32_t polls) {
+    return guarded([&] { S(h)->persist_spin_limit = polls; });
+}
+
 int sg_get_split(sg_solver* h, int32_t* on) {
     return guarded([&] {
         need(on, "on");
@@ -2265,8 +2559,6 @@ int sg_add_ghk(sg_solver* h, int32_t patch, int32_t sspec, int32_t ion, int32_t 
         s->check_spec(ion);
         if (valence == 0) throw sg::ArgErr("GHK current of an ion without valence");
         if (!(perm > 0.0)) throw sg::ArgErr("GHK permeability must be positive (setP or setPInfo)");
-        if (!(voconc >= 0.0))
-            throw sg::NotImplErr("GHK current without a virtual outer concentration (no outer tets here)");
         sg_ghk g{};
         g.patch = patch;
         g.sspec = sspec;
@@ -2274,7 +2566,7 @@ int sg_add_ghk(sg_solver* h, int32_t patch, int32_t sspec, int32_t ion, int32_t 
         g.valence = valence;
         g.perm = perm;
         g.vshift = vshift;
-        g.voconc = voconc;
+        g.voconc = voconc >= 0.0 ? voconc : -1.0;  // < 0: the outer tet's concentration
         g.realflux = realflux ? 1 : 0;
         s->ghks.push_back(g);
         if (out_idx) *out_idx = (int32_t)s->ghks.size() - 1;
@@ -2419,6 +2711,60 @@ int sg_add_vdep_sreac(sg_solver* h, int32_t patch, const uint32_t* slhs, const u
         s->sreacs.push_back(r);
         s->skcst.push_back(0.0);
         if (out_idx) *out_idx = (int32_t)s->sreacs.size() - 1;
+    });
+}
+
+int sg_set_tri_outer(sg_solver* h, const int32_t* tri_outer_tet) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (s->ntris <= 0) throw sg::ProgErr("call sg_set_surface first");
+        need(tri_outer_tet, "tri_outer_tet");
+        s->tri_outer.assign(tri_outer_tet, tri_outer_tet + s->ntris);
+        for (int m = 0; m < s->ntris; ++m) {
+            const int o = s->tri_outer[m];
+            if (o < -1 || o >= s->ntets) throw sg::ArgErr("outer tet index out of range");
+            if (o >= 0 && o == s->tri_inner[m]) throw sg::ArgErr("a triangle's outer tet equals its inner tet");
+        }
+    });
+}
+
+int sg_set_sreac_outer(sg_solver* h, int32_t sreac, const uint32_t* olhs, const int32_t* oupd) {
+    return guarded([&] {
+        Solver* s = S(h);
+        s->require_not_setup();
+        if (sreac < 0 || sreac >= (int32_t)s->sreacs.size()) throw sg::ArgErr("surface reaction index out of range");
+        need(olhs, "olhs");
+        need(oupd, "oupd");
+        sg_sreac& r = s->sreacs[sreac];
+        int n = 0, order = 0;
+        for (int i = 0; i < s->nspec; ++i) {
+            if (!olhs[i]) continue;
+            if (olhs[i] > 4 || n == SG_MAX_LHS) throw sg::ArgErr("volume reactant stoichiometry");
+            ++n;
+            order += (int)olhs[i];
+        }
+        if (n > 0 && r.nilhs > 0)
+            throw sg::ArgErr("a surface reaction has volume reactants on one side only (inner or outer)");
+        if (n > 0) {
+            r.nilhs = 0;
+            for (int i = 0; i < s->nspec; ++i) {
+                if (!olhs[i]) continue;
+                r.ilhs_spec[r.nilhs] = i;
+                r.ilhs_ord[r.nilhs++] = (int32_t)olhs[i];
+            }
+            r.order += order;
+            if (r.order > 4) throw sg::ArgErr("reaction order above 4 is not supported");
+            r.vside = 1;
+            r.surf_surf = 0;
+        }
+        r.noupd = 0;
+        for (int i = 0; i < s->nspec; ++i) {
+            if (!oupd[i]) continue;
+            if (r.noupd == SG_MAX_UPD) throw sg::ArgErr("too many changed volume species");
+            r.oupd_spec[r.noupd] = i;
+            r.oupd_delta[r.noupd++] = oupd[i];
+        }
     });
 }
 

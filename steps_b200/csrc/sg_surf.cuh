@@ -91,6 +91,17 @@ __device__ inline double ghk_rate(const sg_ghk& g, double vm, uint32_t c_ion, ui
     return I / (SG_E_CHARGE * (double)g.valence) * (double)n;
 }
 
+// Signed rate of a GHK current whose outer concentration is that of the outer tet, c_out
+// ions in a tet of 1/(1e3 V N_A) = ivs_out (ghkcurr.cpp:176-181 with voconc < 0).
+__device__ inline double ghk_rate_outer(const sg_ghk& g, double vm, uint32_t c_ion, uint32_t n, double ivs,
+                                        uint32_t c_out, double ivs_out, double temp, uint32_t* status) {
+    if (n == 0) return 0.0;
+    const double ci = (double)c_ion * ivs * 1.0e3;
+    const double co = (double)c_out * ivs_out * 1.0e3;
+    const double I = ghk_current(g.perm, vm * 1.0e-3 + g.vshift, g.valence, temp, ci, co, status);
+    return I / (SG_E_CHARGE * (double)g.valence) * (double)n;
+}
+
 // Scaled constant of a surface reaction on triangle m whose inner tet has 1/(1e3 V N_A) = ivs.
 __device__ inline double sreac_ccst(const sg_sreac& r, double k, double ivs, double area) {
     if (r.surf_surf) {
@@ -125,6 +136,26 @@ __device__ inline double sreac_h(const sg_sreac& r, const uint32_t* scnt_slot, c
     }
     for (int i = 0; i < r.nilhs; ++i) {
         uint32_t c = vcnt[r.ilhs_spec[i] * stride];
+        uint32_t o = (uint32_t)r.ilhs_ord[i];
+        if (o > c) return 0.0;
+        h = h * falling(c, o);
+    }
+    return h;
+}
+
+// The same product with the surface and volume counts at their own strides (the merged
+// units read them from the global count arrays); vcnt is the tet on the reactants' side.
+__device__ inline double sreac_h2(const sg_sreac& r, const uint32_t* scnt, int sstride, const uint32_t* vcnt,
+                                  int vstride) {
+    double h = 1.0;
+    for (int i = 0; i < r.nslhs; ++i) {
+        uint32_t c = scnt[(size_t)r.slhs_spec[i] * sstride];
+        uint32_t o = (uint32_t)r.slhs_ord[i];
+        if (o > c) return 0.0;
+        h = h * falling(c, o);
+    }
+    for (int i = 0; i < r.nilhs; ++i) {
+        uint32_t c = vcnt[(size_t)r.ilhs_spec[i] * vstride];
         uint32_t o = (uint32_t)r.ilhs_ord[i];
         if (o > c) return 0.0;
         h = h * falling(c, o);

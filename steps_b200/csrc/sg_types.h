@@ -69,7 +69,9 @@ static inline uint32_t sg_reac_fast_code(const sg_reac* r) {
 // One surface reaction of a patch (Patchdef sreac_lhs_S/I, sreac_upd_S/I,
 // src/steps/solver/patchdef.hpp), optionally with a voltage-dependent constant
 // (VDepSReacdef, src/steps/solver/vdepsreacdef.cpp:194-218).  Reactants and products on
-// the triangle (S) and in its inner tet (I); outer-volume terms are not supported.
+// the triangle (S), in its inner tet (I) and in its outer tet (O).  As in the reference
+// (SReacdef::inside / outside), the volume reactants are all on one side: ilhs holds them
+// and vside says which tet they are counted in (and whose volume scales the constant).
 typedef struct sg_sreac {
     int32_t patch;
     int32_t order;                     // total lhs stoichiometry (surface + volume)
@@ -80,6 +82,9 @@ typedef struct sg_sreac {
     int32_t ilhs_spec[SG_MAX_LHS], ilhs_ord[SG_MAX_LHS];
     int32_t supd_spec[SG_MAX_UPD], supd_delta[SG_MAX_UPD];
     int32_t iupd_spec[SG_MAX_UPD], iupd_delta[SG_MAX_UPD];
+    int32_t vside;                     // 0: volume reactants in the inner tet, 1: in the outer tet
+    int32_t noupd;                     // outer-tet species changed
+    int32_t oupd_spec[SG_MAX_UPD], oupd_delta[SG_MAX_UPD];
 } sg_sreac;
 
 // k(V) table of a voltage-dependent surface reaction: k at vmin + i dv, i < n (V, /s ...).
@@ -99,7 +104,9 @@ typedef struct sg_ohmic {
 } sg_ohmic;
 
 // GHK current (ghkcurr.cpp:168-280): channel state sspec of a patch passes ion (valence z)
-// with permeability perm (m^3/s per channel) against a fixed outer concentration voconc (M).
+// with permeability perm (m^3/s per channel) against a fixed outer concentration voconc (M),
+// or, with voconc < 0, against the concentration in the triangle's outer tet (the ions then
+// move between the two tets).
 typedef struct sg_ghk {
     int32_t patch;
     int32_t sspec;
@@ -107,7 +114,7 @@ typedef struct sg_ghk {
     int32_t valence;
     double perm;
     double vshift;                     // V
-    double voconc;                     // M
+    double voconc;                     // M; < 0: the outer tet's concentration
     int32_t realflux;                  // ions move (else charge only)
     int32_t pad_;
 } sg_ghk;
@@ -134,6 +141,7 @@ typedef struct sg_surf_args {
     const int32_t* snbr;               // [M][4]: (neighbour << 2) | its edge, -1 = none
     const float* sgeo;                 // [M][4]: conditional selectors c0, c1, 1, G = sum l/(A d)
     const int32_t* tri_inner;          // [M] inner tet (its realization owns the triangle)
+    const int32_t* tri_outer;          // [M] outer tet, -1 none (null when no triangle has one)
     int32_t nsdiff;
     const sg_ghk* ghks;                // [nghk]
     long long* tri_echarge;            // [M] elementary charges carried out by GHK events this EField step
@@ -164,6 +172,50 @@ typedef struct sg_real {
 #define SG_ERR_TABLE 4u                // a table index out of range
 #define SG_ERR_CG 8u                   // EField CG did not converge
 #define SG_ERR_NEGATIVE 16u            // a count would go below zero
+#define SG_ERR_WAIT 32u                // a persistent window launch gave up waiting on a realization
+
+// Merged SSA units.  A membrane triangle whose patch has surface reactions or GHK currents
+// that count or change species of its outer tet couples that tet to its inner one (the
+// reference keeps the triangle and both tets in one rank's SSA, sreac.cpp:200-300).  A
+// connected group of coupled tets, together with every membrane triangle whose inner tet is
+// in the group, is one SSA unit: elements are its tets (ascending) then its triangles
+// (ascending), each with its own reactions; the unit's direct-method SSA selects the
+// element through a binary sum tree of element propensities.
+typedef struct sg_unit_args {
+    const int32_t* tet_begin;          // [U + 1] into tets
+    const int32_t* tets;               // tets of each unit, ascending
+    const int32_t* tri_begin;          // [U + 1] into tris
+    const int32_t* tris;               // membrane triangles of each unit, ascending
+    const int32_t* elem_base;          // [U + 1]: first element of each unit (tets, then triangles)
+    const int32_t* tree_base;          // [U + 1]: first node of each unit's tree (2 P doubles, P = 2^k >= elements)
+    const int32_t* tet_unit;           // [T]: unit of a merged tet, -1 otherwise
+    const int32_t* tet_adj;            // [E][4]: for tet elements, the unit's triangle elements whose rates read the tet (-1)
+    const int32_t* tri_side;           // [M][2]: unit elements of a merged triangle's inner tet and coupled outer tet (-1)
+    double* prop;                      // [E][rmax] element reaction propensities (scratch)
+    double* tree;                      // sum trees (scratch)
+    double* socc;                      // [SS][M] surface occupancy integrals within the window (scratch)
+    double* slast;                     // [SS][M] time of the last change within the window (scratch)
+    int32_t nunits;
+    int32_t rmax;                      // reactions (and GHK currents) per element, at most
+} sg_unit_args;
+
+// One persistent launch that runs nwin windows of every batched realization.  Work items
+// are (window, chunk) in window-major order; a chunk is tpw consecutive tets of one
+// realization (32 lanes x tets per lane).  A warp takes the next item from the counter and
+// waits (bounded) until its realization has completed the previous window; the warp that
+// finishes the last chunk of a realization's window advances that realization's time and
+// publishes the window.
+typedef struct sg_persist_args {
+    const int32_t* chunk_begin;        // [nreal + 1] first chunk of each realization
+    unsigned int* done;                // [nreal] chunks finished in this launch
+    unsigned int* ready;               // [nreal] windows completed in this launch
+    unsigned long long* next;          // [1] next work item
+    unsigned int* abort;               // [1] set when a wait gave up
+    unsigned int spin_limit;           // polls of one wait before it gives up
+    int32_t nchunks;                   // chunks of one window over all realizations
+    int32_t nwin;                      // windows of this launch
+    int32_t tpw;                       // tets per chunk
+} sg_persist_args;
 
 // Window-kernel arguments.
 typedef struct sg_window_args {
@@ -210,6 +262,7 @@ typedef struct sg_window_args {
     const int32_t* bcomps;
     const double* btab;
     int32_t nbnd;
+    sg_unit_args units;                // merged SSA units (nunits = 0: none)
     int32_t ntets;                     // total tets over realizations
     int32_t nspec;
     int32_t ndiff;

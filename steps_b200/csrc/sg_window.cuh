@@ -838,6 +838,8 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
                 const int4 tr = __ldg(reinterpret_cast<const int4*>(a.surf.tet_tris) + t);
                 if (tr.x >= 0 || tr.y >= 0 || tr.z >= 0 || tr.w >= 0) active = false;
             }
+            // Tets of merged units run in unit_ssa_kernel.
+            if (SPLIT && a.units.tet_unit && __ldg(&a.units.tet_unit[t]) >= 0) active = false;
         }
         int4 nb = make_int4(-1, -1, -1, -1);
         uint32_t clampm = 0u;
@@ -1169,6 +1171,542 @@ __global__ void __launch_bounds__(BLOCK) sdiffuse_kernel(sg_window_args a) {
     if (lane == 0 && moved) atomicAdd(&s_moved, moved);
     __syncthreads();
     if (tid == 0 && s_moved) atomicAdd(a.diff_total, s_moved);
+}
+
+// ---- batched realizations in one persistent launch ----------------------------------
+
+__device__ __forceinline__ unsigned int sg_ld_acquire(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void sg_st_release(unsigned int* p, unsigned int v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// One tet's whole window (gather, SSA, diffusion leave, store) as the fused window kernel
+// runs it, with the counts and the inflow read through L2: inside a persistent launch they
+// were written by other SMs earlier in the same launch.
+__device__ __forceinline__ void fused_tet_coherent(const sg_window_args& a, const smem_layout& L, int tid, int BLOCK,
+                                                   int t, int r, int tlocal, double T, unsigned long long w,
+                                                   int pending, const double* s_rcp, unsigned long long* moved) {
+    const int S = a.nspec, R = a.nreac;
+    const size_t plane = (size_t)a.ntets * 4;
+    const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
+    if (comp < 0) return;
+    const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
+    const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
+    const double* Dc = a.dcst + ((size_t)r * a.ncomp + comp) * S;
+    const uint32_t* in = a.outflow + (size_t)((w + 1) & 1ull) * a.ndiff * plane;
+    for (int s = 0; s < S; ++s) {
+        uint32_t c = __ldcg(&a.counts[(size_t)s * a.ntets + t]);
+        const int ds = __ldg(&a.diff_slot[s]);
+        if (pending && ds >= 0 && __ldg(&Dc[s]) > 0.0 && !((clampm >> s) & 1u)) {
+            const uint4 v = __ldcg(reinterpret_cast<const uint4*>(in + (size_t)ds * plane) + t);
+            unsigned long long sum = c;
+            if (nb.x >= 0) sum += v.x;
+            if (nb.y >= 0) sum += v.y;
+            if (nb.z >= 0) sum += v.z;
+            if (nb.w >= 0) sum += v.w;
+            if (a.bface) sum += bnd_inflow(a, t, r, s, v);
+            if (sum > 0xFFFFFFFFull) {
+                atomicOr(a.status, SG_ERR_OVERFLOW);
+                sum = 0xFFFFFFFFull;
+            }
+            c = (uint32_t)sum;
+        }
+        L.tdel[s * BLOCK + tid] = 0.0;
+        L.cnt[s * BLOCK + tid] = c;
+    }
+    sg_stream st;
+    sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)tlocal, w, SG_PURPOSE_WINDOW);
+    const int rb = __ldg(&a.comp_reac_begin[comp]);
+    const int re = __ldg(&a.comp_reac_begin[comp + 1]);
+    if (re > rb) tet_ssa(a, L, tid, BLOCK, rb, re, a.kcst + (size_t)r * R, __ldg(&a.ivs[t]), clampm, T, &st);
+    const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
+    const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
+    const double cs[3] = {(double)g.x, (double)g.y, (double)g.z};
+    const double odd1 = sg_binom_odds(cs[0]);
+    const double odd2 = sg_binom_odds(cs[1]);
+    const double odd3 = sg_binom_odds(cs[2]);
+    uint32_t* out = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane;
+    const double invT = 1.0 / T;
+    for (int s = 0; s < S; ++s) {
+        const int ds = __ldg(&a.diff_slot[s]);
+        if (ds < 0) continue;
+        const double D = __ldg(&Dc[s]);
+        if (!(D > 0.0)) continue;
+        const uint32_t pop = L.cnt[s * BLOCK + tid];
+        uint4 k = make_uint4(0u, 0u, 0u, 0u);
+        if (pop > 0u) {
+            uint32_t Kn = 0u;
+            if (bt) {
+                float4 gb;
+                const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
+                const double cb[3] = {(double)gb.x, (double)gb.y, (double)gb.z};
+                k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
+                                  invT, T * tot, cb, sg_binom_odds(cb[0]), sg_binom_odds(cb[1]),
+                                  sg_binom_odds(cb[2]), s_rcp, nullptr, nullptr, &st, &Kn);
+            } else {
+                k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
+                                  invT, T * (D * (double)g.w), cs, odd1, odd2, odd3, s_rcp, nullptr, nullptr, &st,
+                                  &Kn);
+            }
+            if (Kn > 0u) {
+                if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
+                *moved += Kn;
+            }
+        }
+        uint32_t* po = out + (size_t)ds * plane;
+        if (nb.x >= 0) po[nb.x] = k.x;
+        if (nb.y >= 0) po[nb.y] = k.y;
+        if (nb.z >= 0) po[nb.z] = k.z;
+        if (nb.w >= 0) po[nb.w] = k.w;
+        if (bt) bnd_scatter(a, t, po, k);
+    }
+    for (int s = 0; s < S; ++s) a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
+}
+
+// P.nwin windows of every batched realization in one launch (all blocks resident: a
+// cooperative launch).  Items are taken in window-major order, so every item a warp waits
+// for was taken earlier by a resident warp that itself only waits on earlier items: the
+// waits end.  Each wait is still bounded (P.spin_limit polls); a wait that runs out sets
+// SG_ERR_WAIT and the abort word, and every warp then stops at its next wait or item.
+// Reaction extents go straight to the run totals; the per-window conservation check of
+// the window launches is replaced by the host's check over the whole run() call.
+template <int BLOCK, int TPL>
+__global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
+    persistent_window_kernel(sg_window_args a, sg_persist_args P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double s_rcp[SG_RCP_TABLE];
+    const int S = a.nspec, R = a.nreac, tid = threadIdx.x, lane = tid & 31;
+    smem_layout L = carve(smem_raw, BLOCK, S, R);
+    for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
+    for (int i = tid; i < R; i += BLOCK) L.reac[i] = a.reacs[i];
+    for (int i = tid; i < R; i += BLOCK) L.ext[i] = 0u;
+    if (tid == 0) L.moved[0] = 0ull;
+    __syncthreads();
+    unsigned long long moved = 0ull;
+    const unsigned long long nitems = (unsigned long long)P.nwin * (unsigned long long)P.nchunks;
+    for (;;) {
+        unsigned long long item = 0ull;
+        if (lane == 0) item = atomicAdd(P.next, 1ull);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= nitems) break;
+        const int wrel = (int)(item / (unsigned long long)P.nchunks);
+        const int j = (int)(item - (unsigned long long)wrel * (unsigned long long)P.nchunks);
+        int lo = 0, hi = a.nreal - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&P.chunk_begin[mid]) <= j) lo = mid;
+            else hi = mid - 1;
+        }
+        const int r = lo;
+        const int c0 = __ldg(&P.chunk_begin[r]);
+        const unsigned int nch = (unsigned int)(__ldg(&P.chunk_begin[r + 1]) - c0);
+        int ok = 1;
+        if (lane == 0) {
+            unsigned int polls = 0u;
+            while (sg_ld_acquire(&P.ready[r]) < (unsigned int)wrel) {
+                if (__ldcg(P.abort) != 0u || ++polls > P.spin_limit) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+            if (lane == 0) {
+                atomicOr(P.abort, 1u);
+                atomicOr(a.status, SG_ERR_WAIT);
+            }
+            break;
+        }
+        (void)sg_ld_acquire(&P.ready[r]);  // every lane reads the previous window's writes after this
+        const sg_real* rl = &a.reals[r];
+        const double rt = __ldcg(&rl->t), rend = __ldcg(&rl->t_end), per = __ldcg(&rl->period);
+        const unsigned long long w = __ldcg(&rl->window);
+        const int pending = __ldcg(&rl->pending);
+        const int tb = __ldg(&rl->tet_begin), te = __ldg(&rl->tet_end);
+        const bool live = rt < rend;
+        const double T = (rt + per > rend) ? rend - rt : per;
+#pragma unroll 1
+        for (int k = 0; k < TPL; ++k) {
+            const int t = tb + (j - c0) * 32 * TPL + k * 32 + lane;
+            if (live && t < te) fused_tet_coherent(a, L, tid, BLOCK, t, r, t - tb, T, w, pending, s_rcp, &moved);
+        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) {
+            const unsigned int prev = atomicAdd(&P.done[r], 1u);
+            if (prev + 1u == (unsigned int)(wrel + 1) * nch) {
+                // Last chunk of this realization's window: advance it (as window_last_block)
+                // and publish the window.
+                sg_real* rw = &a.reals[r];
+                if (live) {
+                    rw->t = (rt + per > rend) ? rend : rt + per;
+                    rw->window = w + 1ull;
+                    rw->pending = 1;
+                }
+                __threadfence();
+                sg_st_release(&P.ready[r], (unsigned int)(wrel + 1));
+            }
+        }
+    }
+    moved = warp_sum_u64(moved);
+    if (lane == 0 && moved) atomicAdd(L.moved, moved);
+    __syncthreads();
+    for (int i = tid; i < R; i += BLOCK)
+        if (L.ext[i]) atomicAdd(&a.ext_total[i], (unsigned long long)L.ext[i]);
+    if (tid == 0 && L.moved[0]) atomicAdd(a.diff_total, L.moved[0]);
+}
+
+// ---- merged SSA units (surface reactions and GHK currents that reach the outer tet) ----
+//
+// The reference keeps a triangle, its inner tet and its outer tet in one rank's SSA
+// (sreac.cpp:200-300 rejects any other placement), so the events of all tets linked through
+// such triangles form one SSA.  Here each such unit runs on one thread: elements are the
+// unit's tets (their volume reactions, reac.cpp:184-251) and triangles (surface reactions
+// sreac.cpp:305-520, with inner or outer volume reactants and products, then GHK currents
+// ghkcurr.cpp:168-280), selected through a binary tree of element propensity sums; after an
+// event only the elements whose rates read a changed count are re-evaluated.  State lives in
+// the global count arrays (units are few and touch scattered tets).
+
+// Number of reactions (and GHK currents) of element e.
+__device__ __forceinline__ int unit_elem_nq(const sg_window_args& a, int e, int nt, const int32_t* tets,
+                                            const int32_t* tris) {
+    if (e < nt) {
+        const int comp = a.comp ? __ldg(&a.comp[tets[e]]) : 0;
+        return __ldg(&a.comp_reac_begin[comp + 1]) - __ldg(&a.comp_reac_begin[comp]);
+    }
+    const sg_surf_args& sa = a.surf;
+    const int p = sa.tri_patch[tris[e - nt]];
+    int n = sa.patch_sreac_begin[p + 1] - sa.patch_sreac_begin[p];
+    for (int g = 0; g < sa.nghk; ++g) n += sa.ghks[g].patch == p ? 1 : 0;
+    return n;
+}
+
+// Propensities of element e into prop[0..nq); returns their sum in reaction order.
+static __device__ __noinline__ double unit_elem_props(const sg_window_args& a, int e, int nt, const int32_t* tets,
+                                                      const int32_t* tris, int r, double* prop) {
+    const sg_surf_args& sa = a.surf;
+    double sum = 0.0;
+    if (e < nt) {
+        const int t = tets[e];
+        const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
+        const int rb = __ldg(&a.comp_reac_begin[comp]), re = __ldg(&a.comp_reac_begin[comp + 1]);
+        const double ivs = __ldg(&a.ivs[t]);
+        const double* K = a.kcst + (size_t)r * a.nreac;
+        for (int q = rb; q < re; ++q) {
+            const sg_reac* rc = &a.reacs[q];
+            const double p = reac_prop(rc, a.counts + t, a.ntets, reac_ccst(rc, __ldg(&K[q]), ivs));
+            prop[q - rb] = p;
+            sum = sum + p;
+        }
+        return sum;
+    }
+    const int M = sa.ntris;
+    const int m = tris[e - nt];
+    const int p = sa.tri_patch[m];
+    const int pb = sa.patch_sreac_begin[p], pe = sa.patch_sreac_begin[p + 1];
+    const int ti = sa.tri_inner[m];
+    const int to = sa.tri_outer ? sa.tri_outer[m] : -1;
+    const double area = sa.tri_area[m];
+    const double vm = sa.tri_V ? sa.tri_V[m] : 0.0;
+    const double ivs_i = __ldg(&a.ivs[ti]);
+    const double ivs_o = to >= 0 ? __ldg(&a.ivs[to]) : 0.0;
+    int kk = 0;
+    for (int q = pb; q < pe; ++q, ++kk) {
+        const sg_sreac& rs = sa.sreacs[q];
+        const double k = (rs.vdep >= 0) ? vdep_k(sa, rs.vdep, vm, a.status) : sa.skcst[q];
+        const int tv = rs.vside ? to : ti;
+        double pq = 0.0;
+        if (tv >= 0) {
+            const double h = sreac_h2(rs, sa.tri_counts + m, M, a.counts + tv, a.ntets);
+            pq = h * sreac_ccst(rs, k, rs.vside ? ivs_o : ivs_i, area);
+        }
+        prop[kk] = pq;
+        sum = sum + pq;
+    }
+    for (int g = 0; g < sa.nghk; ++g) {
+        const sg_ghk& gh = sa.ghks[g];
+        if (gh.patch != p) continue;
+        const uint32_t n = sa.tri_counts[(size_t)gh.sspec * M + m];
+        const uint32_t ci = a.counts[(size_t)gh.ion * a.ntets + ti];
+        double rt;
+        if (gh.voconc >= 0.0 || to < 0)
+            rt = ghk_rate(gh, vm, ci, n, ivs_i, sa.temp, a.status);
+        else
+            rt = ghk_rate_outer(gh, vm, ci, n, ivs_i, a.counts[(size_t)gh.ion * a.ntets + to], ivs_o, sa.temp,
+                                a.status);
+        const double pq = fabs(rt);
+        prop[kk++] = pq;
+        sum = sum + pq;
+    }
+    return sum;
+}
+
+// Count of volume species s in tet t changes by d at time tt of the window (skipped when
+// clamped): bounds, and the change-time sum of a diffusing species.
+__device__ __forceinline__ void unit_bump_tet(const sg_window_args& a, int t, int s, int d, double tt) {
+    const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
+    if ((clampm >> s) & 1u) return;
+    uint32_t* pc = a.counts + (size_t)s * a.ntets + t;
+    const uint32_t old = *pc;
+    long long nc = (long long)old + d;
+    if (nc < 0 || nc > 0xFFFFFFFFll) {
+        atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
+        nc = nc < 0 ? 0 : 0xFFFFFFFFll;
+    }
+    const int ds = __ldg(&a.diff_slot[s]);
+    if (ds >= 0) {
+        double* pd = a.tdel + (size_t)ds * a.ntets + t;
+        *pd = *pd + (double)(nc - (long long)old) * tt;
+    }
+    *pc = (uint32_t)nc;
+}
+
+// Re-evaluate element f and the sums on its path to the root.
+__device__ __forceinline__ void unit_refresh(const sg_window_args& a, int f, int nt, const int32_t* tets,
+                                             const int32_t* tris, int r, double* prop, double* tree, int P) {
+    int i = P + f;
+    tree[i] = unit_elem_props(a, f, nt, tets, tris, r, prop + (size_t)f * a.units.rmax);
+    for (i >>= 1; i >= 1; i >>= 1) tree[i] = tree[2 * i] + tree[2 * i + 1];
+}
+
+// Element f (a tet) and the unit's triangles whose rates read it.
+__device__ __forceinline__ void unit_refresh_tet(const sg_window_args& a, int f, int eb, int nt, const int32_t* tets,
+                                                 const int32_t* tris, int r, double* prop, double* tree, int P) {
+    if (f < 0) return;
+    unit_refresh(a, f, nt, tets, tris, r, prop, tree, P);
+    const int4 adj = __ldg(reinterpret_cast<const int4*>(a.units.tet_adj) + eb + f);
+    if (adj.x >= 0) unit_refresh(a, adj.x, nt, tets, tris, r, prop, tree, P);
+    if (adj.y >= 0) unit_refresh(a, adj.y, nt, tets, tris, r, prop, tree, P);
+    if (adj.z >= 0) unit_refresh(a, adj.z, nt, tets, tris, r, prop, tree, P);
+    if (adj.w >= 0) unit_refresh(a, adj.w, nt, tets, tris, r, prop, tree, P);
+}
+
+// SSA of every merged unit over its window, one thread per unit, between the volume and
+// membrane SSA passes and the diffusion leave of a split window: gathers the unit's inflow,
+// writes its tets' counts, change-time sums and tmask, its triangles' counts and occupancy
+// integrals.  The unit draws from the window stream of its first tet.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) unit_ssa_kernel(sg_window_args a) {
+    const sg_unit_args& U = a.units;
+    const sg_surf_args& sa = a.surf;
+    const unsigned long long parity = __ldcg(&a.launch_state[1]) & 1ull;
+    const size_t plane = (size_t)a.ntets * 4;
+    const int S = a.nspec, SS = sa.nsspec, M = sa.ntris;
+    for (int u = blockIdx.x * BLOCK + threadIdx.x; u < U.nunits; u += gridDim.x * BLOCK) {
+        const int tb = U.tet_begin[u], nt = U.tet_begin[u + 1] - tb;
+        const int mb = U.tri_begin[u], nm = U.tri_begin[u + 1] - mb;
+        const int32_t* tets = U.tets + tb;
+        const int32_t* tris = U.tris + mb;
+        const int r = find_real(a.reals, a.nreal, tets[0]);
+        const sg_real* rl = &a.reals[r];
+        const double rt = rl->t, rend = rl->t_end, per = rl->period;
+        if (!(rt < rend)) continue;
+        const double T = (rt + per > rend) ? rend - rt : per;
+        const unsigned long long w = rl->window;
+        const int pending = rl->pending;
+        // Gather the last window's inflow into the unit's tets and triangles.
+        const uint32_t* in = a.outflow + (size_t)((w + 1) & 1ull) * a.ndiff * plane;
+        for (int k = 0; k < nt; ++k) {
+            const int t = tets[k];
+            const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
+            const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
+            const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
+            const double* Dc = a.dcst + ((size_t)r * a.ncomp + comp) * S;
+            for (int s = 0; s < S; ++s) {
+                uint32_t c = a.counts[(size_t)s * a.ntets + t];
+                const int ds = __ldg(&a.diff_slot[s]);
+                if (pending && ds >= 0 && __ldg(&Dc[s]) > 0.0 && !((clampm >> s) & 1u)) {
+                    const uint4 v = __ldg(reinterpret_cast<const uint4*>(in + (size_t)ds * plane) + t);
+                    unsigned long long sum = c;
+                    if (nb.x >= 0) sum += v.x;
+                    if (nb.y >= 0) sum += v.y;
+                    if (nb.z >= 0) sum += v.z;
+                    if (nb.w >= 0) sum += v.w;
+                    if (a.bface) sum += bnd_inflow(a, t, r, s, v);
+                    if (sum > 0xFFFFFFFFull) {
+                        atomicOr(a.status, SG_ERR_OVERFLOW);
+                        sum = 0xFFFFFFFFull;
+                    }
+                    c = (uint32_t)sum;
+                }
+                if (ds >= 0) a.tdel[(size_t)ds * a.ntets + t] = 0.0;
+                a.counts[(size_t)s * a.ntets + t] = c;
+                if (c) atomicAdd(&a.totals[parity * S + s], (unsigned long long)c);
+            }
+        }
+        for (int j = 0; j < nm; ++j) {
+            const int m = tris[j];
+            const int p = sa.tri_patch[m];
+            for (int s = 0; s < SS; ++s) {
+                const size_t o = (size_t)s * M + m;
+                uint32_t c = sa.tri_counts[o];
+                if (pending && sa.tri_outflow) {
+                    const int sd = sa.sdiff_slot[s];
+                    if (sd >= 0 && sa.sdcst[(size_t)p * SS + s] > 0.0) {
+                        const uint4 v = reinterpret_cast<const uint4*>(
+                            sa.tri_outflow + (size_t)((w + 1) & 1ull) * sa.nsdiff * M * 4)[(size_t)sd * M + m];
+                        const int4 nb = reinterpret_cast<const int4*>(sa.snbr)[m];
+                        unsigned long long sum = c;
+                        if (nb.x >= 0) sum += v.x;
+                        if (nb.y >= 0) sum += v.y;
+                        if (nb.z >= 0) sum += v.z;
+                        if (sum > 0xFFFFFFFFull) {
+                            atomicOr(a.status, SG_ERR_OVERFLOW);
+                            sum = 0xFFFFFFFFull;
+                        }
+                        c = (uint32_t)sum;
+                    }
+                }
+                sa.tri_counts[o] = c;
+                U.socc[o] = 0.0;
+                U.slast[o] = 0.0;
+            }
+        }
+        // Element sums and the tree (node i = node 2i + node 2i + 1; leaves P..2P-1).
+        const int E = nt + nm;
+        const int eb = U.elem_base[u];
+        double* tree = U.tree + U.tree_base[u];
+        const int P = (U.tree_base[u + 1] - U.tree_base[u]) >> 1;
+        double* prop = U.prop + (size_t)eb * U.rmax;
+        for (int e = 0; e < P; ++e)
+            tree[P + e] = e < E ? unit_elem_props(a, e, nt, tets, tris, r, prop + (size_t)e * U.rmax) : 0.0;
+        for (int i = P - 1; i >= 1; --i) tree[i] = tree[2 * i] + tree[2 * i + 1];
+        sg_stream st;
+        sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)(tets[0] - rl->tet_begin), w, SG_PURPOSE_WINDOW);
+        double tt = 0.0;
+        for (;;) {
+            const double a0 = tree[1];
+            if (!(a0 > 0.0)) break;
+            const double dt = -sg_log(sg_u01_oc(sg_next_u32(&st))) / a0;
+            if (tt + dt > T) break;
+            tt = tt + dt;
+            double target = sg_u01_co(sg_next_u32(&st)) * a0;
+            // Descend: left while the target falls below the left sum (or nothing is right).
+            int node = 1;
+            while (node < P) {
+                const double l = tree[2 * node], rr = tree[2 * node + 1];
+                if (target < l || !(rr > 0.0)) {
+                    node = 2 * node;
+                } else {
+                    target = target - l;
+                    node = 2 * node + 1;
+                }
+            }
+            const int e = node - P;
+            const double* pq = prop + (size_t)e * U.rmax;
+            const int nq = unit_elem_nq(a, e, nt, tets, tris);
+            double cum = 0.0;
+            int sel = -1, lastnz = -1;
+            for (int q = 0; q < nq; ++q) {
+                const double p = pq[q];
+                if (p > 0.0) {
+                    lastnz = q;
+                    cum = cum + p;
+                    if (target < cum) {
+                        sel = q;
+                        break;
+                    }
+                }
+            }
+            if (sel < 0) sel = lastnz;
+            if (sel < 0) break;
+            if (e < nt) {
+                const int t = tets[e];
+                const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
+                const int q = __ldg(&a.comp_reac_begin[comp]) + sel;
+                const sg_reac* rc = &a.reacs[q];
+                for (int i = 0; i < rc->nupd; ++i) unit_bump_tet(a, t, rc->upd_spec[i], rc->upd_delta[i], tt);
+                atomicAdd(&a.ext[parity * a.nreac + q], 1ull);
+                unit_refresh_tet(a, e, eb, nt, tets, tris, r, prop, tree, P);
+                continue;
+            }
+            const int j = e - nt, m = tris[j];
+            const int p = sa.tri_patch[m];
+            const int pb = sa.patch_sreac_begin[p], npr = sa.patch_sreac_begin[p + 1] - pb;
+            const int ti = sa.tri_inner[m];
+            const int to = sa.tri_outer ? sa.tri_outer[m] : -1;
+            const int ei = U.tri_side[2 * m], eo = U.tri_side[2 * m + 1];
+            bool ci = false, co = false;  // inner / outer tet counts changed
+            if (sel < npr) {
+                const sg_sreac& rs = sa.sreacs[pb + sel];
+                for (int i = 0; i < rs.nsupd; ++i) {
+                    const size_t o = (size_t)rs.supd_spec[i] * M + m;
+                    const uint32_t old = sa.tri_counts[o];
+                    U.socc[o] = U.socc[o] + (double)old * (tt - U.slast[o]);
+                    U.slast[o] = tt;
+                    long long nc = (long long)old + rs.supd_delta[i];
+                    if (nc < 0 || nc > 0xFFFFFFFFll) {
+                        atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
+                        nc = nc < 0 ? 0 : 0xFFFFFFFFll;
+                    }
+                    sa.tri_counts[o] = (uint32_t)nc;
+                }
+                for (int i = 0; i < rs.niupd; ++i) unit_bump_tet(a, ti, rs.iupd_spec[i], rs.iupd_delta[i], tt);
+                for (int i = 0; i < rs.noupd && to >= 0; ++i)
+                    unit_bump_tet(a, to, rs.oupd_spec[i], rs.oupd_delta[i], tt);
+                ci = rs.niupd > 0;
+                co = rs.noupd > 0;
+            } else {
+                // GHK current number sel - npr of the patch: one ion out of (efflux) or into
+                // the inner tet, into or out of the outer tet when its concentration is
+                // used; z elementary charges for the triangle's current.
+                int g = 0, left = sel - npr;
+                for (; g < sa.nghk; ++g)
+                    if (sa.ghks[g].patch == p && left-- == 0) break;
+                const sg_ghk& gh = sa.ghks[g];
+                const uint32_t n = sa.tri_counts[(size_t)gh.sspec * M + m];
+                const uint32_t cin = a.counts[(size_t)gh.ion * a.ntets + ti];
+                const double vm = sa.tri_V ? sa.tri_V[m] : 0.0;
+                const bool outer = gh.voconc < 0.0 && to >= 0;
+                const double rtg = outer ? ghk_rate_outer(gh, vm, cin, n, __ldg(&a.ivs[ti]),
+                                                          a.counts[(size_t)gh.ion * a.ntets + to], __ldg(&a.ivs[to]),
+                                                          sa.temp, a.status)
+                                         : ghk_rate(gh, vm, cin, n, __ldg(&a.ivs[ti]), sa.temp, a.status);
+                const bool eff = rtg >= 0.0;
+                if (gh.realflux) {
+                    unit_bump_tet(a, ti, gh.ion, eff ? -1 : 1, tt);
+                    if (outer) unit_bump_tet(a, to, gh.ion, eff ? 1 : -1, tt);
+                    ci = true;
+                    co = outer;
+                }
+                atomicAdd((unsigned long long*)&sa.tri_echarge[m],
+                          (unsigned long long)(long long)(eff ? gh.valence : -gh.valence));
+            }
+            atomicAdd(a.surf_ext, 1ull);
+            unit_refresh(a, e, nt, tets, tris, r, prop, tree, P);
+            if (ci) unit_refresh_tet(a, ei, eb, nt, tets, tris, r, prop, tree, P);
+            if (co) unit_refresh_tet(a, eo, eb, nt, tets, tris, r, prop, tree, P);
+        }
+        // Occupancy integrals of the triangles, change-time masks of the tets.
+        for (int j = 0; j < nm; ++j) {
+            const int m = tris[j];
+            for (int s = 0; s < SS; ++s) {
+                const size_t o = (size_t)s * M + m;
+                const uint32_t c = sa.tri_counts[o];
+                const double occ = U.socc[o] + (double)c * (T - U.slast[o]);
+                sa.spec_int[o] += occ;
+                if (sa.tri_occ) {
+                    const int sd = sa.sdiff_slot[s];
+                    if (sd >= 0) sa.tri_occ[(size_t)sd * M + m] = occ;
+                }
+            }
+        }
+        for (int k = 0; k < nt && a.tmask; ++k) {
+            const int t = tets[k];
+            uint32_t tm = 0u;
+            for (int s = 0; s < S; ++s) {
+                const int ds = __ldg(&a.diff_slot[s]);
+                if (ds >= 0 && a.tdel[(size_t)ds * a.ntets + t] != 0.0) tm |= 1u << s;
+            }
+            a.tmask[t] = tm;
+        }
+    }
 }
 
 // Apply the pending surface-diffusion inflow to the triangle counts (before host reads).

@@ -166,7 +166,8 @@ class GHKcurr:
     """GHK current through channel state chanstate of ion (src/steps/model/ghkcurr.hpp):
     per channel I = P z F nu (c_in - c_out e^-nu) / (1 - e^-nu), nu = z (V + vshift) F / (R T).
     computeflux moves the ions (one per z e of charge); virtual_oconc (M) fixes the outer
-    concentration (required here: surface units hold no outer tets)."""
+    concentration, and a negative virtual_oconc (the default) takes it from the triangle's
+    outer tet, between which and the inner tet the ions then move."""
 
     def __init__(self, id, surfsys, chanstate, ion, computeflux=True, virtual_oconc=-1.0, vshift=0.0):
         self.id = id

@@ -97,9 +97,11 @@ def flatten(model, geom):
 def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
     """Patches -> membrane triangle tables (the role of Patchdef, src/steps/solver/patchdef.hpp):
     the sorted union of all patch triangles, each with its inner tet (the tet on the side of
-    the patch's inner compartment), patch and area; the surface species; the surface
-    reactions (dense slhs/ilhs/supd/iupd rows), k(V) tables of voltage-dependent ones, and
-    the ohmic currents.  None when the mesh has no patch with a surface system."""
+    the patch's inner compartment), its outer tet (on the side of the outer compartment, -1
+    none), patch and area; the surface species; the surface reactions (dense slhs/ilhs/supd/
+    iupd rows, and olhs/oupd rows of their outer-volume terms), k(V) tables of
+    voltage-dependent ones, and the ohmic currents.  None when the mesh has no patch with a
+    surface system."""
     patches = [p for p in getattr(geom, "patches", {}).values() if p.surfsys]
     if not patches:
         return None
@@ -107,8 +109,10 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
     tri_index = {int(t): i for i, t in enumerate(tris)}
     tri_patch = np.full(len(tris), -1, dtype=np.int32)
     inner = np.full(len(tris), -1, dtype=np.int32)
+    outer = np.full(len(tris), -1, dtype=np.int32)
     for pi, p in enumerate(patches):
         ci = comp_index[p.icomp.id] if p.icomp is not None else -1
+        co = comp_index[p.ocomp.id] if getattr(p, "ocomp", None) is not None else -2
         for t in p.tris:
             m = tri_index[int(t)]
             if tri_patch[m] >= 0:
@@ -118,6 +122,9 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
             inner[m] = a if (a >= 0 and tet_comp[a] == ci) else b
             if inner[m] < 0 or tet_comp[inner[m]] != ci:
                 raise ArgErr(f"triangle {t} has no tet in the inner compartment of patch {p.id}")
+            o = b if inner[m] == a else a
+            if o >= 0 and tet_comp[o] == co:
+                outer[m] = o
     sspecs = []
 
     def sid(name):
@@ -129,8 +136,11 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
         for ssn in p.surfsys:
             ss = model.surfsys[ssn]
             for r in list(ss.sreacs.values()) + list(ss.vdepsreacs.values()):
-                if r.olhs or r.orhs:
-                    raise _lib.NotImplErr("surface reactions with outer-volume species")
+                if r.olhs and r.ilhs:
+                    raise ArgErr(f"surface reaction '{r.id}' has reactants in both volumes")
+                if (r.olhs or r.orhs) and getattr(p, "ocomp", None) is None:
+                    raise ArgErr(f"surface reaction '{r.id}' reaches the outer volume of patch {p.id}, "
+                                 "which has no outer compartment")
                 for s in r.slhs + r.srhs:
                     sid(s)
             for oc in ss.ohmiccurrs.values():
@@ -156,7 +166,19 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
             iupd[spec_index[s]] += 1
         return slhs, ilhs, supd, iupd
 
-    sreacs, ohmics, sdiffs, ghks = [], [], [], []
+    def outer_rows(r):
+        if not (r.olhs or r.orhs):
+            return None
+        olhs = np.zeros(S, np.uint32)
+        oupd = np.zeros(S, np.int32)
+        for s in r.olhs:
+            olhs[spec_index[s]] += 1
+            oupd[spec_index[s]] -= 1
+        for s in r.orhs:
+            oupd[spec_index[s]] += 1
+        return olhs, oupd
+
+    sreacs, ohmics, sdiffs, ghks, sreac_outer = [], [], [], [], []
     for pi, p in enumerate(patches):
         for ssn in p.surfsys:
             ss = model.surfsys[ssn]
@@ -164,16 +186,21 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
                 sdiffs.append((pi, did, sid(d.lig), d.dcst))
             for rid, r in ss.sreacs.items():
                 sreacs.append((pi, rid, rows(r), r.kcst, None))
+                sreac_outer.append(outer_rows(r))
             for rid, r in ss.vdepsreacs.items():
                 vmin, vmax, dv = r.vrange
                 n = int(round((vmax - vmin) / dv)) + 1
                 tab = np.array([r.kfunc(vmin + i * dv) for i in range(n)], dtype=np.float64)
                 sreacs.append((pi, rid, rows(r), 0.0, (vmin, dv, tab)))
+                sreac_outer.append(outer_rows(r))
             for oid, oc in ss.ohmiccurrs.items():
                 ohmics.append((pi, oid, sid(oc.chanstate), oc.g, oc.erev))
             for gid, gh in ss.ghkcurrs.items():
                 if gh.perm is None:
                     raise ArgErr(f"GHK current '{gid}' has no permeability (setP or setPInfo)")
+                if gh.voconc < 0.0 and getattr(p, "ocomp", None) is None:
+                    raise ArgErr(f"GHK current '{gid}' has no virtual outer concentration and patch {p.id} "
+                                 "has no outer compartment")
                 ghks.append((pi, gid, sid(gh.chanstate), spec_index[gh.ion], gh.valence, gh.perm, gh.vshift,
                              gh.voconc, gh.computeflux))
     # Edge neighbours of every membrane triangle (sdiff.cpp:62-83, TOS:585-630): across edge j
@@ -207,6 +234,7 @@ def flatten_surface(model, geom, spec_index, comp_index, tet_comp):
         "tri_dist": np.ascontiguousarray(tri_dist, dtype=np.float64),
         "patch_names": [p.id for p in patches], "tris": tris, "tri_index": tri_index,
         "tri_patch": tri_patch, "tri_inner": inner,
+        "tri_outer": outer if (outer >= 0).any() else None, "sreac_outer": sreac_outer,
         "tri_area": np.ascontiguousarray(geom.tri_area[tris], dtype=np.float64),
         "sspec_names": sspecs, "sspec_index": {n: i for i, n in enumerate(sspecs)},
         "sreacs": sreacs, "ohmics": ohmics, "nsspec": SS,
@@ -275,8 +303,11 @@ class TetOpSplit:
             check(L.sg_set_surface(h, sf["nsspec"], len(sf["tris"]), ptr(tri_inner, C.c_int32),
                                    ptr(tri_patch, C.c_int32), ptr(sf["tri_area"], C.c_double),
                                    len(sf["patch_names"])))
+            if sf["tri_outer"] is not None:
+                tri_outer = np.ascontiguousarray(sf["tri_outer"], dtype=np.int32)
+                check(L.sg_set_tri_outer(h, ptr(tri_outer, C.c_int32)))
             self.sreac_index = {}
-            for (pi, rid, (slhs, ilhs, supd, iupd), k, vdep) in sf["sreacs"]:
+            for (pi, rid, (slhs, ilhs, supd, iupd), k, vdep), orow in zip(sf["sreacs"], sf["sreac_outer"]):
                 out = C.c_int32()
                 args = (h, pi, ptr(slhs, C.c_uint32), ptr(ilhs, C.c_uint32), ptr(supd, C.c_int32),
                         ptr(iupd, C.c_int32))
@@ -285,6 +316,8 @@ class TetOpSplit:
                 else:
                     vmin, dv, tab = vdep
                     check(L.sg_add_vdep_sreac(*args, vmin, dv, len(tab), ptr(tab, C.c_double), C.byref(out)))
+                if orow is not None:
+                    check(L.sg_set_sreac_outer(h, out.value, ptr(orow[0], C.c_uint32), ptr(orow[1], C.c_int32)))
                 self.sreac_index[(sf["patch_names"][pi], rid)] = out.value
             for (pi, oid, ss, g, erev) in sf["ohmics"]:
                 out = C.c_int32()
@@ -691,6 +724,23 @@ class TetOpSplit:
         x = C.c_int32()
         check(self._L.sg_get_split(self._h, C.byref(x)))
         return bool(x.value)
+
+    def setPersistent(self, on, tets_per_lane=1):
+        """Run the windows of every realization in one persistent launch per run() call (up
+        to 64 windows each), warps taking chunks of 32 * tets_per_lane tets; the same results
+        as the window launches.  Only for models without membrane triangles whose
+        realizations take the same windows (otherwise the window launches run)."""
+        check(self._L.sg_set_persistent(self._h, 1 if on else 0, int(tets_per_lane)))
+
+    def getPersistent(self):
+        on, tpl = C.c_int32(), C.c_int32()
+        check(self._L.sg_get_persistent(self._h, C.byref(on), C.byref(tpl)))
+        return bool(on.value), tpl.value
+
+    def setWindowWaitLimit(self, polls):
+        """Polls a persistent launch's wait on a realization makes before it gives up (and
+        run() fails)."""
+        check(self._L.sg_set_window_wait_limit(self._h, int(polls)))
 
     def getCarveout(self):
         """Preferred shared-memory carveout (percent) of the window kernels."""

@@ -20,6 +20,7 @@
 #include "rng/rng.hpp"
 #include "solver/compdef.hpp"
 #include "solver/diffdef.hpp"
+#include "solver/ghkcurrdef.hpp"
 #include "solver/ohmiccurrdef.hpp"
 #include "solver/patchdef.hpp"
 #include "solver/reacdef.hpp"
@@ -218,8 +219,7 @@ void TetOpSplitB200::build_tables() {
             ptris[p].push_back((int)t.get());
             patch_area_[p] += mesh->getTriArea(t);
         }
-        if (pd.countSReacs() + pd.countVDepSReacs() + pd.countOhmicCurrs() == 0) continue;
-        if (pd.countGHKcurrs() > 0) NotImplErrLog("GHK currents through TetOpSplitB200");
+        if (pd.countSReacs() + pd.countVDepSReacs() + pd.countOhmicCurrs() + pd.countGHKcurrs() == 0) continue;
         if (pd.countSurfDiffs() > 0) NotImplErrLog("surface diffusion through TetOpSplitB200");
         for (int t : ptris[p]) tris.insert(t);
         for (uint l = 0; l < pd.countSpecs(); ++l) sspecs.insert((int)pd.specL2G(spec_local_id(l)).get());
@@ -230,15 +230,18 @@ void TetOpSplitB200::build_tables() {
     const int M = (int)memb_tris_.size();
     for (int i = 0; i < M; ++i) memb_index_[memb_tris_[i]] = i;
     tri_patch_.assign(M, -1);
-    std::vector<int32_t> inner(M, -1), tpatch(M, -1);
+    std::vector<int32_t> inner(M, -1), outer(M, -1), tpatch(M, -1);
     std::vector<double> tarea(M, 0.0);
+    bool any_outer = false;
     for (int p = 0; p < P; ++p) {
         auto& pd = sd.patchdef(patch_global_id(p));
-        if (pd.countSReacs() + pd.countVDepSReacs() + pd.countOhmicCurrs() == 0) continue;
+        if (pd.countSReacs() + pd.countVDepSReacs() + pd.countOhmicCurrs() + pd.countGHKcurrs() == 0) continue;
         auto& pt = geom().getPatch(pd.name());
-        int ic = -1;
-        for (int c = 0; c < C; ++c)
+        int ic = -1, oc = -2;
+        for (int c = 0; c < C; ++c) {
             if (sd.compdef(comp_global_id(c)).name() == pt.getIComp().getID()) ic = c;
+            if (pt.getOComp() != nullptr && sd.compdef(comp_global_id(c)).name() == pt.getOComp()->getID()) oc = c;
+        }
         for (int t : ptris[p]) {
             const int m = memb_index_[t];
             if (tpatch[m] >= 0) ArgErrLog("a triangle belongs to two patches");
@@ -249,21 +252,40 @@ void TetOpSplitB200::build_tables() {
                 if (x.valid() && tet_comp_[x.get()] == ic) in = (int)x.get();
             if (in < 0) ArgErrLog("a patch triangle has no tet in the patch's inner compartment");
             inner[m] = in;
+            // Tri::oTet: the other tet, when it lies in the patch's outer compartment.
+            for (const auto& x : tt)
+                if (x.valid() && (int)x.get() != in && tet_comp_[x.get()] == oc) {
+                    outer[m] = (int)x.get();
+                    any_outer = true;
+                }
             tarea[m] = mesh->getTriArea(triangle_global_id(t));
         }
     }
     tri_patch_.assign(tpatch.begin(), tpatch.end());
     const int SS = (int)sspec_global_.size();
     check(sg_set_surface(h_, SS, M, inner.data(), tpatch.data(), tarea.data(), P));
+    if (any_outer) check(sg_set_tri_outer(h_, outer.data()));
+    std::vector<uint32_t> ol;
+    std::vector<int32_t> ou;
+    bool has_outer = false;
     auto rows = [&](auto& r, std::vector<uint32_t>& sl, std::vector<uint32_t>& il, std::vector<int32_t>& su,
                     std::vector<int32_t>& iu) {
         sl.assign(SS, 0);
         su.assign(SS, 0);
         il.assign(S, 0);
         iu.assign(S, 0);
+        ol.assign(S, 0);
+        ou.assign(S, 0);
+        has_outer = false;
         for (uint s = 0; s < sd.countSpecs(); ++s) {
             const spec_global_id g(s);
-            if (r.lhs_O(g) || r.upd_O(g)) NotImplErrLog("surface reactions with outer-volume species");
+            if (r.lhs_O(g) || r.upd_O(g)) {
+                const int v = vol_of[s];
+                if (v < 0) ArgErrLog("outer-volume term on a channel state");
+                ol[v] = r.lhs_O(g);
+                ou[v] = r.upd_O(g);
+                has_outer = true;
+            }
             if (r.lhs_S(g) || r.upd_S(g)) {
                 const int k = surf_spec(g);
                 sl[k] = r.lhs_S(g);
@@ -286,6 +308,7 @@ void TetOpSplitB200::build_tables() {
             rows(r, sl, il, su, iu);
             int32_t idx = 0;
             check(sg_add_sreac(h_, p, sl.data(), il.data(), su.data(), iu.data(), r.kcst(), &idx));
+            if (has_outer) check(sg_set_sreac_outer(h_, idx, ol.data(), ou.data()));
         }
         for (uint l = 0; l < pd.countVDepSReacs(); ++l) {
             const auto g = pd.vdepsreacL2G(vdepsreac_local_id(l));
@@ -296,11 +319,21 @@ void TetOpSplitB200::build_tables() {
             int32_t idx = 0;
             check(sg_add_vdep_sreac(h_, p, sl.data(), il.data(), su.data(), iu.data(), mv._getVMin(), mv._getDV(),
                                     (int32_t)tab.size(), tab.data(), &idx));
+            if (has_outer) check(sg_set_sreac_outer(h_, idx, ol.data(), ou.data()));
         }
         for (uint l = 0; l < pd.countOhmicCurrs(); ++l) {
             auto& oc = sd.ohmiccurrdef(pd.ohmiccurrL2G(ohmiccurr_local_id(l)));
             int32_t idx = 0;
             check(sg_add_ohmic(h_, p, surf_spec(oc.chanstate()), oc.getG(), oc.getERev(), &idx));
+        }
+        // GHKcurr (ghkcurr.cpp:168-280): voconc < 0 reads the triangle's outer tet.
+        for (uint l = 0; l < pd.countGHKcurrs(); ++l) {
+            auto& gd = pd.ghkcurrdef(ghkcurr_local_id(l));
+            const int v = vol_of[gd.ion().get()];
+            if (v < 0) ArgErrLog("GHK current of a channel state");
+            int32_t idx = 0;
+            check(sg_add_ghk(h_, p, surf_spec(gd.chanstate()), v, gd.valence(), gd.perm(), gd.vshift(), gd.voconc(),
+                             gd.realflux() ? 1 : 0, &idx));
         }
     }
 }

@@ -17,6 +17,13 @@ oracle/refsim.py — and stores their trajectories:
                            every 2 ms from 0 to 40 ms.  Arrays tos / tetexact
                            [seed][record][slab].
 
+  ref_ensemble_outer.npz   a membrane between two compartments (tests/outer_membrane.py:
+                           6x4x4 Kuhn cubes cut at the middle plane into cyto and ecs, the
+                           triangles between them the patch memb; pump and channel surface
+                           reactions with inner- and outer-volume reactants and products);
+                           Ca in cyto, Ca in ecs, CaB, PCa and Ko every 0.5 ms from 0 to
+                           10 ms.  Arrays tos / tetexact [seed][record][column].
+
   ref_placement.npz        placement law of setCompSpecCount on the reference's 37-tet
                            sphere mesh (tets of unequal volume): 1000.5 molecules of A
                            placed by TetOpSplitP; per-tet counts [seed][tet] for seeds
@@ -84,9 +91,41 @@ def _place_one(seed):
     return sim.get_tet_counts(0).astype(np.uint16)
 
 
+OUTER_RECORDS = np.arange(0, 21) * 0.5e-3
+OUTER_K = (2.0e-12, 5.0e-13, 5.0e7, 40.0, 1.0e-12, 1.0e8, 60.0, 120.0, 90.0, 2.0e7)
+OUTER_COLUMNS = (("cyto", "Ca"), ("ecs", "Ca"), ("cyto", "CaB"), ("memb", "PCa"), ("memb", "Ko"))
+
+
+def _run_outer(kind, seed):
+    from oracle.refsim import RefOuter
+    from steps_b200 import geom as sgeom
+    from steps_b200 import workloads as W
+    from tests.outer_membrane import INITIAL, outer_split
+
+    base = sgeom.kuhn_box(6, 4, 4, W.H)
+    _, outer, _ = outer_split(base)
+    flag = np.zeros(base.ntets, np.int32)
+    flag[outer] = 1
+    sim = RefOuter(base, flag, OUTER_K, seed, kind=kind)
+    sim.set_comp("cyto", "Ca", INITIAL["Ca_in"])
+    sim.set_comp("ecs", "Ca", INITIAL["Ca_out"])
+    sim.set_comp("cyto", "B", INITIAL["B"])
+    sim.set_patch_count("P", INITIAL["P"])
+    sim.set_patch_count("Kc", INITIAL["Kc"])
+    out = np.zeros((len(OUTER_RECORDS), len(OUTER_COLUMNS)), dtype=np.uint16)
+    for i, t in enumerate(OUTER_RECORDS):
+        if t > 0:
+            sim.run(t)
+        out[i] = [sim.get_patch_count(sp) if c == "memb" else sim.get_comp(c, sp) for c, sp in OUTER_COLUMNS]
+    return out
+
+
 def _run_one(args):
     kind, case, seed = args
     from oracle.refsim import RefSim
+
+    if case == "outer":
+        return _run_outer(kind, seed)
 
     mesh, F = c0_case()
     sim = RefSim(mesh, F, seed, kind=kind)
@@ -115,21 +154,26 @@ def main():
     ap.add_argument("--seeds", type=int, default=200)
     ap.add_argument("-j", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--placement-only", action="store_true")
+    ap.add_argument("--cases", default="placement,c0,spread,outer", help="comma-separated cases to regenerate")
     a = ap.parse_args()
     from oracle import build_ref_tetopsplit
 
     if build_ref_tetopsplit.build() is None:
         raise SystemExit("the reference tree is absent")
     ctx = mp.get_context("spawn")
-    with ctx.Pool(a.j) as pool:
-        pl = np.stack(pool.map(_place_one, range(1, PLACEMENT_SEEDS + 1)))
-    np.savez_compressed(os.path.join(HERE, "ref_placement.npz"), counts=pl, x=PLACEMENT_X,
-                        seeds=np.arange(1, PLACEMENT_SEEDS + 1))
-    print("placement", pl.shape, flush=True)
+    cases = a.cases.split(",")
+    if "placement" in cases:
+        with ctx.Pool(a.j) as pool:
+            pl = np.stack(pool.map(_place_one, range(1, PLACEMENT_SEEDS + 1)))
+        np.savez_compressed(os.path.join(HERE, "ref_placement.npz"), counts=pl, x=PLACEMENT_X,
+                            seeds=np.arange(1, PLACEMENT_SEEDS + 1))
+        print("placement", pl.shape, flush=True)
     if a.placement_only:
         return
     seeds = list(range(1, a.seeds + 1))
-    for case, recs in (("c0", C0_RECORDS), ("spread", SPREAD_RECORDS)):
+    for case, recs in (("c0", C0_RECORDS), ("spread", SPREAD_RECORDS), ("outer", OUTER_RECORDS)):
+        if case not in cases:
+            continue
         res = {}
         for kind in ("tetopsplit", "tetexact"):
             with ctx.Pool(a.j) as pool:

@@ -12,6 +12,7 @@ own public methods on the reference's Model / Tetmesh / RNG objects:
     src/steps/solver/efield/dVsolver.hpp:126-180) at every vertex after every step.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -123,3 +124,41 @@ def test_dropin_passive_efield_matches_reference_efield(steps_lib):
         assert np.max(np.abs(dv_ref)) > 0  # the clamp moves the potential
         worst = max(worst, float(np.max(np.abs(vv[1] - vv[0]) / np.abs(vv[0]))))
     assert worst < 1e-8, worst
+
+
+def test_dropin_outer_membrane_matches_python_solver(steps_lib):
+    """A patch between two compartments whose surface reactions reach both volumes (merged
+    SSA units), built by the reference's own model classes (SReac with outer-volume
+    reactants and products, model/sreac.hpp:67) and run by the drop-in: every tet's counts
+    and the patch totals equal the Python solver's on the same model, bit for bit."""
+    import sys
+
+    from tests.outer_membrane import INITIAL, outer_mesh, outer_model, outer_split
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_ref_ensembles as MR
+
+    seed = 23
+    mesh = outer_mesh()
+    _, outer, _ = outer_split(mesh)
+    flag = np.zeros(mesh.ntets, np.int32)
+    flag[outer] = 1
+    dr = refsim.RefOuter(mesh, flag, MR.OUTER_K, seed, kind="b200")
+    py = TetOpSplit(outer_model(ghk=False), mesh, make_rng(seed))
+    for c, s, n in (("cyto", "Ca", INITIAL["Ca_in"]), ("ecs", "Ca", INITIAL["Ca_out"]), ("cyto", "B", INITIAL["B"])):
+        py.setCompSpecCount(c, s, n)
+        dr.set_comp(c, s, n)
+    for s in ("P", "Kc"):
+        py.setPatchSpecCount("memb", s, INITIAL[s])
+        dr.set_patch_count(s, INITIAL[s])
+    for k in range(1, 7):
+        t = k * 0.5e-3
+        py.run(t)
+        dr.run(t)
+        for s in ("B", "Ca", "CaB"):
+            g = py.getSpecCounts(s)
+            d = np.array([dr.get_tet_count(i, s) for i in range(mesh.ntets)])
+            assert np.array_equal(g, d), (t, s)
+        for s in ("P", "PCa", "Kc", "Ko"):
+            assert py.getPatchSpecCount("memb", s) == dr.get_patch_count(s), (t, s)
+    assert py.getCompSpecCount("ecs", "Ca") != INITIAL["Ca_out"]

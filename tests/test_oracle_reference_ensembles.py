@@ -88,3 +88,51 @@ def test_plain_small_matches_reference_tetopsplit_and_tetexact():
     for arm in ("tos", "tetexact"):
         rep = compare(out, fx[arm][:, :nrec], cols=[0, 2])
         assert rep["ok"], (arm, rep)
+
+
+def _oracle_outer(n, seed0):
+    """The outer-membrane configuration of make_ref_ensembles (same records and columns)
+    run by the oracle, with the reference's placement law for the compartment and patch
+    counts (util/distribute.hpp:102-193 over tet volumes and triangle areas)."""
+    from tests.outer_membrane import INITIAL, outer_mesh, outer_model
+
+    mesh = outer_mesh()
+    F = flatten(outer_model(ghk=False), mesh)
+    S = F["spec_index"]
+    sf = F["surf"]
+    ss = sf["sspec_index"]
+    comp = F["tet_comp"]
+    ci, co = F["comp_index"]["cyto"], F["comp_index"]["ecs"]
+    inner, outer = np.nonzero(comp == ci)[0], np.nonzero(comp == co)[0]
+    times = M.OUTER_RECORDS
+    out = np.zeros((n, len(times), len(M.OUTER_COLUMNS)))
+    for k in range(n):
+        seed = seed0 + k
+        o = Oracle(F, seed=seed)
+
+        def place(call, tets, x):
+            row = np.zeros(mesh.ntets, dtype=np.uint32)
+            row[tets] = distribute(seed, call, F["vol"][tets], x)
+            return row
+
+        o.set_counts(S["Ca"], place(0, inner, INITIAL["Ca_in"]) + place(1, outer, INITIAL["Ca_out"]))
+        o.set_counts(S["B"], place(2, inner, INITIAL["B"]))
+        for call, name in ((3, "P"), (4, "Kc")):
+            o.set_tri_counts(ss[name], distribute(seed, call, sf["tri_area"], INITIAL[name]))
+        for i, t in enumerate(times):
+            if t > 0:
+                o.run(t)
+            ca = o.get_counts(S["Ca"])
+            out[k, i] = [ca[inner].sum(), ca[outer].sum(), o.get_counts(S["CaB"]).sum(),
+                         o.get_tri_counts(ss["PCa"]).sum(), o.get_tri_counts(ss["Ko"]).sum()]
+    return out
+
+
+def test_outer_membrane_matches_reference_tetopsplit():
+    """Merged SSA units (a patch whose surface reactions take reactants from and put products
+    into both volumes, sreac.cpp:305-520): the oracle's ensemble against the reference
+    TetOpSplitP's, five columns every 0.5 ms to 10 ms."""
+    fx = np.load(os.path.join(GOLD, "ref_ensemble_outer.npz"))
+    out = _oracle_outer(200, 9000)
+    rep = compare(out, fx["tos"])
+    assert rep["ok"], rep
