@@ -434,6 +434,7 @@ def run_ours(args):
             "config": dict(config_dict(mesh), parallelism=f"replicas{world}",
                            launch={"block": sim.getLaunch()[0], "grid": sim.getLaunch()[1],
                                    "smem_carveout_pct": sim.getCarveout(), "split": sim.getSplit(),
+                                   "persistent": sim.getPersistent()[0],
                                    "autotune_ms": sim.getAutotuneTimes()}),
             "sim_ms_per_wall_s": (STEP_SIM_S * 1e3 * args.steps) / (t_max * 1e-3),
             "windows_per_step": windows / args.steps,
@@ -443,7 +444,9 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6650 GB/s",
-                         "kernel": (f"sg::window_kernel<{sim.getLaunch()[0]}, split> + sg::leave_kernel<256>"
+                         "kernel": (f"sg::persistent_window_kernel<{256 if sim.getLaunch()[0] >= 256 else 128}, "
+                                    f"{sim.getPersistent()[1]}>" if sim.getPersistent()[0] else
+                                    f"sg::window_kernel<{sim.getLaunch()[0]}, split> + sg::leave_kernel<256>"
                                     if sim.getSplit() else f"sg::window_kernel<{sim.getLaunch()[0]}>"),
                          "algorithmic_bytes_per_launch": bytes_per_window,
                          "avg_launch_us": avg_win_s * 1e6},
@@ -502,6 +505,8 @@ def batched_extra(args):
     torch.cuda.synchronize()
     launch = sim.getLaunch()
     sim_split = sim.getSplit()
+    sim_persist = sim.getPersistent()
+    tune_ms = sim.getAutotuneTimes()
     it0 = sim.getNIteration()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(ext)
@@ -546,7 +551,9 @@ def batched_extra(args):
         "config": {"workload": f"batched: {nreal} realizations of n^3 Kuhn cubes, n in 8..30, "
                                f"{mesh.ntets} tets, 8 species, 12 reactions, rate jitter 0.2",
                    "sim_ms_per_step": 1.0, "steps": args.bx_steps, "warmup": args.bx_warmup,
-                   "launch": {"block": launch[0], "grid": launch[1], "split": sim_split}},
+                   "launch": {"block": launch[0], "grid": launch[1], "split": sim_split,
+                              "persistent": sim_persist[0], "tets_per_lane": sim_persist[1],
+                              "autotune_ms": tune_ms}},
         "windows": windows, "ms": ms, "setup_s": setup_s,
         "plain_sequential": {"value": plain, "realizations_sampled": len(sample), "ms": plain_ms},
         "batched_over_plain": batched / plain,
