@@ -696,6 +696,49 @@ __device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, dou
     return k;
 }
 
+// Leave of one (tet, species) with the face selectors and their odds read from this
+// thread's slots in shared memory (sel[k * stride], k = c0, c1, c2, odd1, odd2, odd3)
+// instead of registers held across the species loop.
+__device__ __forceinline__ uint4 leave_split_sh(sg_stream* st, uint32_t mean_n, double t1, const double* sel,
+                                                int stride, const double* rcp, const double* rcpl,
+                                                const double* lnf, uint32_t* out_kn) {
+    if (mean_n <= SG_PM_MAX) {
+        if (mean_n == 0u || !(t1 > 0.0)) {
+            *out_kn = 0u;
+            return make_uint4(0u, 0u, 0u, 0u);
+        }
+        return leave_molecules(st, mean_n, t1 < 1.0 ? t1 : 1.0, sel[0], sel[stride], sel[2 * stride], out_kn);
+    }
+    uint4 k = make_uint4(0u, 0u, 0u, 0u);
+    uint32_t n = mean_n, Kn = 0u;
+    double pst = t1;
+    double ost = (t1 > 0.0 && t1 < 1.0) ? sg_binom_odds(t1) : 0.0;
+#pragma unroll 1
+    for (int stage = 0; stage < 4; ++stage) {
+        uint32_t v = sg_binom_o(st, n, pst, ost, rcp, rcpl, lnf);
+        if (stage == 0) {
+            Kn = v;
+            n = v;
+        } else if (stage == 1) {
+            k.x = v;
+            n -= v;
+        } else if (stage == 2) {
+            k.y = v;
+            n -= v;
+        } else {
+            k.z = v;
+            n -= v;
+        }
+        if (stage < 3) {
+            pst = sel[stage * stride];
+            ost = sel[(3 + stage) * stride];
+        }
+    }
+    k.w = n;
+    *out_kn = Kn;
+    return k;
+}
+
 // Last block of a window: conservation check, counters, device-side time advance.
 // flag is a 2-int shared scratch; parity is the launch parity read at kernel start.
 __device__ __forceinline__ void window_last_block(const sg_window_args& a, int check, unsigned long long parity,
@@ -1018,6 +1061,12 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
     __shared__ double s_rcp[SG_RCP_TABLE];
     __shared__ double s_rcpl[SG_MODE_TABLE];  // 1/x and ln x! of the mode search
     __shared__ double s_lnf[SG_MODE_TABLE];
+    // Per-thread slots for what the species loop reads after each sampler call: the face
+    // selectors c0, c1, c2 and their odds, the window length and its inverse, the window
+    // index.  Held in registers across the loop they forced spills at the 64-register cap.
+    __shared__ double s_sel[6 * BLOCK];
+    __shared__ double s_T[2 * BLOCK];
+    __shared__ unsigned long long s_w[BLOCK];
     __shared__ int flag[2];
     __shared__ unsigned long long s_moved;
     const int tid = threadIdx.x, lane = tid & 31;
@@ -1032,6 +1081,7 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
     unsigned int* wctr = a.work ? a.work + parity * 4 + 2 : nullptr;
     const size_t plane = (size_t)a.ntets * 4;
     const int S = a.nspec;
+    double* sel = s_sel + tid;
     unsigned long long moved = 0ull;
     for (int it = 0;; ++it) {
         const int base = next_warp_base(wctr, it, BLOCK);
@@ -1044,23 +1094,28 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
         if (!(rt < rend)) continue;
         const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
         if (comp < 0) continue;
-        const double T = (rt + per > rend) ? rend - rt : per;
-        const unsigned long long w = rl->window;
+        const double Tw = (rt + per > rend) ? rend - rt : per;
         const uint32_t tl = (uint32_t)(t - rl->tet_begin);
         const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
-        const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
-        const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
         const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
         const double* Dc = a.dcst + ((size_t)r * a.ncomp + comp) * S;
-        uint32_t* out = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane;
-        // The face selectors and their odds, once per tet.
-        const double cs[3] = {(double)g.x, (double)g.y, (double)g.z};
-        const double odd1 = sg_binom_odds(cs[0]);
-        const double odd2 = sg_binom_odds(cs[1]);
-        const double odd3 = sg_binom_odds(cs[2]);
-        const double invT = 1.0 / T;
+        const float G = __ldg(reinterpret_cast<const float*>(a.geo) + (size_t)t * 4 + 3);
+        if (!bt) {
+            const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
+            sel[0] = (double)g.x;
+            sel[BLOCK] = (double)g.y;
+            sel[2 * BLOCK] = (double)g.z;
+            sel[3 * BLOCK] = sg_binom_odds((double)g.x);
+            sel[4 * BLOCK] = sg_binom_odds((double)g.y);
+            sel[5 * BLOCK] = sg_binom_odds((double)g.z);
+        }
+        s_T[tid] = Tw;
+        s_T[BLOCK + tid] = 1.0 / Tw;  // one division per tet for the occupancy means
+        s_w[tid] = rl->window;
         const uint32_t tm = a.tmask ? a.tmask[t] : 0u;
         for (int s = 0; s < S; ++s) {
+            const double T = s_T[tid], invT = s_T[BLOCK + tid];
+            const unsigned long long w = s_w[tid];
             const int ds = __ldg(&a.diff_slot[s]);
             if (ds < 0) continue;
             const double D = __ldg(&Dc[s]);
@@ -1072,25 +1127,42 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
                 sg_stream st;
                 uint32_t Kn = 0u;
                 const double sd = ((tm >> s) & 1u) ? a.tdel[(size_t)ds * a.ntets + t] : 0.0;
+                double t1;
                 if (bt) {
-                    // Diffusion-boundary tet: face rates, and so selectors, per species.
+                    const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
                     float4 gb;
                     const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
-                    const double cb[3] = {(double)gb.x, (double)gb.y, (double)gb.z};
-                    k = leave_species(a.seed, (uint32_t)r, tl, w, (uint32_t)s, pop, sd, invT, T * tot, cb,
-                                      sg_binom_odds(cb[0]), sg_binom_odds(cb[1]), sg_binom_odds(cb[2]), s_rcp,
-                                      s_rcpl, s_lnf, &st, &Kn);
+                    sel[0] = (double)gb.x;
+                    sel[BLOCK] = (double)gb.y;
+                    sel[2 * BLOCK] = (double)gb.z;
+                    sel[3 * BLOCK] = sg_binom_odds((double)gb.x);
+                    sel[4 * BLOCK] = sg_binom_odds((double)gb.y);
+                    sel[5 * BLOCK] = sg_binom_odds((double)gb.z);
+                    t1 = T * tot;
                 } else {
-                    k = leave_species(a.seed, (uint32_t)r, tl, w, (uint32_t)s, pop, sd, invT, T * (D * (double)g.w),
-                                      cs, odd1, odd2, odd3, s_rcp, s_rcpl, s_lnf, &st, &Kn);
+                    t1 = T * (D * (double)G);
                 }
+                sg_stream_init(&st, a.seed, (uint32_t)r, tl, w, SG_PURPOSE_DIFF + (uint32_t)s);
+                if (t1 >= 1.0) t1 = 1.0;
+                uint32_t mean_n = pop;
+                if (sd != 0.0) {
+                    double nbar = (double)pop - sd * invT;
+                    if (nbar > (double)pop) nbar = (double)pop;
+                    double nint = floor(nbar);
+                    double frc = nbar - nint;
+                    mean_n = (uint32_t)nint;
+                    if (frc > 0.0) {
+                        if (sg_u01_co(sg_next_u32(&st)) < frc) mean_n += 1u;
+                    }
+                }
+                k = leave_split_sh(&st, mean_n, t1, sel, BLOCK, s_rcp, s_rcpl, s_lnf, &Kn);
                 if (Kn > 0u) {
                     if (!((clampm >> s) & 1u)) a.counts[ci] = pop - Kn;
                     moved += Kn;
                 }
             }
-            // Scatter into the receiving tets' slots: nb.f = (neighbour << 2) | its face.
-            uint32_t* po = out + (size_t)ds * plane;
+            const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
+            uint32_t* po = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane + (size_t)ds * plane;
             if (nb.x >= 0) po[nb.x] = k.x;
             if (nb.y >= 0) po[nb.y] = k.y;
             if (nb.z >= 0) po[nb.z] = k.z;
