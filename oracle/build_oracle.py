@@ -53,6 +53,7 @@ def build_ref(force=False):
         import build_ref_tetopsplit
 
     build_ref_tetopsplit.build(force=force)
+    build_ref_tetopsplit.build_cython(force=force)
     os.makedirs(REF_OUT, exist_ok=True)
     exe = os.path.join(REF_OUT, "ref_philox_kat")
     src = os.path.join(HERE, "ref_philox_kat.c")

@@ -37,7 +37,7 @@ DROPIN = os.path.join(REPO, "steps_b200", "steps_api", "tetopsplit_b200.cpp")
 LIB_B200 = os.path.join(OUT, "libsteps_ref_b200.so")
 
 DIRS = ["util", "util/tracker", "math", "geom", "model", "rng", "solver", "solver/efield", "mpi",
-        "mpi/tetopsplit", "tetexact"]
+        "mpi/tetopsplit", "tetexact", "wmdirect", "wmrk4", "wmrssa"]
 EXCLUDE = ("petsc", "lapack")
 FLAGS = ["-std=c++17", "-O2", "-fPIC", "-w", "-DENABLE_ASSERTLOG=1",
          "-I" + SHIM, "-I" + os.path.join(SRC, "steps"), "-I" + SRC, "-I" + os.path.join(SRC, "third_party"),
@@ -122,8 +122,67 @@ def build_dropin(ref_objs, force=False):
     return LIB_B200
 
 
+PYSTEPS = os.path.join(os.path.dirname(SRC), "pysteps")
+CYSRC = os.path.join(REPO, "steps_b200", "steps_api", "cysteps_b200.pyx")
+CYPXD = os.path.join(REPO, "steps_b200", "steps_api", "steps_b200.pxd")
+TETODE_STANDIN = os.path.join(SHIM, "tetode_standin.cpp")
+
+
+def cython_module_path():
+    import sysconfig
+
+    return os.path.join(OUT, "cysteps_b200" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_cython(force=False):
+    """oracle/_ref/cysteps_b200.<ext>: the reference's own Python binding (pysteps/cysteps.pyx,
+    cythonized where it lies, with the compile-time settings of its CMake build for a
+    build without PETSc, the distributed mesh or SUNDIALS) plus the drop-in's binding class
+    steps_b200/steps_api/cysteps_b200.pyx, linked to libsteps_ref_b200.so.  TetODE, which
+    needs SUNDIALS, is replaced by oracle/ref_shim/tetode_standin.cpp.  Returns the module
+    path, or None without the reference tree, Cython or the drop-in library."""
+    if not available() or not os.path.isdir(PYSTEPS) or not os.path.exists(LIB_B200):
+        return None
+    try:
+        import Cython  # noqa: F401
+    except ImportError:
+        return None
+    import sysconfig
+
+    import numpy
+
+    mod = cython_module_path()
+    deps = [CYSRC, CYPXD, TETODE_STANDIN, LIB_B200, os.path.join(REPO, "steps_b200", "steps_api", "tetopsplit_b200.hpp")]
+    if not force and os.path.exists(mod) and os.path.getmtime(mod) >= max(os.path.getmtime(p) for p in deps):
+        return mod
+    cydir = os.path.join(OUT, "cy")
+    os.makedirs(cydir, exist_ok=True)
+    cpp = os.path.join(cydir, "cysteps_b200.cpp")
+    env = ["--compile-time-env", "USE_PETSC=False", "--compile-time-env", "STEPS_USE_DIST_MESH=False",
+           "--compile-time-env", "STEPS_SUNDIALS_VERSION_MAJOR=6"]
+    _run_checked([sys.executable, "-m", "cython", "-3", "--cplus", "-I", PYSTEPS, "-I", os.path.dirname(CYSRC)] + env +
+                 ["-o", cpp, CYSRC], "cythonize")
+    inc = ["-I" + os.path.join(REPO, "steps_b200"), "-I" + os.path.join(REPO, "include"), "-I" + PYSTEPS,
+           "-I" + sysconfig.get_paths()["include"], "-I" + numpy.get_include()]
+    objs = []
+    for src, obj in ((cpp, os.path.join(cydir, "cysteps_b200.o")), (TETODE_STANDIN, os.path.join(cydir, "tetode_standin.o"))):
+        flags = [f for f in FLAGS if f != "-O2"] + ["-O1"]
+        _run_checked(["g++"] + flags + inc + ["-c", src, "-o", obj], "compile " + os.path.basename(src))
+        objs.append(obj)
+    _run_checked(["g++", "-shared", "-o", mod] + objs + ["-L" + OUT, "-lsteps_ref_b200", "-Wl,-rpath,$ORIGIN"],
+                 "link the binding module")
+    return mod
+
+
+def _run_checked(cmd, what):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{what} failed:\n{r.stdout[-2000:]}\n{r.stderr[-3000:]}")
+
+
 if __name__ == "__main__":
     j = None
     if "-j" in sys.argv:
         j = int(sys.argv[sys.argv.index("-j") + 1])
     print(build(force="--force" in sys.argv, jobs=j))
+    print(build_cython(force="--force" in sys.argv))

@@ -162,3 +162,37 @@ def test_dropin_outer_membrane_matches_python_solver(steps_lib):
         for s in ("P", "PCa", "Kc", "Ko"):
             assert py.getPatchSpecCount("memb", s) == dr.get_patch_count(s), (t, s)
     assert py.getCompSpecCount("ecs", "Ca") != INITIAL["Ca_out"]
+
+
+def test_reference_python_binding_drives_the_gpu_solver(steps_lib):
+    """The reference's own Python classes (pysteps/cysteps.pyx: _py_Model, _py_Tetmesh,
+    _py_TmComp, the r123 RNG) with the drop-in's binding class _py_TetOpSplitB200
+    (steps_b200/steps_api/cysteps_b200.pyx), as a STEPS script would call it: the counts
+    equal the Python solver's bit for bit."""
+    from tests.test_cysteps_b200 import _module, build_reference_objects
+
+    S = _module()
+    mesh = sgeom.kuhn_box(8, 8, 8, 1e-7)
+    sgeom.TmComp("comp", mesh, np.arange(mesh.ntets)).addVolsys("vsys")
+    seed = 19
+    mdl, tm, comp, rng = build_reference_objects(S, mesh, seed)
+    dr = S._py_TetOpSplitB200(mdl, tm, rng, 0)
+    assert dr.getSolverName() in (b"TetOpSplitB200", "TetOpSplitB200")
+    py = TetOpSplit(volume_model(), mesh, make_rng(seed))
+    for s, n in (("S0", 5000.5), ("S1", 3000)):
+        py.setCompSpecCount("comp", s, n)
+        dr.setCompSpecCount("comp", s, n)
+    py.setTetSpecCount(17, "S2", 40)
+    dr.setTetSpecCount(17, "S2", 40)
+    idx = np.arange(mesh.ntets, dtype=np.uint32)
+    out = np.zeros(mesh.ntets)
+    for k in range(1, 5):
+        t = k * 1e-3
+        py.run(t)
+        dr.run(t)
+        assert dr.getTime() == t
+        for s in ("S0", "S1", "S2"):
+            dr.getBatchTetSpecCountsNP(idx, s, out)
+            assert np.array_equal(out, py.getSpecCounts(s).astype(np.float64)), (t, s)
+    assert dr.getCompSpecCount("comp", "S0") == py.getCompSpecCount("comp", "S0")
+    assert dr.getNSteps() == py.getNSteps()
