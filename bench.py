@@ -14,8 +14,10 @@ species row from pinned host memory, runs 1 ms and downloads every row.
 parity: after the timed steps the GPU state is copied into the CPU oracle and both run 5
 more windows; every count of every tet must agree bit for bit.
 extra: the batched ensemble (512 realizations) against the same realizations run one at
-a time, and the EField configuration (FP64 and mixed-precision solves, per-step error
-against an FP64 solve), both at reduced step counts.
+a time, the EField configuration (FP64 and mixed-precision solves, per-step error against
+an FP64 solve) and the full coupled batched configuration (16 realizations of 1.2 M tets
+with membrane channels and the mixed-precision EField, 0.03 ms after 0.01 ms), all at
+reduced step counts.
 cpu_baseline: the reference TetOpSplitP itself (compiled from its sources, oracle/_ref),
 one window from the GPU's final state on one host core.
 --impl reference: the reference TetOpSplitP on every host core (independent single-rank
@@ -457,7 +459,9 @@ def run_ours(args):
         }
         if world == 1 and not args.no_extra:
             del sim
-            line["extra"] = {"batched": batched_extra(args), "efield": efield_extra(args)}
+            line["extra"] = {"batched": batched_extra(args), "efield": efield_extra(args),
+                             "coupled": coupled_extra(argparse.Namespace(**dict(vars(args), cp_ms=args.cpx_ms,
+                                                                                cp_warmup_ms=0.01)))}
             sim = None
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -680,7 +684,7 @@ def run_windows(args):
     return 0
 
 
-def run_coupled(args):
+def coupled_extra(args):
     """Full coupled batched configuration: 16 realizations of a 5x5x8 um box (50x50x80 Kuhn
     cubes, 1.2 M tets each) in one launch per window.  Volume: Ca + CB <-> CaCB (kf 1e8 /M/s,
     kb 100 /s), D_Ca 2.2e-10, D_CB = D_CaCB = 2e-11 m^2/s, CB 50 uM, Ca 50 nM.  Membrane (every
@@ -759,7 +763,7 @@ def run_coupled(args):
     windows = sim.getNIteration() - it0
     s1, iters, ms1, rr = sim.getEfieldStats()
     upd = mesh.ntets * 3 * windows
-    print(json.dumps({
+    out = {
         "metric": "tet-species updates/s; sim-ms per wall-s", "value": upd / (ms * 1e-3),
         "unit": "tet-species updates/s",
         "config": {"workload": f"coupled batched: {args.cp_nreal} realizations of {nx}x{ny}x{nz} Kuhn cubes "
@@ -771,8 +775,13 @@ def run_coupled(args):
         "sim_ms_per_wall_s": args.cp_ms / wall,
         "efield_solve_ms_per_step": (ms1 - ms0) / max(s1 - s0, 1),
         "cg_iterations_per_step_overall": iters / max(s1, 1),
-    }), flush=True)
+    }
     del sim
+    return out
+
+
+def run_coupled(args):
+    print(json.dumps(coupled_extra(args)), flush=True)
     return 0
 
 
@@ -791,6 +800,7 @@ def main():
     ap.add_argument("--cp-nreal", type=int, default=16)
     ap.add_argument("--cp-ms", type=float, default=0.5, help="timed simulated ms (the configuration runs 20)")
     ap.add_argument("--cp-warmup-ms", type=float, default=0.02)
+    ap.add_argument("--cpx-ms", type=float, default=0.03, help="coupled extra of the default line: timed simulated ms")
     ap.add_argument("--cp-method", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--ef-inner-tol", type=float, default=1e-4)
     ap.add_argument("--nreal", type=int, default=512)
