@@ -14,7 +14,7 @@ from steps_b200 import model as smodel
 from steps_b200 import workloads as W
 
 
-def outer_model(ghk=True):
+def outer_model(ghk=True, sdiff=False):
     """Species, rules and reactions are created in name order, the order the reference's
     model keeps them in (std::map by name), so that the drop-in built from the reference's
     own model objects sees the same tables as the Python solver."""
@@ -42,6 +42,8 @@ def outer_model(ghk=True):
     smodel.SReac("open", ss, slhs=[kc], srhs=[ko], kcst=120.0)
     smodel.SReac("pin", ss, ilhs=[ca], slhs=[p], srhs=[pc], kcst=1.0e8)
     smodel.SReac("pout", ss, slhs=[pc], srhs=[p], orhs=[ca], kcst=60.0)
+    if sdiff:
+        smodel.Diff("dP", ss, p, 1.0e-13)
     if ghk:
         g = smodel.GHKcurr("ICa", ss, ko, ca, computeflux=True, virtual_oconc=-1.0)
         g.setPInfo(g=20e-12, V=-0.065, T=293.15, oconc=2e-3, iconc=1e-4)

@@ -19,9 +19,9 @@ from tests.outer_membrane import INITIAL, outer_mesh, outer_model
 pytestmark = pytest.mark.gpu
 
 
-def _build(seed, ghk=True, realizations=None):
+def _build(seed, ghk=True, realizations=None, sdiff=False):
     mesh = outer_mesh()
-    sim = TetOpSplit(outer_model(ghk), mesh, make_rng(seed))
+    sim = TetOpSplit(outer_model(ghk, sdiff), mesh, make_rng(seed))
     sim.setCompSpecCount("cyto", "Ca", INITIAL["Ca_in"])
     sim.setCompSpecCount("ecs", "Ca", INITIAL["Ca_out"])
     sim.setCompSpecCount("cyto", "B", INITIAL["B"])
@@ -53,9 +53,11 @@ def _ca_total(sim):
     return int(sim.getSpecCounts("Ca").sum()) + int(sim.getSpecCounts("CaB").sum()) + int(pc)
 
 
-@pytest.mark.parametrize("ghk", [False, True])
-def test_outer_membrane_matches_oracle(steps_lib, ghk):
-    mesh, sim, ora = _build(41, ghk)
+@pytest.mark.parametrize("ghk,sdiff", [(False, False), (True, False), (True, True)])
+def test_outer_membrane_matches_oracle(steps_lib, ghk, sdiff):
+    """With sdiff the pumps also diffuse on the patch (surface diffusion of merged units'
+    triangles, sdiff.cpp:438-560)."""
+    mesh, sim, ora = _build(41, ghk, sdiff=sdiff)
     assert sim.getUpdPeriod() == ora.period()
     total = _ca_total(sim)
     outer = np.unique(sim.tables["surf"]["tri_outer"])
@@ -64,13 +66,15 @@ def test_outer_membrane_matches_oracle(steps_lib, ghk):
         t = k * 0.5e-3
         sim.run(t)
         ora.run(t)
-        _check(sim, ora, f"t={t} ghk={ghk}")
+        _check(sim, ora, f"t={t} ghk={ghk} sdiff={sdiff}")
         assert _ca_total(sim) == total
     assert sim.getNIteration() == ora.window()
     assert ora.surf_extent() > 0
     assert int(sim.getSpecCounts("Ca")[outer].sum()) != ca_out0
     if ghk:
         assert np.any(ora.echarge() != 0)
+    if sdiff:
+        assert ora.diff_extent() > 0
 
 
 def test_outer_membrane_split_setting_is_ignored(steps_lib):

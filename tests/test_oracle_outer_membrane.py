@@ -7,15 +7,16 @@ volumes, the buffer and the pumps, so its total is conserved while both directio
 transport run.
 """
 import numpy as np
+import pytest
 
 from oracle.pyoracle import Oracle
 from steps_b200.solver import flatten
 from tests.outer_membrane import INITIAL, outer_mesh, outer_model
 
 
-def _setup(seed=5, ghk=True):
+def _setup(seed=5, ghk=True, sdiff=False):
     mesh = outer_mesh()
-    mdl = outer_model(ghk)
+    mdl = outer_model(ghk, sdiff)
     F = flatten(mdl, mesh)
     ora = Oracle(F, seed=seed)
     rng = np.random.default_rng(seed)
@@ -58,8 +59,9 @@ def test_outer_tets_are_recorded():
     assert [o is not None for o in sf["sreac_outer"]] == [True, False, False, False, True]
 
 
-def test_calcium_conserved_across_the_membrane():
-    mesh, F, ora = _setup()
+@pytest.mark.parametrize("sdiff", [False, True])
+def test_calcium_conserved_across_the_membrane(sdiff):
+    mesh, F, ora = _setup(sdiff=sdiff)
     S = F["spec_index"]
     total = _ca_total(F, ora)
     outer_tets = F["surf"]["tri_outer"]
