@@ -198,6 +198,7 @@ struct Solver {
     std::vector<int32_t> tri_outer;                 // [M] outer tet, -1 none (empty: not given)
     std::vector<int32_t> tet_unit_h;                // [T] unit of a merged tet, -1
     int nunits = 0, unit_rmax = 0;
+    size_t unit_smem = 0;                           // shared bytes of the largest unit's tree and propensities
     DevBuf<int32_t> d_tri_outer, d_u_tet_begin, d_u_tets, d_u_tri_begin, d_u_tris, d_u_elem_base, d_u_tree_base,
         d_tet_unit, d_u_tet_adj, d_u_tri_side;
     DevBuf<double> d_u_prop, d_u_tree, d_u_socc, d_u_slast;
@@ -307,6 +308,9 @@ struct Solver {
         unit_rmax = max_sreac_per_patch;
         for (int c = 0; c < ncomp; ++c) unit_rmax = std::max(unit_rmax, comp_reac_begin[c + 1] - comp_reac_begin[c]);
         unit_rmax = std::max(unit_rmax, 1);
+        unit_smem = 0;
+        for (int u = 0; u < nunits; ++u)
+            unit_smem = std::max(unit_smem, ((size_t)(trb[u + 1] - trb[u]) + (size_t)(eb[u + 1] - eb[u]) * unit_rmax) * 8);
         if (tri_outer.size() == (size_t)ntris) {
             d_tri_outer.alloc(ntris);
             h2d(d_tri_outer.p, tri_outer.data(), tri_outer.size());
@@ -333,7 +337,11 @@ struct Solver {
         h2d(d_tet_unit.p, tet_unit_h.data(), tet_unit_h.size());
         h2d(d_u_tet_adj.p, adj.data(), adj.size());
         h2d(d_u_tri_side.p, side.data(), side.size());
+        if (unit_smem <= kUnitSmemMax && unit_smem > 48 * 1024)
+            SG_CUDA(cudaFuncSetAttribute(unit_ssa_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)unit_smem));
     }
+    static constexpr size_t kUnitSmemMax = 200 * 1024;
 
     sg_unit_args unit_args() const {
         sg_unit_args u;
@@ -1125,7 +1133,14 @@ struct Solver {
                 SG_CUDA(cudaGetLastError());
             }
             if (nunits > 0) {
-                unit_ssa_kernel<32><<<(nunits + 31) / 32, 32, 0, stream>>>(a);
+                // One warp per unit; the tree and the propensities in shared memory when the
+                // largest unit's fit.
+                const int gu = std::min(nunits, nsm * 32);
+                if (unit_smem <= kUnitSmemMax) {
+                    unit_ssa_kernel<true><<<gu, 32, unit_smem, stream>>>(a);
+                } else {
+                    unit_ssa_kernel<false><<<gu, 32, 0, stream>>>(a);
+                }
                 SG_CUDA(cudaGetLastError());
             }
             if (nsdiff > 0) {

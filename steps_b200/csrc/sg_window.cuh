@@ -1539,38 +1539,114 @@ __device__ __forceinline__ void unit_bump_tet(const sg_window_args& a, int t, in
     *pc = (uint32_t)nc;
 }
 
-// Re-evaluate element f and the sums on its path to the root.
-__device__ __forceinline__ void unit_refresh(const sg_window_args& a, int f, int nt, const int32_t* tets,
-                                             const int32_t* tris, int r, double* prop, double* tree, int P) {
-    int i = P + f;
-    tree[i] = unit_elem_props(a, f, nt, tets, tris, r, prop + (size_t)f * a.units.rmax);
-    for (i >>= 1; i >= 1; i >>= 1) tree[i] = tree[2 * i] + tree[2 * i + 1];
-}
-
-// Element f (a tet) and the unit's triangles whose rates read it.
-__device__ __forceinline__ void unit_refresh_tet(const sg_window_args& a, int f, int eb, int nt, const int32_t* tets,
-                                                 const int32_t* tris, int r, double* prop, double* tree, int P) {
-    if (f < 0) return;
-    unit_refresh(a, f, nt, tets, tris, r, prop, tree, P);
-    const int4 adj = __ldg(reinterpret_cast<const int4*>(a.units.tet_adj) + eb + f);
-    if (adj.x >= 0) unit_refresh(a, adj.x, nt, tets, tris, r, prop, tree, P);
-    if (adj.y >= 0) unit_refresh(a, adj.y, nt, tets, tris, r, prop, tree, P);
-    if (adj.z >= 0) unit_refresh(a, adj.z, nt, tets, tris, r, prop, tree, P);
-    if (adj.w >= 0) unit_refresh(a, adj.w, nt, tets, tris, r, prop, tree, P);
-}
-
-// SSA of every merged unit over its window, one thread per unit, between the volume and
-// membrane SSA passes and the diffusion leave of a split window: gathers the unit's inflow,
-// writes its tets' counts, change-time sums and tmask, its triangles' counts and occupancy
-// integrals.  The unit draws from the window stream of its first tet.
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) unit_ssa_kernel(sg_window_args a) {
+// Apply event (element e, reaction or GHK current sel) of a merged unit at time tt of the
+// window; returns the elements whose propensities read a changed count (into aff, at most
+// 16: the element, and the tets whose counts changed with their triangles).
+static __device__ __noinline__ int unit_apply(const sg_window_args& a, int e, int sel, int eb, int nt,
+                                              const int32_t* tets, const int32_t* tris, unsigned long long parity,
+                                              double tt, int* aff) {
     const sg_unit_args& U = a.units;
     const sg_surf_args& sa = a.surf;
+    const int M = sa.ntris;
+    int n = 0;
+    auto add_tet = [&](int f) {
+        if (f < 0) return;
+        aff[n++] = f;
+        const int4 adj = __ldg(reinterpret_cast<const int4*>(U.tet_adj) + eb + f);
+        if (adj.x >= 0) aff[n++] = adj.x;
+        if (adj.y >= 0) aff[n++] = adj.y;
+        if (adj.z >= 0) aff[n++] = adj.z;
+        if (adj.w >= 0) aff[n++] = adj.w;
+    };
+    if (e < nt) {
+        const int t = tets[e];
+        const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
+        const int q = __ldg(&a.comp_reac_begin[comp]) + sel;
+        const sg_reac* rc = &a.reacs[q];
+        for (int i = 0; i < rc->nupd; ++i) unit_bump_tet(a, t, rc->upd_spec[i], rc->upd_delta[i], tt);
+        atomicAdd(&a.ext[parity * a.nreac + q], 1ull);
+        add_tet(e);
+        return n;
+    }
+    const int j = e - nt, m = tris[j];
+    const int p = sa.tri_patch[m];
+    const int pb = sa.patch_sreac_begin[p], npr = sa.patch_sreac_begin[p + 1] - pb;
+    const int ti = sa.tri_inner[m];
+    const int to = sa.tri_outer ? sa.tri_outer[m] : -1;
+    const int ei = U.tri_side[2 * m], eo = U.tri_side[2 * m + 1];
+    bool ci = false, co = false;
+    if (sel < npr) {
+        const sg_sreac& rs = sa.sreacs[pb + sel];
+        for (int i = 0; i < rs.nsupd; ++i) {
+            const size_t o = (size_t)rs.supd_spec[i] * M + m;
+            const uint32_t old = sa.tri_counts[o];
+            U.socc[o] = U.socc[o] + (double)old * (tt - U.slast[o]);
+            U.slast[o] = tt;
+            long long nc = (long long)old + rs.supd_delta[i];
+            if (nc < 0 || nc > 0xFFFFFFFFll) {
+                atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
+                nc = nc < 0 ? 0 : 0xFFFFFFFFll;
+            }
+            sa.tri_counts[o] = (uint32_t)nc;
+        }
+        for (int i = 0; i < rs.niupd; ++i) unit_bump_tet(a, ti, rs.iupd_spec[i], rs.iupd_delta[i], tt);
+        for (int i = 0; i < rs.noupd && to >= 0; ++i) unit_bump_tet(a, to, rs.oupd_spec[i], rs.oupd_delta[i], tt);
+        ci = rs.niupd > 0;
+        co = rs.noupd > 0;
+    } else {
+        // GHK current number sel - npr of the patch: one ion out of (efflux) or into the
+        // inner tet, into or out of the outer tet when its concentration is used; z
+        // elementary charges for the triangle's current.
+        int g = 0, left = sel - npr;
+        for (; g < sa.nghk; ++g)
+            if (sa.ghks[g].patch == p && left-- == 0) break;
+        const sg_ghk& gh = sa.ghks[g];
+        const uint32_t nch = sa.tri_counts[(size_t)gh.sspec * M + m];
+        const uint32_t cin = a.counts[(size_t)gh.ion * a.ntets + ti];
+        const double vm = sa.tri_V ? sa.tri_V[m] : 0.0;
+        const bool outer = gh.voconc < 0.0 && to >= 0;
+        const double rtg = outer ? ghk_rate_outer(gh, vm, cin, nch, __ldg(&a.ivs[ti]),
+                                                  a.counts[(size_t)gh.ion * a.ntets + to], __ldg(&a.ivs[to]), sa.temp,
+                                                  a.status)
+                                 : ghk_rate(gh, vm, cin, nch, __ldg(&a.ivs[ti]), sa.temp, a.status);
+        const bool eff = rtg >= 0.0;
+        if (gh.realflux) {
+            unit_bump_tet(a, ti, gh.ion, eff ? -1 : 1, tt);
+            if (outer) unit_bump_tet(a, to, gh.ion, eff ? 1 : -1, tt);
+            ci = true;
+            co = outer;
+        }
+        atomicAdd((unsigned long long*)&sa.tri_echarge[m],
+                  (unsigned long long)(long long)(eff ? gh.valence : -gh.valence));
+    }
+    atomicAdd(a.surf_ext, 1ull);
+    aff[n++] = e;
+    if (ci) add_tet(ei);
+    if (co) add_tet(eo);
+    return n;
+}
+
+// SSA of every merged unit over its window, one warp per unit, between the volume and
+// membrane SSA passes and the diffusion leave of a split window: gathers the unit's inflow,
+// writes its tets' counts, change-time sums and tmask, its triangles' counts and occupancy
+// integrals.  The unit draws from the window stream of its first tet.  Lane 0 runs the
+// event loop (draws, the descent of the tree, the reaction within the element, the count
+// changes); the lanes share the gather, the element propensities, the tree build and, after
+// each event, the re-evaluation of the affected elements and of their paths to the root,
+// level by level (a node is always the sum of its two children, so the order of the lanes'
+// updates does not change any value).  SH: the tree and the element propensities sit in
+// shared memory (the largest unit fits the launch's dynamic shared memory).
+template <bool SH>
+__global__ void __launch_bounds__(32) unit_ssa_kernel(sg_window_args a) {
+    extern __shared__ __align__(16) unsigned char smem_u[];
+    __shared__ int s_aff[16];
+    const sg_unit_args& U = a.units;
+    const sg_surf_args& sa = a.surf;
+    const int lane = threadIdx.x;
     const unsigned long long parity = __ldcg(&a.launch_state[1]) & 1ull;
     const size_t plane = (size_t)a.ntets * 4;
     const int S = a.nspec, SS = sa.nsspec, M = sa.ntris;
-    for (int u = blockIdx.x * BLOCK + threadIdx.x; u < U.nunits; u += gridDim.x * BLOCK) {
+    for (int u = blockIdx.x; u < U.nunits; u += gridDim.x) {
         const int tb = U.tet_begin[u], nt = U.tet_begin[u + 1] - tb;
         const int mb = U.tri_begin[u], nm = U.tri_begin[u + 1] - mb;
         const int32_t* tets = U.tets + tb;
@@ -1584,7 +1660,7 @@ __global__ void __launch_bounds__(BLOCK) unit_ssa_kernel(sg_window_args a) {
         const int pending = rl->pending;
         // Gather the last window's inflow into the unit's tets and triangles.
         const uint32_t* in = a.outflow + (size_t)((w + 1) & 1ull) * a.ndiff * plane;
-        for (int k = 0; k < nt; ++k) {
+        for (int k = lane; k < nt; k += 32) {
             const int t = tets[k];
             const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
             const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
@@ -1612,7 +1688,7 @@ __global__ void __launch_bounds__(BLOCK) unit_ssa_kernel(sg_window_args a) {
                 if (c) atomicAdd(&a.totals[parity * S + s], (unsigned long long)c);
             }
         }
-        for (int j = 0; j < nm; ++j) {
+        for (int j = lane; j < nm; j += 32) {
             const int m = tris[j];
             const int p = sa.tri_patch[m];
             for (int s = 0; s < SS; ++s) {
@@ -1640,123 +1716,85 @@ __global__ void __launch_bounds__(BLOCK) unit_ssa_kernel(sg_window_args a) {
                 U.slast[o] = 0.0;
             }
         }
+        __syncwarp();
         // Element sums and the tree (node i = node 2i + node 2i + 1; leaves P..2P-1).
         const int E = nt + nm;
         const int eb = U.elem_base[u];
-        double* tree = U.tree + U.tree_base[u];
         const int P = (U.tree_base[u + 1] - U.tree_base[u]) >> 1;
-        double* prop = U.prop + (size_t)eb * U.rmax;
-        for (int e = 0; e < P; ++e)
+        double* tree = SH ? reinterpret_cast<double*>(smem_u) : U.tree + U.tree_base[u];
+        double* prop = SH ? reinterpret_cast<double*>(smem_u) + 2 * P : U.prop + (size_t)eb * U.rmax;
+        for (int e = lane; e < P; e += 32)
             tree[P + e] = e < E ? unit_elem_props(a, e, nt, tets, tris, r, prop + (size_t)e * U.rmax) : 0.0;
-        for (int i = P - 1; i >= 1; --i) tree[i] = tree[2 * i] + tree[2 * i + 1];
+        __syncwarp();
+        for (int h = P >> 1; h >= 1; h >>= 1) {
+            for (int i = h + lane; i < 2 * h; i += 32) tree[i] = tree[2 * i] + tree[2 * i + 1];
+            __syncwarp();
+        }
         sg_stream st;
         sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)(tets[0] - rl->tet_begin), w, SG_PURPOSE_WINDOW);
         double tt = 0.0;
         for (;;) {
-            const double a0 = tree[1];
-            if (!(a0 > 0.0)) break;
-            const double dt = -sg_log(sg_u01_oc(sg_next_u32(&st))) / a0;
-            if (tt + dt > T) break;
-            tt = tt + dt;
-            double target = sg_u01_co(sg_next_u32(&st)) * a0;
-            // Descend: left while the target falls below the left sum (or nothing is right).
-            int node = 1;
-            while (node < P) {
-                const double l = tree[2 * node], rr = tree[2 * node + 1];
-                if (target < l || !(rr > 0.0)) {
-                    node = 2 * node;
-                } else {
-                    target = target - l;
-                    node = 2 * node + 1;
-                }
-            }
-            const int e = node - P;
-            const double* pq = prop + (size_t)e * U.rmax;
-            const int nq = unit_elem_nq(a, e, nt, tets, tris);
-            double cum = 0.0;
-            int sel = -1, lastnz = -1;
-            for (int q = 0; q < nq; ++q) {
-                const double p = pq[q];
-                if (p > 0.0) {
-                    lastnz = q;
-                    cum = cum + p;
-                    if (target < cum) {
-                        sel = q;
-                        break;
+            int naff = 0;
+            if (lane == 0) {
+                const double a0 = tree[1];
+                int e = -1, sel = -1;
+                if (a0 > 0.0) {
+                    const double dt = -sg_log(sg_u01_oc(sg_next_u32(&st))) / a0;
+                    if (tt + dt <= T) {
+                        tt = tt + dt;
+                        double target = sg_u01_co(sg_next_u32(&st)) * a0;
+                        // Descend: left while the target falls below the left sum (or nothing is right).
+                        int node = 1;
+                        while (node < P) {
+                            const double l = tree[2 * node], rr = tree[2 * node + 1];
+                            if (target < l || !(rr > 0.0)) {
+                                node = 2 * node;
+                            } else {
+                                target = target - l;
+                                node = 2 * node + 1;
+                            }
+                        }
+                        e = node - P;
+                        const double* pq = prop + (size_t)e * U.rmax;
+                        const int nq = unit_elem_nq(a, e, nt, tets, tris);
+                        double cum = 0.0;
+                        int lastnz = -1;
+                        for (int q = 0; q < nq; ++q) {
+                            const double pv = pq[q];
+                            if (pv > 0.0) {
+                                lastnz = q;
+                                cum = cum + pv;
+                                if (target < cum) {
+                                    sel = q;
+                                    break;
+                                }
+                            }
+                        }
+                        if (sel < 0) sel = lastnz;
                     }
                 }
+                if (sel >= 0) naff = unit_apply(a, e, sel, eb, nt, tets, tris, parity, tt, s_aff);
             }
-            if (sel < 0) sel = lastnz;
-            if (sel < 0) break;
-            if (e < nt) {
-                const int t = tets[e];
-                const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
-                const int q = __ldg(&a.comp_reac_begin[comp]) + sel;
-                const sg_reac* rc = &a.reacs[q];
-                for (int i = 0; i < rc->nupd; ++i) unit_bump_tet(a, t, rc->upd_spec[i], rc->upd_delta[i], tt);
-                atomicAdd(&a.ext[parity * a.nreac + q], 1ull);
-                unit_refresh_tet(a, e, eb, nt, tets, tris, r, prop, tree, P);
-                continue;
+            naff = __shfl_sync(0xffffffffu, naff, 0);
+            if (naff == 0) break;
+            __syncwarp();
+            // The affected elements' propensities, then their paths to the root by levels.
+            int node = 0;
+            if (lane < naff) {
+                const int f = s_aff[lane];
+                node = P + f;
+                tree[node] = unit_elem_props(a, f, nt, tets, tris, r, prop + (size_t)f * U.rmax);
             }
-            const int j = e - nt, m = tris[j];
-            const int p = sa.tri_patch[m];
-            const int pb = sa.patch_sreac_begin[p], npr = sa.patch_sreac_begin[p + 1] - pb;
-            const int ti = sa.tri_inner[m];
-            const int to = sa.tri_outer ? sa.tri_outer[m] : -1;
-            const int ei = U.tri_side[2 * m], eo = U.tri_side[2 * m + 1];
-            bool ci = false, co = false;  // inner / outer tet counts changed
-            if (sel < npr) {
-                const sg_sreac& rs = sa.sreacs[pb + sel];
-                for (int i = 0; i < rs.nsupd; ++i) {
-                    const size_t o = (size_t)rs.supd_spec[i] * M + m;
-                    const uint32_t old = sa.tri_counts[o];
-                    U.socc[o] = U.socc[o] + (double)old * (tt - U.slast[o]);
-                    U.slast[o] = tt;
-                    long long nc = (long long)old + rs.supd_delta[i];
-                    if (nc < 0 || nc > 0xFFFFFFFFll) {
-                        atomicOr(a.status, nc < 0 ? SG_ERR_NEGATIVE : SG_ERR_OVERFLOW);
-                        nc = nc < 0 ? 0 : 0xFFFFFFFFll;
-                    }
-                    sa.tri_counts[o] = (uint32_t)nc;
-                }
-                for (int i = 0; i < rs.niupd; ++i) unit_bump_tet(a, ti, rs.iupd_spec[i], rs.iupd_delta[i], tt);
-                for (int i = 0; i < rs.noupd && to >= 0; ++i)
-                    unit_bump_tet(a, to, rs.oupd_spec[i], rs.oupd_delta[i], tt);
-                ci = rs.niupd > 0;
-                co = rs.noupd > 0;
-            } else {
-                // GHK current number sel - npr of the patch: one ion out of (efflux) or into
-                // the inner tet, into or out of the outer tet when its concentration is
-                // used; z elementary charges for the triangle's current.
-                int g = 0, left = sel - npr;
-                for (; g < sa.nghk; ++g)
-                    if (sa.ghks[g].patch == p && left-- == 0) break;
-                const sg_ghk& gh = sa.ghks[g];
-                const uint32_t n = sa.tri_counts[(size_t)gh.sspec * M + m];
-                const uint32_t cin = a.counts[(size_t)gh.ion * a.ntets + ti];
-                const double vm = sa.tri_V ? sa.tri_V[m] : 0.0;
-                const bool outer = gh.voconc < 0.0 && to >= 0;
-                const double rtg = outer ? ghk_rate_outer(gh, vm, cin, n, __ldg(&a.ivs[ti]),
-                                                          a.counts[(size_t)gh.ion * a.ntets + to], __ldg(&a.ivs[to]),
-                                                          sa.temp, a.status)
-                                         : ghk_rate(gh, vm, cin, n, __ldg(&a.ivs[ti]), sa.temp, a.status);
-                const bool eff = rtg >= 0.0;
-                if (gh.realflux) {
-                    unit_bump_tet(a, ti, gh.ion, eff ? -1 : 1, tt);
-                    if (outer) unit_bump_tet(a, to, gh.ion, eff ? 1 : -1, tt);
-                    ci = true;
-                    co = outer;
-                }
-                atomicAdd((unsigned long long*)&sa.tri_echarge[m],
-                          (unsigned long long)(long long)(eff ? gh.valence : -gh.valence));
+            __syncwarp();
+            for (int h = P >> 1; h >= 1; h >>= 1) {
+                node >>= 1;
+                if (lane < naff) tree[node] = tree[2 * node] + tree[2 * node + 1];
+                __syncwarp();
             }
-            atomicAdd(a.surf_ext, 1ull);
-            unit_refresh(a, e, nt, tets, tris, r, prop, tree, P);
-            if (ci) unit_refresh_tet(a, ei, eb, nt, tets, tris, r, prop, tree, P);
-            if (co) unit_refresh_tet(a, eo, eb, nt, tets, tris, r, prop, tree, P);
         }
+        __syncwarp();
         // Occupancy integrals of the triangles, change-time masks of the tets.
-        for (int j = 0; j < nm; ++j) {
+        for (int j = lane; j < nm; j += 32) {
             const int m = tris[j];
             for (int s = 0; s < SS; ++s) {
                 const size_t o = (size_t)s * M + m;
@@ -1769,7 +1807,7 @@ __global__ void __launch_bounds__(BLOCK) unit_ssa_kernel(sg_window_args a) {
                 }
             }
         }
-        for (int k = 0; k < nt && a.tmask; ++k) {
+        for (int k = lane; k < nt && a.tmask; k += 32) {
             const int t = tets[k];
             uint32_t tm = 0u;
             for (int s = 0; s < S; ++s) {
@@ -1778,6 +1816,7 @@ __global__ void __launch_bounds__(BLOCK) unit_ssa_kernel(sg_window_args a) {
             }
             a.tmask[t] = tm;
         }
+        __syncwarp();
     }
 }
 
