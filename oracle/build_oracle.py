@@ -42,7 +42,7 @@ def build_oracle(force=False):
 
 
 def build_ref(force=False):
-    """Reference-side pieces; skipped when the reference tree is absent (GPU box): the
+    """Reference-side pieces; skipped when the reference tree is absent: the
     Philox known-answer generator and the reference solvers (build_ref_tetopsplit)."""
     third = os.path.join(REFERENCE, "src", "third_party")
     if not os.path.isdir(third):

@@ -1,6 +1,6 @@
 // Project-written stand-in for the reference's deterministic solver TetODE
-// (src/steps/tetode/tetode.cpp), which needs the SUNDIALS CVODE library that this
-// container lacks.  The reference's Python binding (pysteps/cysteps_solver.pyx, class
+// (src/steps/tetode/tetode.cpp), which needs the SUNDIALS CVODE library, absent here.  The
+// reference's Python binding (pysteps/cysteps_solver.pyx, class
 // _py_TetODE) calls three of its members; here they throw instead of building the
 // solver, so the binding module loads and every other class in it works.  The symbols are
 // the members' own (Itanium-mangled) names; all arguments are pointers, integers or
@@ -9,7 +9,7 @@
 
 namespace {
 [[noreturn]] void tetode_absent() {
-    throw std::runtime_error("TetODE needs the SUNDIALS CVODE library, which this build lacks");
+    throw std::runtime_error("TetODE needs the SUNDIALS CVODE library, which is absent");
 }
 }  // namespace
 

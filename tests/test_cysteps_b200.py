@@ -74,7 +74,7 @@ def test_dropin_class_has_the_solver_api():
 
 
 def test_tetode_standin_raises():
-    """TetODE needs SUNDIALS, which this build lacks: its stand-in raises instead."""
+    """TetODE needs SUNDIALS, which is absent: its stand-in raises instead."""
     from steps_b200 import geom as sgeom
 
     S = _module()
