@@ -385,22 +385,19 @@ def run_ours(args):
     sim.setProfiling(False)
     updates = mesh.ntets * NSPEC * windows
 
-    # End-to-end through the C ABI with pinned host buffers.
-    host = [torch.empty(mesh.ntets, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-            for _ in range(NSPEC)]
-    for i, s in enumerate(sim.spec_names):
-        sim.getSpecCounts(s, host[i])
+    # End-to-end through the C ABI with a pinned host buffer of every species row: each step
+    # uploads all rows, runs 1 ms and downloads all rows.
+    host = torch.empty((NSPEC, mesh.ntets), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    sim.getAllSpecCounts(host)
     barrier()
     e2e_s, e2e_upd = 0.0, 0
     for _ in range(args.steps):
         it_a = sim.getNIteration()
         t0 = time.perf_counter()
-        for i, s in enumerate(sim.spec_names):
-            sim.setSpecCounts(s, host[i])
+        sim.setAllSpecCounts(host)
         t_sim += STEP_SIM_S
         sim.run(t_sim)
-        for i, s in enumerate(sim.spec_names):
-            sim.getSpecCounts(s, host[i])
+        sim.getAllSpecCounts(host)
         e2e_s += time.perf_counter() - t0
         e2e_upd += mesh.ntets * NSPEC * (sim.getNIteration() - it_a)
     t_max, upd_all, e2e_val = replica_totals(dist, f"cuda:{local}", total_ms, updates, e2e_s, e2e_upd)

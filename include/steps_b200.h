@@ -122,6 +122,10 @@ int sg_set_comp_count(sg_solver* h, int32_t comp, int32_t spec, int32_t real, do
  * and its setter counterpart.  out/in hold ntets uint32 values. */
 int sg_get_spec_counts(sg_solver* h, int32_t spec, uint32_t* out);
 int sg_set_spec_counts(sg_solver* h, int32_t spec, const uint32_t* in);
+/* Every species row at once ([nspec][ntets] uint32, species-major as the device state):
+ * one copy and one stream synchronisation each way instead of one per species. */
+int sg_get_all_counts(sg_solver* h, uint32_t* out);
+int sg_set_all_counts(sg_solver* h, const uint32_t* in);
 /* getBatchTetSpecCountsNP (TOS:5715): out[i] = count of spec in tets[i], gathered on the
  * device so that only the n selected values cross to the host. */
 int sg_get_batch_tet_counts(sg_solver* h, int32_t spec, const int32_t* tets, int32_t n, double* out);

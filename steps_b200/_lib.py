@@ -75,6 +75,8 @@ PROTOTYPES = {
     "sg_get_spec_counts": [_P, _i32, _pu32],
     "sg_get_batch_tet_counts": [_P, _i32, _pi32, _i32, _pf64],
     "sg_set_spec_counts": [_P, _i32, _pu32],
+    "sg_get_all_counts": [_P, _pu32],
+    "sg_set_all_counts": [_P, _pu32],
     "sg_set_tet_clamped": [_P, _i32, _i32, _i32],
     "sg_set_reac_k": [_P, _i32, _i32, _f64],
     "sg_get_reac_k": [_P, _i32, _i32, _pf64],

@@ -1765,6 +1765,21 @@ struct Solver {
         sync();
     }
 
+    void get_all_rows(uint32_t* out) {
+        require_setup();
+        flush();
+        d2h(out, d_counts.p, (size_t)nspec * ntets);
+        sync();
+    }
+
+    void set_all_rows(const uint32_t* in) {
+        require_setup();
+        flush();
+        h2d(d_counts.p, in, (size_t)nspec * ntets);
+        invalidate_check();
+        sync();
+    }
+
     void set_tet_clamped(int t, int s, bool on) {
         require_setup();
         check_tet(t);
@@ -2390,6 +2405,20 @@ int sg_set_spec_counts(sg_solver* h, int32_t spec, const uint32_t* in) {
     return guarded([&] {
         need(in, "in");
         S(h)->set_spec_row(spec, in);
+    });
+}
+
+int sg_get_all_counts(sg_solver* h, uint32_t* out) {
+    return guarded([&] {
+        need(out, "out");
+        S(h)->get_all_rows(out);
+    });
+}
+
+int sg_set_all_counts(sg_solver* h, const uint32_t* in) {
+    return guarded([&] {
+        need(in, "in");
+        S(h)->set_all_rows(in);
     });
 }
 

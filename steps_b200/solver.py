@@ -506,6 +506,24 @@ class TetOpSplit:
             raise ArgErr("need one count per tet")
         check(self._L.sg_set_spec_counts(self._h, self._spec(s), ptr(a, C.c_uint32)))
 
+    def getAllSpecCounts(self, out=None):
+        """Every species row at once, [species][tet] uint32 in spec_names order (one
+        device -> host copy)."""
+        n = len(self.spec_names) * self.geom.ntets
+        if out is None:
+            out = np.empty((len(self.spec_names), self.geom.ntets), dtype=np.uint32)
+        if out.dtype != np.uint32 or out.size != n or not out.flags.c_contiguous:
+            raise ArgErr("need a contiguous uint32 array of species x tets")
+        check(self._L.sg_get_all_counts(self._h, ptr(out, C.c_uint32)))
+        return out
+
+    def setAllSpecCounts(self, counts):
+        """Set every species row at once from a [species][tet] array (one host -> device copy)."""
+        a = np.ascontiguousarray(counts, dtype=np.uint32)
+        if a.size != len(self.spec_names) * self.geom.ntets:
+            raise ArgErr("need species x tets counts")
+        check(self._L.sg_set_all_counts(self._h, ptr(a, C.c_uint32)))
+
     def getBatchTetSpecCountsNP(self, tets, s, counts):
         """Reference getBatchTetSpecCountsNP (TOS:5715): counts[i] = count of s in tets[i],
         gathered on the device."""
