@@ -53,7 +53,10 @@ def build_ref(force=False):
         import build_ref_tetopsplit
 
     build_ref_tetopsplit.build(force=force)
-    build_ref_tetopsplit.build_cython(force=force)
+    try:
+        build_ref_tetopsplit.build_cython(force=force)
+    except RuntimeError as e:  # the binding module is optional test infrastructure
+        print(f"reference Python binding not built: {e}", file=sys.stderr)
     os.makedirs(REF_OUT, exist_ok=True)
     exe = os.path.join(REF_OUT, "ref_philox_kat")
     src = os.path.join(HERE, "ref_philox_kat.c")
