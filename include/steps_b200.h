@@ -252,9 +252,8 @@ int sg_get_launch(sg_solver* h, int32_t* block, int32_t* grid);
  * more in reverse order (drift of the per-window work cancels): block {64,128,256} x grid
  * {occupancy-sized (0), one tet per thread (-1)}; block 256, grid -1 at a shared-memory
  * carveout of 75%; split windows at block 128 and 256, grid -1; the persistent form
- * (sg_set_persistent) at block 128 and 256 with one tet per lane and at block 256 with
- * two (skipped unless every realization takes the same windows and the model has no
- * membrane).  The fastest is kept (the sample path does not depend on the shape).  The
+ * (sg_set_persistent) at block 256 with 2, 4 and 8 tets per lane (skipped unless every
+ * realization takes the same windows and the model has no membrane).  The fastest is kept (the sample path does not depend on the shape).  The
  * twelve sums (ms, in that order) are read back with sg_get_autotune_ms, the kept
  * carveout with sg_get_carveout. */
 int sg_set_autotune(sg_solver* h, int32_t on);
@@ -267,9 +266,10 @@ int sg_set_split(sg_solver* h, int32_t on);
 int sg_get_split(sg_solver* h, int32_t* on);
 /* Persistent form of the batched window loop (TOS:1528-1839 for every realization): the
  * windows of a run() call (up to 64 per launch) of every realization in one cooperative
- * launch, warps taking chunks of 32 x tets_per_lane (1 or 2) tets of one realization in
- * window order and waiting, bounded, until that realization has finished the previous
- * window.  The same results as the window launches, bit for bit.  Used when the model has
+ * launch, warps taking chunks of 32 x tets_per_lane (1, 2, 4 or 8) tets of one realization
+ * in window order and waiting, bounded, until that realization has finished the previous
+ * window; inside a chunk the tets whose first draw falls in the window run their SSA 32 at
+ * a time.  The same results as the window launches, bit for bit.  Used when the model has
  * no membrane triangles and every realization takes the same windows; the per-window
  * conservation check does not run inside it. */
 int sg_set_persistent(sg_solver* h, int32_t on, int32_t tets_per_lane);

@@ -139,6 +139,7 @@ struct Solver {
     DevBuf<int32_t> d_pchunk;                   // [nreal + 1] first chunk of each realization
     DevBuf<unsigned int> d_pstate;              // done [nreal], ready [nreal], abort [1]
     DevBuf<unsigned long long> d_pnext;         // [1] next work item
+    DevBuf<double> d_mode_tab;                  // [2][SG_MODE_TABLE]: 1/x, ln x! (persistent form)
     int pchunk_tpl = 0;                         // tets per lane d_pchunk was built for
     int pchunks = 0;
     DevBuf<float> d_geo;
@@ -1190,6 +1191,11 @@ struct Solver {
         d_pchunk.alloc(cb.size());
         h2d(d_pchunk.p, cb.data(), cb.size());
         if (!d_pstate.p) d_pstate.alloc((size_t)2 * nreal + 1);
+        if (!d_mode_tab.p) {
+            d_mode_tab.alloc((size_t)2 * SG_MODE_TABLE);
+            mode_tables_kernel<<<4, 256, 0, stream>>>(d_mode_tab.p, d_mode_tab.p + SG_MODE_TABLE);
+            SG_CUDA(cudaGetLastError());
+        }
         if (!d_pnext.p) d_pnext.alloc(1);
         pchunks = cb[nreal];
         pchunk_tpl = persist_tpl;
@@ -1203,6 +1209,8 @@ struct Solver {
         if (per_sm < 1) throw NotImplErr("the persistent window kernel does not fit an SM");
         const long need = ((long)P.nchunks * 32 + B - 1) / B;
         const int grid = (int)std::max(1L, std::min(need, (long)per_sm * nsm));
+        a.mode_rcpl = d_mode_tab.p;
+        a.mode_lnf = d_mode_tab.p + SG_MODE_TABLE;
         void* args[] = {&a, &P};
         SG_CUDA(cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(B), args, sm, stream));
     }
@@ -1210,6 +1218,7 @@ struct Solver {
     // its conservation check (the persistent launch keeps no per-window totals).
     void launch_persistent(const sg_window_args& a, int nwin) {
         ensure_persist_tables();
+        if (ndiff > 0 && (!a.tdel || !a.tmask)) throw ProgErr("persistent window without its buffers");
         SG_CUDA(cudaMemsetAsync(d_pstate.p, 0, d_pstate.n * sizeof(unsigned int), stream));
         SG_CUDA(cudaMemsetAsync(d_pnext.p, 0, sizeof(unsigned long long), stream));
         sg_persist_args P;
@@ -1224,13 +1233,21 @@ struct Solver {
         P.nwin = nwin;
         P.tpw = 32 * persist_tpl;
         const int B = block >= 256 ? 256 : 128;
-        const size_t sm = smem_bytes(B, nspec, (int)reacs.size());
+        const size_t sm = smem_bytes(B, nspec, std::max((int)reacs.size(), 6));
         if (B == 256) {
-            if (persist_tpl == 2) persist_launch<256, 2>(a, P, sm);
-            else persist_launch<256, 1>(a, P, sm);
+            switch (persist_tpl) {
+                case 8: persist_launch<256, 8>(a, P, sm); break;
+                case 4: persist_launch<256, 4>(a, P, sm); break;
+                case 2: persist_launch<256, 2>(a, P, sm); break;
+                default: persist_launch<256, 1>(a, P, sm); break;
+            }
         } else {
-            if (persist_tpl == 2) persist_launch<128, 2>(a, P, sm);
-            else persist_launch<128, 1>(a, P, sm);
+            switch (persist_tpl) {
+                case 8: persist_launch<128, 8>(a, P, sm); break;
+                case 4: persist_launch<128, 4>(a, P, sm); break;
+                case 2: persist_launch<128, 2>(a, P, sm); break;
+                default: persist_launch<128, 1>(a, P, sm); break;
+            }
         }
         SG_CUDA(cudaGetLastError());
         SG_CUDA(cudaMemsetAsync(d_launch.p + 3, 0, sizeof(unsigned long long), stream));
@@ -1382,9 +1399,9 @@ struct Solver {
     // reverse order (a palindromic schedule, so that the drift of the per-window work as
     // the run evolves cancels to first order): block {64, 128, 256} x grid {occupancy-
     // sized, one tet per thread}; block 256, one tet per thread at a shared-memory carveout
-    // of 75%; split windows at block 128 and 256; the persistent form at block 128 and 256
-    // with 32 tets per work chunk and at block 256 with 64 (two tets per lane), when every
-    // realization takes the same windows.  The fastest is kept.
+    // of 75%; split windows at block 128 and 256; the persistent form at block 256 with 64,
+    // 128 and 256 tets per work chunk (2, 4, 8 tets per lane), when every realization takes
+    // the same windows.  The fastest is kept.
     static constexpr int kTuneWindows = 2;
     static constexpr int kTuneCands = 12;
     static constexpr uint64_t kPersistMaxWindows = 64;  // windows per persistent launch
@@ -1414,8 +1431,8 @@ struct Solver {
                                         {128, 0, 100, false, 0},  {128, -1, 100, false, 0},
                                         {256, 0, 100, false, 0},  {256, -1, 100, false, 0},
                                         {256, -1, 75, false, 0},  {128, -1, 100, true, 0},
-                                        {256, -1, 100, true, 0},  {128, 0, 100, false, 1},
-                                        {256, 0, 100, false, 1},  {256, 0, 100, false, 2}};
+                                        {256, -1, 100, true, 0},  {256, 0, 100, false, 2},
+                                        {256, 0, 100, false, 4},  {256, 0, 100, false, 8}};
         tune_ms.assign(kTuneCands, 0.0f);
         cudaEvent_t e0, e1;
         SG_CUDA(cudaEventCreate(&e0));
@@ -1477,7 +1494,7 @@ struct Solver {
             done = autotune(a, pok);
             a = window_args();  // the tuner may have allocated the split buffers
         }
-        if (use_split()) {
+        if (use_split() || (persist && pok)) {
             ensure_split_buffers();
             a = window_args();
         }
@@ -2512,7 +2529,8 @@ int sg_set_split(sg_solver* h, int32_t on) {
 
 int sg_set_persistent(sg_solver* h, int32_t on, int32_t tets_per_lane) {
     return guarded([&] {
-        if (tets_per_lane != 1 && tets_per_lane != 2) throw sg::ArgErr("tets per lane must be 1 or 2");
+        if (tets_per_lane != 1 && tets_per_lane != 2 && tets_per_lane != 4 && tets_per_lane != 8)
+            throw sg::ArgErr("tets per lane must be 1, 2, 4 or 8");
         Solver* s = S(h);
         s->persist = on != 0;
         s->persist_tpl = tets_per_lane;

@@ -251,6 +251,10 @@ typedef struct sg_window_args {
     // (3 unused).  Each window's last block zeroes the next parity's counters.  Null:
     // static schedule.
     unsigned int* work;
+    // 1/x and ln x! for x below the mode-search table size in global memory (the values the
+    // leave kernel keeps in shared memory), for kernels without room for them; may be null.
+    const double* mode_rcpl;
+    const double* mode_lnf;
     // Diffusion boundaries (diffboundary.cpp, diff.cpp:307-398), null without any: per tet
     // the boundary of each face (byte f, 0xFF = none), the neighbour behind boundary faces
     // ((n << 2) | its face, -1), the face coefficients A / (V d), the two compartments of

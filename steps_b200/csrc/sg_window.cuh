@@ -1247,6 +1247,15 @@ __global__ void __launch_bounds__(BLOCK) sdiffuse_kernel(sg_window_args a) {
 
 // ---- batched realizations in one persistent launch ----------------------------------
 
+// The mode search's tables in global memory: 1/x and ln x! for x < SG_MODE_TABLE, computed
+// by the same functions as the leave kernel's shared copies.
+static __global__ void mode_tables_kernel(double* rcpl, double* lnf) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < SG_MODE_TABLE; i += gridDim.x * blockDim.x) {
+        rcpl[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
+        lnf[i] = sg_lnfact((uint32_t)i);
+    }
+}
+
 __device__ __forceinline__ unsigned int sg_ld_acquire(const unsigned int* p) {
     unsigned int v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -1256,16 +1265,106 @@ __device__ __forceinline__ void sg_st_release(unsigned int* p, unsigned int v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// One tet's whole window (gather, SSA, diffusion leave, store) as the fused window kernel
-// runs it, with the counts and the inflow read through L2: inside a persistent launch they
-// were written by other SMs earlier in the same launch.
-__device__ __forceinline__ void fused_tet_coherent(const sg_window_args& a, const smem_layout& L, int tid, int BLOCK,
-                                                   int t, int r, int tlocal, double T, unsigned long long w,
-                                                   int pending, const double* s_rcp, unsigned long long* moved) {
+// The diffusion leave of tet t (the split window's leave kernel for one tet): its counts
+// and change-time sums into this thread's shared-memory column, the leave, the scatter of
+// its outflow, then its counts to global memory.  The face selectors and their odds sit in this
+// thread's slots sel[k * BLOCK] (k = c0, c1, c2, odd1, odd2, odd3: its propensity column,
+// free once its SSA is done) for the species loop.
+__device__ __forceinline__ void leave_and_store(const sg_window_args& a, const smem_layout& L, int tid, int BLOCK,
+                                                int t, int r, int tlocal, int comp, double T, unsigned long long w,
+                                                const double* s_rcp, unsigned long long* moved) {
+    const int S = a.nspec;
+    // The counts and change-time sums the first pass or the queued SSA wrote (this warp).
+    const uint32_t tm = a.tmask ? __ldcg(&a.tmask[t]) : 0u;
+    for (int s = 0; s < S; ++s) {
+        L.cnt[s * BLOCK + tid] = __ldcg(&a.counts[(size_t)s * a.ntets + t]);
+        const int ds = __ldg(&a.diff_slot[s]);
+        L.tdel[s * BLOCK + tid] = (ds >= 0 && ((tm >> s) & 1u)) ? __ldcg(&a.tdel[(size_t)ds * a.ntets + t]) : 0.0;
+    }
+    const size_t plane = (size_t)a.ntets * 4;
+    double* sel = L.prop + tid;
+    const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
+    const double* Dc = a.dcst + ((size_t)r * a.ncomp + comp) * S;
+    const float G = __ldg(reinterpret_cast<const float*>(a.geo) + (size_t)t * 4 + 3);
+    const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
+    if (!bt) {
+        const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
+        sel[0] = (double)g.x;
+        sel[BLOCK] = (double)g.y;
+        sel[2 * BLOCK] = (double)g.z;
+        sel[3 * BLOCK] = sg_binom_odds((double)g.x);
+        sel[4 * BLOCK] = sg_binom_odds((double)g.y);
+        sel[5 * BLOCK] = sg_binom_odds((double)g.z);
+    }
+    const double invT = 1.0 / T;
+    for (int s = 0; s < S; ++s) {
+        const int ds = __ldg(&a.diff_slot[s]);
+        if (ds < 0) continue;
+        const double D = __ldg(&Dc[s]);
+        if (!(D > 0.0)) continue;
+        const uint32_t pop = L.cnt[s * BLOCK + tid];
+        uint4 k = make_uint4(0u, 0u, 0u, 0u);
+        if (pop > 0u) {
+            sg_stream st;
+            uint32_t Kn = 0u;
+            double t1;
+            if (bt) {
+                const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
+                float4 gb;
+                const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
+                sel[0] = (double)gb.x;
+                sel[BLOCK] = (double)gb.y;
+                sel[2 * BLOCK] = (double)gb.z;
+                sel[3 * BLOCK] = sg_binom_odds((double)gb.x);
+                sel[4 * BLOCK] = sg_binom_odds((double)gb.y);
+                sel[5 * BLOCK] = sg_binom_odds((double)gb.z);
+                t1 = T * tot;
+            } else {
+                t1 = T * (D * (double)G);
+            }
+            sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)tlocal, w, SG_PURPOSE_DIFF + (uint32_t)s);
+            if (t1 >= 1.0) t1 = 1.0;
+            uint32_t mean_n = pop;
+            const double sd = L.tdel[s * BLOCK + tid];
+            if (sd != 0.0) {
+                double nbar = (double)pop - sd * invT;
+                if (nbar > (double)pop) nbar = (double)pop;
+                const double nint = floor(nbar);
+                const double frc = nbar - nint;
+                mean_n = (uint32_t)nint;
+                if (frc > 0.0) {
+                    if (sg_u01_co(sg_next_u32(&st)) < frc) mean_n += 1u;
+                }
+            }
+            k = leave_split_sh(&st, mean_n, t1, sel, BLOCK, s_rcp, a.mode_rcpl, a.mode_lnf, &Kn);
+            if (Kn > 0u) {
+                if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
+                *moved += Kn;
+            }
+        }
+        const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
+        uint32_t* po = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane + (size_t)ds * plane;
+        if (nb.x >= 0) po[nb.x] = k.x;
+        if (nb.y >= 0) po[nb.y] = k.y;
+        if (nb.z >= 0) po[nb.z] = k.z;
+        if (nb.w >= 0) po[nb.w] = k.w;
+        if (bt) bnd_scatter(a, t, po, k);
+    }
+    for (int s = 0; s < S; ++s) a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
+}
+
+// First pass of tet t inside a persistent launch, as the split window's SSA kernel: its
+// inflow gathered (counts and inflow read through L2: other SMs wrote them earlier in the
+// same launch), its counts stored, its first waiting time drawn.  True when that draw may
+// fall in the window (the tet then waits for coherent_queued); false when its SSA is
+// complete (no change-time sums).
+__device__ __forceinline__ bool coherent_first_pass(const sg_window_args& a, const smem_layout& L, int tid, int BLOCK,
+                                                    int t, int r, int tlocal, double T, unsigned long long w,
+                                                    int pending, const double* s_rcp, unsigned long long* moved) {
     const int S = a.nspec, R = a.nreac;
     const size_t plane = (size_t)a.ntets * 4;
     const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
-    if (comp < 0) return;
+    if (comp < 0) return false;
     const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
     const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
     const double* Dc = a.dcst + ((size_t)r * a.ncomp + comp) * S;
@@ -1290,53 +1389,47 @@ __device__ __forceinline__ void fused_tet_coherent(const sg_window_args& a, cons
         L.tdel[s * BLOCK + tid] = 0.0;
         L.cnt[s * BLOCK + tid] = c;
     }
-    sg_stream st;
-    sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)tlocal, w, SG_PURPOSE_WINDOW);
     const int rb = __ldg(&a.comp_reac_begin[comp]);
     const int re = __ldg(&a.comp_reac_begin[comp + 1]);
-    if (re > rb) tet_ssa(a, L, tid, BLOCK, rb, re, a.kcst + (size_t)r * R, __ldg(&a.ivs[t]), clampm, T, &st);
-    const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
-    const bool bt = a.bface && __ldg(&a.bface[t]) != 0xFFFFFFFFu;
-    const double cs[3] = {(double)g.x, (double)g.y, (double)g.z};
-    const double odd1 = sg_binom_odds(cs[0]);
-    const double odd2 = sg_binom_odds(cs[1]);
-    const double odd3 = sg_binom_odds(cs[2]);
-    uint32_t* out = a.outflow + (size_t)(w & 1ull) * a.ndiff * plane;
-    const double invT = 1.0 / T;
-    for (int s = 0; s < S; ++s) {
-        const int ds = __ldg(&a.diff_slot[s]);
-        if (ds < 0) continue;
-        const double D = __ldg(&Dc[s]);
-        if (!(D > 0.0)) continue;
-        const uint32_t pop = L.cnt[s * BLOCK + tid];
-        uint4 k = make_uint4(0u, 0u, 0u, 0u);
-        if (pop > 0u) {
-            uint32_t Kn = 0u;
-            if (bt) {
-                float4 gb;
-                const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
-                const double cb[3] = {(double)gb.x, (double)gb.y, (double)gb.z};
-                k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
-                                  invT, T * tot, cb, sg_binom_odds(cb[0]), sg_binom_odds(cb[1]),
-                                  sg_binom_odds(cb[2]), s_rcp, nullptr, nullptr, &st, &Kn);
-            } else {
-                k = leave_species(a.seed, (uint32_t)r, (uint32_t)tlocal, w, (uint32_t)s, pop, L.tdel[s * BLOCK + tid],
-                                  invT, T * (D * (double)g.w), cs, odd1, odd2, odd3, s_rcp, nullptr, nullptr, &st,
-                                  &Kn);
-            }
-            if (Kn > 0u) {
-                if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
-                *moved += Kn;
-            }
-        }
-        uint32_t* po = out + (size_t)ds * plane;
-        if (nb.x >= 0) po[nb.x] = k.x;
-        if (nb.y >= 0) po[nb.y] = k.y;
-        if (nb.z >= 0) po[nb.z] = k.z;
-        if (nb.w >= 0) po[nb.w] = k.w;
-        if (bt) bnd_scatter(a, t, po, k);
+    bool fire = false;
+    if (re > rb) {
+        sg_stream st;
+        sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)tlocal, w, SG_PURPOSE_WINDOW);
+        fire = tet_may_fire(L, tid, BLOCK, rb, re, a.kcst + (size_t)r * R, __ldg(&a.ivs[t]), T, &st);
     }
     for (int s = 0; s < S; ++s) a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
+    if (!fire && a.tmask) a.tmask[t] = 0u;  // no change-time sums
+    return fire;
+}
+
+// A queued tet of a persistent launch: its gathered counts back from global memory (this
+// warp wrote them), its whole SSA on its restarted stream (the draws of the first pass
+// again), then its counts, its nonzero change-time sums and tmask to global memory.
+__device__ __forceinline__ void coherent_queued(const sg_window_args& a, const smem_layout& L, int tid, int BLOCK,
+                                                int t, int r, int tlocal, double T, unsigned long long w,
+                                                const double* s_rcp, unsigned long long* moved) {
+    const int S = a.nspec, R = a.nreac;
+    const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
+    const uint32_t clampm = a.clamp ? __ldg(&a.clamp[t]) : 0u;
+    for (int s = 0; s < S; ++s) {
+        L.cnt[s * BLOCK + tid] = __ldcg(&a.counts[(size_t)s * a.ntets + t]);
+        L.tdel[s * BLOCK + tid] = 0.0;
+    }
+    sg_stream st;
+    sg_stream_init(&st, a.seed, (uint32_t)r, (uint32_t)tlocal, w, SG_PURPOSE_WINDOW);
+    tet_ssa(a, L, tid, BLOCK, __ldg(&a.comp_reac_begin[comp]), __ldg(&a.comp_reac_begin[comp + 1]),
+            a.kcst + (size_t)r * R, __ldg(&a.ivs[t]), clampm, T, &st);
+    uint32_t tm = 0u;
+    for (int s = 0; s < S; ++s) {
+        const int ds = __ldg(&a.diff_slot[s]);
+        const double sdv = L.tdel[s * BLOCK + tid];
+        if (ds >= 0 && sdv != 0.0) {
+            a.tdel[(size_t)ds * a.ntets + t] = sdv;
+            tm |= 1u << s;
+        }
+        a.counts[(size_t)s * a.ntets + t] = L.cnt[s * BLOCK + tid];
+    }
+    if (a.tmask) a.tmask[t] = tm;
 }
 
 // P.nwin windows of every batched realization in one launch (all blocks resident: a
@@ -1351,13 +1444,17 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
     persistent_window_kernel(sg_window_args a, sg_persist_args P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double s_rcp[SG_RCP_TABLE];
+    __shared__ int s_q[2 * BLOCK];  // per warp: up to 63 queued tets
     const int S = a.nspec, R = a.nreac, tid = threadIdx.x, lane = tid & 31;
-    smem_layout L = carve(smem_raw, BLOCK, S, R);
+    // At least six propensity slots per thread: the leave keeps the selectors there.
+    smem_layout L = carve(smem_raw, BLOCK, S, R > 6 ? R : 6);
     for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
     for (int i = tid; i < R; i += BLOCK) L.reac[i] = a.reacs[i];
     for (int i = tid; i < R; i += BLOCK) L.ext[i] = 0u;
     if (tid == 0) L.moved[0] = 0ull;
     __syncthreads();
+    int* wq = s_q + (tid & ~31) * 2;
+    int qn = 0;
     unsigned long long moved = 0ull;
     const unsigned long long nitems = (unsigned long long)P.nwin * (unsigned long long)P.nchunks;
     for (;;) {
@@ -1403,11 +1500,42 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
         const int tb = __ldg(&rl->tet_begin), te = __ldg(&rl->tet_end);
         const bool live = rt < rend;
         const double T = (rt + per > rend) ? rend - rt : per;
+        // The split window inside the chunk: first passes of its tets 32 at a time, tets
+        // whose first draw may fall in the window waiting in the warp's queue and running
+        // their SSA 32 at a time (all lanes busy); then the leave of every tet of the chunk.
 #pragma unroll 1
         for (int k = 0; k < TPL; ++k) {
             const int t = tb + (j - c0) * 32 * TPL + k * 32 + lane;
-            if (live && t < te) fused_tet_coherent(a, L, tid, BLOCK, t, r, t - tb, T, w, pending, s_rcp, &moved);
+            bool fire = false;
+            if (live && t < te) fire = coherent_first_pass(a, L, tid, BLOCK, t, r, t - tb, T, w, pending, s_rcp, &moved);
+            const unsigned bal = __ballot_sync(0xffffffffu, fire);
+            if (fire) wq[qn + __popc(bal & ((1u << lane) - 1u))] = t;
+            qn += __popc(bal);
+            if (qn >= 32) {
+                __syncwarp();
+                const int tq = wq[qn - 32 + lane];
+                coherent_queued(a, L, tid, BLOCK, tq, r, tq - tb, T, w, s_rcp, &moved);
+                qn -= 32;
+                __syncwarp();
+            }
         }
+        __syncwarp();
+        if (lane < qn) {
+            const int tq = wq[lane];
+            coherent_queued(a, L, tid, BLOCK, tq, r, tq - tb, T, w, s_rcp, &moved);
+        }
+        qn = 0;
+        __syncwarp();
+        // The diffusion leave of the chunk's tets, all lanes at once.
+#pragma unroll 1
+        for (int k = 0; k < TPL; ++k) {
+            const int t = tb + (j - c0) * 32 * TPL + k * 32 + lane;
+            if (live && t < te) {
+                const int comp = a.comp ? __ldg(&a.comp[t]) : 0;
+                if (comp >= 0) leave_and_store(a, L, tid, BLOCK, t, r, t - tb, comp, T, w, s_rcp, &moved);
+            }
+        }
+        __syncwarp();
         __threadfence();
         __syncwarp();
         if (lane == 0) {

@@ -745,8 +745,8 @@ class TetOpSplit:
 
     def setPersistent(self, on, tets_per_lane=1):
         """Run the windows of every realization in one persistent launch per run() call (up
-        to 64 windows each), warps taking chunks of 32 * tets_per_lane tets; the same results
-        as the window launches.  Only for models without membrane triangles whose
+        to 64 windows each), warps taking chunks of 32 * tets_per_lane tets (1, 2, 4 or 8 per
+        lane); the same results as the window launches.  Only for models without membrane triangles whose
         realizations take the same windows (otherwise the window launches run)."""
         check(self._L.sg_set_persistent(self._h, 1 if on else 0, int(tets_per_lane)))
 

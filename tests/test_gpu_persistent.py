@@ -17,7 +17,7 @@ from tests.helpers import assert_same, pair, sync_counts, two_comp_mesh, two_com
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("block,tpl", [(128, 1), (256, 1), (256, 2)])
+@pytest.mark.parametrize("block,tpl", [(128, 1), (256, 2), (256, 4), (128, 8)])
 def test_persistent_batched_matches_oracle(steps_lib, block, tpl):
     """Realizations of different sizes with per-realization rate constants; run() calls of
     a few windows, of 70 windows (two launches) and one ending off the window grid."""
