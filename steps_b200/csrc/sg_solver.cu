@@ -1070,6 +1070,12 @@ struct Solver {
     }
 
     bool use_split() const { return split || nsdiff > 0 || nunits > 0; }
+    // Kernels one window launch enqueues (launch_window).
+    int kernels_per_window() const {
+        if (!use_split()) return 1;
+        if (!has_surf()) return 2;
+        return 2 + (nmemb_tets > 0 ? 1 : 0) + (nunits > 0 ? 1 : 0) + (nsdiff > 0 ? 1 : 0);
+    }
     void ensure_split_buffers() {
         if (!d_tdel.p && ndiff > 0) d_tdel.alloc((size_t)ndiff * ntets);
         if (!d_tmask.p && ndiff > 0) d_tmask.alloc((size_t)ntets);
@@ -1516,7 +1522,7 @@ struct Solver {
                 for (; done + kGraphChunk <= n; done += kGraphChunk) SG_CUDA(cudaGraphLaunch(ge, stream));
             }
             for (; done < n; ++done) launch_window(a, g);
-            launches += n;
+            launches += n * (uint64_t)kernels_per_window();
         }
         if (profiling) {
             SG_CUDA(cudaEventRecord(ev_end, stream));
