@@ -697,17 +697,19 @@ __device__ __forceinline__ uint4 leave_split(sg_stream* st, uint32_t mean_n, dou
 }
 
 // Leave of one (tet, species) with the face selectors and their odds read from this
-// thread's slots in shared memory (sel[k * stride], k = c0, c1, c2, odd1, odd2, odd3)
-// instead of registers held across the species loop.
-__device__ __forceinline__ uint4 leave_split_sh(sg_stream* st, uint32_t mean_n, double t1, const double* sel,
-                                                int stride, const double* rcp, const double* rcpl,
-                                                const double* lnf, uint32_t* out_kn) {
+// thread's slots in shared memory (selc[k * stride], k = c0, c1, c2, as float or double;
+// selo[k * stride] their odds) instead of registers held across the species loop.
+template <typename C>
+__device__ __forceinline__ uint4 leave_split_sh(sg_stream* st, uint32_t mean_n, double t1, const C* selc,
+                                                const double* selo, int stride, const double* rcp,
+                                                const double* rcpl, const double* lnf, uint32_t* out_kn) {
     if (mean_n <= SG_PM_MAX) {
         if (mean_n == 0u || !(t1 > 0.0)) {
             *out_kn = 0u;
             return make_uint4(0u, 0u, 0u, 0u);
         }
-        return leave_molecules(st, mean_n, t1 < 1.0 ? t1 : 1.0, sel[0], sel[stride], sel[2 * stride], out_kn);
+        return leave_molecules(st, mean_n, t1 < 1.0 ? t1 : 1.0, (double)selc[0], (double)selc[stride],
+                               (double)selc[2 * stride], out_kn);
     }
     uint4 k = make_uint4(0u, 0u, 0u, 0u);
     uint32_t n = mean_n, Kn = 0u;
@@ -730,8 +732,8 @@ __device__ __forceinline__ uint4 leave_split_sh(sg_stream* st, uint32_t mean_n, 
             n -= v;
         }
         if (stage < 3) {
-            pst = sel[stage * stride];
-            ost = sel[(3 + stage) * stride];
+            pst = (double)selc[stage * stride];
+            ost = selo[stage * stride];
         }
     }
     k.w = n;
@@ -1059,29 +1061,27 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_kernel(sg_window_args a, int check) {
     __shared__ double s_rcp[SG_RCP_TABLE];
-    __shared__ double s_rcpl[SG_MODE_TABLE];  // 1/x and ln x! of the mode search
-    __shared__ double s_lnf[SG_MODE_TABLE];
     // Per-thread slots for what the species loop reads after each sampler call: the face
-    // selectors c0, c1, c2 and their odds, the window length and its inverse, the window
-    // index.  Held in registers across the loop they forced spills at the 64-register cap.
-    __shared__ double s_sel[6 * BLOCK];
+    // selectors c0, c1, c2 (floats, as in the geometry) and their odds, the window length
+    // and its inverse.  Held in registers across the loop they forced spills at the
+    // 64-register cap.  The mode search's tables (a.mode_rcpl, a.mode_lnf) and the
+    // remaining spills are served by L1: the block's shared memory is kept small (about
+    // 14 KB) so that the host can give L1 most of the SM's 256 KB (set_leave_carveout).
+    __shared__ float s_selc[3 * BLOCK];
+    __shared__ double s_selo[3 * BLOCK];
     __shared__ double s_T[2 * BLOCK];
-    __shared__ unsigned long long s_w[BLOCK];
     __shared__ int flag[2];
     __shared__ unsigned long long s_moved;
     const int tid = threadIdx.x, lane = tid & 31;
     for (int i = tid; i < SG_RCP_TABLE; i += BLOCK) s_rcp[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
-    for (int i = tid; i < SG_MODE_TABLE; i += BLOCK) {
-        s_rcpl[i] = (i == 0) ? 0.0 : 1.0 / (double)i;
-        s_lnf[i] = sg_lnfact((uint32_t)i);
-    }
     if (tid == 0) s_moved = 0ull;
     __syncthreads();
     const unsigned long long parity = __ldcg(&a.launch_state[1]) & 1ull;
     unsigned int* wctr = a.work ? a.work + parity * 4 + 2 : nullptr;
     const size_t plane = (size_t)a.ntets * 4;
     const int S = a.nspec;
-    double* sel = s_sel + tid;
+    float* selc = s_selc + tid;
+    double* selo = s_selo + tid;
     unsigned long long moved = 0ull;
     for (int it = 0;; ++it) {
         const int base = next_warp_base(wctr, it, BLOCK);
@@ -1102,20 +1102,19 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
         const float G = __ldg(reinterpret_cast<const float*>(a.geo) + (size_t)t * 4 + 3);
         if (!bt) {
             const float4 g = __ldg(reinterpret_cast<const float4*>(a.geo) + t);
-            sel[0] = (double)g.x;
-            sel[BLOCK] = (double)g.y;
-            sel[2 * BLOCK] = (double)g.z;
-            sel[3 * BLOCK] = sg_binom_odds((double)g.x);
-            sel[4 * BLOCK] = sg_binom_odds((double)g.y);
-            sel[5 * BLOCK] = sg_binom_odds((double)g.z);
+            selc[0] = g.x;
+            selc[BLOCK] = g.y;
+            selc[2 * BLOCK] = g.z;
+            selo[0] = sg_binom_odds((double)g.x);
+            selo[BLOCK] = sg_binom_odds((double)g.y);
+            selo[2 * BLOCK] = sg_binom_odds((double)g.z);
         }
         s_T[tid] = Tw;
         s_T[BLOCK + tid] = 1.0 / Tw;  // one division per tet for the occupancy means
-        s_w[tid] = rl->window;
         const uint32_t tm = a.tmask ? a.tmask[t] : 0u;
         for (int s = 0; s < S; ++s) {
             const double T = s_T[tid], invT = s_T[BLOCK + tid];
-            const unsigned long long w = s_w[tid];
+            const unsigned long long w = a.reals[r].window;
             const int ds = __ldg(&a.diff_slot[s]);
             if (ds < 0) continue;
             const double D = __ldg(&Dc[s]);
@@ -1132,12 +1131,12 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
                     const int4 nb = __ldg(reinterpret_cast<const int4*>(a.nbr) + t);
                     float4 gb;
                     const double tot = bnd_split(a, t, comp, s, D, nb, &gb);
-                    sel[0] = (double)gb.x;
-                    sel[BLOCK] = (double)gb.y;
-                    sel[2 * BLOCK] = (double)gb.z;
-                    sel[3 * BLOCK] = sg_binom_odds((double)gb.x);
-                    sel[4 * BLOCK] = sg_binom_odds((double)gb.y);
-                    sel[5 * BLOCK] = sg_binom_odds((double)gb.z);
+                    selc[0] = gb.x;
+                    selc[BLOCK] = gb.y;
+                    selc[2 * BLOCK] = gb.z;
+                    selo[0] = sg_binom_odds((double)gb.x);
+                    selo[BLOCK] = sg_binom_odds((double)gb.y);
+                    selo[2 * BLOCK] = sg_binom_odds((double)gb.z);
                     t1 = T * tot;
                 } else {
                     t1 = T * (D * (double)G);
@@ -1155,7 +1154,7 @@ __global__ void __launch_bounds__(BLOCK, SG_LEAVE_THREADS_PER_SM / BLOCK) leave_
                         if (sg_u01_co(sg_next_u32(&st)) < frc) mean_n += 1u;
                     }
                 }
-                k = leave_split_sh(&st, mean_n, t1, sel, BLOCK, s_rcp, s_rcpl, s_lnf, &Kn);
+                k = leave_split_sh(&st, mean_n, t1, selc, selo, BLOCK, s_rcp, a.mode_rcpl, a.mode_lnf, &Kn);
                 if (Kn > 0u) {
                     if (!((clampm >> s) & 1u)) a.counts[ci] = pop - Kn;
                     moved += Kn;
@@ -1336,7 +1335,7 @@ __device__ __forceinline__ void leave_and_store(const sg_window_args& a, const s
                     if (sg_u01_co(sg_next_u32(&st)) < frc) mean_n += 1u;
                 }
             }
-            k = leave_split_sh(&st, mean_n, t1, sel, BLOCK, s_rcp, a.mode_rcpl, a.mode_lnf, &Kn);
+            k = leave_split_sh(&st, mean_n, t1, sel, sel + 3 * BLOCK, BLOCK, s_rcp, a.mode_rcpl, a.mode_lnf, &Kn);
             if (Kn > 0u) {
                 if (!((clampm >> s) & 1u)) L.cnt[s * BLOCK + tid] = pop - Kn;
                 *moved += Kn;
