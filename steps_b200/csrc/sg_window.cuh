@@ -108,6 +108,18 @@ __device__ __forceinline__ int next_warp_base(unsigned int* ctr, int it, int BLO
     return (int)((blockIdx.x + (unsigned)it * gridDim.x) * (unsigned)BLOCK + (threadIdx.x & ~31u));
 }
 
+// Asynchronous global -> shared copies (cp.async) of 4 and 8 bytes; a thread reads what it
+// copied after sg_cp_async_wait.
+__device__ __forceinline__ void sg_cp_async4(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void sg_cp_async8(void* sdst, const void* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void sg_cp_async_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Shared-memory carve-up for a block of BLOCK threads.
 struct smem_layout {
     uint32_t* cnt;             // [S][BLOCK]
@@ -894,16 +906,37 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
             if (a.clamp) clampm = __ldg(&a.clamp[t]);
             Dc = a.dcst + ((size_t)r * a.ncomp + comp) * S;
         }
-        // Phase 1: gather last window's inflow, stage counts in shared memory.
+        // Phase 1: gather last window's inflow, stage counts in shared memory.  The counts
+        // and the inflow of the first GS diffusing species are copied in asynchronously, all
+        // in flight at once, the inflow into this thread's change-time and propensity slots
+        // (free until the SSA; two 8-byte halves per slot pair).
         const uint32_t* in = a.outflow + (size_t)((w + 1) & 1ull) * a.ndiff * plane;
+        const int GS = (S + R) / 2 < a.ndiff ? (S + R) / 2 : a.ndiff;
+        if (active) {
+            for (int s = 0; s < S; ++s) sg_cp_async4(&L.cnt[s * BLOCK + tid], &a.counts[(size_t)s * a.ntets + t]);
+            if (pending)
+                for (int ds = 0; ds < GS; ++ds) {
+                    const uint32_t* src = in + (size_t)ds * plane + (size_t)t * 4;
+                    sg_cp_async8(&L.tdel[(2 * ds) * BLOCK + tid], src);
+                    sg_cp_async8(&L.tdel[(2 * ds + 1) * BLOCK + tid], src + 2);
+                }
+            sg_cp_async_wait();
+        }
         for (int s = 0; s < S; ++s) {
             uint32_t c = 0u;
             if (active) {
-                c = a.counts[(size_t)s * a.ntets + t];
+                c = L.cnt[s * BLOCK + tid];
                 int ds = __ldg(&a.diff_slot[s]);
                 if (pending && ds >= 0 && __ldg(&Dc[s]) > 0.0 && !((clampm >> s) & 1u)) {
                     // Slot f of this tet holds what the neighbour behind face f sent.
-                    const uint4 v = __ldg(reinterpret_cast<const uint4*>(in + (size_t)ds * plane) + t);
+                    uint4 v;
+                    if (ds < GS) {
+                        const uint2 lo = *reinterpret_cast<const uint2*>(&L.tdel[(2 * ds) * BLOCK + tid]);
+                        const uint2 hi = *reinterpret_cast<const uint2*>(&L.tdel[(2 * ds + 1) * BLOCK + tid]);
+                        v = make_uint4(lo.x, lo.y, hi.x, hi.y);
+                    } else {
+                        v = __ldg(reinterpret_cast<const uint4*>(in + (size_t)ds * plane) + t);
+                    }
                     unsigned long long sum = c;
                     if (nb.x >= 0) sum += v.x;
                     if (nb.y >= 0) sum += v.y;
@@ -916,12 +949,13 @@ __global__ void __launch_bounds__(BLOCK, SG_WINDOW_THREADS_PER_SM / BLOCK)
                     }
                     c = (uint32_t)sum;
                 }
-                L.tdel[s * BLOCK + tid] = 0.0;
             }
             L.cnt[s * BLOCK + tid] = c;
             const unsigned long long v = warp_total_u32(c);
             if (lane == 0 && v) atomicAdd(&L.tot[s], v);
         }
+        if (active)
+            for (int s = 0; s < S; ++s) L.tdel[s * BLOCK + tid] = 0.0;
         if (SPLIT && !SURF) {
             // First draw only; tets that may see an event join the warp's queue.
             bool fire = false;
