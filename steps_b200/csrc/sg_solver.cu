@@ -1113,7 +1113,7 @@ struct Solver {
     // shares the SM's 256 KB with shared memory: ask for the smallest shared-memory carveout
     // that keeps the kernel's full occupancy (its blocks' static shared memory plus the
     // per-block reservation), leaving the rest to L1 (3% faster a window at 384k tets than
-    // the driver's default choice).  Falls back to the largest carveout if the smaller one
+    // the default carveout).  Falls back to the largest carveout if the smaller one
     // would cost occupancy.
     bool leave_carveout_set = false;
     void set_leave_carveout() {
